@@ -1,0 +1,195 @@
+/*
+ * scattersim_b200 -- C ABI of the B200-native coupled-wave (RCWA) layer solve
+ * and field evaluation.
+ *
+ * Every entry point returns an sc_status; none exits, traps or prints.  The
+ * message of the last failure on the calling thread is sc_last_error_string().
+ * Device pointers are plain CUDA device addresses; `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Complex128 buffers hold
+ * interleaved {re, im} doubles; matrices are column-major (the layout of
+ * Eigen::MatrixXcd and of the reference's LAPACK calls).
+ *
+ * Reference interfaces replaced (STIM-Lab/scattersim):
+ *   sc_fft2_crop            fftw_fft2 + fftShift2d           FourierWave.h:82-195, called at :341,:343
+ *   sc_phi                  volume::phi                      FourierWave.h:336-397
+ *   sc_eigensolve_batched   MKL_eigensolve (zgeev 'N','V')   third_Lapack.h:37-44
+ *   sc_linearsolve_batched  MKL_linearsolve (zgesv, 1 RHS)   third_Lapack.h:46-53
+ *   sc_inverse_batched      MKL_inverse (zgesv against I)    third_Lapack.h:55-63
+ *   sc_zgemm_batched        MKL_multiply (cblas_zgemm)       third_Lapack.h:74-84
+ *   sc_volume_plan/solve    scattervolume main()             ScatterVolume.cpp:506-902
+ *   sc_volume_waves         CoupledWaveStructure build +     ScatterVolume.cpp:907-987,
+ *                           cw_allocate / cw_unpack          cpuEvaluator.cpp:34-102
+ *   sc_cw_evaluate          gpu_cw_evaluate / evaluate       gpuEvaluator.cu:28-165
+ *   sc_mkl_eigensolve       host-buffer MKL_eigensolve       third_Lapack.h:37-44
+ *   sc_gpu_initialize /
+ *   sc_gpu_cw_evaluate      host-buffer gpu_initialize /     gpuEvaluator.cu:15-26,131-165
+ *                           gpu_cw_evaluate
+ */
+#ifndef SCATTERSIM_B200_H
+#define SCATTERSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SC_OK = 0,
+    SC_BADINPUT = 1,     /* invalid sizes, null pointers, non-finite input   */
+    SC_NOCONVERGE = 2,   /* QR iteration cap reached (per-instance info > 0) */
+    SC_SINGULAR = 3,     /* exact zero pivot in an LU factorisation          */
+    SC_OOM = 4,          /* device allocation failed                          */
+    SC_CUDA_ERROR = 5,   /* a CUDA runtime call failed                        */
+    SC_ENERGY_FAIL = 6   /* energy-balance check failed                       */
+} sc_status;
+
+typedef struct sc_context sc_context;
+
+const char* sc_version(void);
+const char* sc_last_error_string(void);
+
+/* One context per GPU; owns pooled device workspace (no per-call cudaMalloc
+ * once warm).  Replaces the process-global state of ScatterVolume.cpp:29-95. */
+sc_status sc_create(sc_context** ctx, int device);
+sc_status sc_destroy(sc_context* ctx);
+/* Number of kernel launches this context issued since creation. */
+uint64_t sc_launch_count(const sc_context* ctx);
+
+/* ---------------------------------------------------------------- stages */
+
+/* a3: for each of Z slices, the Fourier coefficients of n^2 and (1/n)^2
+ * (forward DFT / (S1*S2), fftshift, centred My x Mx crop).  `sample` is the
+ * C-order (Z, S1, S2) complex128 .npy buffer, read with the reference's
+ * column-major reinterpretation (FourierWave.h:283-301).  Nf, Nif: Z blocks of
+ * My x Mx column-major complex128. */
+sc_status sc_fft2_crop(sc_context* ctx, const void* sample, int Z, int S1, int S2,
+                       int Mx, int My, void* Nf, void* Nif, void* stream);
+
+/* a5: dense 4M x 4M layer matrices Phi (column-major) for Z slices from their
+ * coefficients.  up (Mx) and wq (My) are the lattice wave numbers of
+ * volume::UpWq_Cal; k is the vacuum wave number. */
+sc_status sc_phi(sc_context* ctx, const void* Nf, const void* Nif, int Z, int Mx, int My,
+                 const double* up_host, const double* wq_host, double k, void* Phi, void* stream);
+
+/* a7: eigenvalues and right eigenvectors (unit 2-norm columns) of `batch`
+ * n x n complex matrices stored back to back.  A is overwritten.  info[b] = 0
+ * on success, > 0 when the QR iteration cap was reached. */
+sc_status sc_eigensolve_batched(sc_context* ctx, void* A, int n, int batch, void* evl,
+                                void* evt, int* info, void* stream);
+
+/* a13: solves A X = B (LU with partial pivoting) for `batch` systems; A is
+ * overwritten by its LU factors, B by X.  info[b] = j+1 for an exact zero
+ * pivot in column j. */
+sc_status sc_linearsolve_batched(sc_context* ctx, void* A, int n, void* B, int nrhs,
+                                 int batch, int* info, void* stream);
+
+/* a9/a12/a14: Ainv = A^-1 for `batch` matrices (A is not modified). */
+sc_status sc_inverse_batched(sc_context* ctx, const void* A, int n, int batch, void* Ainv,
+                             int* info, void* stream);
+
+/* C = alpha * A * B + beta * C, column-major, strided batch. */
+sc_status sc_zgemm_batched(sc_context* ctx, int m, int n, int k, const double* alpha,
+                           const void* A, int lda, long long strideA, const void* B, int ldb,
+                           long long strideB, const double* beta, void* C, int ldc,
+                           long long strideC, int batch, void* stream);
+
+/* --------------------------------------------------------- volume solve */
+
+typedef struct {
+    double lambda;          /* --lambda     (default 1.0)        */
+    double direction[3];    /* --direction  (default 0 0 1)      */
+    double ex[2];           /* --ex         (default 0 0)        */
+    double ey[2];           /* --ey         (default 1 0)        */
+    double ez[2];           /* --ez         (default 0 0)        */
+    double n[2];            /* --n          (default 1 1)        */
+    double kappa;           /* --kappa      (default 0)          */
+    double size[3];         /* --size       (default 10 10 2)    */
+    double z;               /* --z          (default 0)          */
+    int ncoef;              /* number of --coef values (0, 1, 2) */
+    int coef[2];            /* --coef                            */
+    int psf;                /* --psf                             */
+    int external;           /* --external                        */
+    int npz;                /* --npz                             */
+} sc_volume_params;
+
+typedef struct {
+    int Mx, My, MF;         /* orders after the clamps of ScatterVolume.cpp:599-651 */
+    int Z;                  /* layers (slices)                                       */
+    int clamped;            /* 1 if the evanescent-order clamp fired                 */
+    double k;               /* 2 PI / lambda with PI = 3.141592653                   */
+    double dir[3];          /* normalised direction * n_top                          */
+    double e_re[3], e_im[3];/* orthogonalised incident polarisation                  */
+} sc_volume_dims;
+
+/* Fills the defaults of ScatterVolume.cpp:511-529. */
+void sc_volume_params_default(sc_volume_params* p);
+
+/* Geometry, polarisation and order selection for a (Z, S1, S2) sample. */
+sc_status sc_volume_plan(const sc_volume_params* p, int Z, int S1, int S2, sc_volume_dims* dims);
+
+/* The scattervolume solve (ScatterVolume.cpp:654-902) for one sample resident
+ * on the device.  Outputs (device, any may be NULL):
+ *   x      6*MF complex128: [R_x R_y R_z T_x T_y T_z], column-major order index
+ *   evl    Z * 4*MF eigenvalues, even slots forward (downward) modes, odd the
+ *          paired backward modes
+ *   Qc, Qh Z blocks of 3*MF x 2*MF (column-major) internal mode fields
+ *          (Ex, Ey, Ez rows) of the forward / backward modes, scaled by the
+ *          mode coefficients beta (ScatterVolume.cpp:823-889)
+ * info (host, may be NULL) receives the first nonzero per-layer status. */
+sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void* sample,
+                          int Z, int S1, int S2, void* x, void* evl, void* Qc, void* Qh,
+                          int* info, void* stream);
+
+/* Per-stage device milliseconds of the last sc_volume_solve on this context:
+ * [fft, assemble, eig, chain, boundary, interior]. */
+sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms6);
+
+/* Wave table of a solved volume in cw_unpack order: Pi, then per boundary l
+ * its reflected and transmitted lists (ScatterVolume.cpp:907-987,
+ * cpuEvaluator.cpp:61-102), each wave wound to the origin.  E0 and k are
+ * nw x 3 complex128 (row-major).  ez_mode 0 keeps the solver's E_z (Pz);
+ * ez_mode 1 rebuilds E_z by transversality, as a .cw reader does.  Call with
+ * E0 = k = NULL to obtain *nw, the region index begin/end (Z+2 entries each)
+ * and the boundary planes z_layers (Z+1) as the .cw file stores them. */
+sc_status sc_volume_waves(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
+                          const void* x, const void* evl, const void* Qc, const void* Qh,
+                          int ez_mode, long long* nw, int* begin, int* end, double* z_layers,
+                          void* E0, void* k, void* stream);
+
+/* ------------------------------------------------------ field evaluation */
+
+/* E(r) = sum over the waves of r's region of E0 exp(i k.r)
+ * (gpuEvaluator.cu:28-68).  Waves are structure-of-arrays complex128:
+ * E0 (nw x 3) and k (nw x 3), row-major.  Regions follow cw_allocate
+ * (cpuEvaluator.cpp:34-53): region l = waves [begin[l], end[l]); the region of
+ * a point is #{ l : z >= z_layers[l] - zeps }.  Points (np x 3 doubles).
+ * out: np x 3 complex128 (precision 0: float64 sum) or complex64 written as
+ * complex128 (precision 1: float32 sum with float64 phase range reduction). */
+sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw,
+                         const double* z_layers, const int* begin, const int* end, int layers,
+                         double zeps, const double* points, long long np, void* out,
+                         int precision, void* stream);
+
+/* ----------------------------------------- reference-signature shims (host) */
+
+/* MKL_eigensolve(A, evl, evt, N): host buffers, column-major, A clobbered. */
+sc_status sc_mkl_eigensolve(void* A, void* evl, void* evt, int N);
+
+/* gpu_initialize(): copy the unpacked wave table (UnpackedWave<float>:
+ * 6 complex64 per wave, E0[3] then k[3]) and the region index to the device. */
+sc_status sc_gpu_initialize(int layers, const float* z_layers, const int* waves_begin,
+                            const int* waves_end, const void* W, long long nW, int device);
+
+/* gpu_cw_evaluate(): three N x N slices (x-y at z, x-z at y, y-z at x) of
+ * E (N x N x 3 complex64, host buffers). */
+sc_status sc_gpu_cw_evaluate(void* E_xy, void* E_xz, void* E_yz, float x_start, float y_start,
+                             float z_start, float x, float y, float z, float d, int N,
+                             int device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCATTERSIM_B200_H */

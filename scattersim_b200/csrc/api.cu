@@ -1,0 +1,387 @@
+// extern "C" entry points of libscattersim_b200 (declared in
+// include/scattersim_b200.h).  Every function validates its arguments, maps
+// CUDA failures to SC_CUDA_ERROR and records a message for
+// sc_last_error_string(); nothing exits or traps.
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "context.cuh"
+
+namespace sc {
+
+static thread_local char g_err[512] = "";
+static std::atomic<uint64_t> g_launches{0};
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+sc_status cuda_status(cudaError_t e, const char* where) {
+    set_error("%s: %s", where, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return SC_OOM;
+    return SC_CUDA_ERROR;
+}
+
+void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+uint64_t launch_total() { return g_launches.load(); }
+
+sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
+                       int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
+                       int* info_host, cudaStream_t st);
+sc_status volume_waves_launch(cudaStream_t st, int MF, int Z, const double2* svec, const double2* x,
+                              const double2* evl, const double2* Qc, const double2* Qh, const double* zpl,
+                              double k, double ntop, double nbot, int external, int ez_mode, long long nw,
+                              double2* E0, double2* K);
+sc_status cw_evaluate_launch(cudaStream_t st, const double2* E0, const double2* K, const double* zl,
+                             const int* begin, const int* end, int layers, double zeps, const double* pts,
+                             long long np, double2* out, int precision);
+
+namespace {
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// region index of a scattervolume wave table (cw_allocate, cpuEvaluator.cpp:34-53)
+void volume_regions(int MF, int Z, int external, long long* nw, int* begin, int* end) {
+    const long long internal = 2LL * MF * MF;
+    long long total = MF;
+    begin[0] = 0;
+    for (int l = 0; l <= Z; ++l) {
+        long long npr = (l == 0) ? MF : (external ? 0 : internal);
+        long long npt = (l == Z) ? MF : (external ? 0 : internal);
+        total += npr;
+        end[l] = (int)total;
+        begin[l + 1] = (int)total;
+        total += npt;
+    }
+    end[Z + 1] = (int)total;
+    *nw = total;
+}
+}  // namespace
+
+}  // namespace sc
+
+using namespace sc;
+
+extern "C" {
+
+const char* sc_version(void) { return "scattersim_b200 0.1 (sm_100a)"; }
+
+const char* sc_last_error_string(void) { return g_err; }
+
+sc_status sc_create(sc_context** ctx, int device) {
+    if (!ctx) {
+        set_error("sc_create: null ctx");
+        return SC_BADINPUT;
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= count) {
+        set_error("sc_create: device %d out of range (%d devices)", device, count);
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(device);
+    cudaFree(nullptr);
+    auto* c = new sc_context();
+    c->device = device;
+    c->launches_at_create = launch_total();
+    *ctx = c;
+    return SC_OK;
+}
+
+sc_status sc_destroy(sc_context* ctx) {
+    if (!ctx) return SC_OK;
+    DeviceGuard g(ctx->device);
+    cudaDeviceSynchronize();
+    ctx->ws.release();
+    for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    delete ctx;
+    return SC_OK;
+}
+
+uint64_t sc_launch_count(const sc_context* ctx) {
+    (void)ctx;
+    return launch_total();
+}
+
+sc_status sc_fft2_crop(sc_context* ctx, const void* sample, int Z, int S1, int S2, int Mx, int My, void* Nf,
+                       void* Nif, void* stream) {
+    if (!ctx || !sample || !Nf || !Nif) {
+        set_error("sc_fft2_crop: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double2 *R2, *Ri2;
+    SC_TRY(ctx->ws.get(&R2, (size_t)Z * S1 * Mx, WS_TMP, st));
+    SC_TRY(ctx->ws.get(&Ri2, (size_t)Z * S1 * Mx, WS_TMP2, st));
+    return fft2_crop(st, (const double2*)sample, Z, S1, S2, Mx, My, (double2*)Nf, (double2*)Nif, R2, Ri2);
+}
+
+sc_status sc_phi(sc_context* ctx, const void* Nf, const void* Nif, int Z, int Mx, int My, const double* up_host,
+                 const double* wq_host, double k, void* Phi, void* stream) {
+    if (!ctx || !Nf || !Nif || !up_host || !wq_host || !Phi || Z <= 0 || Mx <= 0 || My <= 0) {
+        set_error("sc_phi: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double* lat;
+    SC_TRY(ctx->ws.get(&lat, (size_t)Mx + My, WS_LAT, st));
+    std::vector<double> h(up_host, up_host + Mx);
+    h.insert(h.end(), wq_host, wq_host + My);
+    SC_CUDA_TRY(cudaMemcpyAsync(lat, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    SC_TRY(assemble_phi(st, (const double2*)Nf, (const double2*)Nif, Z, Mx, My, lat, k, (double2*)Phi));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    return SC_OK;
+}
+
+sc_status sc_eigensolve_batched(sc_context* ctx, void* A, int n, int batch, void* evl, void* evt, int* info,
+                                void* stream) {
+    if (!ctx || !A || !evl || !evt || n <= 0 || batch <= 0) {
+        set_error("sc_eigensolve_batched: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* dinfo;
+    SC_TRY(ctx->ws.get(&dinfo, (size_t)batch, WS_INFO, st));
+    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * batch, st));
+    SC_TRY(eig_batched(st, (double2*)A, n, batch, (double2*)evl, (double2*)evt, dinfo, ctx->ws));
+    std::vector<int> h(batch);
+    SC_CUDA_TRY(cudaMemcpyAsync(h.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    int bad = 0;
+    for (int b = 0; b < batch; ++b) {
+        if (info) info[b] = h[b];
+        if (h[b]) bad = 1;
+    }
+    if (bad) {
+        set_error("sc_eigensolve_batched: QR iteration cap reached");
+        return SC_NOCONVERGE;
+    }
+    return SC_OK;
+}
+
+sc_status sc_linearsolve_batched(sc_context* ctx, void* A, int n, void* B, int nrhs, int batch, int* info,
+                                 void* stream) {
+    if (!ctx || !A || !B || n <= 0 || nrhs <= 0 || batch <= 0) {
+        set_error("sc_linearsolve_batched: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int *piv, *dinfo;
+    SC_TRY(ctx->ws.get(&piv, (size_t)batch * n, WS_PIV, st));
+    SC_TRY(ctx->ws.get(&dinfo, (size_t)batch, WS_INFO, st));
+    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * batch, st));
+    const long long sA = (long long)n * n, sB = (long long)n * nrhs;
+    SC_TRY(getrf(st, (double2*)A, n, sA, n, batch, piv, dinfo));
+    SC_TRY(getrs(st, (const double2*)A, n, sA, n, piv, (double2*)B, n, sB, nrhs, batch));
+    std::vector<int> h(batch);
+    SC_CUDA_TRY(cudaMemcpyAsync(h.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    int bad = 0;
+    for (int b = 0; b < batch; ++b) {
+        if (info) info[b] = h[b];
+        if (h[b]) bad = 1;
+    }
+    if (bad) {
+        set_error("sc_linearsolve_batched: exactly singular matrix");
+        return SC_SINGULAR;
+    }
+    return SC_OK;
+}
+
+sc_status sc_inverse_batched(sc_context* ctx, const void* A, int n, int batch, void* Ainv, int* info,
+                             void* stream) {
+    if (!ctx || !A || !Ainv || n <= 0 || batch <= 0) {
+        set_error("sc_inverse_batched: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long sA = (long long)n * n;
+    double2* LU;
+    SC_TRY(ctx->ws.get(&LU, (size_t)batch * sA, WS_GD, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(LU, A, sizeof(double2) * batch * sA, cudaMemcpyDeviceToDevice, st));
+    SC_TRY(set_identity(st, (double2*)Ainv, n, sA, n, batch));
+    return sc_linearsolve_batched(ctx, LU, n, Ainv, n, batch, info, stream);
+}
+
+sc_status sc_zgemm_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
+                           long long strideA, const void* B, int ldb, long long strideB, const double* beta,
+                           void* C, int ldc, long long strideC, int batch, void* stream) {
+    if (!ctx || !alpha || !beta || !A || !B || !C || m < 0 || n < 0 || k < 0 || lda < (m > 1 ? m : 1) ||
+        ldb < (k > 1 ? k : 1) || ldc < (m > 1 ? m : 1)) {
+        set_error("sc_zgemm_batched: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return zgemm((cudaStream_t)stream, m, n, k, make_double2(alpha[0], alpha[1]), (const double2*)A, lda, strideA,
+                 (const double2*)B, ldb, strideB, make_double2(beta[0], beta[1]), (double2*)C, ldc, strideC,
+                 batch);
+}
+
+void sc_volume_params_default(sc_volume_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->lambda = 1.0;
+    p->direction[2] = 1.0;
+    p->ey[0] = 1.0;
+    p->n[0] = p->n[1] = 1.0;
+    p->size[0] = 10.0;
+    p->size[1] = 10.0;
+    p->size[2] = 2.0;
+}
+
+sc_status sc_volume_plan(const sc_volume_params* p, int Z, int S1, int S2, sc_volume_dims* dims) {
+    if (!dims) {
+        set_error("sc_volume_plan: null dims");
+        return SC_BADINPUT;
+    }
+    VolumePlan P;
+    SC_TRY(make_plan(p, Z, S1, S2, &P));
+    *dims = P.dims;
+    return SC_OK;
+}
+
+sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void* sample, int Z, int S1, int S2,
+                          void* x, void* evl, void* Qc, void* Qh, int* info, void* stream) {
+    if (!ctx || !p || !sample) {
+        set_error("sc_volume_solve: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return volume_solve(ctx, p, (const double2*)sample, Z, S1, S2, (double2*)x, (double2*)evl, (double2*)Qc,
+                        (double2*)Qh, info, (cudaStream_t)stream);
+}
+
+sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms6) {
+    if (!ctx || !ms6) {
+        set_error("sc_volume_stage_ms: null argument");
+        return SC_BADINPUT;
+    }
+    for (int i = 0; i < 6; ++i) ms6[i] = ctx->stage_ms[i];
+    return SC_OK;
+}
+
+sc_status sc_volume_waves(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2, const void* x,
+                          const void* evl, const void* Qc, const void* Qh, int ez_mode, long long* nw, int* begin,
+                          int* end, double* z_layers, void* E0, void* k, void* stream) {
+    if (!ctx || !p || !nw) {
+        set_error("sc_volume_waves: null argument");
+        return SC_BADINPUT;
+    }
+    VolumePlan P;
+    SC_TRY(make_plan(p, Z, S1, S2, &P));
+    const int MF = P.dims.MF;
+    std::vector<int> b(Z + 2), e(Z + 2);
+    volume_regions(MF, Z, p->external, nw, b.data(), e.data());
+    if (begin) std::memcpy(begin, b.data(), sizeof(int) * (Z + 2));
+    if (end) std::memcpy(end, e.data(), sizeof(int) * (Z + 2));
+    if (z_layers) {
+        // the .cw keeps z = 0 for interior boundaries written with --external
+        for (int l = 0; l <= Z; ++l)
+            z_layers[l] = (p->external && l != 0 && l != Z) ? 0.0 : P.z[l];
+    }
+    if (!E0 || !k) return SC_OK;
+    if (!x || !evl || (!p->external && (!Qc || !Qh))) {
+        set_error("sc_volume_waves: solution buffers missing");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* svec;
+    double* zpl;
+    SC_TRY(ctx->ws.get(&svec, (size_t)7 * MF, WS_EVAL_W, st));
+    SC_TRY(ctx->ws.get(&zpl, (size_t)Z + 1, WS_EVAL_IDX, st));
+    std::vector<cplx> hv;
+    hv.insert(hv.end(), P.Sx.begin(), P.Sx.end());
+    hv.insert(hv.end(), P.Sy.begin(), P.Sy.end());
+    hv.insert(hv.end(), P.Sz0.begin(), P.Sz0.end());
+    hv.insert(hv.end(), P.Sz1.begin(), P.Sz1.end());
+    hv.insert(hv.end(), P.EF.begin(), P.EF.end());
+    SC_CUDA_TRY(cudaMemcpyAsync(svec, hv.data(), hv.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(zpl, P.z.data(), sizeof(double) * (Z + 1), cudaMemcpyHostToDevice, st));
+    SC_TRY(volume_waves_launch(st, MF, Z, svec, (const double2*)x, (const double2*)evl, (const double2*)Qc,
+                               (const double2*)Qh, zpl, P.dims.k, p->n[0], p->n[1], p->external, ez_mode, *nw,
+                               (double2*)E0, (double2*)k));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    return SC_OK;
+}
+
+sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw, const double* z_layers,
+                         const int* begin, const int* end, int layers, double zeps, const double* points,
+                         long long np, void* out, int precision, void* stream) {
+    if (!ctx || !z_layers || !begin || !end || !points || !out || layers < 0 || nw < 0 ||
+        (nw > 0 && (!E0 || !k)) || (precision != 0 && precision != 1)) {
+        set_error("sc_cw_evaluate: bad argument");
+        return SC_BADINPUT;
+    }
+    for (int l = 0; l <= layers; ++l) {
+        if (begin[l] < 0 || end[l] < begin[l] || end[l] > nw) {
+            set_error("sc_cw_evaluate: region %d [%d, %d) outside the %d waves", l, begin[l], end[l], nw);
+            return SC_BADINPUT;
+        }
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* idx;
+    double* zl;
+    SC_TRY(ctx->ws.get(&idx, (size_t)2 * (layers + 1), WS_EVAL_IDX, st));
+    SC_TRY(ctx->ws.get(&zl, (size_t)layers + 1, WS_LAT, st));
+    std::vector<int> hidx(begin, begin + layers + 1);
+    hidx.insert(hidx.end(), end, end + layers + 1);
+    SC_CUDA_TRY(cudaMemcpyAsync(idx, hidx.data(), sizeof(int) * hidx.size(), cudaMemcpyHostToDevice, st));
+    if (layers > 0)
+        SC_CUDA_TRY(cudaMemcpyAsync(zl, z_layers, sizeof(double) * layers, cudaMemcpyHostToDevice, st));
+    SC_TRY(cw_evaluate_launch(st, (const double2*)E0, (const double2*)k, zl, idx, idx + layers + 1, layers, zeps,
+                              points, np, (double2*)out, precision));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    return SC_OK;
+}
+
+// ------------------------------------------------------------ host shims
+sc_status sc_mkl_eigensolve(void* A, void* evl, void* evt, int N) {
+    if (!A || !evl || !evt || N <= 0) {
+        set_error("sc_mkl_eigensolve: bad argument");
+        return SC_BADINPUT;
+    }
+    static sc_context* shim_ctx = nullptr;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!shim_ctx) SC_TRY(sc_create(&shim_ctx, 0));
+    const size_t bytes = sizeof(double2) * (size_t)N * N;
+    double2 *dA, *dV, *dw;
+    SC_TRY(shim_ctx->ws.get(&dA, (size_t)N * N, WS_BMAT, 0));
+    SC_TRY(shim_ctx->ws.get(&dV, (size_t)N * N, WS_CMAT, 0));
+    SC_TRY(shim_ctx->ws.get(&dw, (size_t)N, WS_MU, 0));
+    SC_CUDA_TRY(cudaMemcpy(dA, A, bytes, cudaMemcpyHostToDevice));
+    sc_status s = sc_eigensolve_batched(shim_ctx, dA, N, 1, dw, dV, nullptr, nullptr);
+    if (s != SC_OK && s != SC_NOCONVERGE) return s;
+    SC_CUDA_TRY(cudaMemcpy(evt, dV, bytes, cudaMemcpyDeviceToHost));
+    SC_CUDA_TRY(cudaMemcpy(evl, dw, sizeof(double2) * N, cudaMemcpyDeviceToHost));
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,641 @@
+// Batched non-Hermitian complex128 eigensolver: eigenvalues and right
+// eigenvectors of `batch` n x n matrices, the job of LAPACKE_zgeev('N','V')
+// behind MKL_eigensolve (third_Lapack.h:37-44, called at
+// ScatterVolume.cpp:253-277).
+//
+// Pipeline (one CTA per matrix for the sequential phases):
+//   1. gehrd_kernel   Householder reduction to upper Hessenberg form
+//                     (the zgehd2 recurrence: reflector from the column below
+//                     the subdiagonal, applied from the right to all rows and
+//                     from the left to the trailing block).
+//   2. orghr_kernel   explicit Q = H(0) H(1) ... H(n-2) (initial Schur vectors).
+//   3. hqr_kernel     complex single-shift QR to Schur form T = Z^H A Z with
+//                     Wilkinson shifts, Ahues-Tisseur deflation and exceptional
+//                     shifts.  The bulge is chased through a 64 x 64 window kept
+//                     in shared memory by one warp; the window's rotations are
+//                     recorded and then streamed by the whole CTA over the rows
+//                     to the right, the columns above and the Schur vectors
+//                     (one thread per far row/column, two live values each).
+//                     Active blocks of <= 64 rows are finished entirely in shared
+//                     memory with the accumulated unitary applied afterwards.
+//   4. trevc_kernel   eigenvectors of T by back substitution, one warp per
+//                     eigenvalue, small pivots raised to eps*|lambda|.
+//   5. V = Z * Y      batched zgemm, then unit 2-norm columns (zgeev's
+//                     normalisation; the largest component is made real).
+// Every loop has an iteration cap; a matrix that hits it gets info > 0 and the
+// kernel returns normally.
+#include "common.cuh"
+#include "kernels.cuh"
+
+#include <cfloat>
+
+namespace sc {
+
+namespace {
+constexpr int HT = 512;     // threads per CTA for gehrd / orghr / hqr
+constexpr int W = 64;       // shared-memory window
+constexpr double ULP = DBL_EPSILON;
+constexpr double SAFMIN = DBL_MIN;
+
+__device__ __forceinline__ bool cz(double2 a) { return a.x == 0.0 && a.y == 0.0; }
+
+// [c s; -conj(s) c] [f; g] = [r; 0], c real
+__device__ __forceinline__ void zlartg(double2 f, double2 g, double& c, double2& s) {
+    if (cz(g)) {
+        c = 1.0;
+        s = make_double2(0.0, 0.0);
+        return;
+    }
+    double fa = cabs(f), ga = cabs(g);
+    if (fa == 0.0) {
+        c = 0.0;
+        s = make_double2(g.x / ga, -g.y / ga);
+        return;
+    }
+    double d = hypot(fa, ga);
+    c = fa / d;
+    double2 fs = make_double2(f.x / fa, f.y / fa);
+    s = cscale(cmulc(fs, g), 1.0 / d);   // fs * conj(g) / d
+}
+// rows: a' = c a + s b ; b' = -conj(s) a + c b
+__device__ __forceinline__ void rot_rows(double c, double2 s, double2& a, double2& b) {
+    double2 na = cadd(cscale(a, c), cmul(s, b));
+    double2 nb = csub(cscale(b, c), cmul(cconj(s), a));
+    a = na;
+    b = nb;
+}
+// cols (right multiply by G^H): a' = a c + b conj(s) ; b' = -a s + b c
+__device__ __forceinline__ void rot_cols(double c, double2 s, double2& a, double2& b) {
+    double2 na = cadd(cscale(a, c), cmulc(b, s));
+    double2 nb = csub(cscale(b, c), cmul(a, s));
+    a = na;
+    b = nb;
+}
+
+// ------------------------------------------------------------------ gehrd
+__global__ void __launch_bounds__(HT)
+gehrd_kernel(double2* Aall, int n, long long sA, double2* tauall) {
+    extern __shared__ double2 sv[];          // n
+    __shared__ double red[32];
+    __shared__ double2 s_tau, s_scal;
+    __shared__ double s_beta;
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double2* A = Aall + b * sA;
+    double2* tau = tauall + (long long)b * n;
+    for (int i = 0; i < n - 1; ++i) {
+        const int m = n - i - 1;
+        double2* col = A + (long long)i * n;
+        double loc = 0.0;
+        for (int r = i + 2 + tid; r < n; r += HT) loc += cnorm2(col[r]);
+        double xn2 = block_sum(loc, red);
+        if (tid == 0) {
+            double2 alpha = col[i + 1];
+            if (xn2 == 0.0 && alpha.y == 0.0) {
+                s_tau = make_double2(0.0, 0.0);
+                s_scal = make_double2(1.0, 0.0);
+                s_beta = alpha.x;
+            } else {
+                double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
+                s_tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+                s_scal = cdiv(make_double2(1.0, 0.0), make_double2(alpha.x - beta, alpha.y));
+                s_beta = beta;
+            }
+        }
+        __syncthreads();
+        const double2 tv = s_tau, scal = s_scal;
+        for (int r = i + 2 + tid; r < n; r += HT) {
+            double2 x = cmul(col[r], scal);
+            col[r] = x;
+            sv[r - i - 1] = x;
+        }
+        if (tid == 0) {
+            sv[0] = make_double2(1.0, 0.0);
+            col[i + 1] = make_double2(s_beta, 0.0);
+            tau[i] = tv;
+        }
+        __syncthreads();
+        if (cz(tv)) continue;
+        // right: A[:, i+1:n] -= tau (A[:, i+1:n] v) v^H
+        for (int r = tid; r < n; r += HT) {
+            double2 y = make_double2(0.0, 0.0);
+            const double2* p = A + (long long)(i + 1) * n + r;
+#pragma unroll 4
+            for (int c = 0; c < m; ++c) y = cfma(p[(long long)c * n], sv[c], y);
+            double2 ty = cmul(tv, y);
+            double2* q = A + (long long)(i + 1) * n + r;
+#pragma unroll 4
+            for (int c = 0; c < m; ++c) q[(long long)c * n] = csub(q[(long long)c * n], cmulc(ty, sv[c]));
+        }
+        __syncthreads();
+        // left: A[i+1:n, i+1:n] -= conj(tau) v (v^H A[i+1:n, i+1:n])
+        const double2 ctv = cconj(tv);
+        for (int c = i + 1 + wid; c < n; c += HT / 32) {
+            double2* p = A + (long long)c * n + i + 1;
+            double2 w = make_double2(0.0, 0.0);
+            for (int r = lane; r < m; r += 32) w = cfma(cconj(sv[r]), p[r], w);
+            w = warp_sum2(w);
+            double2 cw = cmul(ctv, w);
+            for (int r = lane; r < m; r += 32) p[r] = csub(p[r], cmul(sv[r], cw));
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && n >= 1) tau[n - 1] = make_double2(0.0, 0.0);
+}
+
+// Q = H(0) ... H(n-2) into Z; clears the reflectors from A (leaving H)
+__global__ void __launch_bounds__(HT)
+orghr_kernel(double2* Aall, int n, long long sA, const double2* tauall, double2* Zall) {
+    extern __shared__ double2 sv[];
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double2* A = Aall + b * sA;
+    double2* Z = Zall + b * sA;
+    const double2* tau = tauall + (long long)b * n;
+    for (long long t = tid; t < (long long)n * n; t += HT) {
+        int r = (int)(t % n), c = (int)(t / n);
+        Z[t] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int i = n - 2; i >= 0; --i) {
+        const int m = n - i - 1;
+        const double2 tv = tau[i];
+        const double2* col = A + (long long)i * n;
+        for (int r = tid; r < m; r += HT) sv[r] = (r == 0) ? make_double2(1.0, 0.0) : col[i + 1 + r];
+        __syncthreads();
+        if (!cz(tv)) {
+            for (int c = i + 1 + wid; c < n; c += HT / 32) {
+                double2* p = Z + (long long)c * n + i + 1;
+                double2 w = make_double2(0.0, 0.0);
+                for (int r = lane; r < m; r += 32) w = cfma(cconj(sv[r]), p[r], w);
+                w = warp_sum2(w);
+                double2 tw = cmul(tv, w);
+                for (int r = lane; r < m; r += 32) p[r] = csub(p[r], cmul(sv[r], tw));
+            }
+        }
+        __syncthreads();
+    }
+    // zero below the subdiagonal
+    for (long long t = tid; t < (long long)n * n; t += HT) {
+        int r = (int)(t % n), c = (int)(t / n);
+        if (r > c + 1) A[t] = make_double2(0.0, 0.0);
+    }
+}
+
+// ------------------------------------------------------------------ hqr
+struct HqrSmem {
+    double2 Hs[W * W];      // window / small block, column-major, ld W
+    double2 U[W * W];       // accumulated unitary of a small block
+    double2 chunk[W * 32];  // staging for the small-block far products
+    double rc[W];           // recorded rotations of a sweep window
+    double2 rs[W];
+    double red_v[HT / 32];
+    int red_i[HT / 32];
+    int s_int[4];
+    double2 s_shift;
+};
+
+__device__ __forceinline__ double2& HS(HqrSmem& S, int i, int j) { return S.Hs[j * W + i]; }
+
+// Ahues-Tisseur deflation test for subdiagonal k (rows/cols relative to a
+// column-major array with leading dimension ld); lo..hi is the active range.
+__device__ bool negligible(const double2* H, long long ld, int k, int lo, int hi) {
+    double2 hkk1 = H[(long long)(k - 1) * ld + k];
+    double sub = cabs1(hkk1);
+    if (sub <= SAFMIN * 1e3) return true;
+    double2 a = H[(long long)(k - 1) * ld + k - 1], d = H[(long long)k * ld + k];
+    double tst = cabs1(a) + cabs1(d);
+    if (tst == 0.0) {
+        if (k - 2 >= lo) tst += fabs(H[(long long)(k - 2) * ld + k - 1].x);
+        if (k + 1 <= hi) tst += fabs(H[(long long)k * ld + k + 1].x);
+    }
+    if (sub <= ULP * tst) {
+        double2 up = H[(long long)k * ld + k - 1];
+        double ab = fmax(sub, cabs1(up)), ba = fmin(sub, cabs1(up));
+        double2 dd = csub(a, d);
+        double aa = fmax(cabs1(d), cabs1(dd)), bb = fmin(cabs1(d), cabs1(dd));
+        double s = aa + ab;
+        if (ba * (ab / s) <= fmax(SAFMIN * 1e3, ULP * (bb * (aa / s)))) return true;
+    }
+    return false;
+}
+
+// Wilkinson shift from the trailing 2x2 of the active block (zlahqr)
+__device__ double2 wilkinson(double2 h11, double2 h12, double2 h21, double2 h22) {
+    double2 t = h22;
+    double2 u = cmul(csqrt(h12), csqrt(h21));
+    double s = cabs1(u);
+    if (s != 0.0) {
+        double2 x = cscale(csub(h11, h22), 0.5);
+        double sx = cabs1(x);
+        s = fmax(s, sx);
+        double2 xs = cscale(x, 1.0 / s), us = cscale(u, 1.0 / s);
+        double2 y = cscale(csqrt(cadd(cmul(xs, xs), cmul(us, us))), s);
+        if (sx > 0.0) {
+            double2 xx = cscale(x, 1.0 / sx);
+            if (xx.x * y.x + xx.y * y.y < 0.0) y = cneg(y);
+        }
+        t = csub(t, cmul(u, cdiv(u, cadd(x, y))));
+    }
+    return t;
+}
+
+// The small-block QR inside shared memory, run by warp 0.  Returns false on
+// iteration cap.  Block size m, accumulates U.
+__device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
+    const int lane = threadIdx.x & 31;
+    int hi = m - 1;
+    int its = 0, total = 0;
+    while (hi >= 0) {
+        int lo = hi;
+        while (lo > 0 && !negligible(S.Hs, W, lo, 0, hi)) --lo;
+        if (lo > 0) {
+            if (lane == 0) HS(S, lo, lo - 1) = make_double2(0.0, 0.0);
+            __syncwarp();
+        }
+        if (lo == hi) {
+            --hi;
+            its = 0;
+            continue;
+        }
+        if (++total > maxit) return false;
+        ++its;
+        double2 sh;
+        if (its == 10) {
+            sh = cadd(make_double2(0.75 * fabs(HS(S, lo + 1, lo).x), 0.0), HS(S, lo, lo));
+        } else if (its == 20) {
+            sh = cadd(make_double2(0.75 * fabs(HS(S, hi, hi - 1).x), 0.0), HS(S, hi, hi));
+        } else {
+            sh = wilkinson(HS(S, hi - 1, hi - 1), HS(S, hi - 1, hi), HS(S, hi, hi - 1), HS(S, hi, hi));
+        }
+        for (int k = lo; k < hi; ++k) {
+            double c;
+            double2 s;
+            if (k == lo)
+                zlartg(csub(HS(S, lo, lo), sh), HS(S, lo + 1, lo), c, s);
+            else
+                zlartg(HS(S, k, k - 1), HS(S, k + 1, k - 1), c, s);
+            // rows k, k+1 over columns max(k-1, lo)..m-1 (full block width)
+            const int c0 = (k == lo) ? lo : k - 1;
+            for (int j = c0 + lane; j < m; j += 32) {
+                double2 a = HS(S, k, j), bb = HS(S, k + 1, j);
+                rot_rows(c, s, a, bb);
+                HS(S, k, j) = a;
+                HS(S, k + 1, j) = bb;
+            }
+            __syncwarp();
+            if (k > lo && lane == 0) HS(S, k + 1, k - 1) = make_double2(0.0, 0.0);
+            const int r1 = (k + 2 < hi ? k + 2 : hi);
+            for (int i = lane; i <= r1; i += 32) {
+                double2 a = HS(S, i, k), bb = HS(S, i, k + 1);
+                rot_cols(c, s, a, bb);
+                HS(S, i, k) = a;
+                HS(S, i, k + 1) = bb;
+            }
+            for (int i = lane; i < m; i += 32) {
+                double2 a = S.U[k * W + i], bb = S.U[(k + 1) * W + i];
+                rot_cols(c, s, a, bb);
+                S.U[k * W + i] = a;
+                S.U[(k + 1) * W + i] = bb;
+            }
+            __syncwarp();
+        }
+    }
+    return true;
+}
+
+// Far updates after a small block [lo, lo+m) finished with unitary U.
+__device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int lo, int m) {
+    const int tid = threadIdx.x;
+    const int hi1 = lo + m;  // exclusive
+    // right: H[lo:hi1, hi1:n] <- U^H * H[lo:hi1, hi1:n]
+    for (int j0 = hi1; j0 < n; j0 += 32) {
+        const int nc = (n - j0) < 32 ? (n - j0) : 32;
+        for (int t = tid; t < m * nc; t += HT) {
+            int r = t % m, c = t / m;
+            S.chunk[c * W + r] = H[(long long)(j0 + c) * n + lo + r];
+        }
+        __syncthreads();
+        for (int t = tid; t < m * nc; t += HT) {
+            int r = t % m, c = t / m;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int l = 0; l < m; ++l) acc = cfma(cconj(S.U[r * W + l]), S.chunk[c * W + l], acc);
+            H[(long long)(j0 + c) * n + lo + r] = acc;
+        }
+        __syncthreads();
+    }
+    // above: H[0:lo, lo:hi1] <- H[0:lo, lo:hi1] * U ; Z[0:n, lo:hi1] <- Z * U
+    for (int pass = 0; pass < 2; ++pass) {
+        double2* X = pass == 0 ? H : Z;
+        const int rows = pass == 0 ? lo : n;
+        for (int i0 = 0; i0 < rows; i0 += 32) {
+            const int nr = (rows - i0) < 32 ? (rows - i0) : 32;
+            for (int t = tid; t < m * nr; t += HT) {
+                int r = t % nr, c = t / nr;
+                S.chunk[c * 32 + r] = X[(long long)(lo + c) * n + i0 + r];
+            }
+            __syncthreads();
+            for (int t = tid; t < m * nr; t += HT) {
+                int r = t % nr, c = t / nr;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int l = 0; l < m; ++l) acc = cfma(S.chunk[l * 32 + r], S.U[c * W + l], acc);
+                X[(long long)(lo + c) * n + i0 + r] = acc;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(HT, 1)
+hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int* info,
+           int maxsweeps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HqrSmem& S = *reinterpret_cast<HqrSmem*>(smem_raw);
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double2* H = Hall + b * sA;
+    double2* Z = Zall + b * sA;
+    double2* w = wall + (long long)b * n;
+    int ihi = n - 1, its = 0, sweeps = 0;
+    bool failed = false;
+    while (ihi >= 0) {
+        // ---- deflation point: largest k in (0, ihi] with negligible H[k, k-1]
+        int best = 0;
+        for (int k = ihi - tid; k >= 1; k -= HT) {
+            if (negligible(H, n, k, 0, ihi)) {
+                best = k;
+                break;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) S.red_i[wid] = best;
+        __syncthreads();
+        if (tid == 0) {
+            int bb = 0;
+            for (int q = 0; q < HT / 32; ++q) bb = max(bb, S.red_i[q]);
+            S.s_int[0] = bb;
+            if (bb > 0) H[(long long)(bb - 1) * n + bb] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const int lo = S.s_int[0];
+        if (lo == ihi) {
+            if (tid == 0) w[ihi] = H[(long long)ihi * n + ihi];
+            --ihi;
+            its = 0;
+            __syncthreads();
+            continue;
+        }
+        const int m = ihi - lo + 1;
+        if (m <= W) {
+            // ---- finish the block in shared memory
+            for (int t = tid; t < W * W; t += HT) {
+                int i = t % W, j = t / W;
+                S.Hs[t] = (i < m && j < m) ? H[(long long)(lo + j) * n + lo + i] : make_double2(0.0, 0.0);
+                S.U[t] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            }
+            __syncthreads();
+            if (wid == 0) {
+                bool ok = small_qr_warp(S, m, 30 * m + 30);
+                if (lane == 0) S.s_int[1] = ok ? 1 : 0;
+            }
+            __syncthreads();
+            if (!S.s_int[1]) failed = true;
+            for (int t = tid; t < m * m; t += HT) {
+                int i = t % m, j = t / m;
+                H[(long long)(lo + j) * n + lo + i] = S.Hs[j * W + i];
+            }
+            __syncthreads();
+            small_block_far(S, H, Z, n, lo, m);
+            for (int k = lo + tid; k <= ihi; k += HT) w[k] = S.Hs[(k - lo) * W + (k - lo)];
+            __syncthreads();
+            if (failed) break;
+            ihi = lo - 1;
+            its = 0;
+            continue;
+        }
+        // ---- one single-shift sweep over [lo, ihi] through shared-memory windows
+        if (++sweeps > maxsweeps) {
+            failed = true;
+            break;
+        }
+        ++its;
+        if (tid == 0) {
+            double2 sh;
+            if (its % 30 == 10) {
+                sh = cadd(make_double2(0.75 * fabs(H[(long long)lo * n + lo + 1].x), 0.0), H[(long long)lo * n + lo]);
+            } else if (its % 30 == 20) {
+                sh = cadd(make_double2(0.75 * fabs(H[(long long)(ihi - 1) * n + ihi].x), 0.0),
+                          H[(long long)ihi * n + ihi]);
+            } else {
+                sh = wilkinson(H[(long long)(ihi - 1) * n + ihi - 1], H[(long long)ihi * n + ihi - 1],
+                               H[(long long)(ihi - 1) * n + ihi], H[(long long)ihi * n + ihi]);
+            }
+            S.s_shift = sh;
+        }
+        __syncthreads();
+        const double2 sh = S.s_shift;
+        int k = lo;
+        while (k <= ihi - 1) {
+            const int ws = (k == lo) ? lo : k - 1;
+            const int we = (ws + W < ihi + 1) ? ws + W : ihi + 1;   // exclusive
+            const int kend = (we == ihi + 1) ? ihi - 1 : we - 3;
+            const int wm = we - ws;
+            for (int t = tid; t < W * W; t += HT) {
+                int i = t % W, j = t / W;
+                S.Hs[t] = (i < wm && j < wm) ? H[(long long)(ws + j) * n + ws + i] : make_double2(0.0, 0.0);
+            }
+            __syncthreads();
+            if (wid == 0) {
+                for (int kk = k; kk <= kend; ++kk) {
+                    const int lk = kk - ws;
+                    double c;
+                    double2 s;
+                    if (kk == lo)
+                        zlartg(csub(HS(S, lk, lk), sh), HS(S, lk + 1, lk), c, s);
+                    else
+                        zlartg(HS(S, lk, lk - 1), HS(S, lk + 1, lk - 1), c, s);
+                    const int c0 = (kk == lo) ? lk : lk - 1;
+                    for (int j = c0 + lane; j < wm; j += 32) {
+                        double2 a = HS(S, lk, j), bb = HS(S, lk + 1, j);
+                        rot_rows(c, s, a, bb);
+                        HS(S, lk, j) = a;
+                        HS(S, lk + 1, j) = bb;
+                    }
+                    __syncwarp();
+                    if (kk > lo && lane == 0) HS(S, lk + 1, lk - 1) = make_double2(0.0, 0.0);
+                    const int r1 = ((kk + 2 < ihi) ? kk + 2 : ihi) - ws;
+                    for (int i = lane; i <= r1; i += 32) {
+                        double2 a = HS(S, i, lk), bb = HS(S, i, lk + 1);
+                        rot_cols(c, s, a, bb);
+                        HS(S, i, lk) = a;
+                        HS(S, i, lk + 1) = bb;
+                    }
+                    if (lane == 0) {
+                        S.rc[kk - k] = c;
+                        S.rs[kk - k] = s;
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            for (int t = tid; t < wm * wm; t += HT) {
+                int i = t % wm, j = t / wm;
+                H[(long long)(ws + j) * n + ws + i] = S.Hs[j * W + i];
+            }
+            const int nrot = kend - k + 1;
+            // far right: rows k..kend+1, columns we..n-1 (row rotations, streamed)
+            for (int j = we + tid; j < n; j += HT) {
+                double2* p = H + (long long)j * n + k;
+                double2 carry = p[0];
+                for (int t = 0; t < nrot; ++t) {
+                    double2 nx = p[t + 1];
+                    rot_rows(S.rc[t], S.rs[t], carry, nx);
+                    p[t] = carry;
+                    carry = nx;
+                }
+                p[nrot] = carry;
+            }
+            // far above: rows 0..ws-1, columns k..kend+1 ; and Z rows 0..n-1
+            for (int r = tid; r < ws + n; r += HT) {
+                double2* base = (r < ws) ? (H + r) : (Z + (r - ws));
+                double2* p = base + (long long)k * n;
+                double2 carry = p[0];
+                for (int t = 0; t < nrot; ++t) {
+                    double2 nx = p[(long long)(t + 1) * n];
+                    rot_cols(S.rc[t], S.rs[t], carry, nx);
+                    p[(long long)t * n] = carry;
+                    carry = nx;
+                }
+                p[(long long)nrot * n] = carry;
+            }
+            __syncthreads();
+            k = kend + 1;
+        }
+    }
+    if (tid == 0 && info != nullptr) info[b] = failed ? (ihi + 1 > 0 ? ihi + 1 : 1) : 0;
+}
+
+// ------------------------------------------------------------------ trevc
+// Y[:, k] = eigenvector of upper triangular T for T[k,k] (Y upper triangular).
+__global__ void trevc_kernel(const double2* Tall, double2* Yall, int n, long long sA) {
+    const int b = blockIdx.y;
+    const int warps = blockDim.x >> 5;
+    const int k = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= n) return;
+    const double2* T = Tall + b * sA;
+    double2* y = Yall + b * sA + (long long)k * n;
+    const double2 lam = T[(long long)k * n + k];
+    const double smin = fmax(ULP * cabs1(lam), SAFMIN * 1e3);
+    for (int i = lane; i < n; i += 32) {
+        if (i < k) y[i] = cneg(T[(long long)k * n + i]);
+        else y[i] = make_double2(i == k ? 1.0 : 0.0, 0.0);
+    }
+    __syncwarp();
+    for (int j = k - 1; j >= 0; --j) {
+        double2 d = csub(T[(long long)j * n + j], lam);
+        if (cabs1(d) < smin) d = make_double2(smin, 0.0);
+        double2 xj = cdiv(y[j], d);
+        __syncwarp();
+        if (lane == 0) y[j] = xj;
+        const double2* tc = T + (long long)j * n;
+        for (int i = lane; i < j; i += 32) y[i] = csub(y[i], cmul(tc[i], xj));
+        __syncwarp();
+    }
+}
+
+// unit 2-norm columns, largest-magnitude component made real and positive
+__global__ void normalize_cols_kernel(double2* Vall, int rows, int cols, int ld, long long sA) {
+    const int b = blockIdx.y;
+    const int warps = blockDim.x >> 5;
+    const int c = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (c >= cols) return;
+    double2* v = Vall + b * sA + (long long)c * ld;
+    double s = 0.0, best = -1.0;
+    int bi = 0;
+    for (int i = lane; i < rows; i += 32) {
+        double q = cnorm2(v[i]);
+        s += q;
+        if (q > best) { best = q; bi = i; }
+    }
+    s = warp_sum(s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (s == 0.0) return;
+    double2 big = v[bi];
+    double bm = cabs(big);
+    double inv = 1.0 / sqrt(s);
+    double2 ph = (bm > 0.0) ? make_double2(big.x / bm * inv, -big.y / bm * inv) : make_double2(inv, 0.0);
+    __syncwarp();
+    for (int i = lane; i < rows; i += 32) v[i] = cmul(v[i], ph);
+}
+
+}  // namespace
+
+size_t hqr_smem_bytes() { return sizeof(HqrSmem); }
+
+sc_status eig_batched(cudaStream_t st, double2* A, int n, int batch, double2* evl, double2* V,
+                      int* info, Workspace& ws) {
+    if (n <= 0 || batch <= 0) return SC_OK;
+    if (batch > 65535) {
+        set_error("eig: batch %d too large", batch);
+        return SC_BADINPUT;
+    }
+    const long long sA = (long long)n * n;
+    double2* tau = nullptr;
+    double2* Z = nullptr;
+    SC_TRY(ws.get(&tau, (size_t)batch * n, WS_EIG_TAU, st));
+    SC_TRY(ws.get(&Z, (size_t)batch * sA, WS_EIG_Z, st));
+    const size_t vsm = (size_t)n * sizeof(double2);
+    if (vsm > 200 * 1024) {
+        set_error("eig: n=%d exceeds the shared-memory reflector buffer", n);
+        return SC_BADINPUT;
+    }
+    // per-device attributes; cheap host calls, set on every use so that any
+    // device current on this thread is covered
+    SC_CUDA_TRY(cudaFuncSetAttribute(gehrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    SC_CUDA_TRY(cudaFuncSetAttribute(orghr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    SC_CUDA_TRY(cudaFuncSetAttribute(hqr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(HqrSmem)));
+    gehrd_kernel<<<batch, HT, vsm, st>>>(A, n, sA, tau);
+    count_launch();
+    orghr_kernel<<<batch, HT, vsm, st>>>(A, n, sA, tau, Z);
+    count_launch();
+    hqr_kernel<<<batch, HT, sizeof(HqrSmem), st>>>(A, Z, n, sA, evl, info, 60 * n + 100);
+    count_launch();
+    SC_CHECK_LAUNCH("hqr");
+    // Y (upper triangular eigenvectors of T) into V, then V = Z * Y
+    double2* Y = nullptr;
+    SC_TRY(ws.get(&Y, (size_t)batch * sA, WS_EIG_Y, st));
+    {
+        const int warps = 8;
+        dim3 g((n + warps - 1) / warps, batch);
+        trevc_kernel<<<g, 32 * warps, 0, st>>>(A, Y, n, sA);
+        count_launch();
+    }
+    SC_TRY(zgemm(st, n, n, n, make_double2(1.0, 0.0), Z, n, sA, Y, n, sA, make_double2(0.0, 0.0), V, n,
+                 sA, batch));
+    {
+        const int warps = 8;
+        dim3 g((n + warps - 1) / warps, batch);
+        normalize_cols_kernel<<<g, 32 * warps, 0, st>>>(V, n, n, n, sA);
+        count_launch();
+    }
+    SC_CHECK_LAUNCH("eig");
+    return SC_OK;
+}
+
+sc_status normalize_columns(cudaStream_t st, double2* V, int rows, int cols, int ld, long long sA,
+                            int batch) {
+    const int warps = 8;
+    dim3 g((cols + warps - 1) / warps, batch);
+    normalize_cols_kernel<<<g, 32 * warps, 0, st>>>(V, rows, cols, ld, sA);
+    count_launch();
+    SC_CHECK_LAUNCH("normalize");
+    return SC_OK;
+}
+
+}  // namespace sc

@@ -1,0 +1,90 @@
+// Internal declarations shared by the scattersim_b200 translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace sc {
+
+// Pooled device workspace owned by a context.  Each slot is a growable buffer
+// (stream-ordered cudaMallocAsync/cudaFreeAsync); once warm, no call allocates.
+enum WsSlot {
+    WS_EIG_TAU = 0, WS_EIG_Z, WS_EIG_Y,
+    WS_NF, WS_NIF, WS_OMEGA, WS_BMAT, WS_CMAT, WS_MU, WS_W, WS_CW,
+    WS_V, WS_EVL, WS_GD, WS_GC, WS_PIV, WS_INFO, WS_T, WS_T2,
+    WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
+    WS_EVAL_W, WS_EVAL_IDX,
+    WS_COUNT
+};
+
+struct Workspace {
+    void* ptr[WS_COUNT] = {};
+    size_t bytes[WS_COUNT] = {};
+    template <typename T>
+    sc_status get(T** out, size_t count, int slot, cudaStream_t st) {
+        size_t need = count * sizeof(T);
+        if (need == 0) need = 16;
+        if (bytes[slot] < need) {
+            if (ptr[slot]) {
+                cudaError_t e = cudaFreeAsync(ptr[slot], st);
+                if (e != cudaSuccess) return cuda_status(e, "cudaFreeAsync");
+                ptr[slot] = nullptr;
+                bytes[slot] = 0;
+            }
+            size_t alloc = need + need / 8;
+            cudaError_t e = cudaMallocAsync(&ptr[slot], alloc, st);
+            if (e != cudaSuccess) {
+                ptr[slot] = nullptr;
+                if (e == cudaErrorMemoryAllocation) {
+                    cudaGetLastError();
+                    set_error("device allocation of %zu bytes failed", alloc);
+                    return SC_OOM;
+                }
+                return cuda_status(e, "cudaMallocAsync");
+            }
+            bytes[slot] = alloc;
+        }
+        *out = reinterpret_cast<T*>(ptr[slot]);
+        return SC_OK;
+    }
+    void release() {
+        for (int i = 0; i < WS_COUNT; ++i) {
+            if (ptr[i]) cudaFree(ptr[i]);
+            ptr[i] = nullptr;
+            bytes[i] = 0;
+        }
+    }
+};
+
+// kernel launch accounting (per process, atomic)
+void count_launch(int n = 1);
+uint64_t launch_total();
+
+// zgemm.cu
+sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
+                long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
+                int ldc, long long sC, int batch);
+
+// lu.cu
+sc_status getrf(cudaStream_t st, double2* A, int lda, long long sA, int n, int batch, int* ipiv,
+                int* info);
+sc_status getrs(cudaStream_t st, const double2* LU, int lda, long long sA, int n, const int* ipiv,
+                double2* B, int ldb, long long sB, int nrhs, int batch);
+sc_status set_identity(cudaStream_t st, double2* B, int ldb, long long sB, int n, int batch);
+
+// eig.cu
+size_t hqr_smem_bytes();
+sc_status eig_batched(cudaStream_t st, double2* A, int n, int batch, double2* evl, double2* V,
+                      int* info, Workspace& ws);
+sc_status normalize_columns(cudaStream_t st, double2* V, int rows, int cols, int ld, long long sA,
+                            int batch);
+
+// fourier.cu
+// R2, Ri2: scratch of Z*S1*Mx entries each
+sc_status fft2_crop(cudaStream_t st, const double2* sample, int Z, int S1, int S2, int Mx, int My,
+                    double2* Nf, double2* Nif, double2* R2, double2* Ri2);
+sc_status assemble_phi(cudaStream_t st, const double2* Nf, const double2* Nif, int Z, int Mx, int My,
+                       const double* lat, double k, double2* Phi);
+sc_status assemble_bc(cudaStream_t st, const double2* Nf, const double2* Nif, int Z, int Mx, int My,
+                      const double* lat, double k, double2* Bm, double2* Cm);
+
+}  // namespace sc

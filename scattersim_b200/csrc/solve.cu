@@ -1,0 +1,632 @@
+// The scattervolume solve on the device (ScatterVolume.cpp:573-902).
+//
+// Stage map (reference -> here):
+//   volume::CalculateD, phi         fft2_crop + assemble_bc (Phi = [[0,B],[C,0]])
+//   EigenDecompositionD / zgeev     eig of Omega = B C (2M x 2M), then the 4M
+//                                   eigenpairs of Phi: lambda = +-sqrt(mu),
+//                                   vector [w; C w / lambda]
+//   Eigen_Sort pairing              even slot = root with Im > 0 (Re > 0 if
+//                                   real): the forward mode; odd = its negative
+//   Gd/Gc + Gc_static chain         GD_i = V diag(1|Di), GC_i = V diag(Ci|1);
+//                                   Gc_static <- GC_i GD_i^-1 Gc_static via
+//                                   LU(GD_i) and a solve with Gc_static
+//   SetBoundaryConditions + zgesv   A[2M:, 3M:] = GD_0 Gc_static^-1 f3, LU solve
+//   Beta chain, Q, Pz               LU solves with the stored GD_i factors,
+//                                   column scaling, Pz as a batched product
+// Eigenvalue pairing and eigenvector scale differ from the reference's MKL
+// output; every quantity passed out (x, fields of Qc/Qh at each boundary)
+// is invariant to both.
+#include "context.cuh"
+
+#include <cmath>
+#include <cstring>
+
+namespace sc {
+
+namespace {
+
+// ------------------------------------------------------------------ kernels
+
+// V (n4 x n4) and evl (n4) of one layer from mu (n2), W (n2 x n2), CW = C W
+__global__ void build_v_kernel(const double2* __restrict__ mu, const double2* __restrict__ Wm,
+                               const double2* __restrict__ CW, int n2, double2* __restrict__ V,
+                               double2* __restrict__ evl) {
+    const int z = blockIdx.y;
+    const int n4 = 2 * n2;
+    const long long tot = (long long)n4 * n4;
+    const double2* m = mu + (long long)z * n2;
+    const double2* w = Wm + (long long)z * n2 * n2;
+    const double2* cw = CW + (long long)z * n2 * n2;
+    double2* v = V + (long long)z * tot;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % n4), c = (int)(t / n4);
+        const int j = c >> 1;
+        double2 lam = csqrt(m[j]);
+        if (lam.y < 0.0 || (lam.y == 0.0 && lam.x < 0.0)) lam = cneg(lam);
+        if (cabs1(lam) == 0.0) lam = make_double2(1e-300, 0.0);
+        const bool odd = (c & 1);
+        double2 val;
+        if (r < n2) {
+            val = w[(long long)j * n2 + r];
+        } else {
+            val = cdiv(cw[(long long)j * n2 + (r - n2)], lam);
+            if (odd) val = cneg(val);
+        }
+        v[t] = val;
+        if (r == 0) evl[(long long)z * n4 + c] = odd ? cneg(lam) : lam;
+    }
+}
+
+// per-layer column scales: dG = (1 even, Di odd), cG = (Ci even, 1 odd)
+// (ScatterVolume.cpp:297-321)
+__global__ void gdgc_scale_kernel(const double2* __restrict__ evl, int n4, int Z, const double* __restrict__ zpl,
+                                  double k, double2* __restrict__ dG, double2* __restrict__ cG) {
+    const int z = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n4) return;
+    double dzc, dzd;
+    if (Z == 1) {
+        dzc = zpl[Z] - zpl[0];
+        dzd = zpl[0] - zpl[Z];
+    } else {
+        dzc = zpl[z + 1] - zpl[z];
+        dzd = zpl[z] - zpl[z + 1];
+    }
+    const double2 lam = evl[(long long)z * n4 + j];
+    // i * k * lambda * dz
+    const double2 ik = make_double2(0.0, k);
+    const double2 ac = cscale(cmul(ik, lam), dzc);
+    const double2 ad = cscale(cmul(ik, lam), dzd);
+    double2 d, c;
+    if (j & 1) {
+        d = cexp(ad);
+        c = make_double2(1.0, 0.0);
+    } else {
+        d = make_double2(1.0, 0.0);
+        c = cexp(ac);
+    }
+    dG[(long long)z * n4 + j] = d;
+    cG[(long long)z * n4 + j] = c;
+}
+
+// out = in * diag(s) (column scaling), batched with strides
+__global__ void scale_cols_kernel(const double2* __restrict__ in, long long sIn, const double2* __restrict__ s,
+                                  long long sS, int rows, int cols, double2* __restrict__ out, long long sOut) {
+    const int z = blockIdx.y;
+    const long long tot = (long long)rows * cols;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / rows);
+        out[z * sOut + t] = cmul(in[z * sIn + t], s[z * sS + c]);
+    }
+}
+
+// X = diag(s) X (row scaling) in place
+__global__ void scale_rows_kernel(double2* __restrict__ X, int rows, int cols, int ld,
+                                  const double2* __restrict__ s) {
+    const long long tot = (long long)rows * cols;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % rows), c = (int)(t / rows);
+        double2* p = X + (long long)c * ld + r;
+        *p = cmul(*p, s[r]);
+    }
+}
+
+// f3 dense (4MF x 3MF) (ScatterVolume.cpp:377-382)
+__global__ void f3_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
+                          const double2* __restrict__ Sz1, double2* __restrict__ F) {
+    const int n4 = 4 * MF;
+    const long long tot = (long long)n4 * 3 * MF;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % n4), c = (int)(t / n4);
+        const int rb = r / MF, ri = r % MF, cb = c / MF, ci = c % MF;
+        double2 v = make_double2(0.0, 0.0);
+        if (ri == ci) {
+            if (rb == 0 && cb == 0) v = make_double2(-1.0, 0.0);
+            else if (rb == 1 && cb == 1) v = make_double2(-1.0, 0.0);
+            else if (rb == 2 && cb == 1) v = Sz1[ri];
+            else if (rb == 2 && cb == 2) v = cneg(Sy[ri]);
+            else if (rb == 3 && cb == 0) v = cneg(Sz1[ri]);
+            else if (rb == 3 && cb == 2) v = Sx[ri];
+        }
+        F[t] = v;
+    }
+}
+
+// The 6MF x 6MF boundary system except the Gd*inv(Gc)*f3 block, and b
+// (ScatterVolume.cpp:398-414, 446, 456; f1/f2 of :357-373)
+__global__ void system_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
+                              const double2* __restrict__ Sz0, const double2* __restrict__ Sz1,
+                              const double2* __restrict__ EF, double k, double z0, double2* __restrict__ A,
+                              double2* __restrict__ b) {
+    const int n6 = 6 * MF;
+    const long long tot = (long long)n6 * 3 * MF;   // columns 0..3MF
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % n6), c = (int)(t / n6);
+        const int cb = c / MF, ci = c % MF;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < MF) {
+            // reflected Gauss row r: Sx R_x + Sy R_y - Sz0 R_z
+            if (ci == r) v = (cb == 0) ? Sx[r] : (cb == 1) ? Sy[r] : cneg(Sz0[r]);
+        } else if (r < 2 * MF) {
+            v = make_double2(0.0, 0.0);   // transmitted Gauss rows live in columns 3MF..6MF
+        } else {
+            // f2 block at rows 2MF.., columns 0..3MF
+            const int rr = r - 2 * MF, rb = rr / MF, ri = rr % MF;
+            if (ri == ci) {
+                if (rb == 0 && cb == 0) v = make_double2(1.0, 0.0);
+                else if (rb == 1 && cb == 1) v = make_double2(1.0, 0.0);
+                else if (rb == 2 && cb == 1) v = Sz0[ri];
+                else if (rb == 2 && cb == 2) v = Sy[ri];
+                else if (rb == 3 && cb == 0) v = cneg(Sz0[ri]);
+                else if (rb == 3 && cb == 2) v = cneg(Sx[ri]);
+            }
+        }
+        A[(long long)c * n6 + r] = v;
+    }
+    // transmitted Gauss rows (MF..2MF) in columns 3MF..6MF, rows 0..2MF of those columns
+    const long long tot2 = (long long)(2 * MF) * 3 * MF;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot2;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % (2 * MF)), c = 3 * MF + (int)(t / (2 * MF));
+        const int cb = (c - 3 * MF) / MF, ci = (c - 3 * MF) % MF;
+        double2 v = make_double2(0.0, 0.0);
+        if (r >= MF && ci == r - MF) v = (cb == 0) ? Sx[ci] : (cb == 1) ? Sy[ci] : Sz1[ci];
+        A[(long long)c * n6 + r] = v;
+    }
+    // b = [0 (2MF); -f1 EF]
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n6; r += gridDim.x * blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        if (r >= 2 * MF) {
+            const int rr = r - 2 * MF, rb = rr / MF, ri = rr % MF;
+            // phase = exp(i k z0 Sz0)
+            const double2 ph = cexp(cscale(cmul(make_double2(0.0, k), Sz0[ri]), z0));
+            const double2 ex = EF[ri], ey = EF[MF + ri], ez = EF[2 * MF + ri];
+            double2 f;
+            if (rb == 0) f = cmul(ph, ex);
+            else if (rb == 1) f = cmul(ph, ey);
+            else if (rb == 2) f = cadd(cneg(cmul(cmul(ph, Sz0[ri]), ey)), cmul(cmul(ph, Sy[ri]), ez));
+            else f = csub(cmul(cmul(ph, Sz0[ri]), ex), cmul(cmul(ph, Sx[ri]), ez));
+            v = cneg(f);
+        }
+        b[r] = v;
+    }
+}
+
+// rhs0 = f1 EF + f2 R  (ScatterVolume.cpp:768-772)
+__global__ void beta0_rhs_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
+                                 const double2* __restrict__ Sz0, const double2* __restrict__ EF,
+                                 const double2* __restrict__ x, double k, double z0, double2* __restrict__ out) {
+    const int n4 = 4 * MF;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n4; r += gridDim.x * blockDim.x) {
+        const int rb = r / MF, ri = r % MF;
+        const double2 ph = cexp(cscale(cmul(make_double2(0.0, k), Sz0[ri]), z0));
+        const double2 ex = EF[ri], ey = EF[MF + ri], ez = EF[2 * MF + ri];
+        const double2 rx = x[ri], ry = x[MF + ri], rz = x[2 * MF + ri];
+        double2 f1, f2;
+        if (rb == 0) {
+            f1 = cmul(ph, ex);
+            f2 = rx;
+        } else if (rb == 1) {
+            f1 = cmul(ph, ey);
+            f2 = ry;
+        } else if (rb == 2) {
+            f1 = cadd(cneg(cmul(cmul(ph, Sz0[ri]), ey)), cmul(cmul(ph, Sy[ri]), ez));
+            f2 = cadd(cmul(Sz0[ri], ry), cmul(Sy[ri], rz));
+        } else {
+            f1 = csub(cmul(cmul(ph, Sz0[ri]), ex), cmul(cmul(ph, Sx[ri]), ez));
+            f2 = cneg(cadd(cmul(Sz0[ri], rx), cmul(Sx[ri], rz)));
+        }
+        out[r] = cadd(f1, f2);
+    }
+}
+
+// Qc/Qh rows 0..2MF, and G = up*J - wq*I for the Pz product (ScatterVolume.cpp:823-881)
+__global__ void q_kernel(const double2* __restrict__ V, const double2* __restrict__ beta, int MF,
+                         const double* __restrict__ upk, const double* __restrict__ wqk, int Mx,
+                         double2* __restrict__ Qc, double2* __restrict__ Qh, double2* __restrict__ Gc,
+                         double2* __restrict__ Gh) {
+    const int z = blockIdx.y;
+    const int n4 = 4 * MF, n2 = 2 * MF, n3 = 3 * MF;
+    const double2* v = V + (long long)z * n4 * n4;
+    const double2* be = beta + (long long)z * n4;
+    const long long tot = (long long)n2 * n2;   // 2MF rows x 2MF cols
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % n2), j = (int)(t / n2);
+        const double2 bev = be[2 * j], bod = be[2 * j + 1];
+        const double2* ce = v + (long long)(2 * j) * n4;
+        const double2* co = v + (long long)(2 * j + 1) * n4;
+        Qc[(long long)z * n3 * n2 + (long long)j * n3 + r] = cmul(ce[r], bev);
+        Qh[(long long)z * n3 * n2 + (long long)j * n3 + r] = cmul(co[r], bod);
+        if (r < MF) {
+            // r is the Phi-order index qj*Mx + pj of the H rows
+            const double up = upk[r % Mx], wq = wqk[r / Mx];
+            const double2 I1 = cmul(ce[n2 + r], bev), J1 = cmul(ce[n2 + MF + r], bev);
+            const double2 I2 = cmul(co[n2 + r], bod), J2 = cmul(co[n2 + MF + r], bod);
+            Gc[(long long)z * MF * n2 + (long long)j * MF + r] = csub(cscale(J1, up), cscale(I1, wq));
+            Gh[(long long)z * MF * n2 + (long long)j * MF + r] = csub(cscale(J2, up), cscale(I2, wq));
+        }
+    }
+}
+
+// KP (MF x MF): NIf[lin] with lin = ((indR+My/2)%My)*Mx + (indC+Mx/2)%Mx read
+// as a linear index into the column-major My x Mx coefficients
+// (ScatterVolume.cpp:867-875), scaled by -1/k.
+__global__ void kp_kernel(const double2* __restrict__ Nif, int Mx, int My, double k, double2* __restrict__ KP) {
+    const int z = blockIdx.y;
+    const int MF = Mx * My;
+    const long long tot = (long long)MF * MF;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % MF), c = (int)(t / MF);
+        const int qi = r / Mx, pi_ = r % Mx, qj = c / Mx, pj = c % Mx;
+        const int indR = (qi - qj + My) % My, indC = (pi_ - pj + Mx) % Mx;
+        const int lin = ((indR + My / 2) % My) * Mx + (indC + Mx / 2) % Mx;
+        KP[(long long)z * tot + t] = cscale(Nif[(long long)z * MF + lin], -1.0 / k);
+    }
+}
+
+unsigned grid_for(long long tot, int tpb = 256) {
+    long long b = (tot + tpb - 1) / tpb;
+    if (b < 1) b = 1;
+    if (b > 8192) b = 8192;
+    return (unsigned)b;
+}
+
+template <typename T>
+sc_status upload(cudaStream_t st, T* dst, const std::vector<T>& src) {
+    if (src.empty()) return SC_OK;
+    SC_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return SC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- the plan
+sc_status make_plan(const sc_volume_params* p, int Z, int S1, int S2, VolumePlan* plan) {
+    if (!p || !plan || Z <= 0 || S1 <= 0 || S2 <= 0) {
+        set_error("volume plan: bad sample shape (%d, %d, %d)", Z, S1, S2);
+        return SC_BADINPUT;
+    }
+    if (!(p->lambda > 0.0) || !(p->size[0] > 0.0) || !(p->size[1] > 0.0) || !(p->size[2] > 0.0)) {
+        set_error("volume plan: lambda and size must be positive");
+        return SC_BADINPUT;
+    }
+    VolumePlan& P = *plan;
+    P = VolumePlan();
+    P.S1 = S1;
+    P.S2 = S2;
+    sc_volume_dims& D = P.dims;
+    // direction and polarisation (ScatterVolume.cpp:575-583, FourierWave.h:32-39)
+    double dn = std::sqrt(p->direction[0] * p->direction[0] + p->direction[1] * p->direction[1] +
+                          p->direction[2] * p->direction[2]);
+    if (!(dn > 0.0)) {
+        set_error("volume plan: zero direction");
+        return SC_BADINPUT;
+    }
+    double d[3] = {p->direction[0] / dn, p->direction[1] / dn, p->direction[2] / dn};
+    cplx E[3] = {cplx(p->ex[0], p->ex[1]), cplx(p->ey[0], p->ey[1]), cplx(p->ez[0], p->ez[1])};
+    cplx mag = std::sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+    for (auto& e : E) e /= mag;
+    auto cross = [](const cplx* a, const cplx* b, cplx* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    cplx dc[3] = {d[0], d[1], d[2]}, s[3], e2[3];
+    cross(E, dc, s);
+    cross(dc, s, e2);
+    for (int i = 0; i < 3; ++i) {
+        D.e_re[i] = e2[i].real();
+        D.e_im[i] = e2[i].imag();
+        D.dir[i] = d[i] * p->n[0];
+    }
+    D.k = 2 * PI_TRUNC / p->lambda;
+    D.Z = Z;
+    P.n_top = cplx(p->n[0], 0.0);
+    P.n_bot = cplx(p->n[1], p->kappa);
+    // z planes (ScatterVolume.cpp:162-168)
+    P.z.resize(Z + 1);
+    P.z[0] = p->z - p->size[2] / 2.0;
+    for (int i = 1; i <= Z; ++i) P.z[i] = P.z[i - 1] + p->size[2] / Z;
+    // orders (ScatterVolume.cpp:599-651)
+    int M0 = S2, M1 = S1;
+    if (p->ncoef == 1) {
+        M0 = M1 = (int)std::sqrt((double)p->coef[0]);
+    } else if (p->ncoef >= 2) {
+        M0 = p->coef[0];
+        M1 = p->coef[1];
+    }
+    const double lam = p->lambda, *sz = p->size, *n = p->n, *dir = D.dir;
+    D.clamped = 0;
+    if (std::pow((double)(M0 / 2) / sz[0] * lam + dir[0], 2) + std::pow((double)(M1 / 2) / sz[1] * lam + dir[1], 2) >=
+        std::pow(n[0], 2)) {
+        D.clamped = 1;
+        if (M0 != 1 && M1 != 1) {
+            if ((double)(M0 / 2) / sz[0] * lam + dir[0] > 0.71 * n[0]) M0 = (int)(0.707 * n[0] * 2 * sz[0] / lam) - 1;
+            if ((double)(M1 / 2) / sz[1] * lam + dir[1] > 0.71 * n[0]) M1 = (int)(0.707 * n[1] * 2 * sz[1] / lam) - 1;
+        }
+        if (M0 == 1) {
+            if ((double)(M1 / 2) / sz[1] * lam + std::fabs(dir[1]) >= n[0]) {
+                M1 = (int)(n[1] * 2 * sz[1] / lam - 1e-10);
+                if (M1 % 2 == 0) M1 -= 1;
+            }
+        }
+        if (M1 == 1) {
+            if ((double)(M0 / 2) / sz[1] * lam + std::fabs(dir[0]) >= n[0]) {
+                M0 = (int)(n[0] * 2 * sz[0] / lam - 1e-10);
+                if (M0 % 2 == 0) M0 -= 1;
+            }
+        }
+    }
+    if (M0 > S2) M0 = S2;
+    if (M1 > S1) M1 = S1;
+    if (M0 < 1 || M1 < 1) {
+        set_error("volume plan: no Fourier orders left (Mx=%d, My=%d)", M0, M1);
+        return SC_BADINPUT;
+    }
+    D.Mx = M0;
+    D.My = M1;
+    D.MF = M0 * M1;
+    const int Mx = M0, My = M1, MF = D.MF;
+    // lattice (FourierWave.h:319-334) and the Pz lattice (ScatterVolume.cpp:811-814)
+    P.up.resize(Mx);
+    P.wq.resize(My);
+    P.UP.resize(Mx);
+    P.WQ.resize(My);
+    for (int i = 0; i < Mx; ++i) {
+        double ps = (Mx == 1) ? (double)((Mx - 1) / 2) : -(double)(Mx / 2) + i * (((double)((Mx - 1) / 2) + (double)(Mx / 2)) / (Mx - 1));
+        P.up[i] = 2 * PI_TRUNC * ps / sz[0] + dir[0] * D.k;
+        P.UP[i] = 2.0 * ps * M_PI / sz[0];
+    }
+    for (int i = 0; i < My; ++i) {
+        double qs = (My == 1) ? (double)((My - 1) / 2) : -(double)(My / 2) + i * (((double)((My - 1) / 2) + (double)(My / 2)) / (My - 1));
+        P.wq[i] = 2 * PI_TRUNC * qs / sz[1] + dir[1] * D.k;
+        P.WQ[i] = 2.0 * qs * M_PI / sz[1];
+    }
+    P.Sx.resize(MF);
+    P.Sy.resize(MF);
+    P.Sz0.resize(MF);
+    P.Sz1.resize(MF);
+    for (int pidx = 0; pidx < MF; ++pidx) {
+        const int r = pidx % My, c = pidx / My;   // column-major (My x Mx) flattening
+        cplx sx = P.up[c] / D.k, sy = P.wq[r] / D.k;
+        P.Sx[pidx] = sx;
+        P.Sy[pidx] = sy;
+        P.Sz0[pidx] = std::sqrt(P.n_top * P.n_top - sx * sx - sy * sy);
+        P.Sz1[pidx] = std::sqrt(P.n_bot * P.n_bot - sx * sx - sy * sy);
+    }
+    // incident spectrum (ScatterVolume.cpp:661-679): DC order only, or all with --psf
+    P.EF.assign(3 * MF, cplx(0.0, 0.0));
+    const int dcidx = (My / 2) + (Mx / 2) * My;
+    for (int c = 0; c < 3; ++c) {
+        cplx e(D.e_re[c], D.e_im[c]);
+        if (p->psf) {
+            for (int i = 0; i < MF; ++i) P.EF[c * MF + i] = e;
+        } else {
+            P.EF[c * MF + dcidx] = e;
+        }
+    }
+    return SC_OK;
+}
+
+// ---------------------------------------------------------------- the solve
+sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
+                       int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
+                       int* info_host, cudaStream_t st) {
+    VolumePlan P;
+    SC_TRY(make_plan(p, Z, S1, S2, &P));
+    const int Mx = P.dims.Mx, My = P.dims.My, MF = P.dims.MF;
+    const int n2 = 2 * MF, n4 = 4 * MF, n6 = 6 * MF;
+    const long long s2 = (long long)n2 * n2, s4 = (long long)n4 * n4;
+    const double k = P.dims.k;
+    Workspace& ws = ctx->ws;
+    for (int i = 0; i < 7; ++i)
+        if (!ctx->ev[i]) SC_CUDA_TRY(cudaEventCreate(&ctx->ev[i]));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
+
+    // small host-built arrays: lattice, S vectors, EF, z planes
+    double* lat = nullptr;     // up (Mx), wq (My), UPk (Mx), WQk (My), z (Z+1)
+    const size_t nlat = (size_t)2 * (Mx + My) + Z + 1;
+    SC_TRY(ws.get(&lat, nlat, WS_LAT, st));
+    std::vector<double> hl(nlat);
+    for (int i = 0; i < Mx; ++i) hl[i] = P.up[i];
+    for (int i = 0; i < My; ++i) hl[Mx + i] = P.wq[i];
+    for (int i = 0; i < Mx; ++i) hl[Mx + My + i] = P.UP[i] + P.dims.dir[0] * k;
+    for (int i = 0; i < My; ++i) hl[2 * Mx + My + i] = P.WQ[i] + P.dims.dir[1] * k;
+    for (int i = 0; i <= Z; ++i) hl[2 * (Mx + My) + i] = P.z[i];
+    SC_TRY(upload(st, lat, hl));
+    const double* d_up = lat;
+    const double* d_upk = lat + Mx + My;
+    const double* d_wqk = lat + 2 * Mx + My;
+    const double* d_z = lat + 2 * (Mx + My);
+    double2* svec = nullptr;   // Sx, Sy, Sz0, Sz1, EF (7 MF)
+    SC_TRY(ws.get(&svec, (size_t)7 * MF, WS_EVAL_W, st));
+    {
+        std::vector<cplx> hv;
+        hv.reserve(7 * MF);
+        hv.insert(hv.end(), P.Sx.begin(), P.Sx.end());
+        hv.insert(hv.end(), P.Sy.begin(), P.Sy.end());
+        hv.insert(hv.end(), P.Sz0.begin(), P.Sz0.end());
+        hv.insert(hv.end(), P.Sz1.begin(), P.Sz1.end());
+        hv.insert(hv.end(), P.EF.begin(), P.EF.end());
+        SC_CUDA_TRY(cudaMemcpyAsync(svec, hv.data(), hv.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));
+    }
+    const double2 *dSx = svec, *dSy = svec + MF, *dSz0 = svec + 2 * MF, *dSz1 = svec + 3 * MF,
+                  *dEF = svec + 4 * MF;
+
+    // ---- a3: Fourier coefficients
+    double2 *Nf, *Nif, *R2, *Ri2;
+    SC_TRY(ws.get(&Nf, (size_t)Z * MF, WS_NF, st));
+    SC_TRY(ws.get(&Nif, (size_t)Z * MF, WS_NIF, st));
+    SC_TRY(ws.get(&R2, (size_t)Z * S1 * Mx, WS_TMP, st));
+    SC_TRY(ws.get(&Ri2, (size_t)Z * S1 * Mx, WS_TMP2, st));
+    SC_TRY(fft2_crop(st, sample, Z, S1, S2, Mx, My, Nf, Nif, R2, Ri2));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
+
+    // ---- a5: B, C blocks and Omega = B C
+    double2 *Bm, *Cm, *Om;
+    SC_TRY(ws.get(&Bm, (size_t)Z * s2, WS_BMAT, st));
+    SC_TRY(ws.get(&Cm, (size_t)Z * s2, WS_CMAT, st));
+    SC_TRY(ws.get(&Om, (size_t)Z * s2, WS_OMEGA, st));
+    SC_TRY(assemble_bc(st, Nf, Nif, Z, Mx, My, d_up, k, Bm, Cm));
+    SC_TRY(zgemm(st, n2, n2, n2, make_double2(1.0, 0.0), Bm, n2, s2, Cm, n2, s2, make_double2(0.0, 0.0), Om, n2,
+                 s2, Z));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
+
+    // ---- a7/a8: eigenpairs
+    double2 *mu, *Wm, *CW, *V, *evl;
+    int* dinfo;
+    SC_TRY(ws.get(&mu, (size_t)Z * n2, WS_MU, st));
+    SC_TRY(ws.get(&Wm, (size_t)Z * s2, WS_W, st));
+    SC_TRY(ws.get(&CW, (size_t)Z * s2, WS_CW, st));
+    SC_TRY(ws.get(&V, (size_t)Z * s4, WS_V, st));
+    SC_TRY(ws.get(&evl, (size_t)Z * n4, WS_EVL, st));
+    SC_TRY(ws.get(&dinfo, (size_t)Z + 4, WS_INFO, st));
+    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * (Z + 4), st));
+    SC_TRY(eig_batched(st, Om, n2, Z, mu, Wm, dinfo, ws));
+    SC_TRY(zgemm(st, n2, n2, n2, make_double2(1.0, 0.0), Cm, n2, s2, Wm, n2, s2, make_double2(0.0, 0.0), CW, n2,
+                 s2, Z));
+    {
+        dim3 g(grid_for(s4), Z);
+        build_v_kernel<<<g, 256, 0, st>>>(mu, Wm, CW, n2, V, evl);
+        count_launch();
+    }
+    SC_TRY(normalize_columns(st, V, n4, n4, n4, s4, Z));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
+
+    // ---- a9: GD/GC and the chain
+    double2 *dG, *cG, *LU, *Gcs, *X;
+    int* piv;
+    SC_TRY(ws.get(&dG, (size_t)Z * n4, WS_TMP, st));
+    SC_TRY(ws.get(&cG, (size_t)Z * n4, WS_TMP2, st));
+    SC_TRY(ws.get(&LU, (size_t)Z * s4, WS_GD, st));
+    SC_TRY(ws.get(&piv, (size_t)Z * n4, WS_PIV, st));
+    SC_TRY(ws.get(&Gcs, (size_t)s4, WS_T, st));
+    SC_TRY(ws.get(&X, (size_t)s4, WS_T2, st));
+    {
+        dim3 g((n4 + 255) / 256, Z);
+        gdgc_scale_kernel<<<g, 256, 0, st>>>(evl, n4, Z, d_z, k, dG, cG);
+        count_launch();
+        dim3 g2(grid_for(s4), Z);
+        scale_cols_kernel<<<g2, 256, 0, st>>>(V, s4, dG, n4, n4, n4, LU, s4);
+        count_launch();
+        scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, cG, n4, n4, n4, Gcs, s4);
+        count_launch();
+    }
+    SC_TRY(getrf(st, LU, n4, s4, n4, Z, piv, nullptr));
+    for (int i = 1; i < Z; ++i) {
+        // X = GD_i^-1 Gc_static ; Gc_static = V_i diag(cG_i) X
+        SC_CUDA_TRY(cudaMemcpyAsync(X, Gcs, sizeof(double2) * s4, cudaMemcpyDeviceToDevice, st));
+        SC_TRY(getrs(st, LU + i * s4, n4, s4, n4, piv + (long long)i * n4, X, n4, s4, n4, 1));
+        scale_rows_kernel<<<grid_for(s4), 256, 0, st>>>(X, n4, n4, n4, cG + (long long)i * n4);
+        count_launch();
+        SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), V + i * s4, n4, s4, X, n4, s4,
+                     make_double2(0.0, 0.0), Gcs, n4, s4, 1));
+    }
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[4], st));
+
+    // ---- a10-a13: boundary system and its solve
+    double2 *F, *A6, *b6;
+    int* piv6;
+    SC_TRY(ws.get(&F, (size_t)n4 * 3 * MF, WS_F, st));
+    SC_TRY(ws.get(&A6, (size_t)n6 * n6, WS_A6, st));
+    SC_TRY(ws.get(&b6, (size_t)n6, WS_B6, st));
+    SC_TRY(ws.get(&piv6, (size_t)n6 + n4, WS_PIV6, st));
+    f3_kernel<<<grid_for((long long)n4 * 3 * MF), 256, 0, st>>>(MF, dSx, dSy, dSz1, F);
+    count_launch();
+    SC_TRY(getrf(st, Gcs, n4, s4, n4, 1, piv6 + n6, nullptr));
+    SC_TRY(getrs(st, Gcs, n4, s4, n4, piv6 + n6, F, n4, 0, 3 * MF, 1));
+    // GD_0 = V_0 diag(dG_0) into X, then A6[2MF:, 3MF:] = GD_0 * F
+    scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, dG, n4, n4, n4, X, s4);
+    count_launch();
+    system_kernel<<<grid_for((long long)n6 * 3 * MF), 256, 0, st>>>(MF, dSx, dSy, dSz0, dSz1, dEF, k, P.z[0], A6, b6);
+    count_launch();
+    SC_TRY(zgemm(st, n4, 3 * MF, n4, make_double2(1.0, 0.0), X, n4, s4, F, n4, 0, make_double2(0.0, 0.0),
+                 A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0, 1));
+    SC_TRY(getrf(st, A6, n6, 0, n6, 1, piv6, dinfo + Z));
+    SC_TRY(getrs(st, A6, n6, 0, n6, piv6, b6, n6, 0, 1, 1));
+    if (x_out) SC_CUDA_TRY(cudaMemcpyAsync(x_out, b6, sizeof(double2) * n6, cudaMemcpyDeviceToDevice, st));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[5], st));
+
+    // ---- a14/a15: beta chain, Q, Pz
+    if (!p->external && (Qc_out || Qh_out)) {
+        double2 *beta, *tv;
+        SC_TRY(ws.get(&beta, (size_t)Z * n4 + n4, WS_BETA, st));
+        tv = beta + (long long)Z * n4;
+        beta0_rhs_kernel<<<grid_for(n4), 256, 0, st>>>(MF, dSx, dSy, dSz0, dEF, b6, k, P.z[0], beta);
+        count_launch();
+        SC_TRY(getrs(st, LU, n4, s4, n4, piv, beta, n4, 0, 1, 1));
+        for (int i = 1; i < Z; ++i) {
+            // t = V_{i-1} (cG_{i-1} .* beta_{i-1}) ; beta_i = GD_i^-1 t
+            scale_cols_kernel<<<dim3(grid_for(n4), 1), 256, 0, st>>>(beta + (long long)(i - 1) * n4, 0,
+                                                                      cG + (long long)(i - 1) * n4, 0, 1, n4,
+                                                                      tv, 0);
+            count_launch();
+            // scale_cols with rows=1: out[c] = in[c] * s[c]
+            SC_TRY(zgemm(st, n4, 1, n4, make_double2(1.0, 0.0), V + (i - 1) * s4, n4, s4, tv, n4, 0,
+                         make_double2(0.0, 0.0), beta + (long long)i * n4, n4, 0, 1));
+            SC_TRY(getrs(st, LU + i * s4, n4, s4, n4, piv + (long long)i * n4, beta + (long long)i * n4, n4, 0,
+                         1, 1));
+        }
+        double2 *Gc, *Gh, *KP;
+        SC_TRY(ws.get(&Gc, (size_t)Z * MF * n2 * 2, WS_PZ, st));
+        Gh = Gc + (long long)Z * MF * n2;
+        SC_TRY(ws.get(&KP, (size_t)Z * MF * MF, WS_OMEGA, st));
+        double2* Qc = Qc_out;
+        double2* Qh = Qh_out;
+        const long long sq = (long long)3 * MF * n2;
+        {
+            dim3 g(grid_for((long long)n2 * n2), Z);
+            q_kernel<<<g, 256, 0, st>>>(V, beta, MF, d_upk, d_wqk, Mx, Qc, Qh, Gc, Gh);
+            count_launch();
+        }
+        if (!p->npz) {
+            dim3 g(grid_for((long long)MF * MF), Z);
+            kp_kernel<<<g, 256, 0, st>>>(Nif, Mx, My, k, KP);
+            count_launch();
+            SC_TRY(zgemm(st, MF, n2, MF, make_double2(1.0, 0.0), KP, MF, (long long)MF * MF, Gc, MF,
+                         (long long)MF * n2, make_double2(0.0, 0.0), Qc + n2, 3 * MF, sq, Z));
+            SC_TRY(zgemm(st, MF, n2, MF, make_double2(1.0, 0.0), KP, MF, (long long)MF * MF, Gh, MF,
+                         (long long)MF * n2, make_double2(0.0, 0.0), Qh + n2, 3 * MF, sq, Z));
+        } else {
+            for (int z = 0; z < Z; ++z) {
+                SC_CUDA_TRY(cudaMemset2DAsync(Qc + z * sq + n2, sizeof(double2) * 3 * MF, 0, sizeof(double2) * MF,
+                                              n2, st));
+                SC_CUDA_TRY(cudaMemset2DAsync(Qh + z * sq + n2, sizeof(double2) * 3 * MF, 0, sizeof(double2) * MF,
+                                              n2, st));
+            }
+        }
+    }
+    if (evl_out) SC_CUDA_TRY(cudaMemcpyAsync(evl_out, evl, sizeof(double2) * Z * n4, cudaMemcpyDeviceToDevice, st));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[6], st));
+
+    // ---- status: eig info per layer + boundary LU info
+    std::vector<int> hinfo(Z + 4, 0);
+    SC_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * (Z + 4), cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < 6; ++i) {
+        float ms = 0.f;
+        SC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
+        ctx->stage_ms[i] = ms;
+    }
+    int first = 0;
+    for (int i = 0; i < Z && !first; ++i) first = hinfo[i];
+    if (info_host) *info_host = first ? first : hinfo[Z];
+    if (first) {
+        set_error("eigensolve did not converge (layer status %d)", first);
+        return SC_NOCONVERGE;
+    }
+    if (hinfo[Z]) {
+        set_error("boundary system is singular (zero pivot in column %d)", hinfo[Z] - 1);
+        return SC_SINGULAR;
+    }
+    return SC_OK;
+}
+
+}  // namespace sc

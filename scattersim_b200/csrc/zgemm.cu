@@ -1,0 +1,120 @@
+// Batched complex128 GEMM, C = alpha * A * B + beta * C (column-major).
+//
+// Replaces cblas_zgemm behind MKL_multiply (third_Lapack.h:74-84) and every
+// dense product of the layer chain, the boundary system and the interior
+// fields (ScatterVolume.cpp:331-334, 447-449, 769-779, 838-839).
+//
+// FP64 throughput on B200 is the same through DFMA and DMMA, so the tile is a
+// register-blocked SIMT DFMA tile: 64 x 64 complex outputs per CTA of 256
+// threads, each thread owning a 4 x 4 complex block strided by 16 so that
+// shared-memory reads and global stores are contiguous across a warp.  The
+// K dimension is staged through shared memory 16 deep; the next tile's global
+// loads are issued into registers before the current tile's math.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sc {
+
+namespace {
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+__global__ void __launch_bounds__(NT, 2)
+zgemm_nn_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
+                long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
+                double2* __restrict__ C, int ldc, long long sC) {
+    __shared__ double2 As[BK][BM];
+    __shared__ double2 Bs[BK][BN + 1];
+    const int bz = blockIdx.z;
+    A += bz * sA;
+    B += bz * sB;
+    C += bz * sC;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+    // global -> register staging: A tile 64x16 (4 per thread), B tile 16x64 (4 per thread)
+    double2 ra[4], rb[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            int r = tid & 63, kk = (tid >> 6) + 4 * i;
+            int gr = m0 + r, gk = k0 + kk;
+            ra[i] = (gr < m && gk < k) ? A[(long long)gk * lda + gr] : make_double2(0.0, 0.0);
+            int kb = tid & 15, c = (tid >> 4) + 16 * i;
+            int gkb = k0 + kb, gc = n0 + c;
+            rb[i] = (gkb < k && gc < n) ? B[(long long)gc * ldb + gkb] : make_double2(0.0, 0.0);
+        }
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            As[(tid >> 6) + 4 * i][tid & 63] = ra[i];
+            Bs[tid & 15][(tid >> 4) + 16 * i] = rb[i];
+        }
+    };
+
+    double2 acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+
+    int nk = (k + BK - 1) / BK;
+    if (nk > 0) {
+        load(0);
+        store();
+    }
+    __syncthreads();
+    for (int t = 0; t < nk; ++t) {
+        if (t + 1 < nk) load((t + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            double2 a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+        if (t + 1 < nk) {
+            store();
+            __syncthreads();
+        }
+    }
+    const bool beta_zero = (beta.x == 0.0 && beta.y == 0.0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        int gc = n0 + ty + 16 * j;
+        if (gc >= n) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            int gr = m0 + tx + 16 * i;
+            if (gr >= m) continue;
+            double2* p = C + (long long)gc * ldc + gr;
+            double2 v = cmul(alpha, acc[i][j]);
+            if (!beta_zero) v = cfma(beta, *p, v);
+            *p = v;
+        }
+    }
+}
+}  // namespace
+
+sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
+                long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
+                int ldc, long long sC, int batch) {
+    if (m <= 0 || n <= 0 || batch <= 0) return SC_OK;
+    dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN, batch);
+    if (grid.y > 65535 || grid.z > 65535) {
+        set_error("zgemm: grid too large (n=%d, batch=%d)", n, batch);
+        return SC_BADINPUT;
+    }
+    zgemm_nn_kernel<<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    count_launch();
+    SC_CHECK_LAUNCH("zgemm");
+    return SC_OK;
+}
+
+}  // namespace sc

@@ -1,0 +1,173 @@
+"""ScatterVolume: the scattervolume solve through the C ABI.
+
+Mirrors the reference's command-line surface (ScatterVolume.cpp:511-529:
+--sample --lambda --direction --ex --ey --ez --n --kappa --size --z --coef
+--psf --external --npz) as keyword arguments with the same defaults.  Device
+buffers are torch tensors (plumbing only); every computation runs in
+libscattersim_b200.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import VolumeDims, VolumeParams, check
+
+
+def _stream_ptr(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Context:
+    """One sc_context per GPU (pooled device workspace)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        self.device = device
+        h = ctypes.c_void_p()
+        check(self.lib.sc_create(ctypes.byref(h), device))
+        self.handle = h
+
+    def close(self):
+        if self.handle is not None and self.handle.value:
+            self.lib.sc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def launches(self) -> int:
+        return int(self.lib.sc_launch_count(self.handle))
+
+    def stage_ms(self):
+        out = (ctypes.c_double * 6)()
+        check(self.lib.sc_volume_stage_ms(self.handle, out))
+        return dict(zip(("fft", "assemble", "eig", "chain", "boundary", "interior"), list(out)))
+
+
+def make_params(lambda_=1.0, direction=(0, 0, 1), ex=(0, 0), ey=(1, 0), ez=(0, 0), n=(1, 1), kappa=0.0,
+                size=(10, 10, 2), z=0.0, coef=(), psf=False, external=False, npz=False) -> VolumeParams:
+    """sc_volume_params with the reference's defaults (ScatterVolume.cpp:511-529)."""
+    p = VolumeParams()
+    p.lambda_ = float(lambda_)
+    for i in range(3):
+        p.direction[i] = float(direction[i])
+        p.size[i] = float(size[i])
+    for i in range(2):
+        p.ex[i], p.ey[i], p.ez[i], p.n[i] = float(ex[i]), float(ey[i]), float(ez[i]), float(n[i])
+    kap = kappa[0] if isinstance(kappa, (tuple, list)) else kappa
+    p.kappa = float(kap)
+    p.z = float(z)
+    coef = tuple(coef)
+    p.ncoef = len(coef)
+    for i, c in enumerate(coef[:2]):
+        p.coef[i] = int(c)
+    p.psf, p.external, p.npz = int(psf), int(external), int(npz)
+    return p
+
+
+def plan(params: VolumeParams, shape) -> VolumeDims:
+    Z, S1, S2 = shape
+    d = VolumeDims()
+    check(_lib.load().sc_volume_plan(ctypes.byref(params), Z, S1, S2, ctypes.byref(d)))
+    return d
+
+
+@dataclass
+class VolumeSolution:
+    dims: VolumeDims
+    shape: tuple
+    x: torch.Tensor          # (6 MF,) complex128: [R_x R_y R_z T_x T_y T_z]
+    evl: torch.Tensor        # (Z, 4 MF)
+    Qc: torch.Tensor         # (Z, 2MF, 3MF) -> column-major 3MF x 2MF blocks
+    Qh: torch.Tensor
+
+
+def solve(ctx: Context, params: VolumeParams, sample: torch.Tensor, fields: bool = True, stream=None):
+    """One scattervolume solve of a device-resident (Z, S1, S2) complex128 sample."""
+    if sample.dim() == 2:
+        sample = sample.unsqueeze(0)
+    if sample.dtype != torch.complex128 or not sample.is_cuda:
+        raise TypeError("sample must be a complex128 CUDA tensor")
+    sample = sample.contiguous()
+    shape = tuple(sample.shape)
+    d = plan(params, shape)
+    MF, Z = d.MF, shape[0]
+    dev = sample.device
+    x = torch.empty(6 * MF, dtype=torch.complex128, device=dev)
+    evl = torch.empty((Z, 4 * MF), dtype=torch.complex128, device=dev)
+    want = fields and not params.external
+    Qc = torch.empty((Z, 2 * MF, 3 * MF), dtype=torch.complex128, device=dev) if want else None
+    Qh = torch.empty((Z, 2 * MF, 3 * MF), dtype=torch.complex128, device=dev) if want else None
+    info = ctypes.c_int(0)
+    check(ctx.lib.sc_volume_solve(ctx.handle, ctypes.byref(params), _ptr(sample), *shape, _ptr(x), _ptr(evl),
+                                  _ptr(Qc), _ptr(Qh), ctypes.byref(info), _stream_ptr(stream)))
+    return VolumeSolution(d, shape, x, evl, Qc, Qh)
+
+
+@dataclass
+class WaveTable:
+    E0: torch.Tensor         # (nw, 3) complex128
+    k: torch.Tensor          # (nw, 3) complex128
+    begin: np.ndarray        # (Z + 2,)
+    end: np.ndarray
+    z_layers: np.ndarray     # (Z + 1,)
+
+
+def waves(ctx: Context, params: VolumeParams, sol: VolumeSolution, ez_mode: int = 0, stream=None) -> WaveTable:
+    """The CoupledWaveStructure wave list of a solution, on the device (cw_unpack order)."""
+    Z, S1, S2 = sol.shape
+    nw = ctypes.c_longlong(0)
+    begin = (ctypes.c_int * (Z + 2))()
+    end = (ctypes.c_int * (Z + 2))()
+    zl = (ctypes.c_double * (Z + 1))()
+    check(ctx.lib.sc_volume_waves(ctx.handle, ctypes.byref(params), Z, S1, S2, None, None, None, None, ez_mode,
+                                  ctypes.byref(nw), begin, end, zl, None, None, None))
+    E0 = torch.empty((nw.value, 3), dtype=torch.complex128, device=sol.x.device)
+    K = torch.empty((nw.value, 3), dtype=torch.complex128, device=sol.x.device)
+    check(ctx.lib.sc_volume_waves(ctx.handle, ctypes.byref(params), Z, S1, S2, _ptr(sol.x), _ptr(sol.evl),
+                                  _ptr(sol.Qc), _ptr(sol.Qh), ez_mode, ctypes.byref(nw), begin, end, zl, _ptr(E0),
+                                  _ptr(K), _stream_ptr(stream)))
+    return WaveTable(E0, K, np.array(begin[:]), np.array(end[:]), np.array(zl[:]))
+
+
+def evaluate(ctx: Context, E0: torch.Tensor, K: torch.Tensor, z_layers, begin, end, points: torch.Tensor,
+             zeps: float = 0.001, precision: int = 0, stream=None) -> torch.Tensor:
+    """E at (P, 3) float64 device points: the gpuEvaluator sum (gpuEvaluator.cu:28-68)."""
+    layers = len(z_layers)
+    zl = (ctypes.c_double * max(layers, 1))(*list(z_layers))
+    b = (ctypes.c_int * (layers + 1))(*[int(v) for v in begin[:layers + 1]])
+    e = (ctypes.c_int * (layers + 1))(*[int(v) for v in end[:layers + 1]])
+    points = points.to(torch.float64).contiguous()
+    out = torch.empty((points.shape[0], 3), dtype=torch.complex128, device=points.device)
+    check(ctx.lib.sc_cw_evaluate(ctx.handle, _ptr(E0.contiguous()), _ptr(K.contiguous()), int(E0.shape[0]), zl, b,
+                                 e, layers, float(zeps), _ptr(points), int(points.shape[0]), _ptr(out),
+                                 int(precision), _stream_ptr(stream)))
+    return out
+
+
+def eigensolve(ctx: Context, A: torch.Tensor, stream=None):
+    """Batched eigenvalues / right eigenvectors of (B, n, n) complex128 matrices (row-major torch view)."""
+    if A.dim() == 2:
+        A = A.unsqueeze(0)
+    B, n, _ = A.shape
+    # C ABI is column-major: pass A^T's storage, i.e. the transpose of each matrix
+    Acm = A.transpose(1, 2).contiguous()
+    w = torch.empty((B, n), dtype=torch.complex128, device=A.device)
+    V = torch.empty((B, n, n), dtype=torch.complex128, device=A.device)
+    info = (ctypes.c_int * B)()
+    check(ctx.lib.sc_eigensolve_batched(ctx.handle, _ptr(Acm), n, B, _ptr(w), _ptr(V), info,
+                                        _stream_ptr(stream)))
+    return w, V.transpose(1, 2)      # V[b][:, j] is eigenvector j
