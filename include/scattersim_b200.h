@@ -142,9 +142,19 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
                           int Z, int S1, int S2, void* x, void* evl, void* Qc, void* Qh,
                           int* info, void* stream);
 
-/* Per-stage device milliseconds of the last sc_volume_solve on this context:
- * [fft, assemble, eig, chain, boundary, interior]. */
-sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms6);
+/* Device milliseconds of the last sc_volume_solve on this context:
+ * [fft, assemble, eig, chain, boundary, interior, qr-kernel, total]. */
+sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8);
+
+/* QR statistics per matrix of the last eigensolve on this context, 8 values
+ * each: multishift sweeps, then SM cycles spent on shifts, bulge chase,
+ * far-right updates, far-row/Schur-vector updates, small blocks, (unused),
+ * total.  Zero-filled beyond the last batch. */
+sc_status sc_qr_stats(sc_context* ctx, long long* out, int count);
+
+/* Measured FP64 FMA throughput of this device (TFLOP/s): the roofline
+ * denominator of the FP64 kernels. */
+sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops);
 
 /* Wave table of a solved volume in cw_unpack order: Pi, then per boundary l
  * its reflected and transmitted lists (ScatterVolume.cpp:907-987,

@@ -10,7 +10,7 @@ struct sc_context {
     int device = 0;
     sc::Workspace ws;
     cudaEvent_t ev[8] = {};
-    double stage_ms[6] = {};
+    double stage_ms[8] = {};   // fft assemble eig chain boundary interior | qr | total
     uint64_t launches_at_create = 0;
 };
 

@@ -10,14 +10,15 @@
 //                     from the left to the trailing block).
 //   2. orghr_kernel   explicit Q = H(0) H(1) ... H(n-2) (initial Schur vectors).
 //   3. hqr_kernel     complex single-shift QR to Schur form T = Z^H A Z with
-//                     Wilkinson shifts, Ahues-Tisseur deflation and exceptional
-//                     shifts.  The bulge is chased through a 64 x 64 window kept
-//                     in shared memory by one warp; the window's rotations are
-//                     recorded and then streamed by the whole CTA over the rows
-//                     to the right, the columns above and the Schur vectors
-//                     (one thread per far row/column, two live values each).
-//                     Active blocks of <= 64 rows are finished entirely in shared
-//                     memory with the accumulated unitary applied afterwards.
+//                     Ahues-Tisseur deflation.  Large active blocks take
+//                     multishift sweeps: 16 shifts (eigenvalues of the trailing
+//                     16 x 16 block) as a chain of single-shift bulges chased in
+//                     lockstep by 16 warps through a 96 x 96 shared-memory
+//                     window; the window's rotations are then streamed over the
+//                     rows to the right, the columns above and the Schur vectors.
+//                     Active blocks of <= 64 rows are finished in shared memory
+//                     (Wilkinson shifts) with the accumulated unitary applied
+//                     afterwards.
 //   4. trevc_kernel   eigenvectors of T by back substitution, one warp per
 //                     eigenvalue, small pivots raised to eps*|lambda|.
 //   5. V = Z * Y      batched zgemm, then unit 2-norm columns (zgeev's
@@ -39,23 +40,24 @@ constexpr double SAFMIN = DBL_MIN;
 
 __device__ __forceinline__ bool cz(double2 a) { return a.x == 0.0 && a.y == 0.0; }
 
-// [c s; -conj(s) c] [f; g] = [r; 0], c real
+// [c s; -conj(s) c] [f; g] = [r; 0], c real (no overflow scaling: the
+// matrices here are O(1)-scaled; two FP64 rsqrt instead of hypot/divisions)
 __device__ __forceinline__ void zlartg(double2 f, double2 g, double& c, double2& s) {
-    if (cz(g)) {
+    const double f2 = cnorm2(f), g2 = cnorm2(g);
+    if (g2 == 0.0) {
         c = 1.0;
         s = make_double2(0.0, 0.0);
         return;
     }
-    double fa = cabs(f), ga = cabs(g);
-    if (fa == 0.0) {
+    if (f2 == 0.0) {
+        const double rg = rsqrt(g2);
         c = 0.0;
-        s = make_double2(g.x / ga, -g.y / ga);
+        s = make_double2(g.x * rg, -g.y * rg);
         return;
     }
-    double d = hypot(fa, ga);
-    c = fa / d;
-    double2 fs = make_double2(f.x / fa, f.y / fa);
-    s = cscale(cmulc(fs, g), 1.0 / d);   // fs * conj(g) / d
+    const double rf = rsqrt(f2), rd = rsqrt(f2 + g2);
+    c = f2 * rf * rd;
+    s = cscale(cmulc(f, g), rf * rd);   // f conj(g) / (|f| d)
 }
 // rows: a' = c a + s b ; b' = -conj(s) a + c b
 __device__ __forceinline__ void rot_rows(double c, double2 s, double2& a, double2& b) {
@@ -181,19 +183,29 @@ orghr_kernel(double2* Aall, int n, long long sA, const double2* tauall, double2*
 }
 
 // ------------------------------------------------------------------ hqr
+constexpr int NSH = 16;   // shifts (bulges) per multishift sweep, one warp each
+constexpr int WB = 96;    // chase window (rows/cols kept in shared memory)
+constexpr int SEP = 3;    // rows between consecutive bulges of a chain
+
 struct HqrSmem {
-    double2 Hs[W * W];      // window / small block, column-major, ld W
-    double2 U[W * W];       // accumulated unitary of a small block
-    double2 chunk[W * 32];  // staging for the small-block far products
-    double rc[W];           // recorded rotations of a sweep window
-    double2 rs[W];
-    double red_v[HT / 32];
+    union {
+        struct {
+            double2 Hs[W * W];       // small block, column-major, ld W
+            double2 U[W * W];        // its accumulated unitary
+            double2 chunk[W * 32];   // staging for the small-block far products
+        } s;
+        double2 win[WB * WB];        // chase window, column-major, ld WB
+    } u;
+    double rc[WB][NSH];              // rotation q of bulge i in this window: [q][i]
+    double2 rs[WB][NSH];
+    int bpos[NSH], bstart[NSH], bcnt[NSH], boff[NSH];
+    double2 shifts[NSH];
     int red_i[HT / 32];
-    int s_int[4];
-    double2 s_shift;
+    int s_int[8];
 };
 
-__device__ __forceinline__ double2& HS(HqrSmem& S, int i, int j) { return S.Hs[j * W + i]; }
+__device__ __forceinline__ double2& HS(HqrSmem& S, int i, int j) { return S.u.s.Hs[j * W + i]; }
+__device__ __forceinline__ double2& WN(HqrSmem& S, int i, int j) { return S.u.win[j * WB + i]; }
 
 // Ahues-Tisseur deflation test for subdiagonal k (rows/cols relative to a
 // column-major array with leading dimension ld); lo..hi is the active range.
@@ -238,15 +250,18 @@ __device__ double2 wilkinson(double2 h11, double2 h12, double2 h21, double2 h22)
     return t;
 }
 
-// The small-block QR inside shared memory, run by warp 0.  Returns false on
-// iteration cap.  Block size m, accumulates U.
+// Single-shift QR of an m x m block held in S.Hs, run by one warp.  With
+// ACC the rotations are accumulated into S.U (the block then lies in the full
+// Schur form); without it only the eigenvalues (diagonal) matter.  Returns
+// false on the iteration cap.
+template <bool ACC>
 __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
     const int lane = threadIdx.x & 31;
     int hi = m - 1;
     int its = 0, total = 0;
     while (hi >= 0) {
         int lo = hi;
-        while (lo > 0 && !negligible(S.Hs, W, lo, 0, hi)) --lo;
+        while (lo > 0 && !negligible(S.u.s.Hs, W, lo, 0, hi)) --lo;
         if (lo > 0) {
             if (lane == 0) HS(S, lo, lo - 1) = make_double2(0.0, 0.0);
             __syncwarp();
@@ -266,6 +281,8 @@ __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
         } else {
             sh = wilkinson(HS(S, hi - 1, hi - 1), HS(S, hi - 1, hi), HS(S, hi, hi - 1), HS(S, hi, hi));
         }
+        const int jend = ACC ? m : hi + 1;   // row ops extend to the block edge only when accumulating
+        const int ibeg = ACC ? 0 : lo;
         for (int k = lo; k < hi; ++k) {
             double c;
             double2 s;
@@ -273,9 +290,8 @@ __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
                 zlartg(csub(HS(S, lo, lo), sh), HS(S, lo + 1, lo), c, s);
             else
                 zlartg(HS(S, k, k - 1), HS(S, k + 1, k - 1), c, s);
-            // rows k, k+1 over columns max(k-1, lo)..m-1 (full block width)
             const int c0 = (k == lo) ? lo : k - 1;
-            for (int j = c0 + lane; j < m; j += 32) {
+            for (int j = c0 + lane; j < jend; j += 32) {
                 double2 a = HS(S, k, j), bb = HS(S, k + 1, j);
                 rot_rows(c, s, a, bb);
                 HS(S, k, j) = a;
@@ -284,17 +300,19 @@ __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
             __syncwarp();
             if (k > lo && lane == 0) HS(S, k + 1, k - 1) = make_double2(0.0, 0.0);
             const int r1 = (k + 2 < hi ? k + 2 : hi);
-            for (int i = lane; i <= r1; i += 32) {
+            for (int i = ibeg + lane; i <= r1; i += 32) {
                 double2 a = HS(S, i, k), bb = HS(S, i, k + 1);
                 rot_cols(c, s, a, bb);
                 HS(S, i, k) = a;
                 HS(S, i, k + 1) = bb;
             }
-            for (int i = lane; i < m; i += 32) {
-                double2 a = S.U[k * W + i], bb = S.U[(k + 1) * W + i];
-                rot_cols(c, s, a, bb);
-                S.U[k * W + i] = a;
-                S.U[(k + 1) * W + i] = bb;
+            if (ACC) {
+                for (int i = lane; i < m; i += 32) {
+                    double2 a = S.u.s.U[k * W + i], bb = S.u.s.U[(k + 1) * W + i];
+                    rot_cols(c, s, a, bb);
+                    S.u.s.U[k * W + i] = a;
+                    S.u.s.U[(k + 1) * W + i] = bb;
+                }
             }
             __syncwarp();
         }
@@ -311,13 +329,13 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
         const int nc = (n - j0) < 32 ? (n - j0) : 32;
         for (int t = tid; t < m * nc; t += HT) {
             int r = t % m, c = t / m;
-            S.chunk[c * W + r] = H[(long long)(j0 + c) * n + lo + r];
+            S.u.s.chunk[c * W + r] = H[(long long)(j0 + c) * n + lo + r];
         }
         __syncthreads();
         for (int t = tid; t < m * nc; t += HT) {
             int r = t % m, c = t / m;
             double2 acc = make_double2(0.0, 0.0);
-            for (int l = 0; l < m; ++l) acc = cfma(cconj(S.U[r * W + l]), S.chunk[c * W + l], acc);
+            for (int l = 0; l < m; ++l) acc = cfma(cconj(S.u.s.U[r * W + l]), S.u.s.chunk[c * W + l], acc);
             H[(long long)(j0 + c) * n + lo + r] = acc;
         }
         __syncthreads();
@@ -330,13 +348,13 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
             const int nr = (rows - i0) < 32 ? (rows - i0) : 32;
             for (int t = tid; t < m * nr; t += HT) {
                 int r = t % nr, c = t / nr;
-                S.chunk[c * 32 + r] = X[(long long)(lo + c) * n + i0 + r];
+                S.u.s.chunk[c * 32 + r] = X[(long long)(lo + c) * n + i0 + r];
             }
             __syncthreads();
             for (int t = tid; t < m * nr; t += HT) {
                 int r = t % nr, c = t / nr;
                 double2 acc = make_double2(0.0, 0.0);
-                for (int l = 0; l < m; ++l) acc = cfma(S.chunk[l * 32 + r], S.U[c * W + l], acc);
+                for (int l = 0; l < m; ++l) acc = cfma(S.u.s.chunk[l * 32 + r], S.u.s.U[c * W + l], acc);
                 X[(long long)(lo + c) * n + i0 + r] = acc;
             }
             __syncthreads();
@@ -344,9 +362,213 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
     }
 }
 
+// Applies a window's recorded rotations outside the window, in their true
+// step order: tiles of 32 far columns (row rotations, rows [ws, we)) and of
+// 32 far rows (column rotations, columns [ws, we)) are staged in shared
+// memory; each tile vector is owned by 16 lanes, lane i applying bulge i's
+// rotation of the current step (same-step rotations touch disjoint rows).
+__device__ void far_apply(HqrSmem& S, double2* H, double2* Z, int n, int ws, int we, int ns, int steps,
+                          long long* cyc) {
+    const long long tf0 = clock64();
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int wm = we - ws;
+    const int bi = lane & 15;                 // bulge of this lane
+    const int half = lane >> 4;               // which of the warp's two vectors
+    const int vi = 2 * wid + half;            // vector index in the tile (0..31)
+    const bool lane_ok = bi < ns;
+    const int bst = lane_ok ? S.bstart[bi] - ws : 0;
+    const int bof = lane_ok ? S.boff[bi] : 0;
+    const int bct = lane_ok ? S.bcnt[bi] : 0;
+    double2* stage = S.u.win;
+    constexpr int LDC = WB + 1;               // column tile leading dimension
+    constexpr int LDR = 33;                   // row tile leading dimension
+    // rows [ws, we) of columns [we, n): row rotations
+    for (int j0 = we; j0 < n; j0 += 32) {
+        const int nc = (n - j0) < 32 ? (n - j0) : 32;
+        for (int q = tid; q < wm * nc; q += HT) {
+            int r = q % wm, c = q / wm;
+            stage[c * LDC + r] = H[(long long)(j0 + c) * n + ws + r];
+        }
+        __syncthreads();
+        double2* v = stage + vi * LDC;
+        for (int tau = 0; tau < steps; ++tau) {
+            const int q = tau - bof;
+            if (vi < nc && lane_ok && q >= 0 && q < bct) {
+                const int r = bst + q;
+                double2 a = v[r], b2 = v[r + 1];
+                rot_rows(S.rc[q][bi], S.rs[q][bi], a, b2);
+                v[r] = a;
+                v[r + 1] = b2;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int q = tid; q < wm * nc; q += HT) {
+            int r = q % wm, c = q / wm;
+            H[(long long)(j0 + c) * n + ws + r] = stage[c * LDC + r];
+        }
+        __syncthreads();
+    }
+    const long long tf1 = clock64();
+    if (threadIdx.x == 0) cyc[3] += tf1 - tf0;
+    // rows [0, ws) of H and [0, n) of Z, columns [ws, we): column rotations
+    const int rows_total = ws + n;
+    for (int i0 = 0; i0 < rows_total; i0 += 32) {
+        const int nr = (rows_total - i0) < 32 ? (rows_total - i0) : 32;
+        for (int q = tid; q < wm * nr; q += HT) {
+            int rr = q % nr, c = q / nr;
+            const int g = i0 + rr;
+            const double2* src = (g < ws) ? (H + g) : (Z + (g - ws));
+            stage[c * LDR + rr] = src[(long long)(ws + c) * n];
+        }
+        __syncthreads();
+        for (int tau = 0; tau < steps; ++tau) {
+            const int q = tau - bof;
+            if (vi < nr && lane_ok && q >= 0 && q < bct) {
+                const int cc = bst + q;
+                double2 a = stage[cc * LDR + vi], b2 = stage[(cc + 1) * LDR + vi];
+                rot_cols(S.rc[q][bi], S.rs[q][bi], a, b2);
+                stage[cc * LDR + vi] = a;
+                stage[(cc + 1) * LDR + vi] = b2;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int q = tid; q < wm * nr; q += HT) {
+            int rr = q % nr, c = q / nr;
+            const int g = i0 + rr;
+            double2* dst = (g < ws) ? (H + g) : (Z + (g - ws));
+            dst[(long long)(ws + c) * n] = stage[c * LDR + rr];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cyc[4] += clock64() - tf1;
+}
+
+// One multishift sweep over the active block [lo, ihi] with ns shifts in
+// S.shifts.  The ns single-shift bulges are introduced SEP rows apart and
+// advanced in lockstep: every step, warp i computes bulge i's rotation and
+// applies it to its two rows (phase 1), then to its two columns (phase 2).
+// Rotations of different bulges act on disjoint rows / disjoint columns and
+// row and column operations commute, so each phase runs in parallel.  The
+// chase stays inside a WB x WB shared-memory window; at the end of a window
+// the recorded rotations are applied to the rows to its right, the columns
+// above it and the Schur vectors.  There they are applied bulge by bulge
+// (front bulge first): two rotations of different bulges that touch a common
+// row are, in the true step order, already front-bulge first, and all other
+// pairs commute, so the reordering is exact.
+__device__ bool multishift_sweep(HqrSmem& S, double2* H, double2* Z, int n, int lo, int ihi, int ns, long long* cyc) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid < NSH) {
+        S.bpos[tid] = lo;
+        S.bcnt[tid] = 0;
+    }
+    __syncthreads();
+    int t = 0;   // global step (bulge i is introduced at step SEP*i)
+    while (true) {
+        // ---- all bulges finished?
+        int front = -1, rear = -1;
+        for (int i = 0; i < ns; ++i) {
+            bool done = S.bpos[i] > ihi - 1;
+            bool intro = t >= SEP * i || S.bpos[i] > lo;
+            if (!done && front < 0) front = i;
+            if (!done && intro) rear = i;
+        }
+        if (front < 0) break;
+        const bool all_intro = (SEP * (ns - 1) <= t) || S.bpos[ns - 1] > lo;
+        const int ws = all_intro ? (S.bpos[rear] - 1 > lo ? S.bpos[rear] - 1 : lo) : lo;
+        const int we = (ws + WB < ihi + 1) ? ws + WB : ihi + 1;
+        const int wm = we - ws;
+        for (int q = tid; q < WB * WB; q += HT) {
+            int i = q % WB, j = q / WB;
+            S.u.win[q] = (i < wm && j < wm) ? H[(long long)(ws + j) * n + ws + i] : make_double2(0.0, 0.0);
+        }
+        if (tid < NSH) {
+            S.bstart[tid] = S.bpos[tid];
+            S.bcnt[tid] = 0;
+            S.boff[tid] = 0;
+        }
+        __syncthreads();
+        const long long tch = clock64();
+        int steps = 0;
+        while (true) {
+            // front bulge of this step and its room in the window
+            int fr = -1;
+            for (int i = 0; i < ns; ++i)
+                if (S.bpos[i] <= ihi - 1) {
+                    fr = i;
+                    break;
+                }
+            if (fr < 0) break;
+            const int rf = S.bpos[fr];
+            if (!(rf + 2 <= we - 1 || we == ihi + 1)) break;
+            // phase 1: rotations and row operations
+            double c = 1.0;
+            double2 s = make_double2(0.0, 0.0);
+            int r = -1;
+            bool act = false, intro = false;
+            if (wid < ns) {
+                r = S.bpos[wid];
+                intro = (t == SEP * wid);
+                act = (r <= ihi - 1) && (intro || r > lo);
+                if (act) {
+                    const int lr = r - ws;
+                    if (intro)
+                        zlartg(csub(WN(S, lr, lr), S.shifts[wid]), WN(S, lr + 1, lr), c, s);
+                    else
+                        zlartg(WN(S, lr, lr - 1), WN(S, lr + 1, lr - 1), c, s);
+                    const int c0 = intro ? lr : lr - 1;
+                    for (int j = c0 + lane; j < wm; j += 32) {
+                        double2 a = WN(S, lr, j), bb = WN(S, lr + 1, j);
+                        rot_rows(c, s, a, bb);
+                        WN(S, lr, j) = a;
+                        WN(S, lr + 1, j) = bb;
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (!intro) WN(S, lr + 1, lr - 1) = make_double2(0.0, 0.0);
+                        if (S.bcnt[wid] == 0) S.boff[wid] = steps;
+                        S.rc[S.bcnt[wid]][wid] = c;
+                        S.rs[S.bcnt[wid]][wid] = s;
+                    }
+                }
+            }
+            __syncthreads();
+            // phase 2: column operations
+            if (act) {
+                const int lr = r - ws;
+                const int r1 = ((r + 2 < ihi) ? r + 2 : ihi) - ws;
+                for (int i = lane; i <= r1; i += 32) {
+                    double2 a = WN(S, i, lr), bb = WN(S, i, lr + 1);
+                    rot_cols(c, s, a, bb);
+                    WN(S, i, lr) = a;
+                    WN(S, i, lr + 1) = bb;
+                }
+                if (lane == 0) {
+                    S.bcnt[wid] += 1;
+                    S.bpos[wid] = r + 1;
+                }
+            }
+            ++t;
+            ++steps;
+            __syncthreads();
+        }
+        if (steps == 0) return false;   // no room to move: cannot happen with WB >= SEP*NSH + 8
+        if (tid == 0) cyc[2] += clock64() - tch;
+        // ---- write the window back and apply its rotations outside it
+        for (int q = tid; q < wm * wm; q += HT) {
+            int i = q % wm, j = q / wm;
+            H[(long long)(ws + j) * n + ws + i] = S.u.win[j * WB + i];
+        }
+        __syncthreads();
+        far_apply(S, H, Z, n, ws, we, ns, steps, cyc);
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(HT, 1)
 hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int* info,
-           int maxsweeps) {
+           int maxsweeps, long long* stats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HqrSmem& S = *reinterpret_cast<HqrSmem*>(smem_raw);
     const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -355,6 +577,9 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
     double2* w = wall + (long long)b * n;
     int ihi = n - 1, its = 0, sweeps = 0;
     bool failed = false;
+    // phase cycle counters (thread 0): shifts, chase, far-right, far-rows, small blocks, deflation scans
+    long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long t0 = clock64();
     while (ihi >= 0) {
         // ---- deflation point: largest k in (0, ihi] with negligible H[k, k-1]
         int best = 0;
@@ -385,132 +610,72 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
         }
         const int m = ihi - lo + 1;
         if (m <= W) {
+            const long long tsm = clock64();
             // ---- finish the block in shared memory
-            for (int t = tid; t < W * W; t += HT) {
-                int i = t % W, j = t / W;
-                S.Hs[t] = (i < m && j < m) ? H[(long long)(lo + j) * n + lo + i] : make_double2(0.0, 0.0);
-                S.U[t] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            for (int q = tid; q < W * W; q += HT) {
+                int i = q % W, j = q / W;
+                S.u.s.Hs[q] = (i < m && j < m) ? H[(long long)(lo + j) * n + lo + i] : make_double2(0.0, 0.0);
+                S.u.s.U[q] = make_double2(i == j ? 1.0 : 0.0, 0.0);
             }
             __syncthreads();
             if (wid == 0) {
-                bool ok = small_qr_warp(S, m, 30 * m + 30);
+                bool ok = small_qr_warp<true>(S, m, 30 * m + 30);
                 if (lane == 0) S.s_int[1] = ok ? 1 : 0;
             }
             __syncthreads();
             if (!S.s_int[1]) failed = true;
-            for (int t = tid; t < m * m; t += HT) {
-                int i = t % m, j = t / m;
-                H[(long long)(lo + j) * n + lo + i] = S.Hs[j * W + i];
+            for (int q = tid; q < m * m; q += HT) {
+                int i = q % m, j = q / m;
+                H[(long long)(lo + j) * n + lo + i] = S.u.s.Hs[j * W + i];
             }
             __syncthreads();
             small_block_far(S, H, Z, n, lo, m);
-            for (int k = lo + tid; k <= ihi; k += HT) w[k] = S.Hs[(k - lo) * W + (k - lo)];
+            for (int k = lo + tid; k <= ihi; k += HT) w[k] = S.u.s.Hs[(k - lo) * W + (k - lo)];
             __syncthreads();
+            if (tid == 0) cyc[5] += clock64() - tsm;
             if (failed) break;
             ihi = lo - 1;
             its = 0;
             continue;
         }
-        // ---- one single-shift sweep over [lo, ihi] through shared-memory windows
         if (++sweeps > maxsweeps) {
             failed = true;
             break;
         }
         ++its;
-        if (tid == 0) {
-            double2 sh;
-            if (its % 30 == 10) {
-                sh = cadd(make_double2(0.75 * fabs(H[(long long)lo * n + lo + 1].x), 0.0), H[(long long)lo * n + lo]);
-            } else if (its % 30 == 20) {
-                sh = cadd(make_double2(0.75 * fabs(H[(long long)(ihi - 1) * n + ihi].x), 0.0),
-                          H[(long long)ihi * n + ihi]);
-            } else {
-                sh = wilkinson(H[(long long)(ihi - 1) * n + ihi - 1], H[(long long)ihi * n + ihi - 1],
-                               H[(long long)(ihi - 1) * n + ihi], H[(long long)ihi * n + ihi]);
-            }
-            S.s_shift = sh;
+        // ---- shifts: eigenvalues of the trailing ns x ns block
+        const long long tsh = clock64();
+        const int ns = NSH;
+        for (int q = tid; q < W * W; q += HT) {
+            int i = q % W, j = q / W;
+            S.u.s.Hs[q] = (i < ns && j < ns) ? H[(long long)(ihi - ns + 1 + j) * n + ihi - ns + 1 + i]
+                                             : make_double2(0.0, 0.0);
         }
         __syncthreads();
-        const double2 sh = S.s_shift;
-        int k = lo;
-        while (k <= ihi - 1) {
-            const int ws = (k == lo) ? lo : k - 1;
-            const int we = (ws + W < ihi + 1) ? ws + W : ihi + 1;   // exclusive
-            const int kend = (we == ihi + 1) ? ihi - 1 : we - 3;
-            const int wm = we - ws;
-            for (int t = tid; t < W * W; t += HT) {
-                int i = t % W, j = t / W;
-                S.Hs[t] = (i < wm && j < wm) ? H[(long long)(ws + j) * n + ws + i] : make_double2(0.0, 0.0);
+        if (wid == 0) small_qr_warp<false>(S, ns, 30 * ns);
+        __syncthreads();
+        if (tid < ns) {
+            double2 sh = S.u.s.Hs[tid * W + tid];
+            if (its % 6 == 0) {
+                // exceptional shifts: perturb by the size of the last subdiagonal
+                double e = 0.75 * cabs1(H[(long long)(ihi - 1) * n + ihi]);
+                sh = cadd(sh, make_double2(e * (1.0 + 0.1 * tid), 0.0));
             }
-            __syncthreads();
-            if (wid == 0) {
-                for (int kk = k; kk <= kend; ++kk) {
-                    const int lk = kk - ws;
-                    double c;
-                    double2 s;
-                    if (kk == lo)
-                        zlartg(csub(HS(S, lk, lk), sh), HS(S, lk + 1, lk), c, s);
-                    else
-                        zlartg(HS(S, lk, lk - 1), HS(S, lk + 1, lk - 1), c, s);
-                    const int c0 = (kk == lo) ? lk : lk - 1;
-                    for (int j = c0 + lane; j < wm; j += 32) {
-                        double2 a = HS(S, lk, j), bb = HS(S, lk + 1, j);
-                        rot_rows(c, s, a, bb);
-                        HS(S, lk, j) = a;
-                        HS(S, lk + 1, j) = bb;
-                    }
-                    __syncwarp();
-                    if (kk > lo && lane == 0) HS(S, lk + 1, lk - 1) = make_double2(0.0, 0.0);
-                    const int r1 = ((kk + 2 < ihi) ? kk + 2 : ihi) - ws;
-                    for (int i = lane; i <= r1; i += 32) {
-                        double2 a = HS(S, i, lk), bb = HS(S, i, lk + 1);
-                        rot_cols(c, s, a, bb);
-                        HS(S, i, lk) = a;
-                        HS(S, i, lk + 1) = bb;
-                    }
-                    if (lane == 0) {
-                        S.rc[kk - k] = c;
-                        S.rs[kk - k] = s;
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            for (int t = tid; t < wm * wm; t += HT) {
-                int i = t % wm, j = t / wm;
-                H[(long long)(ws + j) * n + ws + i] = S.Hs[j * W + i];
-            }
-            const int nrot = kend - k + 1;
-            // far right: rows k..kend+1, columns we..n-1 (row rotations, streamed)
-            for (int j = we + tid; j < n; j += HT) {
-                double2* p = H + (long long)j * n + k;
-                double2 carry = p[0];
-                for (int t = 0; t < nrot; ++t) {
-                    double2 nx = p[t + 1];
-                    rot_rows(S.rc[t], S.rs[t], carry, nx);
-                    p[t] = carry;
-                    carry = nx;
-                }
-                p[nrot] = carry;
-            }
-            // far above: rows 0..ws-1, columns k..kend+1 ; and Z rows 0..n-1
-            for (int r = tid; r < ws + n; r += HT) {
-                double2* base = (r < ws) ? (H + r) : (Z + (r - ws));
-                double2* p = base + (long long)k * n;
-                double2 carry = p[0];
-                for (int t = 0; t < nrot; ++t) {
-                    double2 nx = p[(long long)(t + 1) * n];
-                    rot_cols(S.rc[t], S.rs[t], carry, nx);
-                    p[(long long)t * n] = carry;
-                    carry = nx;
-                }
-                p[(long long)nrot * n] = carry;
-            }
-            __syncthreads();
-            k = kend + 1;
+            S.shifts[tid] = sh;
+        }
+        __syncthreads();
+        if (tid == 0) cyc[1] += clock64() - tsh;
+        if (!multishift_sweep(S, H, Z, n, lo, ihi, ns, cyc)) {
+            failed = true;
+            break;
         }
     }
     if (tid == 0 && info != nullptr) info[b] = failed ? (ihi + 1 > 0 ? ihi + 1 : 1) : 0;
+    if (tid == 0 && stats != nullptr) {
+        cyc[7] = clock64() - t0;
+        stats[(long long)b * 8 + 0] = sweeps;
+        for (int q = 1; q < 8; ++q) stats[(long long)b * 8 + q] = cyc[q];
+    }
 }
 
 // ------------------------------------------------------------------ trevc
@@ -604,8 +769,14 @@ sc_status eig_batched(cudaStream_t st, double2* A, int n, int batch, double2* ev
     count_launch();
     orghr_kernel<<<batch, HT, vsm, st>>>(A, n, sA, tau, Z);
     count_launch();
-    hqr_kernel<<<batch, HT, sizeof(HqrSmem), st>>>(A, Z, n, sA, evl, info, 60 * n + 100);
+    for (auto& e : ws.ev_hqr)
+        if (!e) SC_CUDA_TRY(cudaEventCreate(&e));
+    SC_TRY(ws.get(&ws.hqr_stats, (size_t)batch * 8, WS_STATS, st));
+    ws.hqr_batch = batch;
+    SC_CUDA_TRY(cudaEventRecord(ws.ev_hqr[0], st));
+    hqr_kernel<<<batch, HT, sizeof(HqrSmem), st>>>(A, Z, n, sA, evl, info, 60 * n + 100, ws.hqr_stats);
     count_launch();
+    SC_CUDA_TRY(cudaEventRecord(ws.ev_hqr[1], st));
     SC_CHECK_LAUNCH("hqr");
     // Y (upper triangular eigenvectors of T) into V, then V = Z * Y
     double2* Y = nullptr;

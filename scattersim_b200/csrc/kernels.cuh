@@ -12,13 +12,18 @@ enum WsSlot {
     WS_NF, WS_NIF, WS_OMEGA, WS_BMAT, WS_CMAT, WS_MU, WS_W, WS_CW,
     WS_V, WS_EVL, WS_GD, WS_GC, WS_PIV, WS_INFO, WS_T, WS_T2,
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
-    WS_EVAL_W, WS_EVAL_IDX,
+    WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_COUNT
 };
 
 struct Workspace {
     void* ptr[WS_COUNT] = {};
     size_t bytes[WS_COUNT] = {};
+    // events bracketing the last QR (hqr_kernel) launch, for live roofline timing
+    cudaEvent_t ev_hqr[2] = {nullptr, nullptr};
+    // per-matrix QR statistics of the last launch: sweeps and phase cycles
+    long long* hqr_stats = nullptr;
+    int hqr_batch = 0;
     template <typename T>
     sc_status get(T** out, size_t count, int slot, cudaStream_t st) {
         size_t need = count * sizeof(T);
@@ -47,6 +52,9 @@ struct Workspace {
         return SC_OK;
     }
     void release() {
+        for (auto& e : ev_hqr)
+            if (e) cudaEventDestroy(e);
+        ev_hqr[0] = ev_hqr[1] = nullptr;
         for (int i = 0; i < WS_COUNT; ++i) {
             if (ptr[i]) cudaFree(ptr[i]);
             ptr[i] = nullptr;

@@ -615,6 +615,13 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         SC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
         ctx->stage_ms[i] = ms;
     }
+    {
+        float ms = 0.f;
+        SC_CUDA_TRY(cudaEventElapsedTime(&ms, ws.ev_hqr[0], ws.ev_hqr[1]));
+        ctx->stage_ms[6] = ms;
+        SC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]));
+        ctx->stage_ms[7] = ms;
+    }
     int first = 0;
     for (int i = 0; i < Z && !first; ++i) first = hinfo[i];
     if (info_host) *info_host = first ? first : hinfo[Z];

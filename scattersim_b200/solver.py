@@ -52,9 +52,22 @@ class Context:
         return int(self.lib.sc_launch_count(self.handle))
 
     def stage_ms(self):
-        out = (ctypes.c_double * 6)()
+        """Device ms of the last solve per stage, plus the QR kernel alone and the total."""
+        out = (ctypes.c_double * 8)()
         check(self.lib.sc_volume_stage_ms(self.handle, out))
-        return dict(zip(("fft", "assemble", "eig", "chain", "boundary", "interior"), list(out)))
+        return dict(zip(("fft", "assemble", "eig", "chain", "boundary", "interior", "qr", "total"), list(out)))
+
+    def qr_stats(self, count: int):
+        """Per matrix of the last eigensolve: sweeps and SM cycles of the QR phases."""
+        out = (ctypes.c_longlong * (8 * count))()
+        check(self.lib.sc_qr_stats(self.handle, out, count))
+        keys = ("sweeps", "shifts", "chase", "far_right", "far_rows", "small", "unused", "total")
+        return [dict(zip(keys, out[8 * i:8 * i + 8])) for i in range(count)]
+
+    def fp64_peak_tflops(self) -> float:
+        v = ctypes.c_double(0.0)
+        check(self.lib.sc_fp64_peak_probe(self.handle, ctypes.byref(v)))
+        return v.value
 
 
 def make_params(lambda_=1.0, direction=(0, 0, 1), ex=(0, 0), ey=(1, 0), ez=(0, 0), n=(1, 1), kappa=0.0,
