@@ -4,11 +4,9 @@
 // ScatterVolume.cpp:253-277).
 //
 // Pipeline (one CTA per matrix for the sequential phases):
-//   1. gehrd_kernel   Householder reduction to upper Hessenberg form
-//                     (the zgehd2 recurrence: reflector from the column below
-//                     the subdiagonal, applied from the right to all rows and
-//                     from the left to the trailing block).
-//   2. orghr_kernel   explicit Q = H(0) H(1) ... H(n-2) (initial Schur vectors).
+//   1-2. hessenberg_blocked (hess.cu)  blocked Householder reduction to upper
+//                     Hessenberg form and the explicit Q = H(0) ... H(n-2)
+//                     (the initial Schur vectors).
 //   3. hqr_kernel     complex single-shift QR to Schur form T = Z^H A Z with
 //                     Ahues-Tisseur deflation.  Large active blocks take
 //                     multishift sweeps: 16 shifts (eigenvalues of the trailing
@@ -30,15 +28,18 @@
 
 #include <cfloat>
 
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
 namespace sc {
 
 namespace {
-constexpr int HT = 512;     // threads per CTA for gehrd / orghr / hqr
+constexpr int HT = 512;     // threads per CTA of the QR kernel
 constexpr int W = 64;       // shared-memory window
 constexpr double ULP = DBL_EPSILON;
 constexpr double SAFMIN = DBL_MIN;
 
-__device__ __forceinline__ bool cz(double2 a) { return a.x == 0.0 && a.y == 0.0; }
 
 // [c s; -conj(s) c] [f; g] = [r; 0], c real (no overflow scaling: the
 // matrices here are O(1)-scaled; two FP64 rsqrt instead of hypot/divisions)
@@ -59,153 +60,55 @@ __device__ __forceinline__ void zlartg(double2 f, double2 g, double& c, double2&
     c = f2 * rf * rd;
     s = cscale(cmulc(f, g), rf * rd);   // f conj(g) / (|f| d)
 }
-// rows: a' = c a + s b ; b' = -conj(s) a + c b
+// rows: a' = c a + s b ; b' = c b - conj(s) a   (12 FP64 mul/fma)
 __device__ __forceinline__ void rot_rows(double c, double2 s, double2& a, double2& b) {
-    double2 na = cadd(cscale(a, c), cmul(s, b));
-    double2 nb = csub(cscale(b, c), cmul(cconj(s), a));
-    a = na;
-    b = nb;
+    const double ax = fma(c, a.x, fma(s.x, b.x, -s.y * b.y));
+    const double ay = fma(c, a.y, fma(s.x, b.y, s.y * b.x));
+    const double bx = fma(c, b.x, -fma(s.x, a.x, s.y * a.y));
+    const double by = fma(c, b.y, -fma(s.x, a.y, -s.y * a.x));
+    a = make_double2(ax, ay);
+    b = make_double2(bx, by);
 }
-// cols (right multiply by G^H): a' = a c + b conj(s) ; b' = -a s + b c
+// cols (right multiply by G^H): a' = a c + b conj(s) ; b' = b c - a s
 __device__ __forceinline__ void rot_cols(double c, double2 s, double2& a, double2& b) {
-    double2 na = cadd(cscale(a, c), cmulc(b, s));
-    double2 nb = csub(cscale(b, c), cmul(a, s));
-    a = na;
-    b = nb;
-}
-
-// ------------------------------------------------------------------ gehrd
-__global__ void __launch_bounds__(HT)
-gehrd_kernel(double2* Aall, int n, long long sA, double2* tauall) {
-    extern __shared__ double2 sv[];          // n
-    __shared__ double red[32];
-    __shared__ double2 s_tau, s_scal;
-    __shared__ double s_beta;
-    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    double2* A = Aall + b * sA;
-    double2* tau = tauall + (long long)b * n;
-    for (int i = 0; i < n - 1; ++i) {
-        const int m = n - i - 1;
-        double2* col = A + (long long)i * n;
-        double loc = 0.0;
-        for (int r = i + 2 + tid; r < n; r += HT) loc += cnorm2(col[r]);
-        double xn2 = block_sum(loc, red);
-        if (tid == 0) {
-            double2 alpha = col[i + 1];
-            if (xn2 == 0.0 && alpha.y == 0.0) {
-                s_tau = make_double2(0.0, 0.0);
-                s_scal = make_double2(1.0, 0.0);
-                s_beta = alpha.x;
-            } else {
-                double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
-                s_tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-                s_scal = cdiv(make_double2(1.0, 0.0), make_double2(alpha.x - beta, alpha.y));
-                s_beta = beta;
-            }
-        }
-        __syncthreads();
-        const double2 tv = s_tau, scal = s_scal;
-        for (int r = i + 2 + tid; r < n; r += HT) {
-            double2 x = cmul(col[r], scal);
-            col[r] = x;
-            sv[r - i - 1] = x;
-        }
-        if (tid == 0) {
-            sv[0] = make_double2(1.0, 0.0);
-            col[i + 1] = make_double2(s_beta, 0.0);
-            tau[i] = tv;
-        }
-        __syncthreads();
-        if (cz(tv)) continue;
-        // right: A[:, i+1:n] -= tau (A[:, i+1:n] v) v^H
-        for (int r = tid; r < n; r += HT) {
-            double2 y = make_double2(0.0, 0.0);
-            const double2* p = A + (long long)(i + 1) * n + r;
-#pragma unroll 4
-            for (int c = 0; c < m; ++c) y = cfma(p[(long long)c * n], sv[c], y);
-            double2 ty = cmul(tv, y);
-            double2* q = A + (long long)(i + 1) * n + r;
-#pragma unroll 4
-            for (int c = 0; c < m; ++c) q[(long long)c * n] = csub(q[(long long)c * n], cmulc(ty, sv[c]));
-        }
-        __syncthreads();
-        // left: A[i+1:n, i+1:n] -= conj(tau) v (v^H A[i+1:n, i+1:n])
-        const double2 ctv = cconj(tv);
-        for (int c = i + 1 + wid; c < n; c += HT / 32) {
-            double2* p = A + (long long)c * n + i + 1;
-            double2 w = make_double2(0.0, 0.0);
-            for (int r = lane; r < m; r += 32) w = cfma(cconj(sv[r]), p[r], w);
-            w = warp_sum2(w);
-            double2 cw = cmul(ctv, w);
-            for (int r = lane; r < m; r += 32) p[r] = csub(p[r], cmul(sv[r], cw));
-        }
-        __syncthreads();
-    }
-    if (tid == 0 && n >= 1) tau[n - 1] = make_double2(0.0, 0.0);
-}
-
-// Q = H(0) ... H(n-2) into Z; clears the reflectors from A (leaving H)
-__global__ void __launch_bounds__(HT)
-orghr_kernel(double2* Aall, int n, long long sA, const double2* tauall, double2* Zall) {
-    extern __shared__ double2 sv[];
-    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    double2* A = Aall + b * sA;
-    double2* Z = Zall + b * sA;
-    const double2* tau = tauall + (long long)b * n;
-    for (long long t = tid; t < (long long)n * n; t += HT) {
-        int r = (int)(t % n), c = (int)(t / n);
-        Z[t] = make_double2(r == c ? 1.0 : 0.0, 0.0);
-    }
-    __syncthreads();
-    for (int i = n - 2; i >= 0; --i) {
-        const int m = n - i - 1;
-        const double2 tv = tau[i];
-        const double2* col = A + (long long)i * n;
-        for (int r = tid; r < m; r += HT) sv[r] = (r == 0) ? make_double2(1.0, 0.0) : col[i + 1 + r];
-        __syncthreads();
-        if (!cz(tv)) {
-            for (int c = i + 1 + wid; c < n; c += HT / 32) {
-                double2* p = Z + (long long)c * n + i + 1;
-                double2 w = make_double2(0.0, 0.0);
-                for (int r = lane; r < m; r += 32) w = cfma(cconj(sv[r]), p[r], w);
-                w = warp_sum2(w);
-                double2 tw = cmul(tv, w);
-                for (int r = lane; r < m; r += 32) p[r] = csub(p[r], cmul(sv[r], tw));
-            }
-        }
-        __syncthreads();
-    }
-    // zero below the subdiagonal
-    for (long long t = tid; t < (long long)n * n; t += HT) {
-        int r = (int)(t % n), c = (int)(t / n);
-        if (r > c + 1) A[t] = make_double2(0.0, 0.0);
-    }
+    const double ax = fma(c, a.x, fma(b.x, s.x, b.y * s.y));
+    const double ay = fma(c, a.y, fma(b.y, s.x, -b.x * s.y));
+    const double bx = fma(c, b.x, -fma(a.x, s.x, -a.y * s.y));
+    const double by = fma(c, b.y, -fma(a.x, s.y, a.y * s.x));
+    a = make_double2(ax, ay);
+    b = make_double2(bx, by);
 }
 
 // ------------------------------------------------------------------ hqr
 constexpr int NSH = 16;   // shifts (bulges) per multishift sweep, one warp each
 constexpr int WB = 96;    // chase window (rows/cols kept in shared memory)
 constexpr int SEP = 3;    // rows between consecutive bulges of a chain
+// odd leading dimensions: a warp's row operation reads one row across 32
+// columns, conflict-free only when the column stride is not a multiple of 32 banks
+constexpr int WL = W + 1;     // small block
+constexpr int WBL = WB + 1;   // chase window
 
 struct HqrSmem {
     union {
         struct {
-            double2 Hs[W * W];       // small block, column-major, ld W
-            double2 U[W * W];        // its accumulated unitary
-            double2 chunk[W * 32];   // staging for the small-block far products
+            double2 Hs[W * WL];      // small block, column-major, ld WL
+            double2 U[W * WL];       // its accumulated unitary
+            double2 chunk[W * 33];   // staging for the small-block far products
         } s;
-        double2 win[WB * WB];        // chase window, column-major, ld WB
+        double2 win[WB * WBL];       // chase window, column-major, ld WBL
     } u;
     double rc[WB][NSH];              // rotation q of bulge i in this window: [q][i]
     double2 rs[WB][NSH];
     int bpos[NSH], bstart[NSH], bcnt[NSH], boff[NSH];
+    int pub[4];                      // published window: ws, we, steps, status (0 ready, 1 done, 2 fail)
     double2 shifts[NSH];
     int red_i[HT / 32];
     int s_int[8];
 };
 
-__device__ __forceinline__ double2& HS(HqrSmem& S, int i, int j) { return S.u.s.Hs[j * W + i]; }
-__device__ __forceinline__ double2& WN(HqrSmem& S, int i, int j) { return S.u.win[j * WB + i]; }
+__device__ __forceinline__ double2& HS(HqrSmem& S, int i, int j) { return S.u.s.Hs[j * WL + i]; }
+__device__ __forceinline__ double2& US(HqrSmem& S, int i, int j) { return S.u.s.U[j * WL + i]; }
+__device__ __forceinline__ double2& WN(HqrSmem& S, int i, int j) { return S.u.win[j * WBL + i]; }
 
 // Ahues-Tisseur deflation test for subdiagonal k (rows/cols relative to a
 // column-major array with leading dimension ld); lo..hi is the active range.
@@ -261,7 +164,7 @@ __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
     int its = 0, total = 0;
     while (hi >= 0) {
         int lo = hi;
-        while (lo > 0 && !negligible(S.u.s.Hs, W, lo, 0, hi)) --lo;
+        while (lo > 0 && !negligible(S.u.s.Hs, WL, lo, 0, hi)) --lo;
         if (lo > 0) {
             if (lane == 0) HS(S, lo, lo - 1) = make_double2(0.0, 0.0);
             __syncwarp();
@@ -308,10 +211,10 @@ __device__ bool small_qr_warp(HqrSmem& S, int m, int maxit) {
             }
             if (ACC) {
                 for (int i = lane; i < m; i += 32) {
-                    double2 a = S.u.s.U[k * W + i], bb = S.u.s.U[(k + 1) * W + i];
+                    double2 a = US(S, i, k), bb = US(S, i, k + 1);
                     rot_cols(c, s, a, bb);
-                    S.u.s.U[k * W + i] = a;
-                    S.u.s.U[(k + 1) * W + i] = bb;
+                    US(S, i, k) = a;
+                    US(S, i, k + 1) = bb;
                 }
             }
             __syncwarp();
@@ -329,13 +232,13 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
         const int nc = (n - j0) < 32 ? (n - j0) : 32;
         for (int t = tid; t < m * nc; t += HT) {
             int r = t % m, c = t / m;
-            S.u.s.chunk[c * W + r] = H[(long long)(j0 + c) * n + lo + r];
+            S.u.s.chunk[c * WL + r] = H[(long long)(j0 + c) * n + lo + r];
         }
         __syncthreads();
         for (int t = tid; t < m * nc; t += HT) {
             int r = t % m, c = t / m;
             double2 acc = make_double2(0.0, 0.0);
-            for (int l = 0; l < m; ++l) acc = cfma(cconj(S.u.s.U[r * W + l]), S.u.s.chunk[c * W + l], acc);
+            for (int l = 0; l < m; ++l) acc = cfma(cconj(US(S, l, r)), S.u.s.chunk[c * WL + l], acc);
             H[(long long)(j0 + c) * n + lo + r] = acc;
         }
         __syncthreads();
@@ -348,13 +251,13 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
             const int nr = (rows - i0) < 32 ? (rows - i0) : 32;
             for (int t = tid; t < m * nr; t += HT) {
                 int r = t % nr, c = t / nr;
-                S.u.s.chunk[c * 32 + r] = X[(long long)(lo + c) * n + i0 + r];
+                S.u.s.chunk[c * 33 + r] = X[(long long)(lo + c) * n + i0 + r];
             }
             __syncthreads();
             for (int t = tid; t < m * nr; t += HT) {
                 int r = t % nr, c = t / nr;
                 double2 acc = make_double2(0.0, 0.0);
-                for (int l = 0; l < m; ++l) acc = cfma(S.u.s.chunk[l * 32 + r], S.u.s.U[c * W + l], acc);
+                for (int l = 0; l < m; ++l) acc = cfma(S.u.s.chunk[l * 33 + r], US(S, l, c), acc);
                 X[(long long)(lo + c) * n + i0 + r] = acc;
             }
             __syncthreads();
@@ -362,49 +265,78 @@ __device__ void small_block_far(HqrSmem& S, double2* H, double2* Z, int n, int l
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
 // Applies a window's recorded rotations outside the window, in their true
-// step order: tiles of 32 far columns (row rotations, rows [ws, we)) and of
-// 32 far rows (column rotations, columns [ws, we)) are staged in shared
-// memory; each tile vector is owned by 16 lanes, lane i applying bulge i's
-// rotation of the current step (same-step rotations touch disjoint rows).
+// step order: tiles of 64 far columns (row rotations, rows [ws, we)) and of
+// 64 far rows (column rotations, columns [ws, we)) are staged in shared
+// memory with cp.async; each tile vector is owned by 16 lanes, lane i applying
+// bulge i's rotation of the current step (same-step rotations touch disjoint
+// rows).  A lane keeps the row its bulge carries forward in a register, so a
+// rotation costs one shared-memory load and one store; each lane serves two
+// vectors for instruction-level parallelism.
 __device__ void far_apply(HqrSmem& S, double2* H, double2* Z, int n, int ws, int we, int ns, int steps,
-                          long long* cyc) {
+                          long long* cyc, int crank, int csize) {
     const long long tf0 = clock64();
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int wm = we - ws;
+    constexpr int TV = 64;                    // vectors per tile
     const int bi = lane & 15;                 // bulge of this lane
-    const int half = lane >> 4;               // which of the warp's two vectors
-    const int vi = 2 * wid + half;            // vector index in the tile (0..31)
+    const int va = 2 * wid + (lane >> 4);     // first vector (0..31); second is va + 32
+    const int vb = va + 32;
     const bool lane_ok = bi < ns;
     const int bst = lane_ok ? S.bstart[bi] - ws : 0;
     const int bof = lane_ok ? S.boff[bi] : 0;
     const int bct = lane_ok ? S.bcnt[bi] : 0;
     double2* stage = S.u.win;
-    constexpr int LDC = WB + 1;               // column tile leading dimension
-    constexpr int LDR = 33;                   // row tile leading dimension
+    constexpr int LDC = WB + 1;               // column tile leading dimension (elements per vector)
+    constexpr int LDR = TV + 1;               // row tile leading dimension (vectors per column)
+    static_assert(TV * LDC <= WB * WBL && WB * LDR <= WB * WBL, "tile exceeds the window buffer");
     // rows [ws, we) of columns [we, n): row rotations
-    for (int j0 = we; j0 < n; j0 += 32) {
-        const int nc = (n - j0) < 32 ? (n - j0) : 32;
+    for (int j0 = we + crank * TV; j0 < n; j0 += TV * csize) {
+        const int nc = (n - j0) < TV ? (n - j0) : TV;
         for (int q = tid; q < wm * nc; q += HT) {
-            int r = q % wm, c = q / wm;
-            stage[c * LDC + r] = H[(long long)(j0 + c) * n + ws + r];
+            const int r = q % wm, c = q / wm;
+            cp_async16(&stage[c * LDC + r], &H[(long long)(j0 + c) * n + ws + r]);
         }
+        cp_async_wait_all();
         __syncthreads();
-        double2* v = stage + vi * LDC;
+        const bool oa = lane_ok && va < nc, ob = lane_ok && vb < nc;
+        double2* pa = stage + va * LDC;
+        double2* pb = stage + vb * LDC;
+        double2 ca = make_double2(0.0, 0.0), cb = make_double2(0.0, 0.0);
         for (int tau = 0; tau < steps; ++tau) {
             const int q = tau - bof;
-            if (vi < nc && lane_ok && q >= 0 && q < bct) {
+            if (q >= 0 && q < bct) {
                 const int r = bst + q;
-                double2 a = v[r], b2 = v[r + 1];
-                rot_rows(S.rc[q][bi], S.rs[q][bi], a, b2);
-                v[r] = a;
-                v[r + 1] = b2;
+                const double c = S.rc[q][bi];
+                const double2 sn = S.rs[q][bi];
+                if (oa) {
+                    if (q == 0) ca = pa[r];
+                    double2 nx = pa[r + 1];
+                    rot_rows(c, sn, ca, nx);
+                    pa[r] = ca;
+                    ca = nx;
+                    if (q == bct - 1) pa[r + 1] = ca;
+                }
+                if (ob) {
+                    if (q == 0) cb = pb[r];
+                    double2 nx = pb[r + 1];
+                    rot_rows(c, sn, cb, nx);
+                    pb[r] = cb;
+                    cb = nx;
+                    if (q == bct - 1) pb[r + 1] = cb;
+                }
             }
             __syncwarp();
         }
         __syncthreads();
         for (int q = tid; q < wm * nc; q += HT) {
-            int r = q % wm, c = q / wm;
+            const int r = q % wm, c = q / wm;
             H[(long long)(j0 + c) * n + ws + r] = stage[c * LDC + r];
         }
         __syncthreads();
@@ -413,29 +345,46 @@ __device__ void far_apply(HqrSmem& S, double2* H, double2* Z, int n, int ws, int
     if (threadIdx.x == 0) cyc[3] += tf1 - tf0;
     // rows [0, ws) of H and [0, n) of Z, columns [ws, we): column rotations
     const int rows_total = ws + n;
-    for (int i0 = 0; i0 < rows_total; i0 += 32) {
-        const int nr = (rows_total - i0) < 32 ? (rows_total - i0) : 32;
+    for (int i0 = crank * TV; i0 < rows_total; i0 += TV * csize) {
+        const int nr = (rows_total - i0) < TV ? (rows_total - i0) : TV;
         for (int q = tid; q < wm * nr; q += HT) {
-            int rr = q % nr, c = q / nr;
+            const int rr = q % nr, c = q / nr;
             const int g = i0 + rr;
             const double2* src = (g < ws) ? (H + g) : (Z + (g - ws));
-            stage[c * LDR + rr] = src[(long long)(ws + c) * n];
+            cp_async16(&stage[c * LDR + rr], &src[(long long)(ws + c) * n]);
         }
+        cp_async_wait_all();
         __syncthreads();
+        const bool oa = lane_ok && va < nr, ob = lane_ok && vb < nr;
+        double2 ca = make_double2(0.0, 0.0), cb = make_double2(0.0, 0.0);
         for (int tau = 0; tau < steps; ++tau) {
             const int q = tau - bof;
-            if (vi < nr && lane_ok && q >= 0 && q < bct) {
+            if (q >= 0 && q < bct) {
                 const int cc = bst + q;
-                double2 a = stage[cc * LDR + vi], b2 = stage[(cc + 1) * LDR + vi];
-                rot_cols(S.rc[q][bi], S.rs[q][bi], a, b2);
-                stage[cc * LDR + vi] = a;
-                stage[(cc + 1) * LDR + vi] = b2;
+                const double c = S.rc[q][bi];
+                const double2 sn = S.rs[q][bi];
+                if (oa) {
+                    if (q == 0) ca = stage[cc * LDR + va];
+                    double2 nx = stage[(cc + 1) * LDR + va];
+                    rot_cols(c, sn, ca, nx);
+                    stage[cc * LDR + va] = ca;
+                    ca = nx;
+                    if (q == bct - 1) stage[(cc + 1) * LDR + va] = ca;
+                }
+                if (ob) {
+                    if (q == 0) cb = stage[cc * LDR + vb];
+                    double2 nx = stage[(cc + 1) * LDR + vb];
+                    rot_cols(c, sn, cb, nx);
+                    stage[cc * LDR + vb] = cb;
+                    cb = nx;
+                    if (q == bct - 1) stage[(cc + 1) * LDR + vb] = cb;
+                }
             }
             __syncwarp();
         }
         __syncthreads();
         for (int q = tid; q < wm * nr; q += HT) {
-            int rr = q % nr, c = q / nr;
+            const int rr = q % nr, c = q / nr;
             const int g = i0 + rr;
             double2* dst = (g < ws) ? (H + g) : (Z + (g - ws));
             dst[(long long)(ws + c) * n] = stage[c * LDR + rr];
@@ -457,113 +406,152 @@ __device__ void far_apply(HqrSmem& S, double2* H, double2* Z, int n, int ws, int
 // (front bulge first): two rotations of different bulges that touch a common
 // row are, in the true step order, already front-bulge first, and all other
 // pairs commute, so the reordering is exact.
-__device__ bool multishift_sweep(HqrSmem& S, double2* H, double2* Z, int n, int lo, int ihi, int ns, long long* cyc) {
+__device__ bool multishift_sweep(HqrSmem& S, double2* H, double2* Z, int n, int lo, int ihi, int ns,
+                                 long long* cyc, int crank, int csize) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid < NSH) {
+    cg::cluster_group cluster = cg::this_cluster();
+    if (crank == 0 && tid < NSH) {
         S.bpos[tid] = lo;
         S.bcnt[tid] = 0;
     }
     __syncthreads();
     int t = 0;   // global step (bulge i is introduced at step SEP*i)
     while (true) {
-        // ---- all bulges finished?
-        int front = -1, rear = -1;
-        for (int i = 0; i < ns; ++i) {
-            bool done = S.bpos[i] > ihi - 1;
-            bool intro = t >= SEP * i || S.bpos[i] > lo;
-            if (!done && front < 0) front = i;
-            if (!done && intro) rear = i;
-        }
-        if (front < 0) break;
-        const bool all_intro = (SEP * (ns - 1) <= t) || S.bpos[ns - 1] > lo;
-        const int ws = all_intro ? (S.bpos[rear] - 1 > lo ? S.bpos[rear] - 1 : lo) : lo;
-        const int we = (ws + WB < ihi + 1) ? ws + WB : ihi + 1;
-        const int wm = we - ws;
-        for (int q = tid; q < WB * WB; q += HT) {
-            int i = q % WB, j = q / WB;
-            S.u.win[q] = (i < wm && j < wm) ? H[(long long)(ws + j) * n + ws + i] : make_double2(0.0, 0.0);
-        }
-        if (tid < NSH) {
-            S.bstart[tid] = S.bpos[tid];
-            S.bcnt[tid] = 0;
-            S.boff[tid] = 0;
-        }
-        __syncthreads();
-        const long long tch = clock64();
-        int steps = 0;
-        while (true) {
-            // front bulge of this step and its room in the window
-            int fr = -1;
-            for (int i = 0; i < ns; ++i)
-                if (S.bpos[i] <= ihi - 1) {
-                    fr = i;
-                    break;
+        if (crank == 0) {
+            // ---- rank 0: next window and the chase through it
+            int front = -1, rear = -1;
+            for (int i = 0; i < ns; ++i) {
+                bool done = S.bpos[i] > ihi - 1;
+                bool intro = t >= SEP * i || S.bpos[i] > lo;
+                if (!done && front < 0) front = i;
+                if (!done && intro) rear = i;
+            }
+            if (front < 0) {
+                if (tid == 0) S.pub[3] = 1;
+            } else {
+                const bool all_intro = (SEP * (ns - 1) <= t) || S.bpos[ns - 1] > lo;
+                const int ws = all_intro ? (S.bpos[rear] - 1 > lo ? S.bpos[rear] - 1 : lo) : lo;
+                const int we = (ws + WB < ihi + 1) ? ws + WB : ihi + 1;
+                const int wm = we - ws;
+                for (int q = tid; q < WB * WB; q += HT) {
+                    int i = q % WB, j = q / WB;
+                    WN(S, i, j) = (i < wm && j < wm) ? H[(long long)(ws + j) * n + ws + i] : make_double2(0.0, 0.0);
                 }
-            if (fr < 0) break;
-            const int rf = S.bpos[fr];
-            if (!(rf + 2 <= we - 1 || we == ihi + 1)) break;
-            // phase 1: rotations and row operations
-            double c = 1.0;
-            double2 s = make_double2(0.0, 0.0);
-            int r = -1;
-            bool act = false, intro = false;
-            if (wid < ns) {
-                r = S.bpos[wid];
-                intro = (t == SEP * wid);
-                act = (r <= ihi - 1) && (intro || r > lo);
-                if (act) {
-                    const int lr = r - ws;
-                    if (intro)
-                        zlartg(csub(WN(S, lr, lr), S.shifts[wid]), WN(S, lr + 1, lr), c, s);
-                    else
-                        zlartg(WN(S, lr, lr - 1), WN(S, lr + 1, lr - 1), c, s);
-                    const int c0 = intro ? lr : lr - 1;
-                    for (int j = c0 + lane; j < wm; j += 32) {
-                        double2 a = WN(S, lr, j), bb = WN(S, lr + 1, j);
-                        rot_rows(c, s, a, bb);
-                        WN(S, lr, j) = a;
-                        WN(S, lr + 1, j) = bb;
+                if (tid < NSH) {
+                    S.bstart[tid] = S.bpos[tid];
+                    S.bcnt[tid] = 0;
+                    S.boff[tid] = 0;
+                }
+                __syncthreads();
+                const long long tch = clock64();
+                int steps = 0;
+                while (true) {
+                    // front bulge of this step and its room in the window
+                    int fr = -1;
+                    for (int i = 0; i < ns; ++i)
+                        if (S.bpos[i] <= ihi - 1) {
+                            fr = i;
+                            break;
+                        }
+                    if (fr < 0) break;
+                    const int rf = S.bpos[fr];
+                    if (!(rf + 2 <= we - 1 || we == ihi + 1)) break;
+                    // phase 1: rotations and row operations
+                    double c = 1.0;
+                    double2 sn = make_double2(0.0, 0.0);
+                    int r = -1;
+                    bool act = false, intro = false;
+                    if (wid < ns) {
+                        r = S.bpos[wid];
+                        intro = (t == SEP * wid);
+                        act = (r <= ihi - 1) && (intro || r > lo);
+                        if (act) {
+                            const int lr = r - ws;
+                            if (intro)
+                                zlartg(csub(WN(S, lr, lr), S.shifts[wid]), WN(S, lr + 1, lr), c, sn);
+                            else
+                                zlartg(WN(S, lr, lr - 1), WN(S, lr + 1, lr - 1), c, sn);
+                            const int c0 = intro ? lr : lr - 1;
+                            for (int j = c0 + lane; j < wm; j += 32) {
+                                double2 a = WN(S, lr, j), bb = WN(S, lr + 1, j);
+                                rot_rows(c, sn, a, bb);
+                                WN(S, lr, j) = a;
+                                WN(S, lr + 1, j) = bb;
+                            }
+                            __syncwarp();
+                            if (lane == 0) {
+                                if (!intro) WN(S, lr + 1, lr - 1) = make_double2(0.0, 0.0);
+                                if (S.bcnt[wid] == 0) S.boff[wid] = steps;
+                                S.rc[S.bcnt[wid]][wid] = c;
+                                S.rs[S.bcnt[wid]][wid] = sn;
+                            }
+                        }
                     }
-                    __syncwarp();
-                    if (lane == 0) {
-                        if (!intro) WN(S, lr + 1, lr - 1) = make_double2(0.0, 0.0);
-                        if (S.bcnt[wid] == 0) S.boff[wid] = steps;
-                        S.rc[S.bcnt[wid]][wid] = c;
-                        S.rs[S.bcnt[wid]][wid] = s;
+                    __syncthreads();
+                    // phase 2: column operations
+                    if (act) {
+                        const int lr = r - ws;
+                        const int r1 = ((r + 2 < ihi) ? r + 2 : ihi) - ws;
+                        for (int i = lane; i <= r1; i += 32) {
+                            double2 a = WN(S, i, lr), bb = WN(S, i, lr + 1);
+                            rot_cols(c, sn, a, bb);
+                            WN(S, i, lr) = a;
+                            WN(S, i, lr + 1) = bb;
+                        }
+                        if (lane == 0) {
+                            S.bcnt[wid] += 1;
+                            S.bpos[wid] = r + 1;
+                        }
                     }
+                    ++t;
+                    ++steps;
+                    __syncthreads();
+                }
+                if (tid == 0) cyc[2] += clock64() - tch;
+                for (int q = tid; q < wm * wm; q += HT) {
+                    int i = q % wm, j = q / wm;
+                    H[(long long)(ws + j) * n + ws + i] = WN(S, i, j);
+                }
+                if (tid == 0) {
+                    S.pub[0] = ws;
+                    S.pub[1] = we;
+                    S.pub[2] = steps;
+                    // no room to move cannot happen with WB >= SEP*NSH + 8; fail instead of spinning
+                    S.pub[3] = steps == 0 ? 2 : 0;
                 }
             }
-            __syncthreads();
-            // phase 2: column operations
-            if (act) {
-                const int lr = r - ws;
-                const int r1 = ((r + 2 < ihi) ? r + 2 : ihi) - ws;
-                for (int i = lane; i <= r1; i += 32) {
-                    double2 a = WN(S, i, lr), bb = WN(S, i, lr + 1);
-                    rot_cols(c, s, a, bb);
-                    WN(S, i, lr) = a;
-                    WN(S, i, lr + 1) = bb;
-                }
-                if (lane == 0) {
-                    S.bcnt[wid] += 1;
-                    S.bpos[wid] = r + 1;
-                }
-            }
-            ++t;
-            ++steps;
-            __syncthreads();
         }
-        if (steps == 0) return false;   // no room to move: cannot happen with WB >= SEP*NSH + 8
-        if (tid == 0) cyc[2] += clock64() - tch;
-        // ---- write the window back and apply its rotations outside it
-        for (int q = tid; q < wm * wm; q += HT) {
-            int i = q % wm, j = q / wm;
-            H[(long long)(ws + j) * n + ws + i] = S.u.win[j * WB + i];
+        // ---- publish the window to the cluster
+        cluster.sync();
+        if (crank != 0) {
+            HqrSmem* S0 = cluster.map_shared_rank(&S, 0);
+            if (tid < 4) S.pub[tid] = S0->pub[tid];
+            if (tid < NSH) {
+                S.bstart[tid] = S0->bstart[tid];
+                S.boff[tid] = S0->boff[tid];
+                S.bcnt[tid] = S0->bcnt[tid];
+            }
+            // rotations recorded per bulge: at most WB - 1 (a bulge crosses the window
+            // once), even when window steps exceed WB while bulges are introduced
+            int qmax = 0;
+            for (int i = 0; i < NSH; ++i) qmax = max(qmax, S0->bcnt[i]);
+            qmax = min(qmax, WB);
+            for (int q = tid; q < qmax * NSH; q += HT) {
+                const int qq = q / NSH, i = q % NSH;
+                S.rc[qq][i] = S0->rc[qq][i];
+                S.rs[qq][i] = S0->rs[qq][i];
+            }
         }
         __syncthreads();
-        far_apply(S, H, Z, n, ws, we, ns, steps, cyc);
+        const int status = S.pub[3];
+        if (status != 0) {
+            // every rank has read rank 0's shared memory before any rank leaves
+            cluster.sync();
+            return status == 1;
+        }
+        far_apply(S, H, Z, n, S.pub[0], S.pub[1], ns, S.pub[2], cyc, crank, csize);
+        cluster.sync();
     }
-    return true;
 }
 
 __global__ void __launch_bounds__(HT, 1)
@@ -571,15 +559,22 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
            int maxsweeps, long long* stats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HqrSmem& S = *reinterpret_cast<HqrSmem*>(smem_raw);
-    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
+    const int b = blockIdx.x / csize, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     double2* H = Hall + b * sA;
     double2* Z = Zall + b * sA;
     double2* w = wall + (long long)b * n;
     int ihi = n - 1, its = 0, sweeps = 0;
     bool failed = false;
-    // phase cycle counters (thread 0): shifts, chase, far-right, far-rows, small blocks, deflation scans
+    // phase cycle counters (thread 0): shifts, chase, far-right, far-rows, small blocks
     long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long t0 = clock64();
+    // Every rank of the cluster evaluates the control decisions (deflation
+    // point, shifts) from the same global data with the same code, so all
+    // ranks take the same branches and the same cluster barriers.  The
+    // negligible subdiagonal is left in place (no rotation ever touches it
+    // again), so no rank's decision depends on another rank's write.
     while (ihi >= 0) {
         // ---- deflation point: largest k in (0, ihi] with negligible H[k, k-1]
         int best = 0;
@@ -597,43 +592,48 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
             int bb = 0;
             for (int q = 0; q < HT / 32; ++q) bb = max(bb, S.red_i[q]);
             S.s_int[0] = bb;
-            if (bb > 0) H[(long long)(bb - 1) * n + bb] = make_double2(0.0, 0.0);
         }
         __syncthreads();
         const int lo = S.s_int[0];
+        __syncthreads();
         if (lo == ihi) {
-            if (tid == 0) w[ihi] = H[(long long)ihi * n + ihi];
+            if (crank == 0 && tid == 0) w[ihi] = H[(long long)ihi * n + ihi];
             --ihi;
             its = 0;
-            __syncthreads();
             continue;
         }
         const int m = ihi - lo + 1;
         if (m <= W) {
+            // ---- rank 0 finishes the block in shared memory
             const long long tsm = clock64();
-            // ---- finish the block in shared memory
-            for (int q = tid; q < W * W; q += HT) {
-                int i = q % W, j = q / W;
-                S.u.s.Hs[q] = (i < m && j < m) ? H[(long long)(lo + j) * n + lo + i] : make_double2(0.0, 0.0);
-                S.u.s.U[q] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            if (crank == 0) {
+                for (int q = tid; q < W * W; q += HT) {
+                    int i = q % W, j = q / W;
+                    HS(S, i, j) = (i < m && j < m) ? H[(long long)(lo + j) * n + lo + i] : make_double2(0.0, 0.0);
+                    US(S, i, j) = make_double2(i == j ? 1.0 : 0.0, 0.0);
+                }
+                __syncthreads();
+                if (wid == 0) {
+                    bool ok = small_qr_warp<true>(S, m, 30 * m + 30);
+                    if (lane == 0) S.s_int[1] = ok ? 1 : 0;
+                }
+                __syncthreads();
+                for (int q = tid; q < m * m; q += HT) {
+                    int i = q % m, j = q / m;
+                    H[(long long)(lo + j) * n + lo + i] = HS(S, i, j);
+                }
+                __syncthreads();
+                small_block_far(S, H, Z, n, lo, m);
+                for (int k = lo + tid; k <= ihi; k += HT) w[k] = HS(S, k - lo, k - lo);
             }
-            __syncthreads();
-            if (wid == 0) {
-                bool ok = small_qr_warp<true>(S, m, 30 * m + 30);
-                if (lane == 0) S.s_int[1] = ok ? 1 : 0;
-            }
-            __syncthreads();
-            if (!S.s_int[1]) failed = true;
-            for (int q = tid; q < m * m; q += HT) {
-                int i = q % m, j = q / m;
-                H[(long long)(lo + j) * n + lo + i] = S.u.s.Hs[j * W + i];
-            }
-            __syncthreads();
-            small_block_far(S, H, Z, n, lo, m);
-            for (int k = lo + tid; k <= ihi; k += HT) w[k] = S.u.s.Hs[(k - lo) * W + (k - lo)];
-            __syncthreads();
+            cluster.sync();
+            const int ok = (crank == 0) ? S.s_int[1] : cluster.map_shared_rank(&S, 0)->s_int[1];
+            cluster.sync();
             if (tid == 0) cyc[5] += clock64() - tsm;
-            if (failed) break;
+            if (!ok) {
+                failed = true;
+                break;
+            }
             ihi = lo - 1;
             its = 0;
             continue;
@@ -643,19 +643,19 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
             break;
         }
         ++its;
-        // ---- shifts: eigenvalues of the trailing ns x ns block
+        // ---- shifts: eigenvalues of the trailing ns x ns block (every rank)
         const long long tsh = clock64();
         const int ns = NSH;
         for (int q = tid; q < W * W; q += HT) {
             int i = q % W, j = q / W;
-            S.u.s.Hs[q] = (i < ns && j < ns) ? H[(long long)(ihi - ns + 1 + j) * n + ihi - ns + 1 + i]
+            HS(S, i, j) = (i < ns && j < ns) ? H[(long long)(ihi - ns + 1 + j) * n + ihi - ns + 1 + i]
                                              : make_double2(0.0, 0.0);
         }
         __syncthreads();
         if (wid == 0) small_qr_warp<false>(S, ns, 30 * ns);
         __syncthreads();
         if (tid < ns) {
-            double2 sh = S.u.s.Hs[tid * W + tid];
+            double2 sh = HS(S, tid, tid);
             if (its % 6 == 0) {
                 // exceptional shifts: perturb by the size of the last subdiagonal
                 double e = 0.75 * cabs1(H[(long long)(ihi - 1) * n + ihi]);
@@ -665,17 +665,18 @@ hqr_kernel(double2* Hall, double2* Zall, int n, long long sA, double2* wall, int
         }
         __syncthreads();
         if (tid == 0) cyc[1] += clock64() - tsh;
-        if (!multishift_sweep(S, H, Z, n, lo, ihi, ns, cyc)) {
+        if (!multishift_sweep(S, H, Z, n, lo, ihi, ns, cyc, crank, csize)) {
             failed = true;
             break;
         }
     }
-    if (tid == 0 && info != nullptr) info[b] = failed ? (ihi + 1 > 0 ? ihi + 1 : 1) : 0;
-    if (tid == 0 && stats != nullptr) {
+    if (crank == 0 && tid == 0 && info != nullptr) info[b] = failed ? (ihi + 1 > 0 ? ihi + 1 : 1) : 0;
+    if (crank == 0 && tid == 0 && stats != nullptr) {
         cyc[7] = clock64() - t0;
         stats[(long long)b * 8 + 0] = sweeps;
         for (int q = 1; q < 8; ++q) stats[(long long)b * 8 + q] = cyc[q];
     }
+    cluster.sync();   // no rank leaves while another may still read its shared memory
 }
 
 // ------------------------------------------------------------------ trevc
@@ -750,32 +751,40 @@ sc_status eig_batched(cudaStream_t st, double2* A, int n, int batch, double2* ev
         return SC_BADINPUT;
     }
     const long long sA = (long long)n * n;
-    double2* tau = nullptr;
     double2* Z = nullptr;
-    SC_TRY(ws.get(&tau, (size_t)batch * n, WS_EIG_TAU, st));
     SC_TRY(ws.get(&Z, (size_t)batch * sA, WS_EIG_Z, st));
-    const size_t vsm = (size_t)n * sizeof(double2);
-    if (vsm > 200 * 1024) {
-        set_error("eig: n=%d exceeds the shared-memory reflector buffer", n);
-        return SC_BADINPUT;
-    }
     // per-device attributes; cheap host calls, set on every use so that any
     // device current on this thread is covered
-    SC_CUDA_TRY(cudaFuncSetAttribute(gehrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    SC_CUDA_TRY(cudaFuncSetAttribute(orghr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     SC_CUDA_TRY(cudaFuncSetAttribute(hqr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(HqrSmem)));
-    gehrd_kernel<<<batch, HT, vsm, st>>>(A, n, sA, tau);
-    count_launch();
-    orghr_kernel<<<batch, HT, vsm, st>>>(A, n, sA, tau, Z);
-    count_launch();
+    SC_TRY(hessenberg_blocked(st, A, n, batch, Z, ws));
     for (auto& e : ws.ev_hqr)
         if (!e) SC_CUDA_TRY(cudaEventCreate(&e));
     SC_TRY(ws.get(&ws.hqr_stats, (size_t)batch * 8, WS_STATS, st));
     ws.hqr_batch = batch;
     SC_CUDA_TRY(cudaEventRecord(ws.ev_hqr[0], st));
-    hqr_kernel<<<batch, HT, sizeof(HqrSmem), st>>>(A, Z, n, sA, evl, info, 60 * n + 100, ws.hqr_stats);
-    count_launch();
+    {
+        // clusters of up to 4 CTAs per matrix when the batch leaves SMs idle
+        int dev = 0, sms = 148;
+        SC_CUDA_TRY(cudaGetDevice(&dev));
+        SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        int cl = 1;
+        while (cl < 4 && (long long)batch * cl * 2 <= sms && n > 2 * W) cl *= 2;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(batch * cl));
+        cfg.blockDim = dim3(HT);
+        cfg.dynamicSmemBytes = sizeof(HqrSmem);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        SC_CUDA_TRY(cudaLaunchKernelEx(&cfg, hqr_kernel, A, Z, n, sA, evl, info, 60 * n + 100, ws.hqr_stats));
+        count_launch();
+    }
     SC_CUDA_TRY(cudaEventRecord(ws.ev_hqr[1], st));
     SC_CHECK_LAUNCH("hqr");
     // Y (upper triangular eigenvectors of T) into V, then V = Z * Y

@@ -1,4 +1,5 @@
-// Batched complex128 GEMM, C = alpha * A * B + beta * C (column-major).
+// Batched complex128 GEMM, C = alpha * op(A) * op(B) + beta * C (column-major,
+// op = identity or conjugate transpose).
 //
 // Replaces cblas_zgemm behind MKL_multiply (third_Lapack.h:74-84) and every
 // dense product of the layer chain, the boundary system and the interior
@@ -18,10 +19,12 @@ namespace sc {
 namespace {
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
+// CA / CB: operand is used conjugate-transposed (op = ^H) instead of as is
+template <bool CA, bool CB>
 __global__ void __launch_bounds__(NT, 2)
-zgemm_nn_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
-                long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
-                double2* __restrict__ C, int ldc, long long sC) {
+zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
+             long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
+             double2* __restrict__ C, int ldc, long long sC) {
     __shared__ double2 As[BK][BM];
     __shared__ double2 Bs[BK][BN + 1];
     const int bz = blockIdx.z;
@@ -33,22 +36,42 @@ zgemm_nn_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ 
 
     // global -> register staging: A tile 64x16 (4 per thread), B tile 16x64 (4 per thread)
     double2 ra[4], rb[4];
+    // index maps chosen so that consecutive threads read consecutive addresses
+    auto a_rk = [&](int i, int& r, int& kk) {
+        if (!CA) { r = tid & 63; kk = (tid >> 6) + 4 * i; }
+        else { r = (tid >> 4) + 16 * i; kk = tid & 15; }
+    };
+    auto b_kc = [&](int i, int& kk, int& c) {
+        if (!CB) { kk = tid & 15; c = (tid >> 4) + 16 * i; }
+        else { kk = (tid >> 6) + 4 * i; c = tid & 63; }
+    };
     auto load = [&](int k0) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            int r = tid & 63, kk = (tid >> 6) + 4 * i;
+            int r, kk;
+            a_rk(i, r, kk);
             int gr = m0 + r, gk = k0 + kk;
-            ra[i] = (gr < m && gk < k) ? A[(long long)gk * lda + gr] : make_double2(0.0, 0.0);
-            int kb = tid & 15, c = (tid >> 4) + 16 * i;
+            if (gr < m && gk < k)
+                ra[i] = CA ? cconj(A[(long long)gr * lda + gk]) : A[(long long)gk * lda + gr];
+            else
+                ra[i] = make_double2(0.0, 0.0);
+            int kb, c;
+            b_kc(i, kb, c);
             int gkb = k0 + kb, gc = n0 + c;
-            rb[i] = (gkb < k && gc < n) ? B[(long long)gc * ldb + gkb] : make_double2(0.0, 0.0);
+            if (gkb < k && gc < n)
+                rb[i] = CB ? cconj(B[(long long)gkb * ldb + gc]) : B[(long long)gc * ldb + gkb];
+            else
+                rb[i] = make_double2(0.0, 0.0);
         }
     };
     auto store = [&]() {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            As[(tid >> 6) + 4 * i][tid & 63] = ra[i];
-            Bs[tid & 15][(tid >> 4) + 16 * i] = rb[i];
+            int r, kk, kb, c;
+            a_rk(i, r, kk);
+            b_kc(i, kb, c);
+            As[kk][r] = ra[i];
+            Bs[kb][c] = rb[i];
         }
     };
 
@@ -102,19 +125,32 @@ zgemm_nn_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ 
 }
 }  // namespace
 
-sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
-                long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
-                int ldc, long long sC, int batch) {
+sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,
+                   const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB,
+                   double2 beta, double2* C, int ldc, long long sC, int batch) {
     if (m <= 0 || n <= 0 || batch <= 0) return SC_OK;
     dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN, batch);
     if (grid.y > 65535 || grid.z > 65535) {
         set_error("zgemm: grid too large (n=%d, batch=%d)", n, batch);
         return SC_BADINPUT;
     }
-    zgemm_nn_kernel<<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    if (!conjA && !conjB)
+        zgemm_kernel<false, false><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    else if (conjA && !conjB)
+        zgemm_kernel<true, false><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    else if (!conjA && conjB)
+        zgemm_kernel<false, true><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    else
+        zgemm_kernel<true, true><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
     count_launch();
     SC_CHECK_LAUNCH("zgemm");
     return SC_OK;
+}
+
+sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
+                long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
+                int ldc, long long sC, int batch) {
+    return zgemm_op(st, false, false, m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch);
 }
 
 }  // namespace sc
