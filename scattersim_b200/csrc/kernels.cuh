@@ -13,7 +13,7 @@ enum WsSlot {
     WS_V, WS_EVL, WS_GD, WS_GC, WS_PIV, WS_INFO, WS_T, WS_T2,
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
-    WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2,
+    WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV,
     WS_COUNT
 };
 
@@ -76,6 +76,11 @@ sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const doubl
 sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,
                    const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB,
                    double2 beta, double2* C, int ldc, long long sC, int batch);
+
+// y = alpha A x + beta y (batched, deterministic two-pass); part: zgemv_part_size entries
+sc_status zgemv(cudaStream_t st, int m, int n, double2 alpha, const double2* A, int lda, long long sA,
+                const double2* x, long long sx, double2 beta, double2* y, long long sy, int batch, double2* part);
+size_t zgemv_part_size(int m, int n, int batch);
 
 // hess.cu: blocked Householder Hessenberg reduction and explicit Q, batched
 sc_status hessenberg_blocked(cudaStream_t st, double2* A, int n, int batch, double2* Q, Workspace& ws);

@@ -246,7 +246,7 @@ sc_status getrf(cudaStream_t st, double2* A, int lda, long long sA, int n, int b
 sc_status getrs(cudaStream_t st, const double2* LU, int lda, long long sA, int n, const int* ipiv,
                 double2* B, int ldb, long long sB, int nrhs, int batch) {
     if (n <= 0 || nrhs <= 0 || batch <= 0) return SC_OK;
-    const int tpb = 128;
+    const int tpb = 64;
     dim3 g((nrhs + tpb - 1) / tpb, batch);
     laswp_rhs_kernel<<<g, tpb, 0, st>>>(B, ldb, sB, n, nrhs, ipiv);
     count_launch();

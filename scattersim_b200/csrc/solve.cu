@@ -102,15 +102,16 @@ __global__ void scale_cols_kernel(const double2* __restrict__ in, long long sIn,
     }
 }
 
-// X = diag(s) X (row scaling) in place
-__global__ void scale_rows_kernel(double2* __restrict__ X, int rows, int cols, int ld,
-                                  const double2* __restrict__ s) {
+// out_z = diag(s_z) in_z (row scaling), batched
+__global__ void scale_rows_batched_kernel(const double2* __restrict__ in, long long sIn,
+                                          const double2* __restrict__ s, long long sS, int rows, int cols,
+                                          double2* __restrict__ out, long long sOut) {
+    const int z = blockIdx.y;
     const long long tot = (long long)rows * cols;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
          t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t % rows), c = (int)(t / rows);
-        double2* p = X + (long long)c * ld + r;
-        *p = cmul(*p, s[r]);
+        const int r = (int)(t % rows);
+        out[z * sOut + t] = cmul(in[z * sIn + t], s[z * sS + r]);
     }
 }
 
@@ -500,15 +501,21 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     SC_TRY(normalize_columns(st, V, n4, n4, n4, s4, Z));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
 
-    // ---- a9: GD/GC and the chain
-    double2 *dG, *cG, *LU, *Gcs, *X;
+    // ---- a9: GD/GC, explicit GD_i^-1 for all layers, and the chain
+    //   Gc_static = T_{Z-1} ... T_1 GC_0,  T_i = GC_i GD_i^-1 = V_i diag(cG_i) GD_i^-1
+    // computed as one batched inverse, one batched product and a pairwise
+    // product tree (ScatterVolume.cpp:326-335 multiplies the same factors in
+    // sequence).
+    double2 *dG, *cG, *LU, *Inv, *Gcs, *X, *tree, *gpart;
     int* piv;
     SC_TRY(ws.get(&dG, (size_t)Z * n4, WS_TMP, st));
     SC_TRY(ws.get(&cG, (size_t)Z * n4, WS_TMP2, st));
     SC_TRY(ws.get(&LU, (size_t)Z * s4, WS_GD, st));
+    SC_TRY(ws.get(&Inv, (size_t)Z * s4, WS_INV, st));
     SC_TRY(ws.get(&piv, (size_t)Z * n4, WS_PIV, st));
     SC_TRY(ws.get(&Gcs, (size_t)s4, WS_T, st));
     SC_TRY(ws.get(&X, (size_t)s4, WS_T2, st));
+    SC_TRY(ws.get(&gpart, zgemv_part_size(n4, n4, 1) + 2 * (size_t)n4, WS_GEMV, st));
     {
         dim3 g((n4 + 255) / 256, Z);
         gdgc_scale_kernel<<<g, 256, 0, st>>>(evl, n4, Z, d_z, k, dG, cG);
@@ -516,18 +523,46 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         dim3 g2(grid_for(s4), Z);
         scale_cols_kernel<<<g2, 256, 0, st>>>(V, s4, dG, n4, n4, n4, LU, s4);
         count_launch();
-        scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, cG, n4, n4, n4, Gcs, s4);
-        count_launch();
     }
     SC_TRY(getrf(st, LU, n4, s4, n4, Z, piv, nullptr));
-    for (int i = 1; i < Z; ++i) {
-        // X = GD_i^-1 Gc_static ; Gc_static = V_i diag(cG_i) X
-        SC_CUDA_TRY(cudaMemcpyAsync(X, Gcs, sizeof(double2) * s4, cudaMemcpyDeviceToDevice, st));
-        SC_TRY(getrs(st, LU + i * s4, n4, s4, n4, piv + (long long)i * n4, X, n4, s4, n4, 1));
-        scale_rows_kernel<<<grid_for(s4), 256, 0, st>>>(X, n4, n4, n4, cG + (long long)i * n4);
+    SC_TRY(set_identity(st, Inv, n4, s4, n4, Z));
+    SC_TRY(getrs(st, LU, n4, s4, n4, piv, Inv, n4, s4, n4, Z));
+    {
+        // level 0 of the tree: M_0 = GC_0 = V_0 diag(cG_0), M_i = T_i (i >= 1)
+        const int nt = Z;
+        SC_TRY(ws.get(&tree, (size_t)(nt + (nt + 1) / 2) * s4, WS_TREE, st));
+        scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, cG, n4, n4, n4, tree, s4);
         count_launch();
-        SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), V + i * s4, n4, s4, X, n4, s4,
-                     make_double2(0.0, 0.0), Gcs, n4, s4, 1));
+        if (Z > 1) {
+            // rows of GD_i^-1 scaled by cG_i, into the spare half of the tree buffer, then T_i = V_i (.)
+            double2* scaled = tree + (long long)nt * s4;
+            for (int i0 = 1; i0 < Z; i0 += (nt + 1) / 2) {
+                const int cnt = (Z - i0) < (nt + 1) / 2 ? (Z - i0) : (nt + 1) / 2;
+                dim3 g(grid_for(s4), cnt);
+                scale_rows_batched_kernel<<<g, 256, 0, st>>>(Inv + i0 * s4, s4, cG + (long long)i0 * n4, n4, n4,
+                                                            n4, scaled, s4);
+                count_launch();
+                SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), V + i0 * s4, n4, s4, scaled, n4, s4,
+                             make_double2(0.0, 0.0), tree + i0 * s4, n4, s4, cnt));
+            }
+        }
+        // pairwise products M_{2j+1} M_{2j}, level by level (order preserved)
+        double2* cur = tree;
+        double2* nxt = tree + (long long)nt * s4;
+        int cnt = nt;
+        while (cnt > 1) {
+            const int pairs = cnt / 2;
+            SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), cur + s4, n4, 2 * s4, cur, n4, 2 * s4,
+                         make_double2(0.0, 0.0), nxt, n4, s4, pairs));
+            if (cnt & 1)
+                SC_CUDA_TRY(cudaMemcpyAsync(nxt + pairs * s4, cur + (cnt - 1) * s4, sizeof(double2) * s4,
+                                            cudaMemcpyDeviceToDevice, st));
+            cnt = pairs + (cnt & 1);
+            double2* t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+        SC_CUDA_TRY(cudaMemcpyAsync(Gcs, cur, sizeof(double2) * s4, cudaMemcpyDeviceToDevice, st));
     }
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[4], st));
 
@@ -557,22 +592,23 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     // ---- a14/a15: beta chain, Q, Pz
     if (!p->external && (Qc_out || Qh_out)) {
         double2 *beta, *tv;
-        SC_TRY(ws.get(&beta, (size_t)Z * n4 + n4, WS_BETA, st));
+        SC_TRY(ws.get(&beta, (size_t)Z * n4 + 2 * n4, WS_BETA, st));
         tv = beta + (long long)Z * n4;
-        beta0_rhs_kernel<<<grid_for(n4), 256, 0, st>>>(MF, dSx, dSy, dSz0, dEF, b6, k, P.z[0], beta);
+        double2* rhs = tv + n4;
+        beta0_rhs_kernel<<<grid_for(n4), 256, 0, st>>>(MF, dSx, dSy, dSz0, dEF, b6, k, P.z[0], rhs);
         count_launch();
-        SC_TRY(getrs(st, LU, n4, s4, n4, piv, beta, n4, 0, 1, 1));
+        // beta_0 = GD_0^-1 (f1 EF + f2 R);  beta_i = GD_i^-1 V_{i-1} (cG_{i-1} .* beta_{i-1})
+        SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), Inv, n4, s4, rhs, 0, make_double2(0.0, 0.0), beta, 0, 1,
+                     gpart));
         for (int i = 1; i < Z; ++i) {
-            // t = V_{i-1} (cG_{i-1} .* beta_{i-1}) ; beta_i = GD_i^-1 t
             scale_cols_kernel<<<dim3(grid_for(n4), 1), 256, 0, st>>>(beta + (long long)(i - 1) * n4, 0,
                                                                       cG + (long long)(i - 1) * n4, 0, 1, n4,
-                                                                      tv, 0);
+                                                                      rhs, 0);
             count_launch();
-            // scale_cols with rows=1: out[c] = in[c] * s[c]
-            SC_TRY(zgemm(st, n4, 1, n4, make_double2(1.0, 0.0), V + (i - 1) * s4, n4, s4, tv, n4, 0,
-                         make_double2(0.0, 0.0), beta + (long long)i * n4, n4, 0, 1));
-            SC_TRY(getrs(st, LU + i * s4, n4, s4, n4, piv + (long long)i * n4, beta + (long long)i * n4, n4, 0,
-                         1, 1));
+            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), V + (i - 1) * s4, n4, s4, rhs, 0,
+                         make_double2(0.0, 0.0), tv, 0, 1, gpart));
+            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), Inv + i * s4, n4, s4, tv, 0, make_double2(0.0, 0.0),
+                         beta + (long long)i * n4, 0, 1, gpart));
         }
         double2 *Gc, *Gh, *KP;
         SC_TRY(ws.get(&Gc, (size_t)Z * MF * n2 * 2, WS_PZ, st));

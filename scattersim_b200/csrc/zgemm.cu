@@ -147,6 +147,59 @@ sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k,
     return SC_OK;
 }
 
+namespace {
+constexpr int VR = 128;   // rows per GEMV CTA
+constexpr int VC = 64;    // columns per GEMV partial
+
+// part[b][ch][r] = sum over columns of chunk ch of A[r, c] x[c]
+__global__ void __launch_bounds__(VR)
+zgemv_part_kernel(int m, int n, const double2* __restrict__ A, int lda, long long sA,
+                  const double2* __restrict__ x, long long sx, double2* __restrict__ part, int nch) {
+    __shared__ double2 xs[VC];
+    const int b = blockIdx.z, ch = blockIdx.x;
+    const int c0 = ch * VC, c1 = (c0 + VC < n) ? c0 + VC : n;
+    for (int q = threadIdx.x; q < c1 - c0; q += VR) xs[q] = x[b * sx + c0 + q];
+    __syncthreads();
+    const int r = blockIdx.y * VR + threadIdx.x;
+    if (r >= m) return;
+    const double2* a = A + b * sA + (long long)c0 * lda + r;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 8
+    for (int q = 0; q < c1 - c0; ++q) acc = cfma(a[(long long)q * lda], xs[q], acc);
+    part[((long long)b * nch + ch) * m + r] = acc;
+}
+
+// y = alpha * sum_ch part + beta * y (fixed summation order)
+__global__ void zgemv_sum_kernel(int m, const double2* __restrict__ part, int nch, double2 alpha, double2 beta,
+                                 double2* __restrict__ y, long long sy) {
+    const int b = blockIdx.y;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int ch = 0; ch < nch; ++ch) acc = cadd(acc, part[((long long)b * nch + ch) * m + r]);
+    double2 v = cmul(alpha, acc);
+    if (beta.x != 0.0 || beta.y != 0.0) v = cfma(beta, y[b * sy + r], v);
+    y[b * sy + r] = v;
+}
+}  // namespace
+
+sc_status zgemv(cudaStream_t st, int m, int n, double2 alpha, const double2* A, int lda, long long sA,
+                const double2* x, long long sx, double2 beta, double2* y, long long sy, int batch, double2* part) {
+    if (m <= 0 || batch <= 0) return SC_OK;
+    const int nch = (n + VC - 1) / VC;
+    if (nch == 0) return SC_OK;
+    dim3 g(nch, (m + VR - 1) / VR, batch);
+    zgemv_part_kernel<<<g, VR, 0, st>>>(m, n, A, lda, sA, x, sx, part, nch);
+    count_launch();
+    dim3 g2((m + 255) / 256, batch);
+    zgemv_sum_kernel<<<g2, 256, 0, st>>>(m, part, nch, alpha, beta, y, sy);
+    count_launch();
+    SC_CHECK_LAUNCH("zgemv");
+    return SC_OK;
+}
+
+size_t zgemv_part_size(int m, int n, int batch) { return (size_t)batch * ((n + VC - 1) / VC) * m; }
+
 sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
                 long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
                 int ldc, long long sC, int batch) {
