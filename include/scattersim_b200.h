@@ -85,6 +85,21 @@ sc_status sc_eigensolve_batched(sc_context* ctx, void* A, int n, int batch, void
 sc_status sc_linearsolve_batched(sc_context* ctx, void* A, int n, void* B, int nrhs,
                                  int batch, int* info, void* stream);
 
+/* Allocation-free variant of sc_linearsolve_batched (no counterpart in the
+ * reference).  Same arguments and results, no context, runs on the current
+ * device, and allocates no device memory: for callers that cannot call
+ * cudaMalloc -- solves recorded into a CUDA graph under stream capture,
+ * real-time loops that must not take cudaMalloc's implicit synchronisation,
+ * frameworks that forbid device allocations after start-up.  Its scratch
+ * (pivots and status words) is a fixed 260 KiB array in the library's device
+ * memory, held by every GPU that loads the library until exit; limits:
+ * n * batch <= 65536 and batch <= 1024, larger sizes return SC_BADINPUT.
+ * The first call on a device looks the array up for that device (make it
+ * before any stream capture).  All calls share the array: calls whose work
+ * overlaps on the GPU race. */
+sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int nrhs, int batch, int* info,
+                                         void* stream);
+
 /* a9/a12/a14: Ainv = A^-1 for `batch` matrices (A is not modified). */
 sc_status sc_inverse_batched(sc_context* ctx, const void* A, int n, int batch, void* Ainv,
                              int* info, void* stream);

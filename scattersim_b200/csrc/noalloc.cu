@@ -1,0 +1,95 @@
+// Allocation-free batched linear solve.
+//
+// sc_linearsolve_batched_noalloc solves A X = B exactly like
+// sc_linearsolve_batched (same LU kernels, same results) but allocates no
+// device memory.  It exists for callers that cannot call cudaMalloc: code
+// that records the solve into a CUDA graph under stream capture (where an
+// allocation would break or invalidate the capture), real-time loops that
+// must not take the implicit device synchronisation of cudaMalloc/cudaFree,
+// and host frameworks that hand the library pre-allocated buffers and forbid
+// further device allocations.
+//
+// Its only scratch -- the pivot indices and one status word per system --
+// lives in g_noalloc_scratch, a fixed array in this library's device memory
+// (NOALLOC_MAX_PIVOTS + NOALLOC_MAX_BATCH ints, 260 KiB).  Every GPU that loads
+// the library's device code holds that array until the process exits.
+//
+// In host code the array's name is only a host-side stand-in for the symbol,
+// not a device address: passed to a kernel it would fault or, where the GPU
+// can reach host memory, silently address the wrong memory.  The device
+// address is therefore looked up with cudaGetSymbolAddress once per device,
+// with that device current, on the first call made on that device; that first
+// call should come before any stream capture starts.
+//
+// All calls share the one array and keep the last call's contents: the status
+// words are cleared on the stream at the start of every call, and calls whose
+// work overlaps on the GPU (different streams, or different host threads
+// without ordering) race on the array.
+#include <mutex>
+
+#include "kernels.cuh"
+
+namespace {
+constexpr int NOALLOC_MAX_PIVOTS = 65536;   // n * batch
+constexpr int NOALLOC_MAX_BATCH = 1024;
+constexpr int MAX_DEVICES = 64;
+
+static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_MAX_PIVOTS + NOALLOC_MAX_BATCH];
+
+int* g_scratch_addr[MAX_DEVICES] = {};
+std::mutex g_scratch_mu;
+}  // namespace
+
+using namespace sc;
+
+extern "C" sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int nrhs, int batch, int* info,
+                                                    void* stream) {
+    if (!A || !B || n <= 0 || nrhs <= 0 || batch <= 0) {
+        set_error("sc_linearsolve_batched_noalloc: bad argument");
+        return SC_BADINPUT;
+    }
+    if (batch > NOALLOC_MAX_BATCH || (long long)n * batch > NOALLOC_MAX_PIVOTS) {
+        set_error("sc_linearsolve_batched_noalloc: n*batch = %lld (batch %d) exceeds the fixed scratch "
+                  "(n*batch <= %d, batch <= %d)",
+                  (long long)n * batch, batch, NOALLOC_MAX_PIVOTS, NOALLOC_MAX_BATCH);
+        return SC_BADINPUT;
+    }
+    int dev = 0;
+    SC_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) {
+        set_error("sc_linearsolve_batched_noalloc: device %d out of range", dev);
+        return SC_BADINPUT;
+    }
+    int* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        if (!g_scratch_addr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+            g_scratch_addr[dev] = static_cast<int*>(p);
+        }
+        base = g_scratch_addr[dev];
+    }
+    int* piv = base;
+    int* dinfo = base + NOALLOC_MAX_PIVOTS;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the previous call's status words are still in the array
+    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * batch, st));
+    const long long sA = (long long)n * n, sB = (long long)n * nrhs;
+    SC_TRY(getrf(st, (double2*)A, n, sA, n, batch, piv, dinfo));
+    SC_TRY(getrs(st, (const double2*)A, n, sA, n, piv, (double2*)B, n, sB, nrhs, batch));
+    int hinfo[NOALLOC_MAX_BATCH];
+    SC_CUDA_TRY(cudaMemcpyAsync(hinfo, dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    int bad = 0;
+    for (int b = 0; b < batch; ++b) {
+        if (info) info[b] = hinfo[b];
+        if (hinfo[b]) bad = 1;
+    }
+    if (bad) {
+        set_error("sc_linearsolve_batched_noalloc: exactly singular matrix");
+        return SC_SINGULAR;
+    }
+    return SC_OK;
+}
