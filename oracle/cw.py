@@ -89,6 +89,36 @@ def get_e0(E2, k):
     return E
 
 
+def _rotation_z_to(kh):
+    """Rodrigues rotation taking z-hat to the unit vector kh (complex kh with kh.kh = 1 allowed)."""
+    z = np.array([0.0, 0.0, 1.0])
+    a = np.cross(z, kh)
+    c = kh[2]
+    s2 = a @ a
+    if abs(s2) < 1e-30:
+        return np.eye(3, dtype=np.complex128) if np.real(c) > 0 else np.diag([1.0, -1.0, -1.0]).astype(np.complex128)
+    sn = np.sqrt(s2)
+    ah = a / sn
+    K = np.array([[0, -ah[2], ah[1]], [ah[2], 0, -ah[0]], [-ah[1], ah[0], 0]])
+    return np.eye(3) + sn * K + (1 - c) * (K @ K)
+
+
+def get_e0_local(E2, k):
+    """Alternative reading of a record: (E0x, E0y) as components in a k-aligned frame.
+
+    The two files the reference ships are continuous across their boundaries
+    only under this reading (psf.cw to ~1e-4): E_world = R (E0x, E0y, 0) with R
+    the rotation taking z-hat to k / sqrt(k.k).  The azimuthal gauge of that
+    frame for oblique waves is not pinned by the data (tira is not available).
+    """
+    out = np.zeros((len(E2), 3), dtype=np.complex128)
+    for i in range(len(E2)):
+        kv = np.asarray(k[i], dtype=np.complex128)
+        R = _rotation_z_to(kv / np.sqrt(kv @ kv))
+        out[i] = R @ np.array([E2[i, 0], E2[i, 1], 0.0])
+    return out
+
+
 def unpack(Pi_E, Pi_k, layers):
     """cpuEvaluator.cpp:34-102.  Returns (z_layers, begin, end, W_E, W_k) with 3-component E."""
     zl = np.array([L[0] for L in layers], dtype=np.float64)

@@ -132,9 +132,13 @@ sc_status sc_fft2_crop(sc_context* ctx, const void* sample, int Z, int S1, int S
     DeviceGuard g(ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
     double2 *R2, *Ri2;
+    int* bins;
     SC_TRY(ctx->ws.get(&R2, (size_t)Z * S1 * Mx, WS_TMP, st));
     SC_TRY(ctx->ws.get(&Ri2, (size_t)Z * S1 * Mx, WS_TMP2, st));
-    return fft2_crop(st, (const double2*)sample, Z, S1, S2, Mx, My, (double2*)Nf, (double2*)Nif, R2, Ri2);
+    SC_TRY(ctx->ws.get(&bins, (size_t)Mx + My, WS_BINS, st));
+    SC_TRY(fft2_crop(st, (const double2*)sample, Z, S1, S2, Mx, My, (double2*)Nf, (double2*)Nif, R2, Ri2, bins));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    return SC_OK;
 }
 
 sc_status sc_phi(sc_context* ctx, const void* Nf, const void* Nif, int Z, int Mx, int My, const double* up_host,

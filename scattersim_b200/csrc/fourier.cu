@@ -4,8 +4,10 @@
 // from volume::phi (FourierWave.h:341, 343).  Only the centred My x Mx block of
 // the shifted spectrum survives the crop, so instead of a full FFT the kernels
 // evaluate that block directly as a separable partial DFT in FP64:
-//   crop index c  <->  frequency c - floor(M/2)   (for any N, even or odd),
-//   rows pass  R(i, pc) = sum_j A(i,j) w_N2^(fp j)       (Mx frequencies)
+//   crop index c  ->  FFT bin given by the reference's own shift tables
+//                     (crop_bins; bin c - floor(M/2) mod N whenever both
+//                     sides of the slice have the same parity),
+//   rows pass  R(i, pc) = sum_j A(i,j) w_N2^(fp j)       (Mx bins)
 //   cols pass  N(qc,pc) = sum_i R(i,pc) w_N1^(fq i) / (N1 N2)
 // with exact twiddles from sincospi on (f j mod N).  A(i, j) is the Eigen
 // column-major view of the C-order .npy slice, A(i,j) = flat[i + j*S1]
@@ -17,6 +19,8 @@
 // B = Phi[0:2M, 2M:4M] and C = Phi[2M:4M, 0:2M].  The convolution entries use
 // the reference's circulant order wrap (FourierWave.h:366-372):
 //   row of Nf = ((qi - qj) mod My + My/2) mod My, col likewise in p.
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -27,8 +31,8 @@ constexpr int RT = 128;     // threads per CTA, rows pass
 constexpr int PCH = 16;     // output frequencies per register chunk
 
 __global__ void __launch_bounds__(RT)
-dft_rows_kernel(const double2* __restrict__ sample, int S1, int S2, int Mx, double2* __restrict__ R2,
-                double2* __restrict__ Ri2) {
+dft_rows_kernel(const double2* __restrict__ sample, int S1, int S2, int Mx, const int* __restrict__ bins_x,
+                double2* __restrict__ R2, double2* __restrict__ Ri2) {
     extern __shared__ double2 tw[];   // S2 twiddles
     const int z = blockIdx.x;
     for (int t = threadIdx.x; t < S2; t += RT) {
@@ -42,7 +46,6 @@ dft_rows_kernel(const double2* __restrict__ sample, int S1, int S2, int Mx, doub
     const double2* A = sample + (long long)z * S1 * S2;
     double2* r2 = R2 + ((long long)z * S1 + i) * Mx;
     double2* ri2 = Ri2 + ((long long)z * S1 + i) * Mx;
-    const int h = Mx / 2;
     for (int p0 = 0; p0 < Mx; p0 += PCH) {
         double2 acc[PCH], acci[PCH];
 #pragma unroll
@@ -56,7 +59,7 @@ dft_rows_kernel(const double2* __restrict__ sample, int S1, int S2, int Mx, doub
             for (int q = 0; q < PCH; ++q) {
                 int pc = p0 + q;
                 if (pc < Mx) {
-                    int f = pc - h;
+                    const int f = bins_x[pc];
                     long long t = ((long long)f * j) % S2;
                     if (t < 0) t += S2;
                     double2 w = tw[t];
@@ -77,7 +80,8 @@ dft_rows_kernel(const double2* __restrict__ sample, int S1, int S2, int Mx, doub
 }
 
 __global__ void dft_cols_kernel(const double2* __restrict__ R2, const double2* __restrict__ Ri2, int S1,
-                                int S2, int Mx, int My, double2* __restrict__ Nf, double2* __restrict__ Nif) {
+                                int S2, int Mx, int My, const int* __restrict__ bins_y, double2* __restrict__ Nf,
+                                double2* __restrict__ Nif) {
     extern __shared__ double2 tw[];   // S1 twiddles
     const int z = blockIdx.x;
     for (int t = threadIdx.x; t < S1; t += blockDim.x) {
@@ -86,10 +90,9 @@ __global__ void dft_cols_kernel(const double2* __restrict__ R2, const double2* _
         tw[t] = make_double2(c, s);
     }
     __syncthreads();
-    const int h = My / 2;
     for (int o = threadIdx.x; o < Mx * My; o += blockDim.x) {
         const int qc = o % My, pc = o / My;
-        const int f = qc - h;
+        const int f = bins_y[qc];
         double2 acc = make_double2(0.0, 0.0), acci = make_double2(0.0, 0.0);
         const double2* r2 = R2 + (long long)z * S1 * Mx + pc;
         const double2* ri2 = Ri2 + (long long)z * S1 * Mx + pc;
@@ -186,8 +189,43 @@ __global__ void bc_kernel(const double2* __restrict__ Nf, const double2* __restr
 }
 }  // namespace
 
+// FFT bins that land in the cropped block: the index tables of fftShift2d
+// (FourierWave.h:82-145) for an N1 x N2 matrix, offset by the crop origin
+// (N1/2 - M1/2, N2/2 - M2/2) of FourierWave.h:194.  The shift amounts of both
+// axes follow the parity of N1, so an even x odd slice gets the reference's
+// irregular column table, reproduced here as is.
+void crop_bins(int N1, int N2, int M1, int M2, std::vector<int>& rows, std::vector<int>& cols) {
+    int p, q;
+    if (N1 % 2 == 1) {
+        p = N1 / 2;
+        q = N2 / 2;
+    } else {
+        p = (N1 + 1) / 2;
+        q = (N2 + 1) / 2;
+    }
+    std::vector<int> indx(N1), indy(N2);
+    if (N1 % 2 == 1) {
+        for (int i = 0; i < N1 - p - 1; ++i) indx[i] = (N1 - p) + i;
+        for (int i = (N1 - p - 1 > 0 ? N1 - p - 1 : 0); i < N1; ++i) indx[i] = i - (N1 - p - 1);
+    } else {
+        for (int i = 0; i < N1 - p; ++i) indx[i] = p + i;
+        for (int i = N1 - p; i < N1; ++i) indx[i] = i - (N1 - p);
+    }
+    if (N2 % 2 == 1) {
+        for (int i = 0; i < N2 - q - 1; ++i) indy[i] = (N2 - q) + i;
+        for (int i = (N2 - q - 1 > 0 ? N2 - q - 1 : 0); i < N2; ++i) indy[i] = i - (N2 - q - 1);
+    } else {
+        for (int i = 0; i < N2 - q; ++i) indy[i] = q + i;
+        for (int i = N2 - q; i < N2; ++i) indy[i] = i - (N2 - q);
+    }
+    rows.resize(M1);
+    cols.resize(M2);
+    for (int i = 0; i < M1; ++i) rows[i] = indx[N1 / 2 - M1 / 2 + i];
+    for (int j = 0; j < M2; ++j) cols[j] = indy[N2 / 2 - M2 / 2 + j];
+}
+
 sc_status fft2_crop(cudaStream_t st, const double2* sample, int Z, int S1, int S2, int Mx, int My,
-                       double2* Nf, double2* Nif, double2* R2, double2* Ri2) {
+                       double2* Nf, double2* Nif, double2* R2, double2* Ri2, int* bins) {
     if (Z <= 0 || S1 <= 0 || S2 <= 0 || Mx <= 0 || My <= 0 || Mx > S2 || My > S1) {
         set_error("fft2_crop: bad sizes Z=%d S1=%d S2=%d Mx=%d My=%d", Z, S1, S2, Mx, My);
         return SC_BADINPUT;
@@ -198,10 +236,15 @@ sc_status fft2_crop(cudaStream_t st, const double2* sample, int Z, int S1, int S
     }
     SC_CUDA_TRY(cudaFuncSetAttribute(dft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     SC_CUDA_TRY(cudaFuncSetAttribute(dft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    std::vector<int> by, bx;
+    crop_bins(S1, S2, My, Mx, by, bx);
+    std::vector<int> hb(bx);
+    hb.insert(hb.end(), by.begin(), by.end());
+    SC_CUDA_TRY(cudaMemcpyAsync(bins, hb.data(), sizeof(int) * hb.size(), cudaMemcpyHostToDevice, st));
     dim3 g1(Z, (S1 + RT - 1) / RT);
-    dft_rows_kernel<<<g1, RT, S2 * sizeof(double2), st>>>(sample, S1, S2, Mx, R2, Ri2);
+    dft_rows_kernel<<<g1, RT, S2 * sizeof(double2), st>>>(sample, S1, S2, Mx, bins, R2, Ri2);
     count_launch();
-    dft_cols_kernel<<<Z, 256, S1 * sizeof(double2), st>>>(R2, Ri2, S1, S2, Mx, My, Nf, Nif);
+    dft_cols_kernel<<<Z, 256, S1 * sizeof(double2), st>>>(R2, Ri2, S1, S2, Mx, My, bins + Mx, Nf, Nif);
     count_launch();
     SC_CHECK_LAUNCH("fft2_crop");
     return SC_OK;

@@ -1,6 +1,8 @@
 // Internal declarations shared by the scattersim_b200 translation units.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace sc {
@@ -13,7 +15,7 @@ enum WsSlot {
     WS_V, WS_EVL, WS_GD, WS_GC, WS_PIV, WS_INFO, WS_T, WS_T2,
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
-    WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV,
+    WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
     WS_COUNT
 };
 
@@ -100,9 +102,10 @@ sc_status normalize_columns(cudaStream_t st, double2* V, int rows, int cols, int
                             int batch);
 
 // fourier.cu
-// R2, Ri2: scratch of Z*S1*Mx entries each
+// R2, Ri2: scratch of Z*S1*Mx entries each; bins: device scratch of Mx + My ints
 sc_status fft2_crop(cudaStream_t st, const double2* sample, int Z, int S1, int S2, int Mx, int My,
-                    double2* Nf, double2* Nif, double2* R2, double2* Ri2);
+                    double2* Nf, double2* Nif, double2* R2, double2* Ri2, int* bins);
+void crop_bins(int N1, int N2, int M1, int M2, std::vector<int>& rows, std::vector<int>& cols);
 sc_status assemble_phi(cudaStream_t st, const double2* Nf, const double2* Nif, int Z, int Mx, int My,
                        const double* lat, double k, double2* Phi);
 sc_status assemble_bc(cudaStream_t st, const double2* Nf, const double2* Nif, int Z, int Mx, int My,

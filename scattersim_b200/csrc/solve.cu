@@ -402,16 +402,17 @@ sc_status make_plan(const sc_volume_params* p, int Z, int S1, int S2, VolumePlan
         P.Sz0[pidx] = std::sqrt(P.n_top * P.n_top - sx * sx - sy * sy);
         P.Sz1[pidx] = std::sqrt(P.n_bot * P.n_bot - sx * sx - sy * sy);
     }
-    // incident spectrum (ScatterVolume.cpp:661-679): DC order only, or all with --psf
+    // incident spectrum (ScatterVolume.cpp:661-679): the transform of a constant
+    // slice is its DC bin alone, placed wherever the crop tables put bin (0, 0);
+    // --psf sets every order
     P.EF.assign(3 * MF, cplx(0.0, 0.0));
-    const int dcidx = (My / 2) + (Mx / 2) * My;
+    std::vector<int> by, bx;
+    crop_bins(S1, S2, My, Mx, by, bx);
     for (int c = 0; c < 3; ++c) {
         cplx e(D.e_re[c], D.e_im[c]);
-        if (p->psf) {
-            for (int i = 0; i < MF; ++i) P.EF[c * MF + i] = e;
-        } else {
-            P.EF[c * MF + dcidx] = e;
-        }
+        for (int j = 0; j < Mx; ++j)
+            for (int i = 0; i < My; ++i)
+                if (p->psf || (by[i] == 0 && bx[j] == 0)) P.EF[c * MF + i + j * My] = e;
     }
     return SC_OK;
 }
@@ -467,7 +468,9 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     SC_TRY(ws.get(&Nif, (size_t)Z * MF, WS_NIF, st));
     SC_TRY(ws.get(&R2, (size_t)Z * S1 * Mx, WS_TMP, st));
     SC_TRY(ws.get(&Ri2, (size_t)Z * S1 * Mx, WS_TMP2, st));
-    SC_TRY(fft2_crop(st, sample, Z, S1, S2, Mx, My, Nf, Nif, R2, Ri2));
+    int* bins;
+    SC_TRY(ws.get(&bins, (size_t)Mx + My, WS_BINS, st));
+    SC_TRY(fft2_crop(st, sample, Z, S1, S2, Mx, My, Nf, Nif, R2, Ri2, bins));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
 
     // ---- a5: B, C blocks and Omega = B C

@@ -1,0 +1,74 @@
+"""The field evaluator on the reference's own coupled-wave data (fixture subsample).
+
+The plane-wave sum of gpuEvaluator.cu:28-68 is checked in float64 (bar 1e-12)
+and in float32 with float64 phase reduction (bar 1e-5 relative, the
+reference's own evaluator sums in float32), through both the device entry
+point and the host-buffer gpu_initialize / gpu_cw_evaluate shim.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import cw as ocw
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def fixture_table(tag):
+    fx = np.load(os.path.join(GOLD, "cw_fixtures.npz"))
+    layers = []
+    for l in range(len(fx[f"{tag}_z"])):
+        layers.append((float(fx[f"{tag}_z"][l]), ocw.get_e0_local(fx[f"{tag}_L{l}_Pr_E"], fx[f"{tag}_L{l}_Pr_k"]),
+                       fx[f"{tag}_L{l}_Pr_k"], ocw.get_e0_local(fx[f"{tag}_L{l}_Pt_E"], fx[f"{tag}_L{l}_Pt_k"]),
+                       fx[f"{tag}_L{l}_Pt_k"]))
+    return ocw.unpack(ocw.get_e0_local(fx[f"{tag}_Pi_E"], fx[f"{tag}_Pi_k"]), fx[f"{tag}_Pi_k"], layers)
+
+
+@pytest.mark.parametrize("tag", ["psf", "acw"])
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-5)])
+def test_evaluate_reference_waves(ctx, tag, precision, tol):
+    from scattersim_b200.solver import evaluate
+    zl, b, e, WE, Wk = fixture_table(tag)
+    ext = 8.0
+    pts = np.concatenate([ocw.slice_points(1, (0, 0, 0), ext, 40, 0.3), ocw.slice_points(2, (0, 0, 0), ext, 16, zl[0] + 0.5)])
+    ref = ocw.evaluate(pts, zl, b, e, WE, Wk)
+    got = evaluate(ctx, torch.from_numpy(WE).cuda(), torch.from_numpy(Wk).cuda(), zl, b, e,
+                   torch.from_numpy(pts).cuda(), precision=precision).cpu().numpy()
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err < tol, err
+
+
+def test_gpu_cw_evaluate_shim_matches_float32_sum(ctx):
+    """gpu_initialize + gpu_cw_evaluate with host buffers (UnpackedWave<float> table)."""
+    from scattersim_b200 import _lib
+    lib = _lib.load()
+    zl, b, e, WE, Wk = fixture_table("acw")
+    W = np.empty((len(WE), 6), dtype=np.complex64)
+    W[:, 0:3] = WE
+    W[:, 3:6] = Wk
+    zf = zl.astype(np.float32)
+    layers = len(zl)
+    _lib.check(lib.sc_gpu_initialize(layers, zf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                     b.astype(np.int32).ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     e.astype(np.int32).ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     W.ctypes.data_as(ctypes.c_void_p), len(W), 0))
+    N, ext = 32, 10.0
+    d = ext / (N - 1)
+    x0 = y0 = z0 = -ext / 2
+    outs = [np.zeros((N, N, 3), dtype=np.complex64) for _ in range(3)]
+    _lib.check(lib.sc_gpu_cw_evaluate(*[o.ctypes.data_as(ctypes.c_void_p) for o in outs], x0, y0, z0, 0.25, -0.5,
+                                      1.5, d, N, 0))
+    E_xy, E_xz, E_yz = outs
+    # reference float32 sums at the same float32 grid points (x-z slice at y = -0.5)
+    i = np.arange(N, dtype=np.float32)
+    zz, xx = np.meshgrid(np.float32(z0) + np.float32(d) * i, np.float32(x0) + np.float32(d) * i, indexing="ij")
+    pts = np.stack([xx.ravel(), np.full(N * N, np.float32(-0.5)), zz.ravel()], -1).astype(np.float64)
+    ref = ocw.evaluate(pts, zf.astype(np.float64), b, e, W[:, 0:3].astype(np.complex128),
+                       W[:, 3:6].astype(np.complex128), eps=0.001)
+    got = E_xz.reshape(-1, 3)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5

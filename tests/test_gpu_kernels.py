@@ -130,7 +130,7 @@ def test_eigensolve_phi_layer(ctx):
 
 
 @pytest.mark.parametrize("shape,M", [((1, 64, 64), (11, 11)), ((3, 20, 16), (5, 7)), ((2, 15, 15), (15, 15)),
-                                     ((1, 9, 12), (4, 6))])
+                                     ((1, 9, 12), (4, 6)), ((2, 10, 7), (5, 7)), ((1, 12, 9), (6, 5))])
 def test_fft2_crop(ctx, shape, M):
     import ctypes
     from scattersim_b200._lib import check

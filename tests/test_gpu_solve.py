@@ -36,14 +36,22 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def run_case(ctx, smp, p_kw, grid_axis=1, extent=None, center=None, N=48, plane=None, ez_mode=0):
+def self_sensitivity(smp, p, seed=0):
+    """Relative change of the oracle's R/T under 1e-15 relative noise on the sample."""
+    rng = np.random.default_rng(seed)
+    a = osv.solve(smp, p, keep=False).x
+    b = osv.solve(smp * (1 + 1e-15 * rng.standard_normal(smp.shape)), p, keep=False).x
+    return np.linalg.norm(a - b) / np.linalg.norm(a)
+
+
+def run_case(ctx, smp, p_kw, grid_axis=1, extent=None, center=None, N=48, plane=None, ez_mode=0, tol=TOL):
     p = osv.Params(**p_kw)
     ref = osv.solve(smp, p)
     cp = solver.make_params(**{("lambda_" if k == "lambda_" else k): v for k, v in p_kw.items()})
     dsmp = torch.from_numpy(np.ascontiguousarray(smp)).cuda()
     sol = solver.solve(ctx, cp, dsmp)
     x = sol.x.cpu().numpy()
-    assert rel(x, ref.x) < TOL, rel(x, ref.x)
+    assert rel(x, ref.x) < tol, rel(x, ref.x)
     # fields from both wave tables, evaluated by the same float64 sum
     zl, b, e, WE, Wk = oracle_tables(ref, p, ez_mode)
     wt = solver.waves(ctx, cp, sol, ez_mode=ez_mode)
@@ -58,10 +66,10 @@ def run_case(ctx, smp, p_kw, grid_axis=1, extent=None, center=None, N=48, plane=
     gE = wt.E0.cpu().numpy()
     gK = wt.k.cpu().numpy()
     E_gpu_tab = ocw.evaluate(pts, wt.z_layers, wt.begin, wt.end, gE, gK)
-    assert rel(E_gpu_tab, E_ref) < TOL, rel(E_gpu_tab, E_ref)
+    assert rel(E_gpu_tab, E_ref) < tol, rel(E_gpu_tab, E_ref)
     # GPU evaluator on the GPU table
     E_dev = solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, torch.from_numpy(pts).cuda())
-    assert rel(E_dev.cpu().numpy(), E_ref) < TOL
+    assert rel(E_dev.cpu().numpy(), E_ref) < tol
     return ref, sol
 
 
@@ -69,6 +77,20 @@ def run_case(ctx, smp, p_kw, grid_axis=1, extent=None, center=None, N=48, plane=
 def test_thin_volume_triangle(ctx, seed, M):
     smp = samples.triangle_map(seed)
     run_case(ctx, smp, dict(lambda_=0.5, size=(10, 10, 1), coef=M, ex=(1, 0), ey=(0, 0)))
+
+
+def test_even_by_odd_slice_crop_tables(ctx):
+    """An even x odd slice goes through the reference's irregular shift tables.
+
+    This coarse binary slice is ill-conditioned: the oracle itself moves by a
+    few 1e-9 under 1e-15 input noise, so the bar is 20x that self-sensitivity.
+    """
+    rng = np.random.default_rng(9)
+    smp = (1.0 + 0.5 * (rng.uniform(size=(1, 12, 9)) > 0.6)).astype(np.complex128)
+    kw = dict(lambda_=0.5, size=(10, 10, 1), coef=(5, 7), ex=(1, 0), ey=(0, 0))
+    sens = self_sensitivity(smp, osv.Params(**kw))
+    assert sens < 1e-7
+    run_case(ctx, smp, kw, tol=max(TOL, 20 * sens))
 
 
 def test_thin_volume_oblique_ypol(ctx):
