@@ -170,6 +170,8 @@ sc_status sc_qr_stats(sc_context* ctx, long long* out, int count);
 /* Measured FP64 FMA throughput of this device (TFLOP/s): the roofline
  * denominator of the FP64 kernels. */
 sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops);
+/* Measured FP64 tensor-core (mma.sync m8n8k4 f64) throughput (TFLOP/s). */
+sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops);
 
 /* Wave table of a solved volume in cw_unpack order: Pi, then per boundary l
  * its reflected and transmitted lists (ScatterVolume.cpp:907-987,

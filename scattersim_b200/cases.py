@@ -1,0 +1,59 @@
+"""Named solve workloads, for timing and profiling one configuration at a time.
+
+    python -m scattersim_b200.cases <case> [repeats]
+
+Cases (seeded synthetic samples, see samples.py):
+  thin          64x64 triangle map, 10x10 um, 1 um slab, lambda 0.5, 11x11 orders
+  volume        128x128x32 sphere volume, 20x20x8 um, lambda 0.6, 10 deg, 21x21 orders
+  volume8       the same geometry with 8 slices
+  small         128x128x4 sphere volume, 11x11 orders (a short QR capture)
+  fp64          measured FP64 throughput: FMA pipe and mma.sync f64
+Prints the per-stage device milliseconds of the last repeat.
+"""
+from __future__ import annotations
+
+import math
+import sys
+
+D10 = (math.sin(math.radians(10.0)), 0.0, math.cos(math.radians(10.0)))
+
+
+def case(name):
+    from . import samples
+    if name == "thin":
+        return samples.triangle_map(0), dict(lambda_=0.5, size=(10.0, 10.0, 1.0), coef=(11, 11), ex=(1.0, 0.0),
+                                              ey=(0.0, 0.0))
+    vol = dict(lambda_=0.6, size=(20.0, 20.0, 8.0), coef=(21, 21), direction=D10, ex=(1.0, 0.0), ey=(0.0, 0.0))
+    if name == "volume":
+        return samples.sphere_volume(0), vol
+    if name == "volume8":
+        return samples.sphere_volume(0, nz=8), vol
+    if name == "small":
+        return samples.sphere_volume(0, nz=4), dict(vol, coef=(11, 11))
+    raise KeyError(name)
+
+
+def main(argv):
+    import torch
+    from . import solver
+    name = argv[1] if len(argv) > 1 else "thin"
+    reps = int(argv[2]) if len(argv) > 2 else 1
+    if name == "fp64":
+        ctx = solver.Context(0)
+        print(f"fp64 FMA pipe {ctx.fp64_peak_tflops():.2f} TFLOP/s, mma.sync f64 {ctx.fp64_peak_tflops(True):.2f} TFLOP/s")
+        ctx.close()
+        return 0
+    smp, kw = case(name)
+    ctx = solver.Context(0)
+    p = solver.make_params(**kw)
+    d = torch.from_numpy(smp).cuda()
+    for _ in range(reps):
+        solver.solve(ctx, p, d)
+    torch.cuda.synchronize()
+    print(name, {k: round(v, 3) for k, v in ctx.stage_ms().items()}, "launches", ctx.launches())
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv))

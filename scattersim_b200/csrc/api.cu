@@ -293,43 +293,55 @@ sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8) {
 
 namespace sc {
 namespace probe {
-// 8 independent FMA chains per thread keep the FP64 pipes busy
-__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
-    double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-3, x2 = x0 + 2e-3, x3 = x0 + 3e-3;
-    double x4 = x0 + 4e-3, x5 = x0 + 5e-3, x6 = x0 + 6e-3, x7 = x0 + 7e-3;
-    for (int i = 0; i < iters; ++i) {
+// FP64 pipe probes: 8 independent DFMA chains per thread, or 4 independent
+// DMMA m8n8k4 accumulators per warp; both sized to keep every SM's FP64 pipe busy
+__global__ void fp64_dfma_kernel(double* out, int iters) {
+    double a[8];
+    for (int i = 0; i < 8; ++i) a[i] = threadIdx.x * 1e-9 + i;
+    for (int it = 0; it < iters; ++it)
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
-            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
-        }
-    }
-    double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
-    if (s == 12345.678) out[0] = s;
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = fma(a[i], 0.999999, 1e-7);
+    double s = 0;
+    for (int i = 0; i < 8; ++i) s += a[i];
+    if (s == 1.2345) out[0] = s;
+}
+__global__ void fp64_dmma_kernel(double* out, int iters) {
+    const double a = threadIdx.x * 1e-9, b = 1.0;
+    double c[4][2];
+    for (int i = 0; i < 4; ++i) c[i][0] = c[i][1] = 0.0;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                             : "+d"(c[i][0]), "+d"(c[i][1])
+                             : "d"(a), "d"(b));
+    double s = 0;
+    for (int i = 0; i < 4; ++i) s += c[i][0] + c[i][1];
+    if (s == 1.2345) out[0] = s;
 }
 }  // namespace probe
-}  // namespace sc
 
-extern "C" {
-
-sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops) {
-    if (!ctx || !tflops) {
-        set_error("sc_fp64_peak_probe: null argument");
-        return SC_BADINPUT;
-    }
+static sc_status fp64_probe(sc_context* ctx, bool dmma, double* tflops) {
     DeviceGuard g(ctx->device);
     int sms = 0;
     SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     double* out;
     SC_TRY(ctx->ws.get(&out, 1, WS_TMP, 0));
-    const int blocks = sms * 8, threads = 256, iters = 2048;
+    const int blocks = sms * 8, threads = 256, iters = 4096;
     cudaEvent_t e0, e1;
     SC_CUDA_TRY(cudaEventCreate(&e0));
     SC_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(e0, 0);
-        probe::fp64_probe_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+        if (dmma)
+            probe::fp64_dmma_kernel<<<blocks, threads>>>(out, iters);
+        else
+            probe::fp64_dfma_kernel<<<blocks, threads>>>(out, iters);
         count_launch();
         cudaEventRecord(e1, 0);
         SC_CUDA_TRY(cudaEventSynchronize(e1));
@@ -339,9 +351,29 @@ sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    const double warps = (double)blocks * threads / 32.0;
+    const double flops = dmma ? warps * iters * 16 * 2.0 * 8 * 8 * 4 : 2.0 * 16 * 8 * (double)iters * blocks * threads;
     *tflops = flops / (best * 1e-3) / 1e12;
     return SC_OK;
+}
+}  // namespace sc
+
+extern "C" {
+
+sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops) {
+    if (!ctx || !tflops) {
+        set_error("sc_fp64_peak_probe: null argument");
+        return SC_BADINPUT;
+    }
+    return fp64_probe(ctx, false, tflops);
+}
+
+sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops) {
+    if (!ctx || !tflops) {
+        set_error("sc_fp64_dmma_probe: null argument");
+        return SC_BADINPUT;
+    }
+    return fp64_probe(ctx, true, tflops);
 }
 
 sc_status sc_qr_stats(sc_context* ctx, long long* out, int count) {

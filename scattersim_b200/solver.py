@@ -64,9 +64,11 @@ class Context:
         keys = ("sweeps", "shifts", "chase", "far_right", "far_rows", "small", "unused", "total")
         return [dict(zip(keys, out[8 * i:8 * i + 8])) for i in range(count)]
 
-    def fp64_peak_tflops(self) -> float:
+    def fp64_peak_tflops(self, tensor: bool = False) -> float:
+        """Measured FP64 throughput: FMA pipe, or mma.sync f64 with tensor=True."""
         v = ctypes.c_double(0.0)
-        check(self.lib.sc_fp64_peak_probe(self.handle, ctypes.byref(v)))
+        f = self.lib.sc_fp64_dmma_probe if tensor else self.lib.sc_fp64_peak_probe
+        check(f(self.handle, ctypes.byref(v)))
         return v.value
 
 

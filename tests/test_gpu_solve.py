@@ -82,15 +82,16 @@ def test_thin_volume_triangle(ctx, seed, M):
 def test_even_by_odd_slice_crop_tables(ctx):
     """An even x odd slice goes through the reference's irregular shift tables.
 
-    This coarse binary slice is ill-conditioned: the oracle itself moves by a
-    few 1e-9 under 1e-15 input noise, so the bar is 20x that self-sensitivity.
+    The slab and wavelength keep the transfer-matrix chain well conditioned
+    (oracle self-sensitivity to 1e-15 input noise ~1e-14), so the 1e-9 bar
+    holds; thicker slabs at shorter wavelengths amplify evanescent orders
+    exponentially in the reference formulation itself.
     """
     rng = np.random.default_rng(9)
     smp = (1.0 + 0.5 * (rng.uniform(size=(1, 12, 9)) > 0.6)).astype(np.complex128)
-    kw = dict(lambda_=0.5, size=(10, 10, 1), coef=(5, 7), ex=(1, 0), ey=(0, 0))
-    sens = self_sensitivity(smp, osv.Params(**kw))
-    assert sens < 1e-7
-    run_case(ctx, smp, kw, tol=max(TOL, 20 * sens))
+    kw = dict(lambda_=1.0, size=(10, 10, 0.3), coef=(5, 7), ex=(1, 0), ey=(0, 0))
+    assert self_sensitivity(smp, osv.Params(**kw)) < 1e-12
+    run_case(ctx, smp, kw)
 
 
 def test_thin_volume_oblique_ypol(ctx):
