@@ -157,8 +157,27 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
                           int Z, int S1, int S2, void* x, void* evl, void* Qc, void* Qh,
                           int* info, void* stream);
 
+/* Precision of sc_sweep_solve. */
+#define SC_SWEEP_FP64 0    /* every stage in FP64                                    */
+#define SC_SWEEP_MIXED 1   /* FP64 layer factors; FP32 chain and boundary LU with
+                              FP64 iterative refinement                             */
+
+/* A batched sweep of independent scattervolume solves, R/T only (the
+ * --external result, ScatterVolume.cpp:739), in place of one scattervolume
+ * process per sweep point (videomaker.py:61-74, spectroscopy.py:66-91).
+ * Host arrays of length count: params, samples (device pointers to (Z, S1, S2)
+ * complex128 index volumes), Z, S1, S2, x (device pointers to 6*MF complex128
+ * outputs, MF from sc_volume_plan) and status (per-instance sc_status,
+ * written).  Instances may differ in wavelength, direction, size, layer count
+ * and orders.  Returns SC_OK when every instance succeeded, else the first
+ * failing status. */
+sc_status sc_sweep_solve(sc_context* ctx, int count, const sc_volume_params* params,
+                         const void* const* samples, const int* Z, const int* S1, const int* S2,
+                         void* const* x, int precision, int* status, void* stream);
+
 /* Device milliseconds of the last sc_volume_solve on this context:
- * [fft, assemble, eig, chain, boundary, interior, qr-kernel, total]. */
+ * [fft, assemble, eig, chain, boundary, interior, qr-kernel, total];
+ * after sc_sweep_solve: [fft, assemble, layer factors, chain, boundary, -, -, total]. */
 sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8);
 
 /* QR statistics per matrix of the last eigensolve on this context, 8 values

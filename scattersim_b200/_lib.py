@@ -18,6 +18,10 @@ STATUS_NAMES = {0: "SC_OK", 1: "SC_BADINPUT", 2: "SC_NOCONVERGE", 3: "SC_SINGULA
                 5: "SC_CUDA_ERROR", 6: "SC_ENERGY_FAIL"}
 
 
+SC_SWEEP_FP64 = 0
+SC_SWEEP_MIXED = 1
+
+
 class ScatterError(RuntimeError):
     """A C-ABI call returned a non-OK sc_status."""
 
@@ -62,6 +66,8 @@ _SIGS = {
                                  c_int, c_void_p]),
     "sc_volume_params_default": (None, [POINTER(VolumeParams)]),
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
+    "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),
+                               POINTER(c_int), POINTER(c_int), POINTER(c_void_p), c_int, POINTER(c_int), c_void_p]),
     "sc_volume_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_void_p, c_int, c_int, c_int, c_void_p,
                                 c_void_p, c_void_p, c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_stage_ms": (c_int, [c_void_p, POINTER(c_double)]),

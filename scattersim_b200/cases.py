@@ -8,6 +8,9 @@ Cases (seeded synthetic samples, see samples.py):
   volume8       the same geometry with 8 slices
   small         128x128x4 sphere volume, 11x11 orders (a short QR capture)
   fp64          measured FP64 throughput: FMA pipe and mma.sync f64
+  sweep [n]     the uneven sweep (first n of 256 instances: 64 wavelengths x 4
+                angles, 4-16 layer disk stacks, 7..25 orders) in one batched call
+  sweep_plain [n]  the same instances, one per-instance solve each
 Prints the per-stage device milliseconds of the last repeat.
 """
 from __future__ import annotations
@@ -43,6 +46,8 @@ def main(argv):
         print(f"fp64 FMA pipe {ctx.fp64_peak_tflops():.2f} TFLOP/s, mma.sync f64 {ctx.fp64_peak_tflops(True):.2f} TFLOP/s")
         ctx.close()
         return 0
+    if name in ("sweep", "sweep_plain"):
+        return sweep_case(name, int(argv[2]) if len(argv) > 2 else 256)
     smp, kw = case(name)
     ctx = solver.Context(0)
     p = solver.make_params(**kw)
@@ -51,6 +56,36 @@ def main(argv):
         solver.solve(ctx, p, d)
     torch.cuda.synchronize()
     print(name, {k: round(v, 3) for k, v in ctx.stage_ms().items()}, "launches", ctx.launches())
+    ctx.close()
+    return 0
+
+
+def sweep_case(name, count):
+    import time
+    import torch
+    from . import samples, solver
+    inst = samples.sweep_instances(0, count=count)
+    params = [solver.make_params(**it.params_kw()) for it in inst]
+    smp = [torch.from_numpy(it.maps).cuda() for it in inst]
+    ctx = solver.Context(0)
+    layers = sum(it.maps.shape[0] for it in inst)
+    orders = {}
+    for it in inst:
+        orders[it.orders] = orders.get(it.orders, 0) + 1
+    print(f"{count} instances, {layers} layers, orders {dict(sorted(orders.items()))}")
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if name == "sweep":
+            solver.sweep(ctx, params, smp)
+        else:
+            for p, s in zip(params, smp):
+                solver.solve(ctx, p, s, fields=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        print(f"{name} rep {rep}: {dt:.3f} s, {count / dt:.2f} solves/s")
+    if name == "sweep":
+        print({k: round(v, 1) for k, v in ctx.stage_ms().items()})
     ctx.close()
     return 0
 

@@ -33,6 +33,9 @@ sc_status cuda_status(cudaError_t e, const char* where) {
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 uint64_t launch_total() { return g_launches.load(); }
 
+sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params, const void* const* samples,
+                      const int* Zs, const int* S1s, const int* S2s, void* const* x_out, int precision,
+                      int* status, cudaStream_t st);
 sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
                        int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
                        int* info_host, cudaStream_t st);
@@ -278,6 +281,17 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
     DeviceGuard g(ctx->device);
     return volume_solve(ctx, p, (const double2*)sample, Z, S1, S2, (double2*)x, (double2*)evl, (double2*)Qc,
                         (double2*)Qh, info, (cudaStream_t)stream);
+}
+
+sc_status sc_sweep_solve(sc_context* ctx, int count, const sc_volume_params* params, const void* const* samples,
+                         const int* Z, const int* S1, const int* S2, void* const* x, int precision, int* status,
+                         void* stream) {
+    if (!ctx) {
+        set_error("sc_sweep_solve: null context");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return sweep_solve(ctx, count, params, samples, Z, S1, S2, x, precision, status, (cudaStream_t)stream);
 }
 
 sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8) {

@@ -171,20 +171,25 @@ __global__ void phi_kernel(const double2* __restrict__ Nf, const double2* __rest
     }
 }
 
-// B (2M x 2M) = Phi[0:2M, 2M:4M], C = Phi[2M:4M, 0:2M]
+// B (2M x 2M) = Phi[0:2M, 2M:4M], C = Phi[2M:4M, 0:2M].  Layer z uses the
+// lattice and 1/k^2 of instance inst[z] (lat + inst * (Mx + My), kinv_arr)
+// when those arrays are given, else the single lattice and kinv.
 __global__ void bc_kernel(const double2* __restrict__ Nf, const double2* __restrict__ Nif, int Mx, int My,
-                          const double* __restrict__ lat, double kinv, double2* __restrict__ Bm,
-                          double2* __restrict__ Cm) {
+                          const double* __restrict__ lat, double kinv, const int* __restrict__ inst,
+                          const double* __restrict__ kinv_arr, double2* __restrict__ Bm, double2* __restrict__ Cm) {
     const int z = blockIdx.y;
     const int MF = Mx * My, n = 2 * MF;
     const long long tot = (long long)n * n;
     const double2* nf = Nf + (long long)z * MF;
     const double2* nif = Nif + (long long)z * MF;
+    const int ii = inst ? inst[z] : 0;
+    const double* L = lat + (long long)ii * (Mx + My);
+    const double kv = kinv_arr ? kinv_arr[ii] : kinv;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
          t += (long long)gridDim.x * blockDim.x) {
         int r = (int)(t % n), c = (int)(t / n);
-        Bm[(long long)z * tot + t] = phi_at(r, c + n, MF, Mx, My, nf, nif, lat, lat + Mx, kinv);
-        Cm[(long long)z * tot + t] = phi_at(r + n, c, MF, Mx, My, nf, nif, lat, lat + Mx, kinv);
+        Bm[(long long)z * tot + t] = phi_at(r, c + n, MF, Mx, My, nf, nif, L, L + Mx, kv);
+        Cm[(long long)z * tot + t] = phi_at(r + n, c, MF, Mx, My, nf, nif, L, L + Mx, kv);
     }
 }
 }  // namespace
@@ -268,9 +273,22 @@ sc_status assemble_bc(cudaStream_t st, const double2* Nf, const double2* Nif, in
     long long blocks = (n * n + 255) / 256;
     if (blocks > 4096) blocks = 4096;
     dim3 g((unsigned)blocks, Z);
-    bc_kernel<<<g, 256, 0, st>>>(Nf, Nif, Mx, My, lat, 1.0 / (k * k), Bm, Cm);
+    bc_kernel<<<g, 256, 0, st>>>(Nf, Nif, Mx, My, lat, 1.0 / (k * k), nullptr, nullptr, Bm, Cm);
     count_launch();
     SC_CHECK_LAUNCH("assemble_bc");
+    return SC_OK;
+}
+
+sc_status assemble_bc_layers(cudaStream_t st, const double2* Nf, const double2* Nif, int L, int Mx, int My,
+                             const double* lat, const int* inst, const double* kinv, double2* Bm, double2* Cm) {
+    const long long n = 2LL * Mx * My;
+    long long blocks = (n * n + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (L <= 0) return SC_OK;
+    dim3 g((unsigned)blocks, L);
+    bc_kernel<<<g, 256, 0, st>>>(Nf, Nif, Mx, My, lat, 0.0, inst, kinv, Bm, Cm);
+    count_launch();
+    SC_CHECK_LAUNCH("assemble_bc_layers");
     return SC_OK;
 }
 

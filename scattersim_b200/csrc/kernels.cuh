@@ -16,6 +16,7 @@ enum WsSlot {
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
+    WS_SWEEP, WS_SWEEP_PTR,
     WS_COUNT
 };
 
@@ -71,6 +72,29 @@ void count_launch(int n = 1);
 uint64_t launch_total();
 
 // zgemm.cu
+// One batched GEMM C_b = alpha * alpha_b * op(A_b) op(B_b) + beta * C_b.  Each
+// operand is addressed either through a device array of per-batch pointers
+// (Ap/Bp/Cp, when non-null) or as base + b * stride; alphas (device, per batch)
+// is optional.
+struct GemmArgs {
+    int m = 0, n = 0, k = 0;
+    double2 alpha = {1.0, 0.0}, beta = {0.0, 0.0};
+    const double2* alphas = nullptr;
+    const double2* A = nullptr;
+    const double2* const* Ap = nullptr;
+    int lda = 1;
+    long long sA = 0;
+    const double2* B = nullptr;
+    const double2* const* Bp = nullptr;
+    int ldb = 1;
+    long long sB = 0;
+    double2* C = nullptr;
+    double2* const* Cp = nullptr;
+    int ldc = 1;
+    long long sC = 0;
+};
+sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch);
+
 sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
                 long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
                 int ldc, long long sC, int batch);
@@ -110,5 +134,27 @@ sc_status assemble_phi(cudaStream_t st, const double2* Nf, const double2* Nif, i
                        const double* lat, double k, double2* Phi);
 sc_status assemble_bc(cudaStream_t st, const double2* Nf, const double2* Nif, int Z, int Mx, int My,
                       const double* lat, double k, double2* Bm, double2* Cm);
+// L layers of several instances: layer z takes lattice lat + inst[z] * (Mx + My)
+// and 1/k^2 = kinv[inst[z]]
+sc_status assemble_bc_layers(cudaStream_t st, const double2* Nf, const double2* Nif, int L, int Mx, int My,
+                             const double* lat, const int* inst, const double* kinv, double2* Bm, double2* Cm);
+
+// mfun.cu: T_l = exp(-i kdz_l Phi_l) (n4 x n4, n4 = 2 n2) for a batch of layers
+// from B, C and Omega = B C (destroyed).  scr: transfer_scratch_blocks() * count
+// * n2^2 entries; dnorm: count doubles; dcoef: 3 * count entries.
+size_t transfer_scratch_blocks();
+sc_status transfer_inv_batched(cudaStream_t st, int n2, int count, const double2* B, const double2* C, double2* Om,
+                               const std::vector<double>& kdz, double2* T, double2* scr, double* dnorm,
+                               double2* dcoef, int* squarings);
+
+// boundary.cu: per-instance blocks of the boundary system (batched over
+// instances; order vectors [Sx, Sy, Sz0, Sz1, EF] at svec + b * sv_stride,
+// (k, z0) pairs at kz0)
+sc_status boundary_f3(cudaStream_t st, int MF, const double2* svec, long long sv_stride, double2* F, long long sF,
+                      int count);
+sc_status boundary_system(cudaStream_t st, int MF, const double2* svec, long long sv_stride, const double* kz0,
+                          double2* A6, long long sA, double2* b6, long long sb, int count);
+sc_status copy_blocks(cudaStream_t st, int rows, int cols, const double2* const* src, int lds, double2* const* dst,
+                      int ldd, int count);
 
 }  // namespace sc

@@ -1,0 +1,237 @@
+// Layer transfer matrices as matrix functions, batched over layers.
+//
+// The reference's layer factor GC_i GD_i^-1 (ScatterVolume.cpp:297-335, with
+// Ci = exp(i k lambda_j dz) on even and 1/Di = exp(i k lambda_j dz) on odd
+// slots) is V exp(t Lambda) V^-1 = exp(t Phi), t = i k dz, for the layer
+// matrix Phi = [[0, B], [C, 0]] of volume::phi (FourierWave.h:378-392).  The
+// boundary block GD_0 Gc_static^-1 f3 (ScatterVolume.cpp:447) is therefore
+//   exp(-t_0 Phi_0) exp(-t_1 Phi_1) ... exp(-t_{L-1} Phi_{L-1}) f3,
+// which needs the inverse factors only, and no eigenvectors.  With
+// Omega = B C (2M x 2M):
+//   exp(-t Phi) = [[ F,        -t G B     ],
+//                  [ -t C G,   I + C H B  ]]
+//   F = cosh(t sqrt Omega), G = sinh(t sqrt Omega) / (t sqrt Omega),
+//   H = (cosh(t sqrt Omega) - I) Omega^-1
+// (all three are power series in t^2 Omega, so no square root or inverse is
+// formed).  They are evaluated by scaling and double-angle squaring:
+//   y = (t / 2^s)^2 Omega with ||y||_1 <= 4;
+//   F = sum_{j<=12} y^j / (2j)!,  G = sum_{j<=12} y^j / (2j+1)!
+//   (Paterson-Stockmeyer in y^4: 3 powers + 2 products per series; the
+//   truncation error is below 4^13/26! ~ 2e-19 in the 1-norm);
+//   s - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
+//   sinh 2a / 2a = (sinh a / a) cosh a);
+//   the last step also forms H_t = (t^2 / 2) G_{t/2}^2 (cosh 2a - 1 = 2 sinh^2 a).
+// Every product is a batched complex GEMM over all layers of the batch, so the
+// whole stage runs on the DFMA GEMM tile with per-layer scalars.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sc {
+
+namespace {
+
+// out_l = c0 I + c1 y + c2 Y2 + c3 Y3 + c4 Y4  (n x n, contiguous, stride n^2)
+__global__ void poly_block_kernel(int n, const double2* __restrict__ y, const double2* __restrict__ Y2,
+                                  const double2* __restrict__ Y3, const double2* __restrict__ Y4, double c0,
+                                  double c1, double c2, double c3, double c4, double2* __restrict__ out) {
+    const long long nn = (long long)n * n;
+    const long long off = (long long)blockIdx.y * nn;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long i = off + t;
+        double2 v = cscale(y[i], c1);
+        v = cadd(v, cscale(Y2[i], c2));
+        v = cadd(v, cscale(Y3[i], c3));
+        if (c4 != 0.0) v = cadd(v, cscale(Y4[i], c4));
+        if (t % (n + 1) == 0) v.x += c0;
+        out[i] = v;
+    }
+}
+
+// block_l (n x n at base + l * stride, leading dimension ld) = val * I
+__global__ void set_diag_kernel(int n, int ld, long long stride, double val, double2* __restrict__ base) {
+    double2* p = base + (long long)blockIdx.y * stride;
+    const long long nn = (long long)n * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t % n), c = (int)(t / n);
+        p[(long long)c * ld + r] = make_double2(r == c ? val : 0.0, 0.0);
+    }
+}
+
+// A_l *= s_l (real per-layer scale, stored in .x)
+__global__ void scale_layers_kernel(long long nn, const double2* __restrict__ s, double2* __restrict__ A) {
+    const double f = s[blockIdx.y].x;
+    double2* p = A + (long long)blockIdx.y * nn;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x)
+        p[t] = cscale(p[t], f);
+}
+
+// norm_l = max_c sum_r |A_l(r, c)|  (one CTA per layer, one warp per column)
+__global__ void __launch_bounds__(256) norm1_kernel(int n, const double2* __restrict__ A, double* __restrict__ norm) {
+    __shared__ double red[8];
+    const double2* a = A + (long long)blockIdx.x * n * n;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double best = 0.0;
+    for (int c = w; c < n; c += 8) {
+        double s = 0.0;
+        for (int r = lane; r < n; r += 32) s += cabs(a[(long long)c * n + r]);
+        s = warp_sum(s);
+        best = fmax(best, s);
+    }
+    if (lane == 0) red[w] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int i = 1; i < 8; ++i) m = fmax(m, red[i]);
+        norm[blockIdx.x] = m;
+    }
+}
+
+unsigned nblocks(long long tot) {
+    long long b = (tot + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 2048) b = 2048;
+    return (unsigned)b;
+}
+
+double factorial(int k) {
+    double f = 1.0;
+    for (int i = 2; i <= k; ++i) f *= i;
+    return f;
+}
+
+}  // namespace
+
+size_t transfer_scratch_blocks() { return 7; }
+
+sc_status transfer_inv_batched(cudaStream_t st, int n2, int count, const double2* B, const double2* C, double2* Om,
+                               const std::vector<double>& kdz, double2* T, double2* scr, double* dnorm,
+                               double2* dcoef, int* squarings) {
+    if (count <= 0) return SC_OK;
+    if ((int)kdz.size() != count || n2 <= 0) {
+        set_error("transfer_inv_batched: %d layer thicknesses for %d layers", (int)kdz.size(), count);
+        return SC_BADINPUT;
+    }
+    const long long nn = (long long)n2 * n2;
+    const int n4 = 2 * n2;
+    const long long s4 = (long long)n4 * n4;
+    double2* Y2 = scr;
+    double2* Y3 = scr + (long long)count * nn;
+    double2* Y4 = scr + 2LL * count * nn;
+    double2* F = scr + 3LL * count * nn;
+    double2* G = scr + 4LL * count * nn;
+    double2* P1 = scr + 5LL * count * nn;
+    double2* P2 = scr + 6LL * count * nn;
+
+    // 1. scaling: s = max over layers so that (kdz/2^s)^2 ||Omega||_1 <= 4, s >= 1
+    norm1_kernel<<<count, 256, 0, st>>>(n2, Om, dnorm);
+    count_launch();
+    SC_CHECK_LAUNCH("norm1");
+    std::vector<double> hn(count);
+    SC_CUDA_TRY(cudaMemcpyAsync(hn.data(), dnorm, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    int s = 1;
+    for (int l = 0; l < count; ++l) {
+        const double v = kdz[l] * kdz[l] * hn[l];
+        if (!std::isfinite(v)) {
+            set_error("transfer_inv_batched: non-finite layer matrix norm (layer %d)", l);
+            return SC_BADINPUT;
+        }
+        while (s < 60 && v / std::ldexp(1.0, 2 * s) > 4.0) ++s;
+    }
+    if (squarings) *squarings = s;
+
+    // per-layer scalars: y scale, H factor t^2/2 = -(kdz)^2/2, off-diagonal factor -t = -i kdz
+    std::vector<double2> hc(3 * (size_t)count);
+    for (int l = 0; l < count; ++l) {
+        const double h = std::ldexp(kdz[l], -s);
+        hc[l] = make_double2(-h * h, 0.0);
+        hc[count + l] = make_double2(-0.5 * kdz[l] * kdz[l], 0.0);
+        hc[2 * count + l] = make_double2(0.0, -kdz[l]);
+    }
+    SC_CUDA_TRY(cudaMemcpyAsync(dcoef, hc.data(), sizeof(double2) * hc.size(), cudaMemcpyHostToDevice, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    const double2* a_y = dcoef;
+    const double2* a_h = dcoef + count;
+    const double2* a_off = dcoef + 2 * count;
+
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+    auto mm = [&](const double2* A, int lda, long long sA, const double2* Bm, int ldb, long long sB, double2* Cm,
+                  int ldc, long long sC, double2 alpha, double2 beta, const double2* alphas) {
+        GemmArgs g;
+        g.m = n2;
+        g.n = n2;
+        g.k = n2;
+        g.alpha = alpha;
+        g.beta = beta;
+        g.alphas = alphas;
+        g.A = A;
+        g.lda = lda;
+        g.sA = sA;
+        g.B = Bm;
+        g.ldb = ldb;
+        g.sB = sB;
+        g.C = Cm;
+        g.ldc = ldc;
+        g.sC = sC;
+        return zgemm_run(st, false, false, g, count);
+    };
+    const dim3 ge(nblocks(nn), count);
+
+    // 2. y = (kdz/2^s)^2 * (-1) * Omega, in place
+    scale_layers_kernel<<<ge, 256, 0, st>>>(nn, a_y, Om);
+    count_launch();
+    const double2* y = Om;
+    SC_TRY(mm(y, n2, nn, y, n2, nn, Y2, n2, nn, one, zero, nullptr));
+    SC_TRY(mm(Y2, n2, nn, y, n2, nn, Y3, n2, nn, one, zero, nullptr));
+    SC_TRY(mm(Y2, n2, nn, Y2, n2, nn, Y4, n2, nn, one, zero, nullptr));
+
+    // 3. F and G by Paterson-Stockmeyer in y^4
+    for (int which = 0; which < 2; ++which) {
+        double c[13];
+        for (int j = 0; j <= 12; ++j) c[j] = 1.0 / factorial(2 * j + which);
+        double2* out = which ? G : F;
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[8], c[9], c[10], c[11], c[12], P1);
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[4], c[5], c[6], c[7], 0.0, P2);
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[0], c[1], c[2], c[3], 0.0, out);
+        count_launch(3);
+        SC_CHECK_LAUNCH("poly_block");
+        SC_TRY(mm(Y4, n2, nn, P1, n2, nn, P2, n2, nn, one, one, nullptr));
+        SC_TRY(mm(Y4, n2, nn, P2, n2, nn, out, n2, nn, one, one, nullptr));
+    }
+
+    // 4. s - 1 double-angle steps
+    for (int step = 1; step < s; ++step) {
+        SC_TRY(mm(G, n2, nn, F, n2, nn, P1, n2, nn, one, zero, nullptr));
+        set_diag_kernel<<<ge, 256, 0, st>>>(n2, n2, nn, -1.0, P2);
+        count_launch();
+        SC_TRY(mm(F, n2, nn, F, n2, nn, P2, n2, nn, make_double2(2.0, 0.0), one, nullptr));
+        std::swap(G, P1);
+        std::swap(F, P2);
+    }
+
+    // 5. last step straight into the quadrants of T (n4 x n4 per layer)
+    double2* T11 = T;
+    double2* T21 = T + n2;
+    double2* T12 = T + (long long)n2 * n4;
+    double2* T22 = T + (long long)n2 * n4 + n2;
+    SC_TRY(mm(G, n2, nn, G, n2, nn, Y2, n2, nn, one, zero, a_h));          // H = (t^2/2) G^2
+    SC_TRY(mm(G, n2, nn, F, n2, nn, P1, n2, nn, one, zero, nullptr));     // G_t = G F
+    set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, -1.0, T11);
+    set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, 1.0, T22);
+    count_launch(2);
+    SC_CHECK_LAUNCH("set_diag");
+    SC_TRY(mm(F, n2, nn, F, n2, nn, T11, n4, s4, make_double2(2.0, 0.0), one, nullptr));   // F_t = 2F^2 - I
+    SC_TRY(mm(P1, n2, nn, B, n2, nn, T12, n4, s4, one, zero, a_off));      // -t G_t B
+    SC_TRY(mm(C, n2, nn, P1, n2, nn, T21, n4, s4, one, zero, a_off));      // -t C G_t
+    SC_TRY(mm(Y2, n2, nn, B, n2, nn, Y3, n2, nn, one, zero, nullptr));     // H B
+    SC_TRY(mm(C, n2, nn, Y3, n2, nn, T22, n4, s4, one, one, nullptr));     // I + C H B
+    return SC_OK;
+}
+
+}  // namespace sc

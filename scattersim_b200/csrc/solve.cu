@@ -115,89 +115,6 @@ __global__ void scale_rows_batched_kernel(const double2* __restrict__ in, long l
     }
 }
 
-// f3 dense (4MF x 3MF) (ScatterVolume.cpp:377-382)
-__global__ void f3_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
-                          const double2* __restrict__ Sz1, double2* __restrict__ F) {
-    const int n4 = 4 * MF;
-    const long long tot = (long long)n4 * 3 * MF;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t % n4), c = (int)(t / n4);
-        const int rb = r / MF, ri = r % MF, cb = c / MF, ci = c % MF;
-        double2 v = make_double2(0.0, 0.0);
-        if (ri == ci) {
-            if (rb == 0 && cb == 0) v = make_double2(-1.0, 0.0);
-            else if (rb == 1 && cb == 1) v = make_double2(-1.0, 0.0);
-            else if (rb == 2 && cb == 1) v = Sz1[ri];
-            else if (rb == 2 && cb == 2) v = cneg(Sy[ri]);
-            else if (rb == 3 && cb == 0) v = cneg(Sz1[ri]);
-            else if (rb == 3 && cb == 2) v = Sx[ri];
-        }
-        F[t] = v;
-    }
-}
-
-// The 6MF x 6MF boundary system except the Gd*inv(Gc)*f3 block, and b
-// (ScatterVolume.cpp:398-414, 446, 456; f1/f2 of :357-373)
-__global__ void system_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
-                              const double2* __restrict__ Sz0, const double2* __restrict__ Sz1,
-                              const double2* __restrict__ EF, double k, double z0, double2* __restrict__ A,
-                              double2* __restrict__ b) {
-    const int n6 = 6 * MF;
-    const long long tot = (long long)n6 * 3 * MF;   // columns 0..3MF
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t % n6), c = (int)(t / n6);
-        const int cb = c / MF, ci = c % MF;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < MF) {
-            // reflected Gauss row r: Sx R_x + Sy R_y - Sz0 R_z
-            if (ci == r) v = (cb == 0) ? Sx[r] : (cb == 1) ? Sy[r] : cneg(Sz0[r]);
-        } else if (r < 2 * MF) {
-            v = make_double2(0.0, 0.0);   // transmitted Gauss rows live in columns 3MF..6MF
-        } else {
-            // f2 block at rows 2MF.., columns 0..3MF
-            const int rr = r - 2 * MF, rb = rr / MF, ri = rr % MF;
-            if (ri == ci) {
-                if (rb == 0 && cb == 0) v = make_double2(1.0, 0.0);
-                else if (rb == 1 && cb == 1) v = make_double2(1.0, 0.0);
-                else if (rb == 2 && cb == 1) v = Sz0[ri];
-                else if (rb == 2 && cb == 2) v = Sy[ri];
-                else if (rb == 3 && cb == 0) v = cneg(Sz0[ri]);
-                else if (rb == 3 && cb == 2) v = cneg(Sx[ri]);
-            }
-        }
-        A[(long long)c * n6 + r] = v;
-    }
-    // transmitted Gauss rows (MF..2MF) in columns 3MF..6MF, rows 0..2MF of those columns
-    const long long tot2 = (long long)(2 * MF) * 3 * MF;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot2;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t % (2 * MF)), c = 3 * MF + (int)(t / (2 * MF));
-        const int cb = (c - 3 * MF) / MF, ci = (c - 3 * MF) % MF;
-        double2 v = make_double2(0.0, 0.0);
-        if (r >= MF && ci == r - MF) v = (cb == 0) ? Sx[ci] : (cb == 1) ? Sy[ci] : Sz1[ci];
-        A[(long long)c * n6 + r] = v;
-    }
-    // b = [0 (2MF); -f1 EF]
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n6; r += gridDim.x * blockDim.x) {
-        double2 v = make_double2(0.0, 0.0);
-        if (r >= 2 * MF) {
-            const int rr = r - 2 * MF, rb = rr / MF, ri = rr % MF;
-            // phase = exp(i k z0 Sz0)
-            const double2 ph = cexp(cscale(cmul(make_double2(0.0, k), Sz0[ri]), z0));
-            const double2 ex = EF[ri], ey = EF[MF + ri], ez = EF[2 * MF + ri];
-            double2 f;
-            if (rb == 0) f = cmul(ph, ex);
-            else if (rb == 1) f = cmul(ph, ey);
-            else if (rb == 2) f = cadd(cneg(cmul(cmul(ph, Sz0[ri]), ey)), cmul(cmul(ph, Sy[ri]), ez));
-            else f = csub(cmul(cmul(ph, Sz0[ri]), ex), cmul(cmul(ph, Sx[ri]), ez));
-            v = cneg(f);
-        }
-        b[r] = v;
-    }
-}
-
 // rhs0 = f1 EF + f2 R  (ScatterVolume.cpp:768-772)
 __global__ void beta0_rhs_kernel(int MF, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
                                  const double2* __restrict__ Sz0, const double2* __restrict__ EF,
@@ -433,8 +350,8 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
 
     // small host-built arrays: lattice, S vectors, EF, z planes
-    double* lat = nullptr;     // up (Mx), wq (My), UPk (Mx), WQk (My), z (Z+1)
-    const size_t nlat = (size_t)2 * (Mx + My) + Z + 1;
+    double* lat = nullptr;     // up (Mx), wq (My), UPk (Mx), WQk (My), z (Z+1), k, z0
+    const size_t nlat = (size_t)2 * (Mx + My) + Z + 3;
     SC_TRY(ws.get(&lat, nlat, WS_LAT, st));
     std::vector<double> hl(nlat);
     for (int i = 0; i < Mx; ++i) hl[i] = P.up[i];
@@ -442,11 +359,14 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     for (int i = 0; i < Mx; ++i) hl[Mx + My + i] = P.UP[i] + P.dims.dir[0] * k;
     for (int i = 0; i < My; ++i) hl[2 * Mx + My + i] = P.WQ[i] + P.dims.dir[1] * k;
     for (int i = 0; i <= Z; ++i) hl[2 * (Mx + My) + i] = P.z[i];
+    hl[2 * (Mx + My) + Z + 1] = k;
+    hl[2 * (Mx + My) + Z + 2] = P.z[0];
     SC_TRY(upload(st, lat, hl));
     const double* d_up = lat;
     const double* d_upk = lat + Mx + My;
     const double* d_wqk = lat + 2 * Mx + My;
     const double* d_z = lat + 2 * (Mx + My);
+    const double* d_kz0 = d_z + Z + 1;
     double2* svec = nullptr;   // Sx, Sy, Sz0, Sz1, EF (7 MF)
     SC_TRY(ws.get(&svec, (size_t)7 * MF, WS_EVAL_W, st));
     {
@@ -459,8 +379,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         hv.insert(hv.end(), P.EF.begin(), P.EF.end());
         SC_CUDA_TRY(cudaMemcpyAsync(svec, hv.data(), hv.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));
     }
-    const double2 *dSx = svec, *dSy = svec + MF, *dSz0 = svec + 2 * MF, *dSz1 = svec + 3 * MF,
-                  *dEF = svec + 4 * MF;
+    const double2 *dSx = svec, *dSy = svec + MF, *dSz0 = svec + 2 * MF, *dEF = svec + 4 * MF;
 
     // ---- a3: Fourier coefficients
     double2 *Nf, *Nif, *R2, *Ri2;
@@ -576,15 +495,13 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     SC_TRY(ws.get(&A6, (size_t)n6 * n6, WS_A6, st));
     SC_TRY(ws.get(&b6, (size_t)n6, WS_B6, st));
     SC_TRY(ws.get(&piv6, (size_t)n6 + n4, WS_PIV6, st));
-    f3_kernel<<<grid_for((long long)n4 * 3 * MF), 256, 0, st>>>(MF, dSx, dSy, dSz1, F);
-    count_launch();
+    SC_TRY(boundary_f3(st, MF, svec, 0, F, 0, 1));
     SC_TRY(getrf(st, Gcs, n4, s4, n4, 1, piv6 + n6, nullptr));
     SC_TRY(getrs(st, Gcs, n4, s4, n4, piv6 + n6, F, n4, 0, 3 * MF, 1));
     // GD_0 = V_0 diag(dG_0) into X, then A6[2MF:, 3MF:] = GD_0 * F
     scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, dG, n4, n4, n4, X, s4);
     count_launch();
-    system_kernel<<<grid_for((long long)n6 * 3 * MF), 256, 0, st>>>(MF, dSx, dSy, dSz0, dSz1, dEF, k, P.z[0], A6, b6);
-    count_launch();
+    SC_TRY(boundary_system(st, MF, svec, 0, d_kz0, A6, 0, b6, 0, 1));
     SC_TRY(zgemm(st, n4, 3 * MF, n4, make_double2(1.0, 0.0), X, n4, s4, F, n4, 0, make_double2(0.0, 0.0),
                  A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0, 1));
     SC_TRY(getrf(st, A6, n6, 0, n6, 1, piv6, dinfo + Z));

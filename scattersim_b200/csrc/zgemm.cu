@@ -21,16 +21,17 @@ constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
 // CA / CB: operand is used conjugate-transposed (op = ^H) instead of as is
 template <bool CA, bool CB>
-__global__ void __launch_bounds__(NT, 2)
-zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
-             long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
-             double2* __restrict__ C, int ldc, long long sC) {
+__global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmArgs g) {
     __shared__ double2 As[BK][BM];
     __shared__ double2 Bs[BK][BN + 1];
     const int bz = blockIdx.z;
-    A += bz * sA;
-    B += bz * sB;
-    C += bz * sC;
+    const int m = g.m, n = g.n, k = g.k, lda = g.lda, ldb = g.ldb, ldc = g.ldc;
+    // per-CTA operand addresses: pointer arrays when given, else strided
+    const double2* __restrict__ A = g.Ap ? g.Ap[bz] : g.A + bz * g.sA;
+    const double2* __restrict__ B = g.Bp ? g.Bp[bz] : g.B + bz * g.sB;
+    double2* __restrict__ C = g.Cp ? g.Cp[bz] : g.C + bz * g.sC;
+    const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[bz]) : g.alpha;
+    const double2 beta = g.beta;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
 
@@ -125,26 +126,45 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
 }
 }  // namespace
 
-sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,
-                   const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB,
-                   double2 beta, double2* C, int ldc, long long sC, int batch) {
-    if (m <= 0 || n <= 0 || batch <= 0) return SC_OK;
-    dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN, batch);
+sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch) {
+    if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
+    dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, batch);
     if (grid.y > 65535 || grid.z > 65535) {
-        set_error("zgemm: grid too large (n=%d, batch=%d)", n, batch);
+        set_error("zgemm: grid too large (n=%d, batch=%d)", g.n, batch);
         return SC_BADINPUT;
     }
     if (!conjA && !conjB)
-        zgemm_kernel<false, false><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+        zgemm_kernel<false, false><<<grid, NT, 0, st>>>(g);
     else if (conjA && !conjB)
-        zgemm_kernel<true, false><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+        zgemm_kernel<true, false><<<grid, NT, 0, st>>>(g);
     else if (!conjA && conjB)
-        zgemm_kernel<false, true><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+        zgemm_kernel<false, true><<<grid, NT, 0, st>>>(g);
     else
-        zgemm_kernel<true, true><<<grid, NT, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+        zgemm_kernel<true, true><<<grid, NT, 0, st>>>(g);
     count_launch();
     SC_CHECK_LAUNCH("zgemm");
     return SC_OK;
+}
+
+sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,
+                   const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB,
+                   double2 beta, double2* C, int ldc, long long sC, int batch) {
+    GemmArgs g;
+    g.m = m;
+    g.n = n;
+    g.k = k;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.A = A;
+    g.lda = lda;
+    g.sA = sA;
+    g.B = B;
+    g.ldb = ldb;
+    g.sB = sB;
+    g.C = C;
+    g.ldc = ldc;
+    g.sC = sC;
+    return zgemm_run(st, conjA, conjB, g, batch);
 }
 
 namespace {

@@ -78,10 +78,14 @@ def disk_map(rng, n: int = 64, period: float = 25.0) -> np.ndarray:
 
 
 def disk_stack(seed: int, n: int = 64, period: float = 25.0):
-    """One sweep instance's stack: (L, n, n) map and per-layer thicknesses (um)."""
+    """One sweep instance's stack: (L, n, n) maps and the layer thickness (um).
+
+    scattervolume slices a sample into equal layers (ScatterVolume.cpp:162-168),
+    so one thickness in [0.1, 0.5] um is drawn per stack; the slab is L times it.
+    """
     rng = np.random.default_rng(seed)
     L = int(rng.integers(4, 17))
-    thick = rng.uniform(0.1, 0.5, size=L)
+    thick = float(rng.uniform(0.1, 0.5))
     maps = np.stack([disk_map(rng, n, period) for _ in range(L)])
     return maps, thick
 
@@ -97,13 +101,22 @@ class SweepInstance:
     angle_deg: float
     orders: int                 # Mx = My
     maps: np.ndarray            # (L, n, n) complex128
-    thickness: np.ndarray       # (L,) um
+    thickness: float            # layer thickness, um
     period: float
 
     @property
     def direction(self):
         a = math.radians(self.angle_deg)
         return (math.sin(a), 0.0, math.cos(a))
+
+    @property
+    def size(self):
+        return (self.period, self.period, self.thickness * self.maps.shape[0])
+
+    def params_kw(self):
+        """scattervolume options of this instance (x-polarised, R/T only)."""
+        return dict(lambda_=self.wavelength, size=self.size, coef=(self.orders, self.orders),
+                    direction=self.direction, ex=(1.0, 0.0), ey=(0.0, 0.0), external=True)
 
 
 def sweep_instances(seed: int = 0, count: int = 256, n: int = 64, period: float = 25.0):

@@ -173,6 +173,45 @@ def evaluate(ctx: Context, E0: torch.Tensor, K: torch.Tensor, z_layers, begin, e
     return out
 
 
+@dataclass
+class SweepResult:
+    x: list                  # per instance: (6 MF,) complex128 device tensor [R; T]
+    status: list             # per instance sc_status
+    dims: list               # per instance VolumeDims
+
+
+def sweep(ctx: Context, params, samples, precision: int = _lib.SC_SWEEP_FP64, stream=None,
+          raise_on_error: bool = True) -> SweepResult:
+    """A batched sweep of independent R/T solves: sc_sweep_solve over device-resident samples.
+
+    params: sequence of VolumeParams; samples: sequence of (Z, S1, S2) (or (S1, S2))
+    complex128 CUDA tensors.  Instances may differ in every parameter.
+    """
+    n = len(params)
+    if len(samples) != n:
+        raise ValueError("params and samples differ in length")
+    smp = []
+    for t in samples:
+        if t.dim() == 2:
+            t = t.unsqueeze(0)
+        if t.dtype != torch.complex128 or not t.is_cuda:
+            raise TypeError("samples must be complex128 CUDA tensors")
+        smp.append(t.contiguous())
+    dims = [plan(p, tuple(t.shape)) for p, t in zip(params, smp)]
+    xs = [torch.empty(6 * d.MF, dtype=torch.complex128, device=t.device) for d, t in zip(dims, smp)]
+    P = (VolumeParams * max(n, 1))(*params)
+    S = (ctypes.c_void_p * max(n, 1))(*[t.data_ptr() for t in smp])
+    Z = (ctypes.c_int * max(n, 1))(*[t.shape[0] for t in smp])
+    S1 = (ctypes.c_int * max(n, 1))(*[t.shape[1] for t in smp])
+    S2 = (ctypes.c_int * max(n, 1))(*[t.shape[2] for t in smp])
+    X = (ctypes.c_void_p * max(n, 1))(*[x.data_ptr() for x in xs])
+    st = (ctypes.c_int * max(n, 1))()
+    rc = ctx.lib.sc_sweep_solve(ctx.handle, n, P, S, Z, S1, S2, X, int(precision), st, _stream_ptr(stream))
+    if raise_on_error:
+        check(rc)
+    return SweepResult(xs, list(st[:n]), dims)
+
+
 def eigensolve(ctx: Context, A: torch.Tensor, stream=None):
     """Batched eigenvalues / right eigenvectors of (B, n, n) complex128 matrices (row-major torch view)."""
     if A.dim() == 2:
