@@ -110,6 +110,18 @@ sc_status sc_zgemm_batched(sc_context* ctx, int m, int n, int k, const double* a
                            long long strideB, const double* beta, void* C, int ldc,
                            long long strideC, int batch, void* stream);
 
+/* The product of sc_zgemm_batched on the int8 tensor cores (tcgen05): each
+ * operand is cut into `slices` signed 7-bit digits (1..7) under power-of-two
+ * row (A) and column (B) scales, digit products are summed exactly in int32
+ * and recombined in FP64; the error is about (slices + 1) 2^-7*slices times
+ * the row scale x column scale x k per element.  No reference counterpart: it
+ * is the arithmetic of the mixed-precision sweep.  Synchronises the stream;
+ * SC_CUDA_ERROR if a tensor-core pipeline wait timed out. */
+sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, int k, const double* alpha,
+                                    const void* A, int lda, long long strideA, const void* B, int ldb,
+                                    long long strideB, const double* beta, void* C, int ldc,
+                                    long long strideC, int batch, void* stream);
+
 /* --------------------------------------------------------- volume solve */
 
 typedef struct {

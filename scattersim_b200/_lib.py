@@ -61,6 +61,9 @@ _SIGS = {
     "sc_linearsolve_batched_noalloc": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int, POINTER(c_int),
                                                c_void_p]),
     "sc_inverse_batched": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, POINTER(c_int), c_void_p]),
+    "sc_zgemm_emulated_batched": (c_int, [c_void_p, c_int, c_int, c_int, c_int, POINTER(c_double), c_void_p, c_int, c_longlong,
+                                 c_void_p, c_int, c_longlong, POINTER(c_double), c_void_p, c_int, c_longlong,
+                                 c_int, c_void_p]),
     "sc_zgemm_batched": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_void_p, c_int, c_longlong, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_int, c_void_p]),

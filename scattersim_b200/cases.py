@@ -11,6 +11,7 @@ Cases (seeded synthetic samples, see samples.py):
   sweep [n]     the uneven sweep (first n of 256 instances: 64 wavelengths x 4
                 angles, 4-16 layer disk stacks, 7..25 orders) in one batched call
   sweep_plain [n]  the same instances, one per-instance solve each
+  gemm          batched complex GEMM throughput at the shapes of the solves
 Prints the per-stage device milliseconds of the last repeat.
 """
 from __future__ import annotations
@@ -46,6 +47,8 @@ def main(argv):
         print(f"fp64 FMA pipe {ctx.fp64_peak_tflops():.2f} TFLOP/s, mma.sync f64 {ctx.fp64_peak_tflops(True):.2f} TFLOP/s")
         ctx.close()
         return 0
+    if name == "gemm":
+        return gemm_case()
     if name in ("sweep", "sweep_plain"):
         return sweep_case(name, int(argv[2]) if len(argv) > 2 else 256)
     smp, kw = case(name)
@@ -56,6 +59,52 @@ def main(argv):
         solver.solve(ctx, p, d)
     torch.cuda.synchronize()
     print(name, {k: round(v, 3) for k, v in ctx.stage_ms().items()}, "launches", ctx.launches())
+    ctx.close()
+    return 0
+
+
+def gemm_case():
+    import ctypes
+    import torch
+    from . import solver
+    from ._lib import check
+    ctx = solver.Context(0)
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    zero = (ctypes.c_double * 2)(0.0, 0.0)
+    for m, n, k, batch in [(98, 98, 98, 512), (242, 242, 242, 256), (450, 450, 450, 128), (882, 882, 882, 64),
+                           (1250, 1250, 1250, 32), (1764, 1764, 1764, 8), (2500, 1875, 2500, 8),
+                           (3528, 3528, 3528, 2)]:
+        A = torch.randn(batch, k, m, dtype=torch.complex128, device="cuda")
+        B = torch.randn(batch, n, k, dtype=torch.complex128, device="cuda")
+        C = torch.empty(batch, n, m, dtype=torch.complex128, device="cuda")
+        args = (ctx.handle, m, n, k, one, ctypes.c_void_p(A.data_ptr()), m, m * k, ctypes.c_void_p(B.data_ptr()), k,
+                k * n, zero, ctypes.c_void_p(C.data_ptr()), m, m * n, batch, None)
+        for _ in range(2):
+            check(ctx.lib.sc_zgemm_batched(*args))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        reps = 5
+        for _ in range(reps):
+            check(ctx.lib.sc_zgemm_batched(*args))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = 8.0 * m * n * k * batch / (ms * 1e-3) / 1e12
+        ref = (A[0].T @ B[0].T).T   # column-major product of batch 0
+        err = (C[0] - ref).abs().max().item() / ref.abs().max().item()
+        print(f"zgemm m={m} n={n} k={k} batch={batch}: {ms:.3f} ms, {tf:.1f} TFLOP/s, err {err:.1e}")
+        for slices in (4, 6, 7):
+            eargs = (ctx.handle, slices) + args[1:]
+            check(ctx.lib.sc_zgemm_emulated_batched(*eargs))
+            e0.record()
+            for _ in range(reps):
+                check(ctx.lib.sc_zgemm_emulated_batched(*eargs))
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            tf = 8.0 * m * n * k * batch / (ms * 1e-3) / 1e12
+            err = (C[0] - ref).abs().max().item() / ref.abs().max().item()
+            print(f"   int8 x{slices}: {ms:.3f} ms, {tf:.1f} FP64-equivalent TFLOP/s, err {err:.1e}")
     ctx.close()
     return 0
 

@@ -235,6 +235,46 @@ sc_status sc_inverse_batched(sc_context* ctx, const void* A, int n, int batch, v
     return sc_linearsolve_batched(ctx, LU, n, Ainv, n, batch, info, stream);
 }
 
+sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, int k, const double* alpha,
+                                    const void* A, int lda, long long strideA, const void* B, int ldb,
+                                    long long strideB, const double* beta, void* C, int ldc, long long strideC,
+                                    int batch, void* stream) {
+    if (!ctx || !alpha || !beta || !A || !B || !C || m < 0 || n < 0 || k < 0 || lda < (m > 1 ? m : 1) ||
+        ldb < (k > 1 ? k : 1) || ldc < (m > 1 ? m : 1)) {
+        set_error("sc_zgemm_emulated_batched: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* err;
+    SC_TRY(ctx->ws.get(&err, 1, WS_OZ_ERR, st));
+    SC_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+    GemmArgs a;
+    a.m = m;
+    a.n = n;
+    a.k = k;
+    a.alpha = make_double2(alpha[0], alpha[1]);
+    a.beta = make_double2(beta[0], beta[1]);
+    a.A = (const double2*)A;
+    a.lda = lda;
+    a.sA = strideA;
+    a.B = (const double2*)B;
+    a.ldb = ldb;
+    a.sB = strideB;
+    a.C = (double2*)C;
+    a.ldc = ldc;
+    a.sC = strideC;
+    SC_TRY(zgemm_ozaki(st, slices, a, batch, ctx->ws, err));
+    int herr = 0;
+    SC_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+        set_error("sc_zgemm_emulated_batched: tensor-core pipeline wait timed out (stage %d)", herr);
+        return SC_CUDA_ERROR;
+    }
+    return SC_OK;
+}
+
 sc_status sc_zgemm_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
                            long long strideA, const void* B, int ldb, long long strideB, const double* beta,
                            void* C, int ldc, long long strideC, int batch, void* stream) {

@@ -16,7 +16,7 @@ enum WsSlot {
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
-    WS_SWEEP, WS_SWEEP_PTR,
+    WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR,
     WS_COUNT
 };
 
@@ -102,6 +102,21 @@ sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const doubl
 sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,
                    const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB,
                    double2 beta, double2* C, int ldc, long long sC, int batch);
+
+// ozaki.cu: the same product (op = N only) on the int8 tensor cores with
+// `slices` 7-bit digits per operand (1..7); err: device word set nonzero if a
+// pipeline wait timed out (never cleared here)
+sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch, Workspace& ws, int* err);
+
+// A GEMM engine: FP64 tensor-pipe tiles (slices == 0) or int8 digit slices
+struct GemmEngine {
+    int slices = 0;
+    Workspace* ws = nullptr;
+    int* err = nullptr;
+    sc_status run(cudaStream_t st, const GemmArgs& g, int batch) const {
+        return slices ? zgemm_ozaki(st, slices, g, batch, *ws, err) : zgemm_run(st, false, false, g, batch);
+    }
+};
 
 // y = alpha A x + beta y (batched, deterministic two-pass); part: zgemv_part_size entries
 sc_status zgemv(cudaStream_t st, int m, int n, double2 alpha, const double2* A, int lda, long long sA,

@@ -1,0 +1,472 @@
+// Complex128 GEMM on the int8 tensor cores (tcgen05.mma kind::i8), exact to
+// the chosen number of 7-bit slices: C_b = alpha * A_b B_b + beta * C_b.
+//
+// Splitting (Ozaki's scheme with power-of-two row / column scales):
+//   the complex product is the real product A' B' of the interleaved
+//   embedding  A'(2i, 2j) = Re a_ij, A'(2i, 2j+1) = -Im a_ij,
+//              A'(2i+1, 2j) = Im a_ij, A'(2i+1, 2j+1) = Re a_ij,
+//              B'(2j, c) = Re b_jc, B'(2j+1, c) = Im b_jc,
+//   so rows 2i / 2i+1 of C' are Re / Im of c_ic.  Row i of A' is divided by
+//   sigma_i = 2^e_i > max_j |a_ij| (one exponent per complex row), column c of
+//   B' by tau_c = 2^f_c; the scaled values (|x| < 1) are cut into s signed
+//   digits x = sum_t d_t 2^-7(t+1), |d_t| <= 127, by truncation (exact in FP64).
+//   Digit products with t + u <= s - 1 are summed in int32, one accumulator
+//   per digit sum d = t + u (|acc| <= (d+1) K' 127^2 < 2^31 for K' <= 2^16 / (d+1)),
+//   and the epilogue forms sigma_i tau_c sum_d 2^-7(d+2) acc_d in FP64.
+//   The dropped terms and the digit tails bound the error by about
+//   (s + 1) 2^-7s sigma_i tau_c K' per element.
+//
+// Data path (one CTA of 128 threads per 128 x 64 tile of C', one CTA per SM):
+//   the pack kernels write every operand tile (128 or 64 rows x 32 bytes of K,
+//   all s digit planes) pre-arranged in the UMMA K-major core-matrix layout
+//   (8 rows x 16 bytes per core matrix, LBO = 128 B along K, SBO = 256 B along
+//   rows) with 16-byte stores, so one stage is two contiguous cp.async.bulk
+//   copies; warp 0 streams stages through a ring of up to 8 slots (as many as
+//   fit in 200 KB; mbarrier complete_tx), warp 1 issues s(s+1)/2 MMAs of
+//   128 x 64 x 32 per stage into TMEM (s accumulators of 64 columns) and
+//   releases slots with tcgen05.commit;
+//   all four warps then read their 32 TMEM lanes (tcgen05.ld 32x32b) and
+//   write C.  Every mbarrier wait is bounded; a timeout sets the error word
+//   and the CTA drains, frees its TMEM and returns.
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sc {
+
+namespace {
+
+constexpr int OZ_BM = 128;       // rows of C' per CTA (TMEM lanes)
+constexpr int OZ_BN = 64;        // columns of C per CTA
+constexpr int OZ_BK = 32;        // bytes (int8 K values) per stage: one MMA K step
+constexpr int OZ_ATILE = OZ_BM * OZ_BK;   // 4 KB per digit plane
+constexpr int OZ_BTILE = OZ_BN * OZ_BK;   // 2 KB per digit plane
+constexpr int OZ_MAXS = 7;
+constexpr int OZ_MAXST = 8;      // pipeline slots
+constexpr int OZ_SMEM_BUDGET = 200 * 1024;
+constexpr int OZ_THREADS = 128;
+constexpr long long OZ_SPIN = 1LL << 24;
+
+// byte offset of (row, kk) inside one K-major core-matrix tile of 32 K bytes:
+// core matrices of 8 rows x 16 bytes, the two along K 128 B apart (LBO), the
+// 8-row groups 256 B apart (SBO)
+__device__ __forceinline__ int tile_off(int r, int kk) {
+    return (r >> 3) * 256 + (kk >> 4) * 128 + (r & 7) * 16 + (kk & 15);
+}
+
+// stages of the ring for s digit planes
+__host__ __device__ __forceinline__ int oz_stages(int s) {
+    const int per = s * (OZ_ATILE + OZ_BTILE);
+    int n = OZ_SMEM_BUDGET / per;
+    return n > OZ_MAXST ? OZ_MAXST : n;
+}
+
+// ------------------------------------------------------------------ scales
+// rowexp[b][i] = smallest e with max_j |Re, Im a_ij| < 2^e (rows of A, column-major)
+__global__ void oz_rowexp_kernel(int m, int k, const double2* __restrict__ A, const double2* const* Ap, int lda,
+                                 long long sA, int* __restrict__ rowexp) {
+    const int b = blockIdx.z;
+    const double2* a = Ap ? Ap[b] : A + b * sA;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int j0 = blockIdx.y * 256, j1 = min(k, j0 + 256);
+    double mx = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        const double2 v = a[(long long)j * lda + i];
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+    if (mx > 0.0) {
+        int e;
+        frexp(mx, &e);   // mx < 2^e
+        atomicMax(rowexp + (long long)b * m + i, e);
+    }
+}
+
+// colexp[b][c] = smallest f with max_j |Re, Im b_jc| < 2^f (one warp per column)
+__global__ void oz_colexp_kernel(int k, int n, const double2* __restrict__ B, const double2* const* Bp, int ldb,
+                                 long long sB, int* __restrict__ colexp) {
+    const int b = blockIdx.y;
+    const double2* bb = Bp ? Bp[b] : B + b * sB;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (c >= n) return;
+    double mx = 0.0;
+    for (int j = lane; j < k; j += 32) {
+        const double2 v = bb[(long long)c * ldb + j];
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+        int e = -1100;
+        if (mx > 0.0) frexp(mx, &e);
+        colexp[(long long)b * n + c] = e;
+    }
+}
+
+// next signed 7-bit digit of x (|x| < 1), leaving the remainder in x
+__device__ __forceinline__ int next_digit(double& x) {
+    x *= 128.0;
+    const double q = trunc(x);
+    x -= q;
+    return (int)q;
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+    return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
+           ((uint32_t)(uint8_t)d << 24);
+}
+
+// ------------------------------------------------------------------ packing
+// A' tiles: [b][rb][kb][t][4 KB]; a thread takes one complex row i and 8
+// complex columns (16 K bytes) and writes one 16-byte core-matrix row per plane
+// for each of A' rows 2i and 2i+1
+__global__ void __launch_bounds__(128) oz_pack_a_kernel(int m, int k, const double2* __restrict__ A,
+                                                        const double2* const* Ap, int lda, long long sA,
+                                                        const int* __restrict__ rowexp, int s, int RB, int KB,
+                                                        int8_t* __restrict__ out) {
+    const int b = blockIdx.z;
+    const int rb = blockIdx.x, kb = blockIdx.y;
+    const double2* a = Ap ? Ap[b] : A + b * sA;
+    int8_t* tile = out + (((long long)b * RB + rb) * KB + kb) * (long long)s * OZ_ATILE;
+    const int il = threadIdx.x & 63, jc = threadIdx.x >> 6;   // 64 rows x 2 chunks
+    const int i = rb * (OZ_BM / 2) + il, j0 = kb * (OZ_BK / 2) + 8 * jc;
+    double xr[8], xi[8];
+    const int ex = (i < m) ? rowexp[(long long)b * m + i] : 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double2 v = make_double2(0.0, 0.0);
+        if (i < m && j0 + q < k) v = a[(long long)(j0 + q) * lda + i];
+        xr[q] = ldexp(v.x, -ex);
+        xi[q] = ldexp(v.y, -ex);
+    }
+    const int o0 = tile_off(2 * il, 16 * jc), o1 = tile_off(2 * il + 1, 16 * jc);
+    for (int t = 0; t < s; ++t) {
+        int dr[8], di[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            dr[q] = next_digit(xr[q]);
+            di[q] = next_digit(xi[q]);
+        }
+        // row 2i: (Re, -Im) pairs; row 2i+1: (Im, Re) pairs
+        const uint4 w0 = make_uint4(pack4(dr[0], -di[0], dr[1], -di[1]), pack4(dr[2], -di[2], dr[3], -di[3]),
+                                    pack4(dr[4], -di[4], dr[5], -di[5]), pack4(dr[6], -di[6], dr[7], -di[7]));
+        const uint4 w1 = make_uint4(pack4(di[0], dr[0], di[1], dr[1]), pack4(di[2], dr[2], di[3], dr[3]),
+                                    pack4(di[4], dr[4], di[5], dr[5]), pack4(di[6], dr[6], di[7], dr[7]));
+        int8_t* pl = tile + (long long)t * OZ_ATILE;
+        *reinterpret_cast<uint4*>(pl + o0) = w0;
+        *reinterpret_cast<uint4*>(pl + o1) = w1;
+    }
+}
+
+// B' tiles (N x K, K-major): [b][cb][kb][t][2 KB]; a thread takes one column c
+// and 8 complex rows (16 K bytes) and writes one 16-byte row per plane
+__global__ void __launch_bounds__(128) oz_pack_b_kernel(int k, int n, const double2* __restrict__ B,
+                                                        const double2* const* Bp, int ldb, long long sB,
+                                                        const int* __restrict__ colexp, int s, int CB, int KB,
+                                                        int8_t* __restrict__ out) {
+    const int b = blockIdx.z;
+    const int cb = blockIdx.x, kb = blockIdx.y;
+    const double2* bb = Bp ? Bp[b] : B + b * sB;
+    int8_t* tile = out + (((long long)b * CB + cb) * KB + kb) * (long long)s * OZ_BTILE;
+    const int cl = threadIdx.x & 63, jc = threadIdx.x >> 6;
+    const int c = cb * OZ_BN + cl, j0 = kb * (OZ_BK / 2) + 8 * jc;
+    double xr[8], xi[8];
+    const int ex = (c < n) ? colexp[(long long)b * n + c] : 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double2 v = make_double2(0.0, 0.0);
+        if (c < n && j0 + q < k) v = bb[(long long)c * ldb + j0 + q];
+        xr[q] = ldexp(v.x, -ex);
+        xi[q] = ldexp(v.y, -ex);
+    }
+    const int o = tile_off(cl, 16 * jc);
+    for (int t = 0; t < s; ++t) {
+        int dr[8], di[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            dr[q] = next_digit(xr[q]);
+            di[q] = next_digit(xi[q]);
+        }
+        const uint4 w = make_uint4(pack4(dr[0], di[0], dr[1], di[1]), pack4(dr[2], di[2], dr[3], di[3]),
+                                   pack4(dr[4], di[4], dr[5], di[5]), pack4(dr[6], di[6], dr[7], di[7]));
+        *reinterpret_cast<uint4*>(tile + (long long)t * OZ_BTILE + o) = w;
+    }
+}
+
+// ------------------------------------------------------------------ tcgen05 plumbing
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false after OZ_SPIN polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (long long it = 0; it < OZ_SPIN; ++it)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+    // K-major, no swizzle: LBO = 128 B (next core matrix along K), SBO = 256 B
+    // (next 8-row group), descriptor version 1
+    return (uint64_t)((smem_u32(p) >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
+           (1ULL << 46);
+}
+// kind::i8: D s32 (bits 4-5 = 2), A and B signed (bits 7-9, 10-12 = 1), K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
+                              ((uint32_t)(OZ_BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+struct OzArgs {
+    int m, n, k, s, RB, CB, KB;
+    const int8_t* Aq;        // packed A' digit tiles
+    const int8_t* Bq;        // packed B' digit tiles
+    const int* rowexp;       // [b][m]
+    const int* colexp;       // [b][n]
+    double2 alpha, beta;
+    const double2* alphas;
+    double2* C;
+    double2* const* Cp;
+    int ldc;
+    long long sC;
+    int* err;
+};
+
+__global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[OZ_MAXST], empty[OZ_MAXST], done;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    const int s = g.s;
+    const int NS = oz_stages(s);
+    const int stageA = s * OZ_ATILE, stageB = s * OZ_BTILE;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // column blocks vary fastest, so the CTAs resident at one time share their
+    // A' row-block tiles through L2
+    const int cb = blockIdx.x, rb = blockIdx.y, b = blockIdx.z;
+    const int KB = g.KB;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NS; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], 1);
+        }
+        mbar_init(&done, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    // TMEM columns: s accumulators of 64, rounded up to a power of two
+    const uint32_t ncols = (s <= 2) ? 128u : (s <= 4) ? 256u : 512u;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    const int8_t* Ab = g.Aq + (((long long)b * g.RB + rb) * KB) * (long long)stageA;
+    const int8_t* Bb = g.Bq + (((long long)b * g.CB + cb) * KB) * (long long)stageB;
+
+    if (warp == 0 && lane == 0) {
+        // producer: stage kb into slot kb % NS once the MMAs of stage kb - NS released it
+        for (int kb = 0; kb < KB; ++kb) {
+            const int slot = kb % NS;
+            if (kb >= NS && !mbar_wait(&empty[slot], ((kb / NS) - 1) & 1)) {
+                atomicExch(g.err, 1);
+                abort_flag = 1;
+                break;
+            }
+            if (abort_flag) break;
+            unsigned char* sa = smem_raw + (size_t)slot * (stageA + stageB);
+            mbar_expect_tx(&full[slot], (uint32_t)(stageA + stageB));
+            bulk_g2s(sa, Ab + (long long)kb * stageA, (uint32_t)stageA, &full[slot]);
+            bulk_g2s(sa + stageA, Bb + (long long)kb * stageB, (uint32_t)stageB, &full[slot]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: every digit pair with t + u < s, one 128 x 64 x 32 MMA per stage
+        uint32_t written = 0;   // accumulators already initialised
+        for (int kb = 0; kb < KB; ++kb) {
+            const int slot = kb % NS;
+            if (!mbar_wait(&full[slot], (kb / NS) & 1)) {
+                atomicExch(g.err, 2);
+                abort_flag = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const unsigned char* sa = smem_raw + (size_t)slot * (stageA + stageB);
+            for (int t = 0; t < s; ++t) {
+                const uint64_t ad = smem_desc(sa + t * OZ_ATILE);
+                for (int u = 0; t + u < s; ++u) {
+                    const int d = t + u;
+                    const uint64_t bd = smem_desc(sa + stageA + u * OZ_BTILE);
+                    mma_i8(tmem + (uint32_t)(d * OZ_BN), ad, bd, (written >> d) & 1u);
+                    written |= 1u << d;
+                }
+            }
+            mma_commit(&empty[slot]);
+        }
+        mma_commit(&done);
+    }
+    __syncwarp();
+    // epilogue: every warp waits for the last MMA
+    bool ready = mbar_wait(&done, 0);
+    ready = __all_sync(0xffffffffu, ready);
+    if (!ready && lane == 0) atomicExch(g.err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const int rowp = rb * OZ_BM + warp * 32 + lane;   // row of C'
+    const int i = rowp >> 1;                           // complex row
+    const bool im = rowp & 1;
+    double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
+    const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
+    const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
+    const int ex = (i < g.m) ? g.rowexp[(long long)b * g.m + i] : 0;
+    for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
+        double acc[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+        if (ready) {
+            for (int d = 0; d < s; ++d) {
+                uint32_t r[16];
+                const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * OZ_BN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];\n"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(addr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+                for (int q = 0; q < 16; ++q) acc[q] = fma((double)(int)r[q], w, acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int c = cb * OZ_BN + c0 + q;
+            const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
+            const double v = ldexp(acc[q], ex + fx);
+            // partner lane holds the other half of the complex value
+            const double o = __shfl_xor_sync(0xffffffffu, v, 1);
+            if (!im && i < g.m && c < g.n && ready) {
+                double2* p = C + (long long)c * g.ldc + i;
+                double2 val = cmul(alpha, make_double2(v, o));
+                if (!beta_zero) val = cfma(g.beta, *p, val);
+                *p = val;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
+}
+
+}  // namespace
+
+size_t ozaki_smem_bytes(int s) { return (size_t)oz_stages(s) * s * (OZ_ATILE + OZ_BTILE) + 1024; }
+
+sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch, Workspace& ws, int* err) {
+    if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
+    if (slices < 1 || slices > OZ_MAXS) {
+        set_error("zgemm_ozaki: slices must be 1..%d", OZ_MAXS);
+        return SC_BADINPUT;
+    }
+    if (2LL * g.k * (slices + 1) > (1LL << 16)) {
+        set_error("zgemm_ozaki: K = %d too deep for exact int32 accumulation", g.k);
+        return SC_BADINPUT;
+    }
+    const int s = slices;
+    const int RB = (2 * g.m + OZ_BM - 1) / OZ_BM, CB = (g.n + OZ_BN - 1) / OZ_BN, KB = (2 * g.k + OZ_BK - 1) / OZ_BK;
+    if (RB > 65535 || KB > 65535 || batch > 65535) {
+        set_error("zgemm_ozaki: grid too large");
+        return SC_BADINPUT;
+    }
+    const size_t aq = (size_t)batch * RB * KB * s * OZ_ATILE;
+    const size_t bq = (size_t)batch * CB * KB * s * OZ_BTILE;
+    int8_t *Aq, *Bq;
+    int* ex;
+    SC_TRY(ws.get(&Aq, aq, WS_OZ_A, st));
+    SC_TRY(ws.get(&Bq, bq, WS_OZ_B, st));
+    SC_TRY(ws.get(&ex, (size_t)batch * (g.m + g.n), WS_OZ_E, st));
+    int* rowexp = ex;
+    int* colexp = ex + (size_t)batch * g.m;
+    if (!err) {
+        set_error("zgemm_ozaki: no error word");
+        return SC_BADINPUT;
+    }
+    // row exponents start at the smallest exponent (all-zero rows pack to zeros)
+    SC_CUDA_TRY(cudaMemsetAsync(rowexp, 0x80, sizeof(int) * (size_t)batch * g.m, st));
+    oz_rowexp_kernel<<<dim3((g.m + 127) / 128, (g.k + 255) / 256, batch), 128, 0, st>>>(g.m, g.k, g.A, g.Ap, g.lda,
+                                                                                       g.sA, rowexp);
+    oz_colexp_kernel<<<dim3((g.n + 7) / 8, batch), 256, 0, st>>>(g.k, g.n, g.B, g.Bp, g.ldb, g.sB, colexp);
+    oz_pack_a_kernel<<<dim3(RB, KB, batch), 128, 0, st>>>(g.m, g.k, g.A, g.Ap, g.lda, g.sA, rowexp, s, RB, KB, Aq);
+    oz_pack_b_kernel<<<dim3(CB, KB, batch), 128, 0, st>>>(g.k, g.n, g.B, g.Bp, g.ldb, g.sB, colexp, s, CB, KB, Bq);
+    count_launch(4);
+    SC_CHECK_LAUNCH("ozaki pack");
+    OzArgs a;
+    a.m = g.m;
+    a.n = g.n;
+    a.k = g.k;
+    a.s = s;
+    a.RB = RB;
+    a.CB = CB;
+    a.KB = KB;
+    a.Aq = Aq;
+    a.Bq = Bq;
+    a.rowexp = rowexp;
+    a.colexp = colexp;
+    a.alpha = g.alpha;
+    a.beta = g.beta;
+    a.alphas = g.alphas;
+    a.C = g.C;
+    a.Cp = g.Cp;
+    a.ldc = g.ldc;
+    a.sC = g.sC;
+    a.err = err;
+    const size_t smem = ozaki_smem_bytes(s);
+    SC_CUDA_TRY(cudaFuncSetAttribute(oz_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    oz_mma_kernel<<<dim3(CB, RB, batch), OZ_THREADS, smem, st>>>(a);
+    count_launch();
+    SC_CHECK_LAUNCH("ozaki mma");
+    return SC_OK;
+}
+
+}  // namespace sc

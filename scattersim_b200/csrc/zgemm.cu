@@ -5,25 +5,59 @@
 // dense product of the layer chain, the boundary system and the interior
 // fields (ScatterVolume.cpp:331-334, 447-449, 769-779, 838-839).
 //
-// FP64 throughput on B200 is the same through DFMA and DMMA, so the tile is a
-// register-blocked SIMT DFMA tile: 64 x 64 complex outputs per CTA of 256
-// threads, each thread owning a 4 x 4 complex block strided by 16 so that
-// shared-memory reads and global stores are contiguous across a warp.  The
-// K dimension is staged through shared memory 16 deep; the next tile's global
-// loads are issued into registers before the current tile's math.
+// The tile runs on the FP64 tensor pipe (mma.sync m8n8k4 f64, measured 37.1
+// TFLOP/s against 36.6 for DFMA): a complex 8 x 8 x 4 product is four real
+// MMAs (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br), so operand reuse happens
+// inside the MMA unit and shared memory feeds one complex fragment value per
+// lane per MMA group instead of a full outer product per thread.  256 threads
+// (8 warps) per CTA; each warp owns MT x NT 8 x 8 complex tiles.  Two CTA
+// shapes: 128 x 64 (warps 4 x 2, 32 x 32 each) for large products and 64 x 64
+// (warps 2 x 4, 32 x 16 each, two CTAs per SM) for short K or when the large
+// tile would leave SMs idle.  K is
+// staged 16 deep through a three-stage cp.async ring (16-byte copies,
+// zero-filled past the edges); op = ^H is applied to fragments as they leave
+// shared memory.
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace sc {
 
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+constexpr int BK = 16, NT = 256, ST = 3;
+
+__device__ __forceinline__ void cp16(void* smem, const void* gmem, bool pred) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = pred ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <int BM>
+constexpr int tile_smem_bytes() {
+    return ST * BK * ((BM + 1) + (64 + 1)) * (int)sizeof(double2);
+}
+
+// d (8x8, two values per lane) += a (8x4 row fragment) * b (4x8 column fragment)
+__device__ __forceinline__ void dmma(double* d, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
 
 // CA / CB: operand is used conjugate-transposed (op = ^H) instead of as is
-template <bool CA, bool CB>
-__global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmArgs g) {
-    __shared__ double2 As[BK][BM];
-    __shared__ double2 Bs[BK][BN + 1];
+template <int BM, bool CA, bool CB>
+__global__ void __launch_bounds__(NT, (BM == 64 ? 2 : 1)) zgemm_kernel(GemmArgs g) {
+    constexpr int BN = 64;
+    constexpr int WM = (BM == 128) ? 4 : 2, WN = 8 / WM;     // warps along m, n
+    constexpr int MT = BM / WM / 8, NT8 = BN / WN / 8;       // 8x8 tiles per warp
+    constexpr int LAS = BM + 1, LBS = BN + 1;
+    extern __shared__ double2 smem[];
+    double2* As = smem;                    // [ST][BK][LAS]
+    double2* Bs = smem + ST * BK * LAS;    // [ST][BK][LBS]
     const int bz = blockIdx.z;
     const int m = g.m, n = g.n, k = g.k, lda = g.lda, ldb = g.ldb, ldc = g.ldc;
     // per-CTA operand addresses: pointer arrays when given, else strided
@@ -33,114 +67,142 @@ __global__ void __launch_bounds__(NT, 2) zgemm_kernel(GemmArgs g) {
     const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[bz]) : g.alpha;
     const double2 beta = g.beta;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp % WM, wn = warp / WM;
+    const int gq = lane >> 2, tq = lane & 3;   // fragment row/col group, thread in group
 
-    // global -> register staging: A tile 64x16 (4 per thread), B tile 16x64 (4 per thread)
-    double2 ra[4], rb[4];
-    // index maps chosen so that consecutive threads read consecutive addresses
-    auto a_rk = [&](int i, int& r, int& kk) {
-        if (!CA) { r = tid & 63; kk = (tid >> 6) + 4 * i; }
-        else { r = (tid >> 4) + 16 * i; kk = tid & 15; }
-    };
-    auto b_kc = [&](int i, int& kk, int& c) {
-        if (!CB) { kk = tid & 15; c = (tid >> 4) + 16 * i; }
-        else { kk = (tid >> 6) + 4 * i; c = tid & 63; }
-    };
-    auto load = [&](int k0) {
+    // consecutive threads copy consecutive global addresses
+    auto load_stage = [&](int slot, int k0) {
+        double2* as = As + slot * BK * LAS;
+        double2* bs = Bs + slot * BK * LBS;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < BM * BK / NT; ++i) {
+            const int e = tid + NT * i;
             int r, kk;
-            a_rk(i, r, kk);
-            int gr = m0 + r, gk = k0 + kk;
-            if (gr < m && gk < k)
-                ra[i] = CA ? cconj(A[(long long)gr * lda + gk]) : A[(long long)gk * lda + gr];
-            else
-                ra[i] = make_double2(0.0, 0.0);
-            int kb, c;
-            b_kc(i, kb, c);
-            int gkb = k0 + kb, gc = n0 + c;
-            if (gkb < k && gc < n)
-                rb[i] = CB ? cconj(B[(long long)gkb * ldb + gc]) : B[(long long)gc * ldb + gkb];
-            else
-                rb[i] = make_double2(0.0, 0.0);
+            if (!CA) { r = e % BM; kk = e / BM; }
+            else { kk = e % BK; r = e / BK; }
+            const int gr = m0 + r, gk = k0 + kk;
+            const bool ok = gr < m && gk < k;
+            const double2* src = ok ? (CA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
+            cp16(as + kk * LAS + r, src, ok);
         }
-    };
-    auto store = [&]() {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            int r, kk, kb, c;
-            a_rk(i, r, kk);
-            b_kc(i, kb, c);
-            As[kk][r] = ra[i];
-            Bs[kb][c] = rb[i];
+        for (int i = 0; i < BN * BK / NT; ++i) {
+            const int e = tid + NT * i;
+            int kk, c;
+            if (!CB) { kk = e % BK; c = e / BK; }
+            else { c = e % BN; kk = e / BN; }
+            const int gk = k0 + kk, gc = n0 + c;
+            const bool ok = gk < k && gc < n;
+            const double2* src = ok ? (CB ? B + (long long)gk * ldb + gc : B + (long long)gc * ldb + gk) : B;
+            cp16(bs + kk * LBS + c, src, ok);
         }
     };
 
-    double2 acc[4][4];
+    double cr[MT][NT8][2], ci[MT][NT8][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+        for (int j = 0; j < NT8; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
 
-    int nk = (k + BK - 1) / BK;
-    if (nk > 0) {
-        load(0);
-        store();
+    const int nk = (k + BK - 1) / BK;
+#pragma unroll
+    for (int s = 0; s < ST - 1; ++s) {
+        if (s < nk) load_stage(s, s * BK);
+        cp_commit();
     }
-    __syncthreads();
+    const int arow = wm * MT * 8 + gq;   // + 8 * mt
+    const int bcol = wn * NT8 * 8 + gq;  // + 8 * nt
     for (int t = 0; t < nk; ++t) {
-        if (t + 1 < nk) load((t + 1) * BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            double2 a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
-        }
+        cp_wait<ST - 2>();
         __syncthreads();
-        if (t + 1 < nk) {
-            store();
-            __syncthreads();
+        const int tn = t + ST - 1;
+        if (tn < nk) load_stage(tn % ST, tn * BK);
+        cp_commit();
+        const double2* as = As + (t % ST) * BK * LAS;
+        const double2* bs = Bs + (t % ST) * BK * LBS;
+#pragma unroll
+        for (int ks = 0; ks < BK; ks += 4) {
+            double2 a[MT], b[NT8];
+#pragma unroll
+            for (int i = 0; i < MT; ++i) {
+                a[i] = as[(ks + tq) * LAS + arow + 8 * i];
+                if (CA) a[i].y = -a[i].y;
+            }
+#pragma unroll
+            for (int j = 0; j < NT8; ++j) {
+                b[j] = bs[(ks + tq) * LBS + bcol + 8 * j];
+                if (CB) b[j].y = -b[j].y;
+            }
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NT8; ++j) {
+                    dmma(cr[i][j], a[i].x, b[j].x);
+                    dmma(ci[i][j], a[i].x, b[j].y);
+                    dmma(ci[i][j], a[i].y, b[j].x);
+                    dmma(cr[i][j], -a[i].y, b[j].y);
+                }
         }
     }
+    cp_wait<0>();
     const bool beta_zero = (beta.x == 0.0 && beta.y == 0.0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        int gc = n0 + ty + 16 * j;
-        if (gc >= n) continue;
+    for (int i = 0; i < MT; ++i) {
+        const int gr = m0 + arow + 8 * i;
+        if (gr >= m) continue;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            int gr = m0 + tx + 16 * i;
-            if (gr >= m) continue;
-            double2* p = C + (long long)gc * ldc + gr;
-            double2 v = cmul(alpha, acc[i][j]);
-            if (!beta_zero) v = cfma(beta, *p, v);
-            *p = v;
+        for (int j = 0; j < NT8; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gc = n0 + wn * NT8 * 8 + 8 * j + 2 * tq + h;
+                if (gc >= n) continue;
+                double2* p = C + (long long)gc * ldc + gr;
+                double2 v = cmul(alpha, make_double2(cr[i][j][h], ci[i][j][h]));
+                if (!beta_zero) v = cfma(beta, *p, v);
+                *p = v;
+            }
         }
     }
+}
+
+template <int BM, bool CA, bool CB>
+sc_status launch_tile(cudaStream_t st, const GemmArgs& g, int batch) {
+    static bool configured = false;
+    constexpr int bytes = tile_smem_bytes<BM>();
+    if (!configured) {
+        SC_CUDA_TRY(cudaFuncSetAttribute(zgemm_kernel<BM, CA, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes));
+        configured = true;
+    }
+    dim3 grid((g.m + BM - 1) / BM, (g.n + 63) / 64, batch);
+    zgemm_kernel<BM, CA, CB><<<grid, NT, bytes, st>>>(g);
+    return SC_OK;
+}
+
+template <int BM>
+sc_status launch_shape(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch) {
+    if (!conjA && !conjB) return launch_tile<BM, false, false>(st, g, batch);
+    if (conjA && !conjB) return launch_tile<BM, true, false>(st, g, batch);
+    if (!conjA && conjB) return launch_tile<BM, false, true>(st, g, batch);
+    return launch_tile<BM, true, true>(st, g, batch);
 }
 }  // namespace
 
 sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch) {
     if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
-    dim3 grid((g.m + BM - 1) / BM, (g.n + BN - 1) / BN, batch);
-    if (grid.y > 65535 || grid.z > 65535) {
+    if ((g.n + 63) / 64 > 65535 || batch > 65535) {
         set_error("zgemm: grid too large (n=%d, batch=%d)", g.n, batch);
         return SC_BADINPUT;
     }
-    if (!conjA && !conjB)
-        zgemm_kernel<false, false><<<grid, NT, 0, st>>>(g);
-    else if (conjA && !conjB)
-        zgemm_kernel<true, false><<<grid, NT, 0, st>>>(g);
-    else if (!conjA && conjB)
-        zgemm_kernel<false, true><<<grid, NT, 0, st>>>(g);
+    // the 128-row tile when it still gives every SM at least one CTA and K is
+    // deep enough to amortise its pipeline fill (rank-32 panel updates of the
+    // LU and Hessenberg reductions stay on the two-CTA-per-SM 64-row tile)
+    const long long big = (long long)((g.m + 127) / 128) * ((g.n + 63) / 64) * batch;
+    if (g.m > 64 && g.k > 48 && big >= 148)
+        SC_TRY(launch_shape<128>(st, conjA, conjB, g, batch));
     else
-        zgemm_kernel<true, true><<<grid, NT, 0, st>>>(g);
+        SC_TRY(launch_shape<64>(st, conjA, conjB, g, batch));
     count_launch();
     SC_CHECK_LAUNCH("zgemm");
     return SC_OK;
