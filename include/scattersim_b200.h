@@ -169,10 +169,17 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
                           int Z, int S1, int S2, void* x, void* evl, void* Qc, void* Qh,
                           int* info, void* stream);
 
-/* Precision of sc_sweep_solve. */
-#define SC_SWEEP_FP64 0    /* every stage in FP64                                    */
-#define SC_SWEEP_MIXED 1   /* FP64 layer factors; FP32 chain and boundary LU with
-                              FP64 iterative refinement                             */
+/* Precision of sc_sweep_solve.  SC_SWEEP_FP64 runs every product on the FP64
+ * tensor pipe.  SC_SWEEP_MIXED lets the layer-factor and chain products run
+ * on the int8 tensor cores with 7 digit slices per operand
+ * (sc_zgemm_emulated_batched; about 1e-13 relative per product) wherever the
+ * context's GEMM autotuner measured that faster than the FP64 tile, which on
+ * the sweep workload keeps R/T within 2e-9 of FP64; SC_SWEEP_SLICES(s) runs
+ * every such product on the int8 engine with s = 1..7 slices.  FFT, assembly,
+ * the boundary systems and their LU stay in FP64. */
+#define SC_SWEEP_FP64 0
+#define SC_SWEEP_MIXED 1
+#define SC_SWEEP_SLICES(s) (0x100 | (s))
 
 /* A batched sweep of independent scattervolume solves, R/T only (the
  * --external result, ScatterVolume.cpp:739), in place of one scattervolume

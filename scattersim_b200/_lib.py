@@ -22,6 +22,10 @@ SC_SWEEP_FP64 = 0
 SC_SWEEP_MIXED = 1
 
 
+def SC_SWEEP_SLICES(s):
+    return 0x100 | int(s)
+
+
 class ScatterError(RuntimeError):
     """A C-ABI call returned a non-OK sc_status."""
 

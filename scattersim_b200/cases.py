@@ -10,8 +10,12 @@ Cases (seeded synthetic samples, see samples.py):
   fp64          measured FP64 throughput: FMA pipe and mma.sync f64
   sweep [n]     the uneven sweep (first n of 256 instances: 64 wavelengths x 4
                 angles, 4-16 layer disk stacks, 7..25 orders) in one batched call
+  sweep_mixed [n]  the sweep with the mixed path (int8 tensor-core products, 7
+                   digit slices, where the autotuner finds them faster)
   sweep_plain [n]  the same instances, one per-instance solve each
   gemm          batched complex GEMM throughput at the shapes of the solves
+  gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
+                twice each (the profiling case of the tcgen05 MMA kernel)
 Prints the per-stage device milliseconds of the last repeat.
 """
 from __future__ import annotations
@@ -49,7 +53,9 @@ def main(argv):
         return 0
     if name == "gemm":
         return gemm_case()
-    if name in ("sweep", "sweep_plain"):
+    if name == "gemm_int8":
+        return gemm_int8_case()
+    if name in ("sweep", "sweep_plain", "sweep_mixed"):
         return sweep_case(name, int(argv[2]) if len(argv) > 2 else 256)
     smp, kw = case(name)
     ctx = solver.Context(0)
@@ -109,6 +115,30 @@ def gemm_case():
     return 0
 
 
+def gemm_int8_case():
+    import ctypes
+    import torch
+    from . import solver
+    from ._lib import check
+    ctx = solver.Context(0)
+    m = n = k = 1250
+    batch = 8
+    A = torch.randn(batch, k, m, dtype=torch.complex128, device="cuda")
+    B = torch.randn(batch, n, k, dtype=torch.complex128, device="cuda")
+    C = torch.empty(batch, n, m, dtype=torch.complex128, device="cuda")
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    zero = (ctypes.c_double * 2)(0.0, 0.0)
+    for s in (7, 4):
+        args = (ctx.handle, s, m, n, k, one, ctypes.c_void_p(A.data_ptr()), m, m * k, ctypes.c_void_p(B.data_ptr()),
+                k, k * n, zero, ctypes.c_void_p(C.data_ptr()), m, m * n, batch, None)
+        for _ in range(2):
+            check(ctx.lib.sc_zgemm_emulated_batched(*args))
+    torch.cuda.synchronize()
+    print("gemm_int8 done")
+    ctx.close()
+    return 0
+
+
 def sweep_case(name, count):
     import time
     import torch
@@ -127,13 +157,15 @@ def sweep_case(name, count):
         t0 = time.perf_counter()
         if name == "sweep":
             solver.sweep(ctx, params, smp)
+        elif name == "sweep_mixed":
+            solver.sweep(ctx, params, smp, precision=1)
         else:
             for p, s in zip(params, smp):
                 solver.solve(ctx, p, s, fields=False)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         print(f"{name} rep {rep}: {dt:.3f} s, {count / dt:.2f} solves/s")
-    if name == "sweep":
+    if name != "sweep_plain":
         print({k: round(v, 1) for k, v in ctx.stage_ms().items()})
     ctx.close()
     return 0

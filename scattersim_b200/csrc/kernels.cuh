@@ -1,6 +1,8 @@
 // Internal declarations shared by the scattersim_b200 translation units.
 #pragma once
 
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -16,7 +18,7 @@ enum WsSlot {
     WS_F, WS_A6, WS_B6, WS_PIV6, WS_TMP, WS_TMP2, WS_BETA, WS_LAT, WS_PZ,
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
-    WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR,
+    WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR, WS_TUNE_C, WS_TUNE_P,
     WS_COUNT
 };
 
@@ -28,6 +30,8 @@ struct Workspace {
     // per-matrix QR statistics of the last launch: sweeps and phase cycles
     long long* hqr_stats = nullptr;
     int hqr_batch = 0;
+    // GEMM autotuner: fastest variant per (m, n, k, batch, slices) shape
+    std::map<std::tuple<int, int, int, int, int>, int> gemm_choice;
     template <typename T>
     sc_status get(T** out, size_t count, int slot, cudaStream_t st) {
         size_t need = count * sizeof(T);
@@ -94,6 +98,8 @@ struct GemmArgs {
     long long sC = 0;
 };
 sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch);
+// the FP64 tensor-pipe product with a given CTA tile (64 or 128 rows)
+sc_status zgemm_tile(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch, int tile);
 
 sc_status zgemm(cudaStream_t st, int m, int n, int k, double2 alpha, const double2* A, int lda,
                 long long sA, const double2* B, int ldb, long long sB, double2 beta, double2* C,
@@ -108,14 +114,17 @@ sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k,
 // pipeline wait timed out (never cleared here)
 sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch, Workspace& ws, int* err);
 
-// A GEMM engine: FP64 tensor-pipe tiles (slices == 0) or int8 digit slices
+// A GEMM engine for op = N products: FP64 tensor-pipe tiles, and with
+// slices > 0 also int8 digit slices on the tcgen05 tensor cores.  The first
+// product of each shape times every candidate once (into scratch output) and
+// caches the fastest in the workspace; later products of that shape reuse it.
+// force_int8 skips the tuning and runs every product on the int8 engine.
 struct GemmEngine {
     int slices = 0;
+    bool force_int8 = false;
     Workspace* ws = nullptr;
     int* err = nullptr;
-    sc_status run(cudaStream_t st, const GemmArgs& g, int batch) const {
-        return slices ? zgemm_ozaki(st, slices, g, batch, *ws, err) : zgemm_run(st, false, false, g, batch);
-    }
+    sc_status run(cudaStream_t st, const GemmArgs& g, int batch) const;
 };
 
 // y = alpha A x + beta y (batched, deterministic two-pass); part: zgemv_part_size entries
@@ -158,9 +167,9 @@ sc_status assemble_bc_layers(cudaStream_t st, const double2* Nf, const double2* 
 // from B, C and Omega = B C (destroyed).  scr: transfer_scratch_blocks() * count
 // * n2^2 entries; dnorm: count doubles; dcoef: 3 * count entries.
 size_t transfer_scratch_blocks();
-sc_status transfer_inv_batched(cudaStream_t st, int n2, int count, const double2* B, const double2* C, double2* Om,
-                               const std::vector<double>& kdz, double2* T, double2* scr, double* dnorm,
-                               double2* dcoef, int* squarings);
+sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, int count, const double2* B,
+                               const double2* C, double2* Om, const std::vector<double>& kdz, double2* T,
+                               double2* scr, double* dnorm, double2* dcoef, int* squarings);
 
 // boundary.cu: per-instance blocks of the boundary system (batched over
 // instances; order vectors [Sx, Sy, Sz0, Sz1, EF] at svec + b * sv_stride,

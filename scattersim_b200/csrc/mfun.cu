@@ -21,8 +21,9 @@
 //   s - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
 //   sinh 2a / 2a = (sinh a / a) cosh a);
 //   the last step also forms H_t = (t^2 / 2) G_{t/2}^2 (cosh 2a - 1 = 2 sinh^2 a).
-// Every product is a batched complex GEMM over all layers of the batch, so the
-// whole stage runs on the DFMA GEMM tile with per-layer scalars.
+// Every product is a batched complex GEMM over all layers of the batch with
+// per-layer scalars, run by the caller's GEMM engine (FP64 tensor-pipe tiles,
+// or int8 digit slices on the tcgen05 tensor cores).
 #include <cmath>
 #include <vector>
 
@@ -109,9 +110,9 @@ double factorial(int k) {
 
 size_t transfer_scratch_blocks() { return 7; }
 
-sc_status transfer_inv_batched(cudaStream_t st, int n2, int count, const double2* B, const double2* C, double2* Om,
-                               const std::vector<double>& kdz, double2* T, double2* scr, double* dnorm,
-                               double2* dcoef, int* squarings) {
+sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, int count, const double2* B,
+                               const double2* C, double2* Om, const std::vector<double>& kdz, double2* T,
+                               double2* scr, double* dnorm, double2* dcoef, int* squarings) {
     if (count <= 0) return SC_OK;
     if ((int)kdz.size() != count || n2 <= 0) {
         set_error("transfer_inv_batched: %d layer thicknesses for %d layers", (int)kdz.size(), count);
@@ -179,7 +180,7 @@ sc_status transfer_inv_batched(cudaStream_t st, int n2, int count, const double2
         g.C = Cm;
         g.ldc = ldc;
         g.sC = sC;
-        return zgemm_run(st, false, false, g, count);
+        return eng.run(st, g, count);
     };
     const dim3 ge(nblocks(nn), count);
 

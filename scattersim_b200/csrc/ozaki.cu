@@ -266,12 +266,15 @@ struct OzArgs {
     int* err;
 };
 
+// S: digit slices (compile time, so the MMA issue loop is fully unrolled with
+// descriptors advanced by constants)
+template <int S>
 __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[OZ_MAXST], empty[OZ_MAXST], done;
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
-    const int s = g.s;
+    constexpr int s = S;
     const int NS = oz_stages(s);
     const int stageA = s * OZ_ATILE, stageB = s * OZ_BTILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -320,8 +323,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
             bulk_g2s(sa + stageA, Bb + (long long)kb * stageB, (uint32_t)stageB, &full[slot]);
         }
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer: every digit pair with t + u < s, one 128 x 64 x 32 MMA per stage
-        uint32_t written = 0;   // accumulators already initialised
+        // MMA issuer: every digit pair with t + u < s, one 128 x 64 x 32 MMA per
+        // stage; descriptors advance in 16-byte units of the start-address field
+        const uint64_t desc0 = smem_desc(smem_raw);
+        const uint64_t slot_step = (uint64_t)((stageA + stageB) >> 4);
         for (int kb = 0; kb < KB; ++kb) {
             const int slot = kb % NS;
             if (!mbar_wait(&full[slot], (kb / NS) & 1)) {
@@ -330,16 +335,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const unsigned char* sa = smem_raw + (size_t)slot * (stageA + stageB);
-            for (int t = 0; t < s; ++t) {
-                const uint64_t ad = smem_desc(sa + t * OZ_ATILE);
-                for (int u = 0; t + u < s; ++u) {
-                    const int d = t + u;
-                    const uint64_t bd = smem_desc(sa + stageA + u * OZ_BTILE);
-                    mma_i8(tmem + (uint32_t)(d * OZ_BN), ad, bd, (written >> d) & 1u);
-                    written |= 1u << d;
-                }
-            }
+            const uint64_t da = desc0 + slot * slot_step;
+            const uint64_t db = da + (uint64_t)(stageA >> 4);
+            const uint32_t later = (kb > 0) ? 1u : 0u;
+#pragma unroll
+            for (int t = 0; t < S; ++t)
+#pragma unroll
+                for (int u = 0; u < S - t; ++u)
+                    mma_i8(tmem + (uint32_t)((t + u) * OZ_BN), da + (uint64_t)(t * (OZ_ATILE >> 4)),
+                           db + (uint64_t)(u * (OZ_BTILE >> 4)), (t > 0) ? 1u : later);
             mma_commit(&empty[slot]);
         }
         mma_commit(&done);
@@ -399,6 +403,31 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
 }
 
+}  // namespace
+
+namespace {
+template <int S>
+sc_status launch_mma_s(dim3 grid, size_t smem, cudaStream_t st, const OzArgs& a) {
+    static bool configured = false;
+    if (!configured) {
+        SC_CUDA_TRY(cudaFuncSetAttribute(oz_mma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    oz_mma_kernel<S><<<grid, OZ_THREADS, smem, st>>>(a);
+    return SC_OK;
+}
+
+sc_status launch_mma(int s, dim3 grid, size_t smem, cudaStream_t st, const OzArgs& a) {
+    switch (s) {
+        case 1: return launch_mma_s<1>(grid, smem, st, a);
+        case 2: return launch_mma_s<2>(grid, smem, st, a);
+        case 3: return launch_mma_s<3>(grid, smem, st, a);
+        case 4: return launch_mma_s<4>(grid, smem, st, a);
+        case 5: return launch_mma_s<5>(grid, smem, st, a);
+        case 6: return launch_mma_s<6>(grid, smem, st, a);
+        default: return launch_mma_s<7>(grid, smem, st, a);
+    }
+}
 }  // namespace
 
 size_t ozaki_smem_bytes(int s) { return (size_t)oz_stages(s) * s * (OZ_ATILE + OZ_BTILE) + 1024; }
@@ -462,11 +491,83 @@ sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch,
     a.sC = g.sC;
     a.err = err;
     const size_t smem = ozaki_smem_bytes(s);
-    SC_CUDA_TRY(cudaFuncSetAttribute(oz_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    oz_mma_kernel<<<dim3(CB, RB, batch), OZ_THREADS, smem, st>>>(a);
+    SC_TRY(launch_mma(s, dim3(CB, RB, batch), smem, st, a));
     count_launch();
     SC_CHECK_LAUNCH("ozaki mma");
     return SC_OK;
+}
+
+// ------------------------------------------------------------------ engine
+namespace {
+enum { VAR_TILE64 = 0, VAR_TILE128 = 1, VAR_INT8 = 2 };
+
+sc_status run_variant(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, int batch, int v) {
+    if (v == VAR_INT8) return zgemm_ozaki(st, e.slices, g, batch, *e.ws, e.err);
+    return zgemm_tile(st, false, false, g, batch, v == VAR_TILE128 ? 128 : 64);
+}
+}  // namespace
+
+sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
+    if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
+    if (force_int8 && slices > 0) return zgemm_ozaki(st, slices, g, batch, *ws, err);
+    const auto key = std::make_tuple(g.m, g.n, g.k, batch, slices);
+    auto it = ws->gemm_choice.find(key);
+    if (it != ws->gemm_choice.end()) return run_variant(st, *this, g, batch, it->second);
+    std::vector<int> cand{VAR_TILE64};
+    if (g.m > 64) cand.push_back(VAR_TILE128);
+    if (slices > 0 && 2LL * g.k * (slices + 1) <= (1LL << 16)) cand.push_back(VAR_INT8);
+    int best = cand[0];
+    if (cand.size() > 1) {
+        // candidates write a compact scratch output (ldc = m, at most 1 GiB: the
+        // trial batch is trimmed to fit, which still fills the GPU for shapes
+        // that large), so the product itself runs once, after the choice
+        GemmArgs t = g;
+        const long long cols = (long long)g.m * g.n;
+        int tb = batch;
+        while (tb > 1 && (long long)tb * cols * (long long)sizeof(double2) > (1LL << 30)) tb = (tb + 1) / 2;
+        double2* scratch;
+        SC_TRY(ws->get(&scratch, (size_t)cols * tb, WS_TUNE_C, st));
+        t.ldc = g.m;
+        t.beta = make_double2(0.0, 0.0);
+        if (g.Cp) {
+            double2** ptrs;
+            SC_TRY(ws->get(&ptrs, (size_t)tb, WS_TUNE_P, st));
+            std::vector<double2*> hp(tb);
+            for (int b = 0; b < tb; ++b) hp[b] = scratch + b * cols;
+            SC_CUDA_TRY(cudaMemcpyAsync(ptrs, hp.data(), sizeof(double2*) * tb, cudaMemcpyHostToDevice, st));
+            t.Cp = ptrs;
+        } else {
+            t.C = scratch;
+            t.sC = cols;
+        }
+        cudaEvent_t e0, e1;
+        SC_CUDA_TRY(cudaEventCreate(&e0));
+        SC_CUDA_TRY(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        sc_status s = SC_OK;
+        for (int v : cand) {
+            s = run_variant(st, *this, t, tb, v);   // warm-up (and attribute setup)
+            if (s == SC_OK && cudaEventRecord(e0, st) != cudaSuccess) s = SC_CUDA_ERROR;
+            if (s == SC_OK) s = run_variant(st, *this, t, tb, v);
+            if (s == SC_OK && cudaEventRecord(e1, st) != cudaSuccess) s = SC_CUDA_ERROR;
+            float ms = 0.f;
+            if (s == SC_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                s = SC_CUDA_ERROR;
+            if (s != SC_OK) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = v;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != SC_OK) {
+            set_error("GEMM autotuner: a candidate failed");
+            return s;
+        }
+    }
+    ws->gemm_choice[key] = best;
+    return run_variant(st, *this, g, batch, best);
 }
 
 }  // namespace sc

@@ -95,7 +95,7 @@ size_t chunk_bytes(const std::vector<Item*>& items, int Mx, int My) {
 }
 
 sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My, cudaStream_t st,
-                      int* status, double* stage_ms) {
+                      const GemmEngine& eng, int* status, double* stage_ms) {
     Workspace& ws = ctx->ws;
     // deepest stacks first: the instances still inside their stack at depth
     // step j are then items[0 .. active(j))
@@ -188,12 +188,24 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
     // 2. B, C, Omega
     const long long s2 = (long long)n2 * n2;
     SC_TRY(assemble_bc_layers(st, b.Nf, b.Nif, Ltot, Mx, My, b.lat, b.inst, b.kinv, b.B, b.C));
-    SC_TRY(zgemm(st, n2, n2, n2, make_double2(1.0, 0.0), b.B, n2, s2, b.C, n2, s2, make_double2(0.0, 0.0), b.Om, n2,
-                 s2, Ltot));
+    {
+        GemmArgs g;
+        g.m = g.n = g.k = n2;
+        g.A = b.B;
+        g.lda = n2;
+        g.sA = s2;
+        g.B = b.C;
+        g.ldb = n2;
+        g.sB = s2;
+        g.C = b.Om;
+        g.ldc = n2;
+        g.sC = s2;
+        SC_TRY(eng.run(st, g, Ltot));
+    }
     SC_CUDA_TRY(cudaEventRecord(ev[2], st));
     // 3. inverse layer factors
     int squarings = 0;
-    SC_TRY(transfer_inv_batched(st, n2, Ltot, b.B, b.C, b.Om, kdz, b.T, b.scr, b.dnorm, b.coef, &squarings));
+    SC_TRY(transfer_inv_batched(st, eng, n2, Ltot, b.B, b.C, b.Om, kdz, b.T, b.scr, b.dnorm, b.coef, &squarings));
     SC_CUDA_TRY(cudaEventRecord(ev[3], st));
     // 4. chain from f3 up through each stack
     SC_TRY(boundary_f3(st, MF, b.svec, 7LL * MF, b.X0, sX, nI));
@@ -211,7 +223,7 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
         g.ldb = n4;
         g.Cp = reinterpret_cast<double2* const*>(row + 2 * nI);
         g.ldc = n4;
-        SC_TRY(zgemm_run(st, false, false, g, act));
+        SC_TRY(eng.run(st, g, act));
     }
     SC_CUDA_TRY(cudaEventRecord(ev[4], st));
     // 5. boundary systems and their solves
@@ -245,7 +257,17 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
         set_error("sweep_solve: null argument");
         return SC_BADINPUT;
     }
-    if (precision != SC_SWEEP_FP64) {
+    int slices = -1;
+    bool force = false;
+    if (precision == SC_SWEEP_FP64) {
+        slices = 0;
+    } else if (precision == SC_SWEEP_MIXED) {
+        slices = 7;
+    } else if ((precision & ~0xFF) == 0x100 && (precision & 0xFF) >= 1 && (precision & 0xFF) <= 7) {
+        slices = precision & 0xFF;
+        force = true;
+    }
+    if (slices < 0) {
         set_error("sweep_solve: unknown precision %d", precision);
         return SC_BADINPUT;
     }
@@ -279,9 +301,16 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
     size_t freeb = 0, totalb = 0;
     SC_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
     const size_t held = ctx->ws.bytes[WS_SWEEP];
-    size_t budget = (size_t)(0.6 * (double)(freeb + held));
+    // the digit-slice engine keeps its packed operands in its own workspace
+    size_t budget = (size_t)((slices ? 0.45 : 0.6) * (double)(freeb + held));
     const size_t cap = (size_t)48 << 30;
     if (budget > cap) budget = cap;
+    GemmEngine eng;
+    eng.slices = slices;
+    eng.force_int8 = force;
+    eng.ws = &ctx->ws;
+    SC_TRY(ctx->ws.get(&eng.err, 1, WS_OZ_ERR, st));
+    SC_CUDA_TRY(cudaMemsetAsync(eng.err, 0, sizeof(int), st));
     const auto t0 = ctx->ev[7];
     SC_CUDA_TRY(cudaEventRecord(t0, st));
     double stage[8] = {};
@@ -309,7 +338,7 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
                 pos = nxt;
                 continue;
             }
-            SC_TRY(solve_chunk(ctx, chunk, Mx, My, st, status, stage));
+            SC_TRY(solve_chunk(ctx, chunk, Mx, My, st, eng, status, stage));
             pos = nxt;
         }
     }
@@ -319,6 +348,14 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
     SC_CUDA_TRY(cudaEventElapsedTime(&total, t0, ctx->ev[6]));
     for (int i = 0; i < 5; ++i) ctx->stage_ms[i] = stage[i];
     ctx->stage_ms[7] = total;
+    if (slices) {
+        int herr = 0;
+        SC_CUDA_TRY(cudaMemcpy(&herr, eng.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) {
+            set_error("sweep_solve: tensor-core pipeline wait timed out (stage %d)", herr);
+            return SC_CUDA_ERROR;
+        }
+    }
     for (int i = 0; i < count && first == SC_OK; ++i)
         if (status[i] != SC_OK) {
             first = (sc_status)status[i];

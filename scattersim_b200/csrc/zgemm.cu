@@ -189,23 +189,28 @@ sc_status launch_shape(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& 
 }
 }  // namespace
 
-sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch) {
+sc_status zgemm_tile(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch, int tile) {
     if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
     if ((g.n + 63) / 64 > 65535 || batch > 65535) {
         set_error("zgemm: grid too large (n=%d, batch=%d)", g.n, batch);
         return SC_BADINPUT;
     }
-    // the 128-row tile when it still gives every SM at least one CTA and K is
-    // deep enough to amortise its pipeline fill (rank-32 panel updates of the
-    // LU and Hessenberg reductions stay on the two-CTA-per-SM 64-row tile)
-    const long long big = (long long)((g.m + 127) / 128) * ((g.n + 63) / 64) * batch;
-    if (g.m > 64 && g.k > 48 && big >= 148)
+    if (tile == 128)
         SC_TRY(launch_shape<128>(st, conjA, conjB, g, batch));
     else
         SC_TRY(launch_shape<64>(st, conjA, conjB, g, batch));
     count_launch();
     SC_CHECK_LAUNCH("zgemm");
     return SC_OK;
+}
+
+sc_status zgemm_run(cudaStream_t st, bool conjA, bool conjB, const GemmArgs& g, int batch) {
+    // the 128-row tile when it still gives every SM at least one CTA and K is
+    // deep enough to amortise its pipeline fill (rank-32 panel updates of the
+    // LU and Hessenberg reductions stay on the two-CTA-per-SM 64-row tile)
+    const long long big = (long long)((g.m + 127) / 128) * ((g.n + 63) / 64) * batch;
+    const int tile = (g.m > 64 && g.k > 48 && big >= 148) ? 128 : 64;
+    return zgemm_tile(st, conjA, conjB, g, batch, tile);
 }
 
 sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k, double2 alpha,

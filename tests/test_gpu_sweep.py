@@ -123,3 +123,40 @@ def test_sweep_per_instance_status(ctx):
     for i in (0, 2):
         ref = osv.solve(inst[i].maps, osv.Params(**inst[i].params_kw()), keep=False).x
         assert rel(xs[i].cpu().numpy(), ref) < TOL
+
+
+MIXED_TOL = 1e-8
+
+
+@pytest.mark.parametrize("precision", [_lib.SC_SWEEP_MIXED, _lib.SC_SWEEP_SLICES(7)])
+def test_sweep_mixed_matches_oracle(ctx, precision):
+    """Autotuned mixed path, and every product forced onto the int8 tensor cores
+    (7 digit slices): R/T within 1e-8 of the FP64 oracle."""
+    inst = small_instances(count=6, seed=4)
+    res = run_sweep(ctx, inst, precision=precision)
+    for it, x in zip(inst, res.x):
+        ref = osv.solve(it.maps, osv.Params(**it.params_kw()), keep=False).x
+        assert rel(x.cpu().numpy(), ref) < MIXED_TOL, (it.index, rel(x.cpu().numpy(), ref))
+
+
+def test_sweep_mixed_matches_fp64_at_large_orders(ctx):
+    inst = samples.sweep_instances(6, count=4)
+    for i, it in enumerate(inst):
+        it.orders = (21, 25)[i % 2]
+    fp = run_sweep(ctx, inst)
+    for precision in (_lib.SC_SWEEP_MIXED, _lib.SC_SWEEP_SLICES(7)):
+        mx = run_sweep(ctx, inst, precision=precision)
+        for a, b in zip(mx.x, fp.x):
+            assert rel(a.cpu().numpy(), b.cpu().numpy()) < MIXED_TOL
+
+
+def test_sweep_slice_count_orders_error(ctx):
+    """Each digit slice buys about 2^-7: the R/T error falls monotonically from 4 to 7 slices."""
+    inst = small_instances(count=3, seed=8)
+    fp = run_sweep(ctx, inst)
+    errs = []
+    for slices in (4, 5, 6, 7):
+        sl = run_sweep(ctx, inst, precision=_lib.SC_SWEEP_SLICES(slices))
+        errs.append(max(rel(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(sl.x, fp.x)))
+    assert all(b < a for a, b in zip(errs, errs[1:])), errs
+    assert errs[-1] < 1e-10 and errs[0] < 1e-3, errs
