@@ -1,16 +1,24 @@
 #!/usr/bin/env python
-"""Benchmark: scattervolume solves/s on B200.
+"""Benchmark: RCWA solves/s on B200 for the scattervolume solve.
 
-Workload (default): the plain 3-D volume -- a 128x128x32-voxel sphere volume
-over 20x20x8 um (seeded), 32 layers, lambda = 0.6 um, 10 deg incidence,
-x-polarised, 21x21 Fourier orders (M = 441, 1764 x 1764 layer matrices),
-solved in FP64 with the interior mode fields (the reference's default, Pz on).
-One step = one full solve of one instance, sample resident in HBM.
+Default workload (--workload sweep): the batched sweep of 256 uneven instances
+-- 64 seeded wavelengths in [0.4, 0.8] um x incidence 0/10/20/30 deg, each a
+seeded 4-16 layer stack of 64x64 random-disk maps (n 1.0-1.6, 25x25 um period,
+layer thickness 0.1-0.5 um), Fourier orders drawn from {7,11,15,21,25}^2 --
+solved for R/T.  One step = the whole 256-instance sweep, samples resident in
+HBM.  The headline value is the batched mixed-precision path (int8 tcgen05
+digit-sliced products, 7 slices, where the GEMM autotuner finds them faster);
+the line also carries the batched FP64 path, the plain per-instance FP64 path
+(timed on every 8th instance) and the R/T error of the mixed path against FP64.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+--workload volume: the plain 3-D volume -- a 128x128x32-voxel sphere volume over
+20x20x8 um (seeded), 32 layers, lambda 0.6 um, 10 deg, x-polarised, 21x21
+orders, FP64 with interior fields; one step = one solve.
 
-Under torchrun each rank solves its own seeded instance (weak scaling, no
-data-path collective); timing is on the device, max over ranks.
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume]
+
+Under torchrun each rank solves its own seeded sweep / instance (weak scaling,
+no data-path collective); timing is on the device, max over ranks.
 """
 from __future__ import annotations
 
@@ -38,6 +46,11 @@ WORKLOAD_NAME = ("plain 3-D volume: 128x128x32 seeded sphere volume over 20x20x8
                  "lambda 0.6 um, 10 deg, x-pol, orders 21x21 (M=441, 1764x1764 per layer), fields on")
 Z_LAYERS = 32
 N_2M = 2 * 441
+SWEEP_NAME = ("uneven sweep: 256 instances = 64 seeded wavelengths in [0.4, 0.8] um x 0/10/20/30 deg incidence; "
+              "each a seeded 4-16 layer stack of 64x64 random-disk maps (n 1.0-1.6, 25x25 um period, 0.1-0.5 um "
+              "layers); orders drawn from {7,11,15,21,25}^2; x-pol; R/T only")
+MIXED = 1          # SC_SWEEP_MIXED: int8 tcgen05 digit-sliced products, 7 slices
+PLAIN_EVERY = 8    # the per-instance FP64 path is timed on every 8th instance
 
 
 def _peaks():
@@ -154,6 +167,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "sweep":
+        return run_sweep_reference(args)
     for _ in range(args.warmup):
         cpu_layer_sample(0)
     ts = [cpu_layer_sample(0) for _ in range(args.steps)]
@@ -205,7 +220,7 @@ def e2e_loop(args, ctx, params, sol, host, flush, stream, barrier, dist, world):
     return world * args.steps / (total / 1e3), h2d, d2h
 
 
-def run_ours(args):
+def run_volume_ours(args):
     import torch
     from scattersim_b200 import samples, solver
 
@@ -308,6 +323,252 @@ def run_ours(args):
     return 0
 
 
+# --------------------------------------------------------------------------- sweep
+def sweep_instances(seed):
+    from scattersim_b200 import samples
+    return samples.sweep_instances(seed, count=256)
+
+
+def cpu_sweep_sample(inst):
+    """The reference CPU path on a bounded sample of the sweep (the oracle port).
+
+    For each order count one layer of one instance is timed -- phi assembly,
+    zgeev of the 4M x 4M layer matrix, the eigen sort and one T-matrix step
+    (ScatterVolume.cpp:235-336); the sweep's time is the sum over instances of
+    layers x that per-layer time (boundary solves excluded, a lower bound).
+    Returns (solves/s, description, seconds spent).
+    """
+    from oracle import scattervolume as osv
+    per_layer, spent = {}, 0.0
+    for m in sorted({it.orders for it in inst}):
+        it = next(i for i in inst if i.orders == m)
+        p = osv.Params(**it.params_kw())
+        d, e, dirv, k, ni, slices, num_pixels, z, M, msgs = osv.setup(it.maps, p)
+        lat = osv.upwq_cal(M, p.size, dirv, k, ni)
+        t0 = time.perf_counter()
+        P, _, _ = osv.phi(slices[0], M, lat, k)
+        w, v = osv.mkl_eigensolve(P)
+        sl, sv = osv.eigen_sort(w, v)
+        dz = z[1] - z[0]
+        odd = (np.arange(sl.size) % 2) != 0
+        Gd = sv * np.where(odd, np.exp(1j * k * sl * (-dz)), 1.0)[None, :]
+        Gc = sv * np.where(odd, 1.0, np.exp(1j * k * sl * dz))[None, :]
+        _ = (Gc @ osv.mkl_inverse(Gd)) @ Gc
+        per_layer[m] = time.perf_counter() - t0
+        spent += per_layer[m]
+    total = sum(it.maps.shape[0] * per_layer[it.orders] for it in inst)
+    desc = ("one layer per order count timed (phi, zgeev n=4M, sort, one T-matrix step: "
+            + ", ".join(f"M={m}x{m}: {t:.2f} s" for m, t in per_layer.items())
+            + f"), times the sweep's {sum(i.maps.shape[0] for i in inst)} layers; numpy/scipy OpenBLAS "
+              "restatement of ScatterVolume.cpp")
+    return len(inst) / total, desc, spent
+
+
+def run_sweep_reference(args):
+    inst = sweep_instances(1000)
+    for _ in range(args.warmup):
+        cpu_sweep_sample([i for i in inst if i.orders == 7][:1])
+    vals, desc = [], ""
+    for _ in range(args.steps):
+        v, desc, _ = cpu_sweep_sample(inst)
+        vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 256e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": SWEEP_NAME, "seed": 1000},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": blas_threads(), "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def run_sweep_ours(args):
+    import torch
+    from scattersim_b200 import solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = solver.Context(local)
+    inst = sweep_instances(1000 + rank)
+    params = [solver.make_params(**it.params_kw()) for it in inst]
+    dev = [torch.from_numpy(it.maps).cuda() for it in inst]
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+    n = len(inst)
+
+    def timed(fn):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):          # the first call also autotunes every GEMM shape
+        solver.sweep(ctx, params, dev, precision=MIXED)
+
+    # ---- headline: batched mixed precision, device-timed, samples resident in HBM
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    ctx.kernel_timing(True)
+    l0 = ctx.launches()
+    step_ms = []
+    res_mixed = None
+    for _ in range(args.steps):
+        res_mixed, ms = timed(lambda: solver.sweep(ctx, params, dev, precision=MIXED))
+        step_ms.append(ms)
+    launches = ctx.launches() - l0
+    kst = ctx.kernel_stats()
+    ctx.kernel_timing(False)
+    stages = ctx.stage_ms()
+    barrier()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * n * args.steps / (total_ms / 1e3)
+
+    # ---- batched FP64 (one warm-up for its own GEMM shapes, then timed)
+    solver.sweep(ctx, params, dev, precision=0)
+    fp_steps = max(1, min(2, args.steps))
+    fp_ms = []
+    res_fp = None
+    for _ in range(fp_steps):
+        res_fp, ms = timed(lambda: solver.sweep(ctx, params, dev, precision=0))
+        fp_ms.append(ms)
+    fp_value = world * n * fp_steps / (max_over_ranks(sum(fp_ms)) / 1e3)
+    errs = [_rel(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(res_mixed.x, res_fp.x)]
+
+    # ---- plain per-instance FP64 path on every 8th instance
+    sub = list(range(0, n, PLAIN_EVERY))
+    solver.solve(ctx, params[sub[0]], dev[sub[0]], fields=False)
+    plain_ms = 0.0
+    for i in sub:
+        _, ms = timed(lambda: solver.solve(ctx, params[i], dev[i], fields=False))
+        plain_ms += ms
+    plain_value = world * len(sub) / (max_over_ranks(plain_ms) / 1e3)
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        sizes = [it.maps.size for it in inst]
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        pin_in = torch.empty(int(offs[-1]), dtype=torch.complex128).pin_memory()
+        for it, o in zip(inst, offs[:-1]):
+            pin_in[int(o):int(o) + it.maps.size].copy_(torch.from_numpy(it.maps.ravel()))
+        outs = [torch.empty(x.numel(), dtype=torch.complex128).pin_memory() for x in res_mixed.x]
+        d_in = torch.empty_like(pin_in, device="cuda")
+        barrier()
+        e2e_ms = []
+        for _ in range(max(1, min(2, args.steps))):
+            def step():
+                d_in.copy_(pin_in, non_blocking=True)
+                views = [d_in[int(o):int(o) + it.maps.size].view(it.maps.shape) for it, o in zip(inst, offs[:-1])]
+                r = solver.sweep(ctx, params, views, precision=MIXED)
+                for o, x in zip(outs, r.x):
+                    o.copy_(x, non_blocking=True)
+                return r
+            _, ms = timed(step)
+            e2e_ms.append(ms)
+        e2e_value = world * n * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) / 1e3)
+        e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(offs[-1]) * 16,
+               "d2h_bytes_per_step": int(sum(x.numel() for x in outs)) * 16}
+
+    # ---- roofline of the dominant kernel (by device time over the timed steps)
+    peaks = _peaks()
+    fp64_peak = ctx.fp64_peak_tflops()
+    d8, dd = kst["int8"], kst["dmma"]
+    if d8["ms"] >= dd["ms"]:
+        int8_peak = 2.0 * float(peaks.get("bf16_tflops", 1590.0))
+        achieved = d8["int8_ops"] / (d8["ms"] / 1e3) / 1e12
+        tr = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "int8_gemm_traffic.json")) as f:
+                rec = json.load(f)
+            tr = rec["bytes_per_fp64_flop"] * d8["flops"] / max(d8["launches"], 1)
+        except Exception:
+            pass
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS (int8)",
+                    "frac": achieved / int8_peak, "traffic": tr,
+                    "kernel": "oz_mma_kernel (int8 tcgen05 MMA, 7 digit slices, TMEM accumulators)",
+                    "peak_source": "2 x measured bf16 dense burst peak (MEASURED_PEAKS.json): int8 dense "
+                                   "is twice bf16 dense on B200",
+                    "launches": int(d8["launches"]), "avg_launch_ms": d8["ms"] / max(d8["launches"], 1),
+                    "fp64_equivalent_tflops": d8["flops"] / (d8["ms"] / 1e3) / 1e12,
+                    "fp64_peak_tflops": fp64_peak,
+                    "traffic_source": "ncu dram bytes of one 1250^3 x 8 capture, scaled by FP64-equivalent "
+                                      "flops per launch (profiles/int8_gemm_traffic.json)"}
+    else:
+        achieved = dd["flops"] / (dd["ms"] / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp64_peak, "traffic": None,
+                    "kernel": "zgemm_kernel (FP64 mma.sync m8n8k4 complex GEMM)",
+                    "peak_source": "FP64 FMA probe measured in this run",
+                    "launches": int(dd["launches"]), "avg_launch_ms": dd["ms"] / max(dd["launches"], 1)}
+    roofline["gemm_time_share"] = (d8["ms"] + dd["ms"]) / (sum(step_ms) or 1.0)
+    roofline["int8_ms_per_step"] = d8["ms"] / args.steps
+    roofline["fp64_tile_ms_per_step"] = dd["ms"] / args.steps
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, desc, spent = cpu_sweep_sample(inst)
+            cpu = {"value": v, "unit": UNIT, "cores": blas_threads(), "kind": "port",
+                   "sample": desc + f"; {spent:.1f} s of host work"}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int8 tensor products (7 digit slices) + f64",
+                "data": "synthetic",
+                "config": {"workload": SWEEP_NAME, "seed": "1000+rank", "path": "batched mixed precision",
+                           "l2": "flushed between steps (256 MB write, untimed); working set >> L2",
+                           "parallelism": f"independent sweep per rank x{world}"},
+                "paths": {"batched_mixed": value, "batched_fp64": fp_value,
+                          "plain_fp64_per_instance": plain_value,
+                          "plain_sample": f"every {PLAIN_EVERY}th instance ({len(sub)} of {n}), one "
+                                          "sc_volume_solve (--external) each",
+                          "mixed_rt_rel_err_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
+                          "speedup_mixed_vs_plain": value / plain_value,
+                          "speedup_fp64_batched_vs_plain": fp_value / plain_value},
+                "clocks": clocks, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e,
+                "stage_ms": {"fft": round(stages["fft"], 1), "assemble": round(stages["assemble"], 1),
+                             "layer_factors": round(stages["eig"], 1), "chain": round(stages["chain"], 1),
+                             "boundary": round(stages["boundary"], 1), "total": round(stages["total"], 1)}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -316,10 +577,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "volume"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    return run_ours(args)
+    if args.workload == "sweep":
+        return run_sweep_ours(args)
+    return run_volume_ours(args)
 
 
 if __name__ == "__main__":

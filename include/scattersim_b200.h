@@ -205,6 +205,23 @@ sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8);
  * total.  Zero-filled beyond the last batch. */
 sc_status sc_qr_stats(sc_context* ctx, long long* out, int count);
 
+/* Per-launch device timing of the GEMM kernels that the sweep's engine runs
+ * (CUDA events on the launching stream).  sc_kernel_timing(ctx, 1) clears the
+ * record and starts timing, 0 stops it; sc_kernel_stats synchronises the
+ * device and sums the record into out[8] = {launches, ms, FP64-equivalent
+ * flops, 0} for the FP64 tensor-pipe tiles, then {launches, ms,
+ * FP64-equivalent flops, int8 ops} for the int8 tcgen05 MMA kernel. */
+sc_status sc_kernel_timing(sc_context* ctx, int on);
+sc_status sc_kernel_stats(sc_context* ctx, double* out8);
+
+/* The GEMM autotuner's choices on this context, as 6-int records (m, n, k,
+ * batch, slices, variant: 0/1 FP64 tile of 64/128 rows, 2 int8 engine).
+ * sc_gemm_choices_get writes up to cap records and returns their count in
+ * *count; sc_gemm_choices_set replaces the table, so that a later run (a
+ * profiler replay, say) makes the same choices without timing them again. */
+sc_status sc_gemm_choices_get(sc_context* ctx, int* rec, int cap, int* count);
+sc_status sc_gemm_choices_set(sc_context* ctx, const int* rec, int count);
+
 /* Measured FP64 FMA throughput of this device (TFLOP/s): the roofline
  * denominator of the FP64 kernels. */
 sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops);

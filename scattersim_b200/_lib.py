@@ -75,6 +75,10 @@ _SIGS = {
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
     "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),
                                POINTER(c_int), POINTER(c_int), POINTER(c_void_p), c_int, POINTER(c_int), c_void_p]),
+    "sc_kernel_timing": (c_int, [c_void_p, c_int]),
+    "sc_kernel_stats": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_gemm_choices_get": (c_int, [c_void_p, POINTER(c_int), c_int, POINTER(c_int)]),
+    "sc_gemm_choices_set": (c_int, [c_void_p, POINTER(c_int), c_int]),
     "sc_volume_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_void_p, c_int, c_int, c_int, c_void_p,
                                 c_void_p, c_void_p, c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_stage_ms": (c_int, [c_void_p, POINTER(c_double)]),

@@ -13,6 +13,8 @@ Cases (seeded synthetic samples, see samples.py):
   sweep_mixed [n]  the sweep with the mixed path (int8 tensor-core products, 7
                    digit slices, where the autotuner finds them faster)
   sweep_plain [n]  the same instances, one per-instance solve each
+    (sweep cases accept --choices-out FILE to save the GEMM autotuner's table
+     and --choices-in FILE to replay one, e.g. under a profiler)
   gemm          batched complex GEMM throughput at the shapes of the solves
   gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
                 twice each (the profiling case of the tcgen05 MMA kernel)
@@ -56,7 +58,9 @@ def main(argv):
     if name == "gemm_int8":
         return gemm_int8_case()
     if name in ("sweep", "sweep_plain", "sweep_mixed"):
-        return sweep_case(name, int(argv[2]) if len(argv) > 2 else 256)
+        count = int(argv[2]) if len(argv) > 2 and not argv[2].startswith("--") else 256
+        opt = dict(zip(argv[3::2], argv[4::2])) if len(argv) > 3 else {}
+        return sweep_case(name, count, opt.get("--choices-in"), opt.get("--choices-out"))
     smp, kw = case(name)
     ctx = solver.Context(0)
     p = solver.make_params(**kw)
@@ -139,7 +143,7 @@ def gemm_int8_case():
     return 0
 
 
-def sweep_case(name, count):
+def sweep_case(name, count, choices_in=None, choices_out=None):
     import time
     import torch
     from . import samples, solver
@@ -147,6 +151,10 @@ def sweep_case(name, count):
     params = [solver.make_params(**it.params_kw()) for it in inst]
     smp = [torch.from_numpy(it.maps).cuda() for it in inst]
     ctx = solver.Context(0)
+    if choices_in:
+        import json
+        with open(choices_in) as f:
+            ctx.set_gemm_choices(json.load(f))
     layers = sum(it.maps.shape[0] for it in inst)
     orders = {}
     for it in inst:
@@ -167,6 +175,10 @@ def sweep_case(name, count):
         print(f"{name} rep {rep}: {dt:.3f} s, {count / dt:.2f} solves/s")
     if name != "sweep_plain":
         print({k: round(v, 1) for k, v in ctx.stage_ms().items()})
+    if choices_out:
+        import json
+        with open(choices_out, "w") as f:
+            json.dump(ctx.gemm_choices(), f)
     ctx.close()
     return 0
 

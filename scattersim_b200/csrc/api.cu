@@ -334,6 +334,83 @@ sc_status sc_sweep_solve(sc_context* ctx, int count, const sc_volume_params* par
     return sweep_solve(ctx, count, params, samples, Z, S1, S2, x, precision, status, (cudaStream_t)stream);
 }
 
+sc_status sc_kernel_timing(sc_context* ctx, int on) {
+    if (!ctx) {
+        set_error("sc_kernel_timing: null context");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    Workspace& ws = ctx->ws;
+    SC_CUDA_TRY(cudaDeviceSynchronize());
+    for (auto& m : ws.marks) {
+        ws.event_pool.push_back(m.e0);
+        ws.event_pool.push_back(m.e1);
+    }
+    ws.marks.clear();
+    ws.time_kernels = on != 0;
+    return SC_OK;
+}
+
+sc_status sc_kernel_stats(sc_context* ctx, double* out8) {
+    if (!ctx || !out8) {
+        set_error("sc_kernel_stats: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    SC_CUDA_TRY(cudaDeviceSynchronize());
+    for (int i = 0; i < 8; ++i) out8[i] = 0.0;
+    for (auto& m : ctx->ws.marks) {
+        float ms = 0.f;
+        SC_CUDA_TRY(cudaEventElapsedTime(&ms, m.e0, m.e1));
+        double* o = out8 + 4 * m.cls;
+        o[0] += 1.0;
+        o[1] += ms;
+        o[2] += m.flops;
+        o[3] += m.int8_ops;
+    }
+    return SC_OK;
+}
+
+sc_status sc_gemm_choices_get(sc_context* ctx, int* rec, int cap, int* count) {
+    if (!ctx || !count || (cap > 0 && !rec)) {
+        set_error("sc_gemm_choices_get: null argument");
+        return SC_BADINPUT;
+    }
+    int i = 0;
+    for (auto& kv : ctx->ws.gemm_choice) {
+        if (i < cap) {
+            int* r = rec + 6 * i;
+            r[0] = std::get<0>(kv.first);
+            r[1] = std::get<1>(kv.first);
+            r[2] = std::get<2>(kv.first);
+            r[3] = std::get<3>(kv.first);
+            r[4] = std::get<4>(kv.first);
+            r[5] = kv.second;
+        }
+        ++i;
+    }
+    *count = i;
+    return SC_OK;
+}
+
+sc_status sc_gemm_choices_set(sc_context* ctx, const int* rec, int count) {
+    if (!ctx || count < 0 || (count > 0 && !rec)) {
+        set_error("sc_gemm_choices_set: bad argument");
+        return SC_BADINPUT;
+    }
+    for (int i = 0; i < count; ++i)
+        if (rec[6 * i + 5] < 0 || rec[6 * i + 5] > 2) {
+            set_error("sc_gemm_choices_set: record %d has unknown variant %d", i, rec[6 * i + 5]);
+            return SC_BADINPUT;
+        }
+    ctx->ws.gemm_choice.clear();
+    for (int i = 0; i < count; ++i) {
+        const int* r = rec + 6 * i;
+        ctx->ws.gemm_choice[std::make_tuple(r[0], r[1], r[2], r[3], r[4])] = r[5];
+    }
+    return SC_OK;
+}
+
 sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8) {
     if (!ctx || !ms8) {
         set_error("sc_volume_stage_ms: null argument");

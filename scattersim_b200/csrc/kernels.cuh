@@ -32,6 +32,40 @@ struct Workspace {
     int hqr_batch = 0;
     // GEMM autotuner: fastest variant per (m, n, k, batch, slices) shape
     std::map<std::tuple<int, int, int, int, int>, int> gemm_choice;
+    // optional per-launch timing of the engine's GEMM kernels (class 0: FP64
+    // tensor-pipe tiles, class 1: int8 tcgen05 MMA kernel): event pairs on the
+    // launching stream, summed by sc_kernel_stats after the stream has drained
+    bool time_kernels = false;
+    struct KernelMark {
+        int cls;
+        double flops;      // FP64-equivalent flops of the product (8 m n k per batch entry)
+        double int8_ops;   // 2 x int8 multiply-adds issued by the MMA kernel (class 1)
+        cudaEvent_t e0, e1;
+    };
+    std::vector<KernelMark> marks;
+    std::vector<cudaEvent_t> event_pool;
+    sc_status mark_begin(cudaStream_t st, int cls, double flops, double int8_ops, size_t* id) {
+        KernelMark m{cls, flops, int8_ops, nullptr, nullptr};
+        for (cudaEvent_t* e : {&m.e0, &m.e1}) {
+            if (event_pool.empty()) {
+                cudaEvent_t ev;
+                cudaError_t r = cudaEventCreate(&ev);
+                if (r != cudaSuccess) return cuda_status(r, "cudaEventCreate");
+                event_pool.push_back(ev);
+            }
+            *e = event_pool.back();
+            event_pool.pop_back();
+        }
+        cudaError_t r = cudaEventRecord(m.e0, st);
+        if (r != cudaSuccess) return cuda_status(r, "cudaEventRecord");
+        marks.push_back(m);
+        *id = marks.size() - 1;
+        return SC_OK;
+    }
+    sc_status mark_end(cudaStream_t st, size_t id) {
+        cudaError_t r = cudaEventRecord(marks[id].e1, st);
+        return r == cudaSuccess ? SC_OK : cuda_status(r, "cudaEventRecord");
+    }
     template <typename T>
     sc_status get(T** out, size_t count, int slot, cudaStream_t st) {
         size_t need = count * sizeof(T);
@@ -60,6 +94,13 @@ struct Workspace {
         return SC_OK;
     }
     void release() {
+        for (auto& m : marks) {
+            cudaEventDestroy(m.e0);
+            cudaEventDestroy(m.e1);
+        }
+        marks.clear();
+        for (auto e : event_pool) cudaEventDestroy(e);
+        event_pool.clear();
         for (auto& e : ev_hqr)
             if (e) cudaEventDestroy(e);
         ev_hqr[0] = ev_hqr[1] = nullptr;

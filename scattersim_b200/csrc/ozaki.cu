@@ -491,8 +491,15 @@ sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch,
     a.sC = g.sC;
     a.err = err;
     const size_t smem = ozaki_smem_bytes(s);
+    size_t mark = 0;
+    if (ws.time_kernels) {
+        const int pairs = s * (s + 1) / 2;
+        const double macs = (double)pairs * batch * (double)RB * OZ_BM * (double)CB * OZ_BN * (double)KB * OZ_BK;
+        SC_TRY(ws.mark_begin(st, 1, 8.0 * g.m * (double)g.n * g.k * batch, 2.0 * macs, &mark));
+    }
     SC_TRY(launch_mma(s, dim3(CB, RB, batch), smem, st, a));
     count_launch();
+    if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark));
     SC_CHECK_LAUNCH("ozaki mma");
     return SC_OK;
 }
@@ -505,6 +512,15 @@ sc_status run_variant(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, i
     if (v == VAR_INT8) return zgemm_ozaki(st, e.slices, g, batch, *e.ws, e.err);
     return zgemm_tile(st, false, false, g, batch, v == VAR_TILE128 ? 128 : 64);
 }
+// the chosen variant; FP64 tiles are bracketed by timing marks here, the int8
+// MMA kernel marks itself (its pack kernels stay outside the mark)
+sc_status run_timed(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, int batch, int v) {
+    if (!e.ws->time_kernels || v == VAR_INT8) return run_variant(st, e, g, batch, v);
+    size_t mark = 0;
+    SC_TRY(e.ws->mark_begin(st, 0, 8.0 * g.m * (double)g.n * g.k * batch, 0.0, &mark));
+    SC_TRY(run_variant(st, e, g, batch, v));
+    return e.ws->mark_end(st, mark);
+}
 }  // namespace
 
 sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
@@ -512,7 +528,7 @@ sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
     if (force_int8 && slices > 0) return zgemm_ozaki(st, slices, g, batch, *ws, err);
     const auto key = std::make_tuple(g.m, g.n, g.k, batch, slices);
     auto it = ws->gemm_choice.find(key);
-    if (it != ws->gemm_choice.end()) return run_variant(st, *this, g, batch, it->second);
+    if (it != ws->gemm_choice.end()) return run_timed(st, *this, g, batch, it->second);
     std::vector<int> cand{VAR_TILE64};
     if (g.m > 64) cand.push_back(VAR_TILE128);
     if (slices > 0 && 2LL * g.k * (slices + 1) <= (1LL << 16)) cand.push_back(VAR_INT8);
@@ -567,7 +583,7 @@ sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
         }
     }
     ws->gemm_choice[key] = best;
-    return run_variant(st, *this, g, batch, best);
+    return run_timed(st, *this, g, batch, best);
 }
 
 }  // namespace sc

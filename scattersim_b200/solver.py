@@ -64,6 +64,30 @@ class Context:
         keys = ("sweeps", "shifts", "chase", "far_right", "far_rows", "small", "unused", "total")
         return [dict(zip(keys, out[8 * i:8 * i + 8])) for i in range(count)]
 
+    def kernel_timing(self, on: bool = True):
+        """Start (clearing the record) or stop per-launch timing of the engine's GEMM kernels."""
+        check(self.lib.sc_kernel_timing(self.handle, int(on)))
+
+    def kernel_stats(self):
+        """{'dmma': {...}, 'int8': {...}}: launches, ms, FP64-equivalent flops, int8 ops."""
+        out = (ctypes.c_double * 8)()
+        check(self.lib.sc_kernel_stats(self.handle, out))
+        keys = ("launches", "ms", "flops", "int8_ops")
+        return {"dmma": dict(zip(keys, out[0:4])), "int8": dict(zip(keys, out[4:8]))}
+
+    def gemm_choices(self):
+        """The autotuner's table: list of (m, n, k, batch, slices, variant)."""
+        n = ctypes.c_int(0)
+        check(self.lib.sc_gemm_choices_get(self.handle, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_int * (6 * max(n.value, 1)))()
+        check(self.lib.sc_gemm_choices_get(self.handle, buf, n.value, ctypes.byref(n)))
+        return [tuple(buf[6 * i:6 * i + 6]) for i in range(n.value)]
+
+    def set_gemm_choices(self, table):
+        flat = [int(v) for rec in table for v in rec]
+        buf = (ctypes.c_int * max(len(flat), 1))(*flat)
+        check(self.lib.sc_gemm_choices_set(self.handle, buf, len(table)))
+
     def fp64_peak_tflops(self, tensor: bool = False) -> float:
         """Measured FP64 throughput: FMA pipe, or mma.sync f64 with tensor=True."""
         v = ctypes.c_double(0.0)
