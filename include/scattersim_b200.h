@@ -270,6 +270,34 @@ sc_status sc_gpu_cw_evaluate(void* E_xy, void* E_xz, void* E_yz, float x_start, 
                              float z_start, float x, float y, float z, float d, int N,
                              int device);
 
+
+/* --------------------------------------------------------- surrogate
+ * A Fourier-neural-operator surrogate of the thin-volume solve (11 x 11
+ * orders): a 64 x 64 real index map and a wavelength in, the R/T vector out
+ * as 726 complex values (1452 floats, [Rx Ry Rz Tx Ty Tz] x 121 orders in the
+ * column-major order index of sc_volume_solve's x, real and imaginary
+ * interleaved).  No reference counterpart: the reference has no learned path;
+ * the plain solve generates its training data, is its fallback, and measures
+ * its error.  Width 64, 4 spectral layers, 16 x 16 modes; every linear map is
+ * a BF16 tensor-core GEMM with FP32 accumulation; training is Adam on FP32
+ * master weights.  All buffers are device pointers; batch <= max_batch. */
+typedef struct sc_fno sc_fno;
+sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long long seed);
+sc_status sc_fno_destroy(sc_fno* f);
+sc_status sc_fno_param_count(const sc_fno* f, long long* n);
+/* direction 0: copy the parameters out to dev_params; 1: load them from it */
+sc_status sc_fno_params(sc_fno* f, void* dev_params, int direction, void* stream);
+/* maps: batch x 64 x 64 floats; lambdas: batch floats (um); out: batch x 1452 */
+sc_status sc_fno_forward(sc_fno* f, const float* maps, const float* lambdas, int batch, float* out, void* stream);
+/* per-sample relative squared error |out - target|^2 / |target|^2 into loss
+ * (batch floats) and the gradient of its batch mean into grad (param_count
+ * floats); either may be NULL */
+sc_status sc_fno_loss_grad(sc_fno* f, const float* maps, const float* lambdas, const float* target, int batch,
+                           float* loss, float* grad, void* stream);
+/* sc_fno_loss_grad followed by one Adam step (beta 0.9 / 0.999) at rate lr */
+sc_status sc_fno_train_step(sc_fno* f, const float* maps, const float* lambdas, const float* target, int batch,
+                            float lr, float* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

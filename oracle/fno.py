@@ -1,0 +1,234 @@
+"""CPU restatement of the surrogate network (test infrastructure only).
+
+The reference has no learned component; this file is the oracle for the
+project's own Fourier neural operator (scattersim_b200/csrc/fno.cu): the same
+parameter layout, the same dense DFT operators, and the same arithmetic
+points -- every GEMM rounds its two operands to BF16 (round to nearest even)
+and accumulates in float64 here (float32 on the GPU), and every stored
+intermediate is float32.  With ``bf16=False`` the network runs in float64
+throughout, which the finite-difference tests use to pin the backward pass.
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.special import erf
+
+G = 64
+NP = G * G
+W = 64
+CIN = 4
+L = 4
+MX = MY = 16
+NM = 2 * MX * MY
+NF = 2 * NM
+HID = 128
+COUT = 12
+NO = 11
+NORD = NO * NO
+NOUT = 6 * NORD * 2
+
+
+def bf16(x):
+    """Round float32 values to bfloat16 (nearest even), returned as float32."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    u = x.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32)
+
+
+class Layout:
+    """Offsets of the flat parameter vector (fno.cu::Layout, 64-float aligned blocks)."""
+
+    def __init__(self):
+        self.o = 0
+
+        def take(n):
+            r = self.o
+            self.o += (n + 63) // 64 * 64
+            return r
+        self.P = take(W * CIN)
+        self.bP = take(W)
+        self.Wl, self.bl, self.SWr, self.SWi = [], [], [], []
+        for _ in range(L):
+            self.Wl.append(take(W * W))
+            self.bl.append(take(W))
+            self.SWr.append(take(NM * W * W))
+            self.SWi.append(take(NM * W * W))
+        self.Q1 = take(HID * W)
+        self.bQ1 = take(HID)
+        self.Q2 = take(COUT * HID)
+        self.bQ2 = take(COUT)
+        self.total = self.o
+
+
+def kx_of(r):
+    return r if r < MX else r - 2 * MX
+
+
+def operators():
+    """F (NP x NF), Gi (NF x NP), R (NP x 2 NORD) as in fno.cu::build_operators."""
+    x = np.arange(G)[:, None]
+    y = np.arange(G)[None, :]
+    F = np.zeros((NP, NF))
+    Gi = np.zeros((NF, NP))
+    R = np.zeros((NP, 2 * NORD))
+    tp = 2 * np.pi / G
+    for r in range(2 * MX):
+        for ky in range(MY):
+            md = r * MY + ky
+            ph = ((kx_of(r) * x + ky * y) % G + G) % G
+            th = (tp * ph).ravel()
+            c, s = np.cos(th), np.sin(th)
+            F[:, md] = c
+            F[:, NM + md] = -s
+            cw = (1.0 if ky == 0 else 2.0) / NP
+            Gi[md] = cw * c
+            Gi[NM + md] = -cw * s
+    for j in range(NORD):
+        qq = j % NO - NO // 2
+        pp = j // NO - NO // 2
+        ph = ((pp * x + qq * y) % G + G) % G
+        th = (tp * ph).ravel()
+        R[:, j] = np.cos(th) / NP
+        R[:, NORD + j] = np.sin(th) / NP
+    return F.astype(np.float32), Gi.astype(np.float32), R.astype(np.float32)
+
+
+class Net:
+    def __init__(self, params, bf16_ops=True):
+        self.lay = Layout()
+        self.w = np.asarray(params, dtype=np.float32)
+        self.q = bf16_ops
+        self.F, self.Gi, self.R = operators()
+        self.dt = np.float32 if bf16_ops else np.float64
+        if not bf16_ops:
+            self.w = self.w.astype(np.float64)
+            self.F, self.Gi, self.R = (a.astype(np.float64) for a in (self.F, self.Gi, self.R))
+
+    # a GEMM the way the GPU does it: BF16 operands, wide accumulation, stored as float32
+    def mm(self, A, B):
+        if self.q:
+            out = bf16(A).astype(np.float64) @ bf16(B).astype(np.float64)
+            return out.astype(np.float32)
+        return A @ B
+
+    def par(self, off, shape):
+        n = int(np.prod(shape))
+        return self.w[off:off + n].reshape(shape)
+
+    def gelu(self, x):
+        return (0.5 * x * (1.0 + erf(x.astype(np.float64) / np.sqrt(2.0)))).astype(self.dt)
+
+    def gelu_grad(self, x):
+        xd = x.astype(np.float64)
+        return (0.5 * (1.0 + erf(xd / np.sqrt(2.0))) + xd * np.exp(-0.5 * xd * xd) / np.sqrt(2 * np.pi)).astype(self.dt)
+
+    def forward(self, maps, lam):
+        Ly = self.lay
+        B = maps.shape[0]
+        c = {}
+        inp = np.zeros((B, CIN, NP), self.dt)
+        inp[:, 0] = maps.reshape(B, NP)
+        inp[:, 1] = ((np.asarray(lam, np.float32) - np.float32(0.6)) / np.float32(0.2))[:, None]
+        p = np.arange(NP)
+        inp[:, 2] = (p // G).astype(np.float32) / np.float32(63)
+        inp[:, 3] = (p % G).astype(np.float32) / np.float32(63)
+        c["in"] = inp
+        P = self.par(Ly.P, (W, CIN))
+        v = np.stack([self.mm(P, inp[b]) for b in range(B)]) + self.par(Ly.bP, (W,))[None, :, None]
+        v = v.astype(self.dt)
+        acts, pres, Xs = [v], [], []
+        for l in range(L):
+            X = np.stack([self.mm(v[b], self.F) for b in range(B)])          # B x W x NF
+            Xs.append(X)
+            Wr = self.par(Ly.SWr[l], (NM, W, W))
+            Wi = self.par(Ly.SWi[l], (NM, W, W))
+            Xr, Xi = X[:, :, :NM], X[:, :, NM:]
+            Y = np.zeros_like(X)
+            for md in range(NM):
+                a, bm = Xr[:, :, md], Xi[:, :, md]
+                Y[:, :, md] = (self.mm(a, Wr[md]).astype(np.float64) - self.mm(bm, Wi[md]).astype(np.float64)).astype(self.dt)
+                Y[:, :, NM + md] = (self.mm(a, Wi[md]).astype(np.float64) + self.mm(bm, Wr[md]).astype(np.float64)).astype(self.dt)
+            Wl = self.par(Ly.Wl[l], (W, W))
+            u = np.stack([(self.mm(Wl, v[b]).astype(np.float64) + self.mm(Y[b], self.Gi).astype(np.float64))
+                          for b in range(B)]).astype(self.dt)
+            u = (u + self.par(Ly.bl[l], (W,))[None, :, None]).astype(self.dt)
+            pres.append(u)
+            v = self.gelu(u) if l < L - 1 else u
+            acts.append(v)
+        Q1 = self.par(Ly.Q1, (HID, W))
+        hpre = (np.stack([self.mm(Q1, v[b]) for b in range(B)]) + self.par(Ly.bQ1, (HID,))[None, :, None]).astype(self.dt)
+        h = self.gelu(hpre)
+        Q2 = self.par(Ly.Q2, (COUT, HID))
+        o = (np.stack([self.mm(Q2, h[b]) for b in range(B)]) + self.par(Ly.bQ2, (COUT,))[None, :, None]).astype(self.dt)
+        Pc = np.stack([self.mm(o[b], self.R) for b in range(B)])             # B x 12 x 242
+        pred = np.zeros((B, 6, NORD, 2), self.dt)
+        for ch in range(6):
+            pr, pi = Pc[:, 2 * ch], Pc[:, 2 * ch + 1]
+            pred[:, ch, :, 0] = pr[:, :NORD] + pi[:, NORD:]
+            pred[:, ch, :, 1] = pi[:, :NORD] - pr[:, NORD:]
+        c.update(acts=acts, pres=pres, Xs=Xs, hpre=hpre, h=h, o=o)
+        self.cache = c
+        return pred.reshape(B, NOUT)
+
+    def loss_grad(self, maps, lam, target):
+        """Mean relative squared error and its gradient (flat, like the parameters)."""
+        Ly = self.lay
+        pred = self.forward(maps, lam)
+        c = self.cache
+        B = pred.shape[0]
+        tgt = np.asarray(target, self.dt)
+        d = pred.astype(np.float64) - tgt
+        nrm = (tgt.astype(np.float64) ** 2).sum(1)
+        loss = (d ** 2).sum(1) / nrm
+        dpred = (2.0 * d / (nrm[:, None] * B)).astype(self.dt).reshape(B, 6, NORD, 2)
+        g = np.zeros(Ly.total, np.float64)
+
+        def acc(off, val):
+            g[off:off + val.size] += val.ravel()
+
+        dP = np.zeros((B, COUT, 2 * NORD), self.dt)
+        for ch in range(6):
+            dP[:, 2 * ch, :NORD] = dpred[:, ch, :, 0]
+            dP[:, 2 * ch + 1, NORD:] = dpred[:, ch, :, 0]
+            dP[:, 2 * ch + 1, :NORD] = dpred[:, ch, :, 1]
+            dP[:, 2 * ch, NORD:] = -dpred[:, ch, :, 1]
+        do = np.stack([self.mm(dP[b], self.R.T) for b in range(B)])
+        acc(Ly.Q2, sum(self.mm(do[b], c["h"][b].T).astype(np.float64) for b in range(B)))
+        acc(Ly.bQ2, do.astype(np.float64).sum((0, 2)))
+        Q2 = self.par(Ly.Q2, (COUT, HID))
+        dh = np.stack([self.mm(Q2.T, do[b]) for b in range(B)])
+        dh = (dh * self.gelu_grad(c["hpre"])).astype(self.dt)
+        acc(Ly.Q1, sum(self.mm(dh[b], c["acts"][L][b].T).astype(np.float64) for b in range(B)))
+        acc(Ly.bQ1, dh.astype(np.float64).sum((0, 2)))
+        Q1 = self.par(Ly.Q1, (HID, W))
+        dv = np.stack([self.mm(Q1.T, dh[b]) for b in range(B)])
+        for l in range(L - 1, -1, -1):
+            du = dv if l == L - 1 else (dv * self.gelu_grad(c["pres"][l])).astype(self.dt)
+            acc(Ly.bl[l], du.astype(np.float64).sum((0, 2)))
+            vin = c["acts"][l]
+            acc(Ly.Wl[l], sum(self.mm(du[b], vin[b].T).astype(np.float64) for b in range(B)))
+            Wl = self.par(Ly.Wl[l], (W, W))
+            dvn = np.stack([self.mm(Wl.T, du[b]) for b in range(B)])
+            dY = np.stack([self.mm(du[b], self.Gi.T) for b in range(B)])
+            X = c["Xs"][l]
+            Xr, Xi = X[:, :, :NM], X[:, :, NM:]
+            dYr, dYi = dY[:, :, :NM], dY[:, :, NM:]
+            Wr = self.par(Ly.SWr[l], (NM, W, W))
+            Wi = self.par(Ly.SWi[l], (NM, W, W))
+            dX = np.zeros_like(X)
+            gWr = np.zeros((NM, W, W))
+            gWi = np.zeros((NM, W, W))
+            for md in range(NM):
+                r, i = dYr[:, :, md], dYi[:, :, md]
+                dX[:, :, md] = (self.mm(r, Wr[md].T).astype(np.float64) + self.mm(i, Wi[md].T).astype(np.float64)).astype(self.dt)
+                dX[:, :, NM + md] = (-self.mm(r, Wi[md].T).astype(np.float64) + self.mm(i, Wr[md].T).astype(np.float64)).astype(self.dt)
+                xr, xi = Xr[:, :, md], Xi[:, :, md]
+                gWr[md] = self.mm(xr.T, r).astype(np.float64) + self.mm(xi.T, i).astype(np.float64)
+                gWi[md] = -self.mm(xi.T, r).astype(np.float64) + self.mm(xr.T, i).astype(np.float64)
+            acc(Ly.SWr[l], gWr)
+            acc(Ly.SWi[l], gWi)
+            dv = (dvn.astype(np.float64) + np.stack([self.mm(dX[b], self.F.T) for b in range(B)]).astype(np.float64)).astype(self.dt)
+        acc(Ly.P, sum(self.mm(dv[b], c["in"][b].T).astype(np.float64) for b in range(B)))
+        acc(Ly.bP, dv.astype(np.float64).sum((0, 2)))
+        return loss, g

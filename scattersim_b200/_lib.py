@@ -79,6 +79,14 @@ _SIGS = {
     "sc_kernel_stats": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_gemm_choices_get": (c_int, [c_void_p, POINTER(c_int), c_int, POINTER(c_int)]),
     "sc_gemm_choices_set": (c_int, [c_void_p, POINTER(c_int), c_int]),
+    "sc_fno_create": (c_int, [POINTER(c_void_p), c_int, c_int, ctypes.c_ulonglong]),
+    "sc_fno_destroy": (c_int, [c_void_p]),
+    "sc_fno_param_count": (c_int, [c_void_p, POINTER(c_longlong)]),
+    "sc_fno_params": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "sc_fno_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "sc_fno_loss_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "sc_fno_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p,
+                                  c_void_p]),
     "sc_volume_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_void_p, c_int, c_int, c_int, c_void_p,
                                 c_void_p, c_void_p, c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_stage_ms": (c_int, [c_void_p, POINTER(c_double)]),

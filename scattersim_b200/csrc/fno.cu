@@ -1,0 +1,793 @@
+// Fourier-neural-operator surrogate of the thin-volume solve: a 64 x 64 index
+// map plus the wavelength in, the R/T amplitudes of the 11 x 11 orders out
+// (the x vector of ScatterVolume.cpp:739 for --coef 11 11).  The plain solve is
+// its training data, its fallback and the judge of its error.
+//
+// Network (width W = 64, 4 spectral layers, 16 x 16 retained modes):
+//   in  = [n(x, y), (lambda - 0.6) / 0.2, x / 63, y / 63]            4 x 64 x 64
+//   v0  = P in + bP                                                   lift
+//   u_l = W_l v_l + b_l + Re IDFT(M_l . DFT(v_l)),  v_{l+1} = GELU(u_l)
+//         (no GELU after the last layer); DFT keeps kx in [-16, 16),
+//         ky in [0, 16) (512 complex modes), M_l is a complex W x W
+//         matrix per mode, IDFT is the real inverse of that half spectrum
+//   h   = GELU(Q1 v4 + bQ1) (128 channels), o = Q2 h + bQ2 (12 channels)
+//   amplitudes of channel pair c: sum_xy (o_2c + i o_2c+1) e^-i theta / 4096
+//         at the 121 orders, theta = 2 pi (p x + q y) / 64, p, q in [-5, 5]
+// Every linear map (lift, pointwise, the forward and inverse DFT as dense
+// 4096 x 1024 operators, the per-mode mixing, projections, readout) is one
+// hand-written tensor-core GEMM: operands rounded to BF16 as they are staged,
+// mma.sync m16n8k16 with FP32 accumulation, FP32 in global memory, arbitrary
+// strides and batches.  Training: relative squared error per sample, Adam on
+// FP32 master weights.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sc {
+namespace fno {
+
+constexpr int G = 64;                 // grid side
+constexpr int NP = G * G;             // pixels
+constexpr int W = 64;                 // width
+constexpr int CIN = 4;                // input channels
+constexpr int L = 4;                  // spectral layers
+constexpr int MX = 16, MY = 16;       // retained modes: kx in [-MX, MX), ky in [0, MY)
+constexpr int NM = 2 * MX * MY;       // 512 complex modes
+constexpr int NF = 2 * NM;            // 1024 real columns: [re | im]
+constexpr int HID = 128;              // projection hidden channels
+constexpr int COUT = 12;              // 6 complex output fields
+constexpr int NO = 11;                // orders per axis
+constexpr int NORD = NO * NO;         // 121
+constexpr int NOUT = 6 * NORD * 2;    // 1452 reals per sample
+
+// ------------------------------------------------------------------ BF16 GEMM
+// C_b[m, n] = alpha * sum_k A_b[m, k] B_b[k, n] + beta * C_b[m, n], element
+// addresses A + b sAb + m sAm + k sAk (likewise B, C).
+struct Gemm {
+    int m, n, k, batch;
+    float alpha, beta;
+    const float* A;
+    long long sAm, sAk, sAb;
+    const float* B;
+    long long sBk, sBn, sBb;
+    float* C;
+    long long sCm, sCn, sCb;
+};
+
+constexpr int TM = 64, TN = 64, TK = 32, GT = 128, PADK = 8;
+
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
+    __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PADK];
+    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PADK];
+    const int b = blockIdx.z;
+    const float* A = g.A + b * g.sAb;
+    const float* B = g.B + b * g.sBb;
+    float* C = g.C + b * g.sCb;
+    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int gq = lane >> 2, tq = lane & 3;
+    const bool a_kfast = (g.sAk == 1), b_kfast = (g.sBk == 1);
+    float ra[TM * TK / GT], rb[TN * TK / GT];
+
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < TM * TK / GT; ++i) {
+            const int e = tid + GT * i;
+            int r, kk;
+            if (a_kfast) { r = e / TK; kk = e % TK; }
+            else { r = e % TM; kk = e / TM; }
+            const int gm = m0 + r, gk = k0 + kk;
+            ra[i] = (gm < g.m && gk < g.k) ? A[gm * g.sAm + gk * g.sAk] : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < TN * TK / GT; ++i) {
+            const int e = tid + GT * i;
+            int c, kk;
+            if (b_kfast) { c = e / TK; kk = e % TK; }
+            else { c = e % TN; kk = e / TN; }
+            const int gn = n0 + c, gk = k0 + kk;
+            rb[i] = (gn < g.n && gk < g.k) ? B[gk * g.sBk + gn * g.sBn] : 0.f;
+        }
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int i = 0; i < TM * TK / GT; ++i) {
+            const int e = tid + GT * i;
+            int r, kk;
+            if (a_kfast) { r = e / TK; kk = e % TK; }
+            else { r = e % TM; kk = e / TM; }
+            As[r][kk] = __float2bfloat16_rn(ra[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < TN * TK / GT; ++i) {
+            const int e = tid + GT * i;
+            int c, kk;
+            if (b_kfast) { c = e / TK; kk = e % TK; }
+            else { c = e % TN; kk = e / TN; }
+            Bs[c][kk] = __float2bfloat16_rn(rb[i]);
+        }
+    };
+
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+    const int nk = (g.k + TK - 1) / TK;
+    if (nk > 0) {
+        load(0);
+        store();
+    }
+    __syncthreads();
+    for (int t = 0; t < nk; ++t) {
+        if (t + 1 < nk) load((t + 1) * TK);
+#pragma unroll
+        for (int ks = 0; ks < TK; ks += 16) {
+            uint32_t af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r0 = wm * 32 + i * 16 + gq;
+                af[i][0] = ld32(&As[r0][ks + 2 * tq]);
+                af[i][1] = ld32(&As[r0 + 8][ks + 2 * tq]);
+                af[i][2] = ld32(&As[r0][ks + 8 + 2 * tq]);
+                af[i][3] = ld32(&As[r0 + 8][ks + 8 + 2 * tq]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c0 = wn * 32 + j * 8 + gq;
+                bf[j][0] = ld32(&Bs[c0][ks + 2 * tq]);
+                bf[j][1] = ld32(&Bs[c0][ks + 8 + 2 * tq]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    asm volatile(
+                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                        "{%8, %9}, {%0, %1, %2, %3};\n"
+                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+                        : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bf[j][0]), "r"(bf[j][1]));
+        }
+        __syncthreads();
+        if (t + 1 < nk) {
+            store();
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gm = m0 + wm * 32 + i * 16 + gq + ((q & 2) ? 8 : 0);
+                const int gn = n0 + wn * 32 + j * 8 + 2 * tq + (q & 1);
+                if (gm < g.m && gn < g.n) {
+                    float* p = C + gm * g.sCm + gn * g.sCn;
+                    const float v = g.alpha * acc[i][j][q];
+                    *p = (g.beta == 0.f) ? v : fmaf(g.beta, *p, v);
+                }
+            }
+}
+
+sc_status gemm(cudaStream_t st, const Gemm& g) {
+    if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return SC_OK;
+    if (g.batch > 65535 || (g.n + TN - 1) / TN > 65535) {
+        set_error("fno gemm: grid too large");
+        return SC_BADINPUT;
+    }
+    dim3 grid((g.m + TM - 1) / TM, (g.n + TN - 1) / TN, g.batch);
+    bf16_gemm_kernel<<<grid, GT, 0, st>>>(g);
+    count_launch();
+    SC_CHECK_LAUNCH("fno gemm");
+    return SC_OK;
+}
+
+// ------------------------------------------------------------------ elementwise
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    return 0.5f * (1.f + erff(x * 0.70710678f)) + x * 0.39894228f * expf(-0.5f * x * x);
+}
+
+// in[b] = [map, (lambda - 0.6) / 0.2, x / 63, y / 63]
+__global__ void input_kernel(const float* __restrict__ maps, const float* __restrict__ lam, int Bn,
+                             float* __restrict__ in) {
+    const long long tot = (long long)Bn * NP;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / NP), p = (int)(t % NP);
+        float* o = in + (long long)b * CIN * NP;
+        o[p] = maps[t];
+        o[NP + p] = (lam[b] - 0.6f) / 0.2f;
+        o[2 * NP + p] = (float)(p / G) / 63.f;
+        o[3 * NP + p] = (float)(p % G) / 63.f;
+    }
+}
+
+// x[b][c][p] += bias[c]; optionally a = GELU(x) (x keeps the pre-activation)
+__global__ void bias_act_kernel(float* __restrict__ x, const float* __restrict__ bias, int C, int Bn, int act,
+                                float* __restrict__ a) {
+    const long long tot = (long long)Bn * C * NP;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)((t / NP) % C);
+        const float v = x[t] + bias[c];
+        x[t] = v;
+        if (act) a[t] = gelu(v);
+    }
+}
+
+// g *= GELU'(pre)
+__global__ void gelu_back_kernel(float* __restrict__ g, const float* __restrict__ pre, long long tot) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x)
+        g[t] *= gelu_grad(pre[t]);
+}
+
+// db[c] += sum_{b, p} g[b][c][p]  (one CTA per channel, fixed order)
+__global__ void bias_grad_kernel(const float* __restrict__ g, int C, int Bn, float* __restrict__ db) {
+    __shared__ float red[8];
+    const int c = blockIdx.x;
+    float s = 0.f;
+    for (int b = 0; b < Bn; ++b)
+        for (int p = threadIdx.x; p < NP; p += blockDim.x) s += g[((long long)b * C + c) * NP + p];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+        db[c] += t;
+    }
+}
+
+// out[i] += sum_b part[b][i]
+__global__ void batch_sum_kernel(const float* __restrict__ part, int Bn, long long n, float* __restrict__ out) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int b = 0; b < Bn; ++b) s += part[(long long)b * n + t];
+        out[t] += s;
+    }
+}
+
+// readout: P[b][12][242] (cos | sin correlations) -> pred[b][6][121][re, im]
+__global__ void readout_kernel(const float* __restrict__ P, int Bn, float* __restrict__ pred) {
+    const int tot = Bn * 6 * NORD;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+        const int b = t / (6 * NORD), c = (t / NORD) % 6, j = t % NORD;
+        const float* pr = P + ((long long)b * COUT + 2 * c) * 2 * NORD;
+        const float* pi = pr + 2 * NORD;
+        float* o = pred + (long long)b * NOUT + 2 * (c * NORD + j);
+        o[0] = pr[j] + pi[NORD + j];
+        o[1] = pi[j] - pr[NORD + j];
+    }
+}
+
+// adjoint of readout_kernel
+__global__ void readout_back_kernel(const float* __restrict__ dpred, int Bn, float* __restrict__ dP) {
+    const int tot = Bn * 6 * NORD;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+        const int b = t / (6 * NORD), c = (t / NORD) % 6, j = t % NORD;
+        const float* d = dpred + (long long)b * NOUT + 2 * (c * NORD + j);
+        float* pr = dP + ((long long)b * COUT + 2 * c) * 2 * NORD;
+        float* pi = pr + 2 * NORD;
+        pr[j] = d[0];
+        pi[NORD + j] = d[0];
+        pi[j] = d[1];
+        pr[NORD + j] = -d[1];
+    }
+}
+
+// per-sample relative squared error; dpred = d loss / d pred; loss[b]
+__global__ void loss_kernel(const float* __restrict__ pred, const float* __restrict__ tgt, int Bn,
+                            float* __restrict__ dpred, float* __restrict__ loss) {
+    __shared__ float r1[8], r2[8];
+    const int b = blockIdx.x;
+    const float* p = pred + (long long)b * NOUT;
+    const float* y = tgt + (long long)b * NOUT;
+    float e = 0.f, n = 0.f;
+    for (int i = threadIdx.x; i < NOUT; i += blockDim.x) {
+        const float d = p[i] - y[i];
+        e += d * d;
+        n += y[i] * y[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        r1[threadIdx.x >> 5] = e;
+        r2[threadIdx.x >> 5] = n;
+    }
+    __syncthreads();
+    float E = 0.f, N = 0.f;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        E += r1[i];
+        N += r2[i];
+    }
+    N = fmaxf(N, 1e-30f);
+    if (threadIdx.x == 0) loss[b] = E / N;
+    if (dpred)
+        for (int i = threadIdx.x; i < NOUT; i += blockDim.x) dpred[(long long)b * NOUT + i] = 2.f * (p[i] - y[i]) / (N * Bn);
+}
+
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[t];
+        const float mi = b1 * m[t] + (1.f - b1) * gi;
+        const float vi = b2 * v[t] + (1.f - b2) * gi * gi;
+        m[t] = mi;
+        v[t] = vi;
+        w[t] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+unsigned blocks(long long tot) {
+    long long b = (tot + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 4096) b = 4096;
+    return (unsigned)b;
+}
+
+// ------------------------------------------------------------------ parameters
+struct Layout {
+    long long P, bP, Wl[L], bl[L], SWr[L], SWi[L], Q1, bQ1, Q2, bQ2, total;
+    Layout() {
+        long long o = 0;
+        auto take = [&](long long n) {
+            long long r = o;
+            o += (n + 63) / 64 * 64;
+            return r;
+        };
+        P = take((long long)W * CIN);
+        bP = take(W);
+        for (int l = 0; l < L; ++l) {
+            Wl[l] = take((long long)W * W);
+            bl[l] = take(W);
+            SWr[l] = take((long long)NM * W * W);
+            SWi[l] = take((long long)NM * W * W);
+        }
+        Q1 = take((long long)HID * W);
+        bQ1 = take(HID);
+        Q2 = take((long long)COUT * HID);
+        bQ2 = take(COUT);
+        total = o;
+    }
+};
+
+}  // namespace fno
+}  // namespace sc
+
+using namespace sc;
+using namespace sc::fno;
+
+struct sc_fno {
+    int device = 0;
+    int max_batch = 0;
+    Layout lay;
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // params, grads, Adam moments
+    float *F = nullptr, *Gi = nullptr, *R = nullptr;                 // DFT operators
+    float *in = nullptr, *act[L + 1] = {}, *pre[L] = {}, *X[L] = {}, *Y = nullptr;
+    float *hpre = nullptr, *h = nullptr, *o12 = nullptr, *P = nullptr, *pred = nullptr;
+    float *dact = nullptr, *dv = nullptr, *dX = nullptr, *dY = nullptr, *dh = nullptr, *do12 = nullptr,
+          *dP = nullptr, *dpred = nullptr, *part = nullptr, *loss = nullptr;
+    long long step = 0;
+};
+
+namespace {
+
+sc_status fno_alloc(float** p, long long n) {
+    cudaError_t e = cudaMalloc(p, sizeof(float) * (size_t)(n > 0 ? n : 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("fno: device allocation of %lld floats failed", n);
+        return SC_OOM;
+    }
+    return SC_OK;
+}
+
+// deterministic uniform [0, 1) stream (splitmix64)
+struct Rng {
+    uint64_t s;
+    double next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    }
+};
+
+// wrapped signed frequency of retained row index r in [0, 2 MX)
+int kx_of(int r) { return r < MX ? r : r - 2 * MX; }
+
+// order index j (the solve's column-major (q, p) index) -> (p, q) in [-5, 5]
+void order_pq(int j, int* p, int* q) {
+    *q = j % NO - NO / 2;
+    *p = j / NO - NO / 2;
+}
+
+Gemm mk(int m, int n, int k, int batch, float alpha, float beta, const float* A, long long sAm, long long sAk,
+        long long sAb, const float* B, long long sBk, long long sBn, long long sBb, float* C, long long sCm,
+        long long sCn, long long sCb) {
+    return Gemm{m, n, k, batch, alpha, beta, A, sAm, sAk, sAb, B, sBk, sBn, sBb, C, sCm, sCn, sCb};
+}
+
+// forward pass for Bn samples; keeps every activation for the backward pass
+sc_status forward(sc_fno* f, const float* maps, const float* lam, int Bn, cudaStream_t st) {
+    const Layout& Ly = f->lay;
+    const float* w = f->w;
+    const long long sv = (long long)W * NP;
+    input_kernel<<<blocks((long long)Bn * NP), 256, 0, st>>>(maps, lam, Bn, f->in);
+    count_launch();
+    // lift: v0_b (W x NP) = P (W x CIN) in_b (CIN x NP)
+    SC_TRY(gemm(st, mk(W, NP, CIN, Bn, 1.f, 0.f, w + Ly.P, CIN, 1, 0, f->in, NP, 1, (long long)CIN * NP, f->act[0], NP,
+                       1, sv)));
+    bias_act_kernel<<<blocks((long long)Bn * sv), 256, 0, st>>>(f->act[0], w + Ly.bP, W, Bn, 0, nullptr);
+    count_launch();
+    for (int l = 0; l < L; ++l) {
+        float* vin = f->act[l];
+        // X_b (W x NF) = v_b (W x NP) F (NP x NF)
+        SC_TRY(gemm(st, mk(W, NF, NP, Bn, 1.f, 0.f, vin, NP, 1, sv, f->F, NF, 1, 0, f->X[l], NF, 1, (long long)W * NF)));
+        // per mode md: Y[b, o] = sum_i X[b, i] M[md][i][o] (complex, as four real products)
+        const float* Xr = f->X[l];
+        const float* Xi = f->X[l] + NM;
+        const float* Wr = w + Ly.SWr[l];
+        const float* Wi = w + Ly.SWi[l];
+        float* Yr = f->Y;
+        float* Yi = f->Y + NM;
+        const long long sb = (long long)W * NF;
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, sb, NF, 1, Wr, W, 1, (long long)W * W, Yr, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 1.f, Xi, sb, NF, 1, Wi, W, 1, (long long)W * W, Yr, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, sb, NF, 1, Wi, W, 1, (long long)W * W, Yi, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, Xi, sb, NF, 1, Wr, W, 1, (long long)W * W, Yi, sb, NF, 1)));
+        // u_b = W_l v_b + Y_b G + b_l
+        float* u = f->pre[l];
+        SC_TRY(gemm(st, mk(W, NP, W, Bn, 1.f, 0.f, w + Ly.Wl[l], W, 1, 0, vin, NP, 1, sv, u, NP, 1, sv)));
+        SC_TRY(gemm(st, mk(W, NP, NF, Bn, 1.f, 1.f, f->Y, NF, 1, sb, f->Gi, NP, 1, 0, u, NP, 1, sv)));
+        const int act = (l < L - 1);
+        bias_act_kernel<<<blocks((long long)Bn * sv), 256, 0, st>>>(u, w + Ly.bl[l], W, Bn, act, f->act[l + 1]);
+        count_launch();
+        if (!act)
+            SC_CUDA_TRY(cudaMemcpyAsync(f->act[l + 1], u, sizeof(float) * Bn * sv, cudaMemcpyDeviceToDevice, st));
+    }
+    // projection
+    const long long sh = (long long)HID * NP;
+    SC_TRY(gemm(st, mk(HID, NP, W, Bn, 1.f, 0.f, w + Ly.Q1, W, 1, 0, f->act[L], NP, 1, sv, f->hpre, NP, 1, sh)));
+    bias_act_kernel<<<blocks((long long)Bn * sh), 256, 0, st>>>(f->hpre, w + Ly.bQ1, HID, Bn, 1, f->h);
+    count_launch();
+    const long long so = (long long)COUT * NP;
+    SC_TRY(gemm(st, mk(COUT, NP, HID, Bn, 1.f, 0.f, w + Ly.Q2, HID, 1, 0, f->h, NP, 1, sh, f->o12, NP, 1, so)));
+    bias_act_kernel<<<blocks((long long)Bn * so), 256, 0, st>>>(f->o12, w + Ly.bQ2, COUT, Bn, 0, nullptr);
+    count_launch();
+    // readout correlations P_b (12 x 242) = o_b (12 x NP) R (NP x 242)
+    SC_TRY(gemm(st, mk(COUT, 2 * NORD, NP, Bn, 1.f, 0.f, f->o12, NP, 1, so, f->R, 2 * NORD, 1, 0, f->P, 2 * NORD, 1,
+                       (long long)COUT * 2 * NORD)));
+    readout_kernel<<<blocks((long long)Bn * 6 * NORD), 256, 0, st>>>(f->P, Bn, f->pred);
+    count_launch();
+    SC_CHECK_LAUNCH("fno forward");
+    return SC_OK;
+}
+
+// gradient of sum_b loss_b / Bn into f->g (zeroed here); loss per sample into f->loss
+sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
+    const Layout& Ly = f->lay;
+    const float* w = f->w;
+    float* g = f->g;
+    const long long sv = (long long)W * NP, sh = (long long)HID * NP, so = (long long)COUT * NP;
+    const long long sb = (long long)W * NF;
+    SC_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(float) * Ly.total, st));
+    loss_kernel<<<Bn, 256, 0, st>>>(f->pred, tgt, Bn, f->dpred, f->loss);
+    readout_back_kernel<<<blocks((long long)Bn * 6 * NORD), 256, 0, st>>>(f->dpred, Bn, f->dP);
+    count_launch(2);
+    // do12_b (12 x NP) = dP_b (12 x 242) R^T
+    SC_TRY(gemm(st, mk(COUT, NP, 2 * NORD, Bn, 1.f, 0.f, f->dP, 2 * NORD, 1, (long long)COUT * 2 * NORD, f->R, 1,
+                       2 * NORD, 0, f->do12, NP, 1, so)));
+    // Q2, bQ2: per-sample partials, then summed over the batch
+    SC_TRY(gemm(st, mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
+                       (long long)COUT * HID)));
+    batch_sum_kernel<<<blocks((long long)COUT * HID), 256, 0, st>>>(f->part, Bn, (long long)COUT * HID, g + Ly.Q2);
+    bias_grad_kernel<<<COUT, 256, 0, st>>>(f->do12, COUT, Bn, g + Ly.bQ2);
+    count_launch(2);
+    // dh_b = Q2^T do12_b, through GELU
+    SC_TRY(gemm(st, mk(HID, NP, COUT, Bn, 1.f, 0.f, w + Ly.Q2, 1, HID, 0, f->do12, NP, 1, so, f->dh, NP, 1, sh)));
+    gelu_back_kernel<<<blocks((long long)Bn * sh), 256, 0, st>>>(f->dh, f->hpre, (long long)Bn * sh);
+    count_launch();
+    SC_TRY(gemm(st, mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
+                       (long long)HID * W)));
+    batch_sum_kernel<<<blocks((long long)HID * W), 256, 0, st>>>(f->part, Bn, (long long)HID * W, g + Ly.Q1);
+    bias_grad_kernel<<<HID, 256, 0, st>>>(f->dh, HID, Bn, g + Ly.bQ1);
+    count_launch(2);
+    // dv4 = Q1^T dh
+    SC_TRY(gemm(st, mk(W, NP, HID, Bn, 1.f, 0.f, w + Ly.Q1, 1, W, 0, f->dh, NP, 1, sh, f->dact, NP, 1, sv)));
+    for (int l = L - 1; l >= 0; --l) {
+        // du = dv_{l+1} * GELU'(u_l) (no activation after the last layer)
+        float* du = f->dact;
+        if (l < L - 1) {
+            gelu_back_kernel<<<blocks((long long)Bn * sv), 256, 0, st>>>(du, f->pre[l], (long long)Bn * sv);
+            count_launch();
+        }
+        bias_grad_kernel<<<W, 256, 0, st>>>(du, W, Bn, g + Ly.bl[l]);
+        count_launch();
+        const float* vin = f->act[l];
+        // W_l
+        SC_TRY(gemm(st, mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1, (long long)W * W)));
+        batch_sum_kernel<<<blocks((long long)W * W), 256, 0, st>>>(f->part, Bn, (long long)W * W, g + Ly.Wl[l]);
+        count_launch();
+        // dv_l = W_l^T du
+        SC_TRY(gemm(st, mk(W, NP, W, Bn, 1.f, 0.f, w + Ly.Wl[l], 1, W, 0, du, NP, 1, sv, f->dv, NP, 1, sv)));
+        // dY_b = du_b G^T
+        SC_TRY(gemm(st, mk(W, NF, NP, Bn, 1.f, 0.f, du, NP, 1, sv, f->Gi, 1, NP, 0, f->dY, NF, 1, sb)));
+        // mode mixing: dX = dY M^H, dM = X^H dY (complex, per mode)
+        const float* Xr = f->X[l];
+        const float* Xi = f->X[l] + NM;
+        const float* Wr = w + Ly.SWr[l];
+        const float* Wi = w + Ly.SWi[l];
+        const float* dYr = f->dY;
+        const float* dYi = f->dY + NM;
+        float* dXr = f->dX;
+        float* dXi = f->dX + NM;
+        const long long ww = (long long)W * W;
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, dYr, sb, NF, 1, Wr, 1, W, ww, dXr, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, sb, NF, 1, Wi, 1, W, ww, dXr, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 0.f, dYr, sb, NF, 1, Wi, 1, W, ww, dXi, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, sb, NF, 1, Wr, 1, W, ww, dXi, sb, NF, 1)));
+        float* gWr = g + Ly.SWr[l];
+        float* gWi = g + Ly.SWi[l];
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 0.f, Xr, NF, sb, 1, dYr, sb, NF, 1, gWr, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xi, NF, sb, 1, dYi, sb, NF, 1, gWr, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, -1.f, 0.f, Xi, NF, sb, 1, dYr, sb, NF, 1, gWi, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xr, NF, sb, 1, dYi, sb, NF, 1, gWi, W, 1, ww)));
+        // dv_l += dX_b F^T
+        SC_TRY(gemm(st, mk(W, NP, NF, Bn, 1.f, 1.f, f->dX, NF, 1, sb, f->F, 1, NF, 0, f->dv, NP, 1, sv)));
+        std::swap(f->dact, f->dv);
+    }
+    // lift
+    SC_TRY(gemm(st, mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part, CIN,
+                       1, (long long)W * CIN)));
+    batch_sum_kernel<<<blocks((long long)W * CIN), 256, 0, st>>>(f->part, Bn, (long long)W * CIN, g + Ly.P);
+    bias_grad_kernel<<<W, 256, 0, st>>>(f->dact, W, Bn, g + Ly.bP);
+    count_launch(2);
+    SC_CHECK_LAUNCH("fno backward");
+    return SC_OK;
+}
+
+void init_params(const Layout& Ly, uint64_t seed, std::vector<float>& w) {
+    w.assign(Ly.total, 0.f);
+    Rng r{seed};
+    auto unif = [&](long long off, long long n, double a) {
+        for (long long i = 0; i < n; ++i) w[off + i] = (float)((2.0 * r.next() - 1.0) * a);
+    };
+    unif(Ly.P, (long long)W * CIN, 1.0 / std::sqrt((double)CIN));
+    unif(Ly.bP, W, 1.0 / std::sqrt((double)CIN));
+    for (int l = 0; l < L; ++l) {
+        unif(Ly.Wl[l], (long long)W * W, 1.0 / std::sqrt((double)W));
+        unif(Ly.bl[l], W, 1.0 / std::sqrt((double)W));
+        const double s = 1.0 / ((double)W * W);
+        for (long long i = 0; i < (long long)NM * W * W; ++i) w[Ly.SWr[l] + i] = (float)(s * r.next());
+        for (long long i = 0; i < (long long)NM * W * W; ++i) w[Ly.SWi[l] + i] = (float)(s * r.next());
+    }
+    unif(Ly.Q1, (long long)HID * W, 1.0 / std::sqrt((double)W));
+    unif(Ly.bQ1, HID, 1.0 / std::sqrt((double)W));
+    unif(Ly.Q2, (long long)COUT * HID, 1.0 / std::sqrt((double)HID));
+    unif(Ly.bQ2, COUT, 1.0 / std::sqrt((double)HID));
+}
+
+// dense DFT operators: F (NP x NF) = [cos | -sin] of the retained modes,
+// Gi (NF x NP) = [c cos; -c sin] / NP (real inverse of the half spectrum,
+// c = 1 for ky = 0 else 2), R (NP x 242) = [cos | sin] / NP at the orders
+void build_operators(std::vector<float>& F, std::vector<float>& Gi, std::vector<float>& R) {
+    F.assign((size_t)NP * NF, 0.f);
+    Gi.assign((size_t)NF * NP, 0.f);
+    R.assign((size_t)NP * 2 * NORD, 0.f);
+    const double tp = 2.0 * M_PI / G;
+    for (int x = 0; x < G; ++x)
+        for (int y = 0; y < G; ++y) {
+            const int p = x * G + y;
+            for (int r = 0; r < 2 * MX; ++r)
+                for (int ky = 0; ky < MY; ++ky) {
+                    const int md = r * MY + ky;
+                    const long long ph = ((long long)kx_of(r) * x + (long long)ky * y) % G;
+                    const double th = tp * (double)((ph + G) % G);
+                    const double c = std::cos(th), s = std::sin(th);
+                    F[(size_t)p * NF + md] = (float)c;
+                    F[(size_t)p * NF + NM + md] = (float)(-s);
+                    const double cw = (ky == 0 ? 1.0 : 2.0) / NP;
+                    Gi[(size_t)md * NP + p] = (float)(cw * c);
+                    Gi[(size_t)(NM + md) * NP + p] = (float)(-cw * s);
+                }
+            for (int j = 0; j < NORD; ++j) {
+                int pp, qq;
+                order_pq(j, &pp, &qq);
+                const long long ph = ((long long)pp * x + (long long)qq * y) % G;
+                const double th = tp * (double)((ph + G) % G);
+                R[(size_t)p * 2 * NORD + j] = (float)(std::cos(th) / NP);
+                R[(size_t)p * 2 * NORD + NORD + j] = (float)(std::sin(th) / NP);
+            }
+        }
+}
+
+struct Guard {
+    int prev = -1;
+    explicit Guard(int dev) {
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+    }
+    ~Guard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+sc_status check_batch(const sc_fno* f, int Bn) {
+    if (!f || Bn <= 0 || Bn > f->max_batch) {
+        set_error("fno: batch %d outside 1..%d", Bn, f ? f->max_batch : 0);
+        return SC_BADINPUT;
+    }
+    return SC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long long seed) {
+    if (!out || max_batch <= 0 || max_batch > 4096) {
+        set_error("sc_fno_create: bad argument (max_batch %d)", max_batch);
+        return SC_BADINPUT;
+    }
+    *out = nullptr;
+    Guard gd(device);
+    sc_fno* f = new sc_fno();
+    f->device = device;
+    f->max_batch = max_batch;
+    const Layout& Ly = f->lay;
+    const long long B = max_batch, sv = (long long)W * NP;
+    sc_status s = SC_OK;
+    auto A = [&](float** p, long long n) {
+        if (s == SC_OK) s = fno_alloc(p, n);
+    };
+    A(&f->w, Ly.total);
+    A(&f->g, Ly.total);
+    A(&f->m, Ly.total);
+    A(&f->v, Ly.total);
+    A(&f->F, (long long)NP * NF);
+    A(&f->Gi, (long long)NF * NP);
+    A(&f->R, (long long)NP * 2 * NORD);
+    A(&f->in, B * CIN * NP);
+    for (int l = 0; l <= L; ++l) A(&f->act[l], B * sv);
+    for (int l = 0; l < L; ++l) {
+        A(&f->pre[l], B * sv);
+        A(&f->X[l], B * W * NF);
+    }
+    A(&f->Y, B * W * NF);
+    A(&f->hpre, B * HID * NP);
+    A(&f->h, B * HID * NP);
+    A(&f->o12, B * COUT * NP);
+    A(&f->P, B * COUT * 2 * NORD);
+    A(&f->pred, B * NOUT);
+    A(&f->dact, B * sv);
+    A(&f->dv, B * sv);
+    A(&f->dX, B * W * NF);
+    A(&f->dY, B * W * NF);
+    A(&f->dh, B * HID * NP);
+    A(&f->do12, B * COUT * NP);
+    A(&f->dP, B * COUT * 2 * NORD);
+    A(&f->dpred, B * NOUT);
+    A(&f->part, B * (long long)HID * W);
+    A(&f->loss, B);
+    if (s == SC_OK) {
+        std::vector<float> w, F, Gi, R;
+        init_params(Ly, seed, w);
+        build_operators(F, Gi, R);
+        cudaError_t e = cudaMemcpy(f->w, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(f->F, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(f->Gi, Gi.data(), sizeof(float) * Gi.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(f->R, R.data(), sizeof(float) * R.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(f->m, 0, sizeof(float) * Ly.total);
+        if (e == cudaSuccess) e = cudaMemset(f->v, 0, sizeof(float) * Ly.total);
+        if (e != cudaSuccess) s = cuda_status(e, "sc_fno_create");
+    }
+    if (s != SC_OK) {
+        sc_fno_destroy(f);
+        return s;
+    }
+    *out = f;
+    return SC_OK;
+}
+
+sc_status sc_fno_destroy(sc_fno* f) {
+    if (!f) return SC_OK;
+    Guard gd(f->device);
+    float* ptrs[] = {f->w, f->g, f->m, f->v, f->F, f->Gi, f->R, f->in, f->Y, f->hpre, f->h, f->o12, f->P, f->pred,
+                     f->dact, f->dv, f->dX, f->dY, f->dh, f->do12, f->dP, f->dpred, f->part, f->loss};
+    for (float* p : ptrs)
+        if (p) cudaFree(p);
+    for (int l = 0; l <= L; ++l)
+        if (f->act[l]) cudaFree(f->act[l]);
+    for (int l = 0; l < L; ++l) {
+        if (f->pre[l]) cudaFree(f->pre[l]);
+        if (f->X[l]) cudaFree(f->X[l]);
+    }
+    delete f;
+    return SC_OK;
+}
+
+sc_status sc_fno_param_count(const sc_fno* f, long long* n) {
+    if (!f || !n) {
+        set_error("sc_fno_param_count: null argument");
+        return SC_BADINPUT;
+    }
+    *n = f->lay.total;
+    return SC_OK;
+}
+
+sc_status sc_fno_params(sc_fno* f, void* dev_params, int direction, void* stream) {
+    if (!f || !dev_params) {
+        set_error("sc_fno_params: null argument");
+        return SC_BADINPUT;
+    }
+    Guard gd(f->device);
+    const size_t bytes = sizeof(float) * (size_t)f->lay.total;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (direction == 0)
+        SC_CUDA_TRY(cudaMemcpyAsync(dev_params, f->w, bytes, cudaMemcpyDeviceToDevice, st));
+    else
+        SC_CUDA_TRY(cudaMemcpyAsync(f->w, dev_params, bytes, cudaMemcpyDeviceToDevice, st));
+    return SC_OK;
+}
+
+sc_status sc_fno_forward(sc_fno* f, const float* maps, const float* lambdas, int batch, float* out, void* stream) {
+    SC_TRY(check_batch(f, batch));
+    if (!maps || !lambdas || !out) {
+        set_error("sc_fno_forward: null argument");
+        return SC_BADINPUT;
+    }
+    Guard gd(f->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    SC_TRY(forward(f, maps, lambdas, batch, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(out, f->pred, sizeof(float) * (size_t)batch * NOUT, cudaMemcpyDeviceToDevice, st));
+    return SC_OK;
+}
+
+sc_status sc_fno_loss_grad(sc_fno* f, const float* maps, const float* lambdas, const float* target, int batch,
+                           float* loss, float* grad, void* stream) {
+    SC_TRY(check_batch(f, batch));
+    if (!maps || !lambdas || !target) {
+        set_error("sc_fno_loss_grad: null argument");
+        return SC_BADINPUT;
+    }
+    Guard gd(f->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    SC_TRY(forward(f, maps, lambdas, batch, st));
+    SC_TRY(backward(f, target, batch, st));
+    if (loss) SC_CUDA_TRY(cudaMemcpyAsync(loss, f->loss, sizeof(float) * batch, cudaMemcpyDeviceToDevice, st));
+    if (grad)
+        SC_CUDA_TRY(cudaMemcpyAsync(grad, f->g, sizeof(float) * (size_t)f->lay.total, cudaMemcpyDeviceToDevice, st));
+    return SC_OK;
+}
+
+sc_status sc_fno_train_step(sc_fno* f, const float* maps, const float* lambdas, const float* target, int batch,
+                            float lr, float* loss, void* stream) {
+    SC_TRY(sc_fno_loss_grad(f, maps, lambdas, target, batch, loss, nullptr, stream));
+    cudaStream_t st = (cudaStream_t)stream;
+    f->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)f->step), c2 = 1.f - std::pow(b2, (float)f->step);
+    adam_kernel<<<blocks(f->lay.total), 256, 0, st>>>(f->w, f->g, f->m, f->v, f->lay.total, lr, b1, b2, 1e-8f, c1, c2);
+    count_launch();
+    SC_CHECK_LAUNCH("fno adam");
+    return SC_OK;
+}
+
+}  // extern "C"
