@@ -278,7 +278,9 @@ sc_status sc_gpu_cw_evaluate(void* E_xy, void* E_xz, void* E_yz, float x_start, 
  * column-major order index of sc_volume_solve's x, real and imaginary
  * interleaved).  No reference counterpart: the reference has no learned path;
  * the plain solve generates its training data, is its fallback, and measures
- * its error.  Width 64, 4 spectral layers, 16 x 16 modes; every linear map is
+ * its error.  Inputs per pixel: n, the scaled wavelength, the coordinates and
+ * the thin-element slab phase 2 pi n (1 um) / lambda as cos and sin (the
+ * workload's slab is 1 um).  Width 64, 4 spectral layers, 16 x 16 modes; every linear map is
  * a BF16 tensor-core GEMM with FP32 accumulation; training is Adam on FP32
  * master weights.  All buffers are device pointers; batch <= max_batch. */
 typedef struct sc_fno sc_fno;

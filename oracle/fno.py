@@ -16,7 +16,8 @@ from scipy.special import erf
 G = 64
 NP = G * G
 W = 64
-CIN = 4
+CIN = 6
+SLAB_UM = 1.0
 L = 4
 MX = MY = 16
 NM = 2 * MX * MY
@@ -133,6 +134,12 @@ class Net:
         p = np.arange(NP)
         inp[:, 2] = (p // G).astype(np.float32) / np.float32(63)
         inp[:, 3] = (p % G).astype(np.float32) / np.float32(63)
+        # thin-element phase of the slab, in turns reduced to [0, 1) in float32
+        turns = (np.asarray(maps, np.float32).reshape(B, NP) * np.float32(SLAB_UM)
+                 / np.asarray(lam, np.float32)[:, None]).astype(np.float32)
+        fr = (turns - np.floor(turns)).astype(np.float32)
+        inp[:, 4] = np.cos(2 * np.pi * fr.astype(np.float64)).astype(np.float32)
+        inp[:, 5] = np.sin(2 * np.pi * fr.astype(np.float64)).astype(np.float32)
         c["in"] = inp
         P = self.par(Ly.P, (W, CIN))
         v = np.stack([self.mm(P, inp[b]) for b in range(B)]) + self.par(Ly.bP, (W,))[None, :, None]

@@ -4,7 +4,10 @@
 // its training data, its fallback and the judge of its error.
 //
 // Network (width W = 64, 4 spectral layers, 16 x 16 retained modes):
-//   in  = [n(x, y), (lambda - 0.6) / 0.2, x / 63, y / 63]            4 x 64 x 64
+//   in  = [n(x, y), (lambda - 0.6) / 0.2, x / 63, y / 63,
+//          cos phi, sin phi], phi = 2 pi n d / lambda                   6 x 64 x 64
+//         (phi is the thin-element phase through the d = 1 um slab: its
+//         mean over the cell is the zero-order transmission to first order)
 //   v0  = P in + bP                                                   lift
 //   u_l = W_l v_l + b_l + Re IDFT(M_l . DFT(v_l)),  v_{l+1} = GELU(u_l)
 //         (no GELU after the last layer); DFT keeps kx in [-16, 16),
@@ -35,7 +38,8 @@ namespace fno {
 constexpr int G = 64;                 // grid side
 constexpr int NP = G * G;             // pixels
 constexpr int W = 64;                 // width
-constexpr int CIN = 4;                // input channels
+constexpr int CIN = 6;                // input channels
+constexpr float SLAB_UM = 1.0f;       // slab thickness of the workload (um)
 constexpr int L = 4;                  // spectral layers
 constexpr int MX = 16, MY = 16;       // retained modes: kx in [-MX, MX), ky in [0, MY)
 constexpr int NM = 2 * MX * MY;       // 512 complex modes
@@ -201,17 +205,25 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.f + erff(x * 0.70710678f)) + x * 0.39894228f * expf(-0.5f * x * x);
 }
 
-// in[b] = [map, (lambda - 0.6) / 0.2, x / 63, y / 63]
+// in[b] = [map, (lambda - 0.6) / 0.2, x / 63, y / 63, cos phi, sin phi]
 __global__ void input_kernel(const float* __restrict__ maps, const float* __restrict__ lam, int Bn,
                              float* __restrict__ in) {
     const long long tot = (long long)Bn * NP;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(t / NP), p = (int)(t % NP);
         float* o = in + (long long)b * CIN * NP;
-        o[p] = maps[t];
+        const float n = maps[t];
+        o[p] = n;
         o[NP + p] = (lam[b] - 0.6f) / 0.2f;
         o[2 * NP + p] = (float)(p / G) / 63.f;
         o[3 * NP + p] = (float)(p % G) / 63.f;
+        // phase in turns, reduced before the trigonometric call
+        const float turns = n * SLAB_UM / lam[b];
+        const float fr = turns - floorf(turns);
+        float sv, cv;
+        sincospif(2.f * fr, &sv, &cv);
+        o[4 * NP + p] = cv;
+        o[5 * NP + p] = sv;
     }
 }
 
