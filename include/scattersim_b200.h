@@ -194,6 +194,14 @@ sc_status sc_sweep_solve(sc_context* ctx, int count, const sc_volume_params* par
                          const void* const* samples, const int* Z, const int* S1, const int* S2,
                          void* const* x, int precision, int* status, void* stream);
 
+/* Precision of the products in later sc_volume_solve calls on this context,
+ * with the codes of sc_sweep_solve: SC_SWEEP_FP64 (the default: the
+ * reference's FP64 arithmetic), SC_SWEEP_MIXED or SC_SWEEP_SLICES(s) for the
+ * transfer-chain, boundary-block and Pz products on the int8 tensor cores.
+ * The FFT, the assembly, Omega = B C, the eigensolve, the eigenvectors and all
+ * LU factorisations stay FP64.  No reference counterpart. */
+sc_status sc_volume_precision(sc_context* ctx, int precision);
+
 /* Device milliseconds of the last sc_volume_solve on this context:
  * [fft, assemble, eig, chain, boundary, interior, qr-kernel, total];
  * after sc_sweep_solve: [fft, assemble, layer factors, chain, boundary, -, -, total]. */

@@ -87,6 +87,7 @@ _SIGS = {
     "sc_fno_loss_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "sc_fno_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p,
                                   c_void_p]),
+    "sc_volume_precision": (c_int, [c_void_p, c_int]),
     "sc_volume_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_void_p, c_int, c_int, c_int, c_void_p,
                                 c_void_p, c_void_p, c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_stage_ms": (c_int, [c_void_p, POINTER(c_double)]),

@@ -15,6 +15,9 @@ Cases (seeded synthetic samples, see samples.py):
   sweep_plain [n]  the same instances, one per-instance solve each
     (sweep cases accept --choices-out FILE to save the GEMM autotuner's table
      and --choices-in FILE to replay one, e.g. under a profiler)
+  volume31      the sphere volume at 31x31 orders (M = 961, 3844 x 3844 layer
+                matrices), solved in FP64 and in mixed precision; prints times
+                and the mixed path's error per stage against the FP64 path
   gemm          batched complex GEMM throughput at the shapes of the solves
   gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
                 twice each (the profiling case of the tcgen05 MMA kernel)
@@ -55,6 +58,8 @@ def main(argv):
         return 0
     if name == "gemm":
         return gemm_case()
+    if name == "volume31":
+        return volume31_case()
     if name == "gemm_int8":
         return gemm_int8_case()
     if name in ("sweep", "sweep_plain", "sweep_mixed"):
@@ -115,6 +120,55 @@ def gemm_case():
             tf = 8.0 * m * n * k * batch / (ms * 1e-3) / 1e12
             err = (C[0] - ref).abs().max().item() / ref.abs().max().item()
             print(f"   int8 x{slices}: {ms:.3f} ms, {tf:.1f} FP64-equivalent TFLOP/s, err {err:.1e}")
+    ctx.close()
+    return 0
+
+
+def volume31_case(N=64):
+    """Mixed precision at 31x31 orders, error per stage against the FP64 path."""
+    import json
+    import time
+    import numpy as np
+    import torch
+    from . import samples, solver
+    from ._lib import SC_SWEEP_FP64, SC_SWEEP_MIXED
+    smp = samples.sphere_volume(0)
+    kw = dict(lambda_=0.6, size=(20.0, 20.0, 8.0), coef=(31, 31), direction=D10, ex=(1.0, 0.0), ey=(0.0, 0.0))
+    p = solver.make_params(**kw)
+    d = torch.from_numpy(smp).cuda()
+    ctx = solver.Context(0)
+    # x-z slice through the volume centre: 6 um of z around the slab, 20 um of x
+    i = np.arange(N)
+    zz, xx = np.meshgrid(-6.0 + 12.0 * i / (N - 1), 20.0 * i / (N - 1), indexing="ij")
+    pts = torch.from_numpy(np.stack([xx.ravel(), np.full(N * N, 10.0), zz.ravel()], -1)).cuda()
+    out = {}
+    sols = {}
+    for name, prec in (("fp64", SC_SWEEP_FP64), ("mixed", SC_SWEEP_MIXED)):
+        ctx.set_precision(prec)
+        solver.solve(ctx, p, d)              # warm-up (allocations, GEMM autotuning)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol = solver.solve(ctx, p, d)
+        torch.cuda.synchronize()
+        out[f"{name}_solve_s"] = time.perf_counter() - t0
+        out[f"{name}_stage_ms"] = {k: round(v, 1) for k, v in ctx.stage_ms().items()}
+        wt = solver.waves(ctx, p, sol)
+        E64 = solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, pts, precision=0)
+        E32 = solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, pts, precision=1)
+        sols[name] = (sol.x.cpu().numpy(), sol.Qc.cpu().numpy(), sol.Qh.cpu().numpy(), E64.cpu().numpy(),
+                      E32.cpu().numpy())
+        del wt
+    ctx.set_precision(SC_SWEEP_FP64)
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    f, m = sols["fp64"], sols["mixed"]
+    out["err_vs_fp64"] = {"R/T x": rel(m[0], f[0]), "interior Qc": rel(m[1], f[1]), "interior Qh": rel(m[2], f[2]),
+                          "field, FP64 evaluator": rel(m[3], f[3]),
+                          "field, FP32 evaluator (FP64 phase reduction)": rel(m[4], f[3]),
+                          "FP32 evaluator alone on the FP64 waves": rel(f[4], f[3])}
+    print(json.dumps(out))
     ctx.close()
     return 0
 

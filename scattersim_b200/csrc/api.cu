@@ -33,6 +33,7 @@ sc_status cuda_status(cudaError_t e, const char* where) {
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 uint64_t launch_total() { return g_launches.load(); }
 
+sc_status set_volume_precision(sc_context* ctx, int precision);
 sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params, const void* const* samples,
                       const int* Zs, const int* S1s, const int* S2s, void* const* x_out, int precision,
                       int* status, cudaStream_t st);
@@ -409,6 +410,14 @@ sc_status sc_gemm_choices_set(sc_context* ctx, const int* rec, int count) {
         ctx->ws.gemm_choice[std::make_tuple(r[0], r[1], r[2], r[3], r[4])] = r[5];
     }
     return SC_OK;
+}
+
+sc_status sc_volume_precision(sc_context* ctx, int precision) {
+    if (!ctx) {
+        set_error("sc_volume_precision: null context");
+        return SC_BADINPUT;
+    }
+    return set_volume_precision(ctx, precision);
 }
 
 sc_status sc_volume_stage_ms(const sc_context* ctx, double* ms8) {

@@ -12,6 +12,7 @@ struct sc_context {
     cudaEvent_t ev[8] = {};
     double stage_ms[8] = {};   // fft assemble eig chain boundary interior | qr | total
     uint64_t launches_at_create = 0;
+    int precision = 0;   // SC_SWEEP_* code for the products of sc_volume_solve (sc_volume_precision)
 };
 
 namespace sc {

@@ -203,7 +203,54 @@ sc_status upload(cudaStream_t st, T* dst, const std::vector<T>& src) {
     return SC_OK;
 }
 
+// slices / forcing of a precision code (SC_SWEEP_FP64, _MIXED, _SLICES(s))
+bool precision_slices(int precision, int* slices, bool* force) {
+    *force = false;
+    if (precision == SC_SWEEP_FP64) *slices = 0;
+    else if (precision == SC_SWEEP_MIXED) *slices = 7;
+    else if ((precision & ~0xFF) == 0x100 && (precision & 0xFF) >= 1 && (precision & 0xFF) <= 7) {
+        *slices = precision & 0xFF;
+        *force = true;
+    } else
+        return false;
+    return true;
+}
+
+// C = A B (alpha 1, beta 0), strided batch: the FP64 tile when the engine has
+// no digit slices (the reference-precision path), else the engine
+sc_status product(cudaStream_t st, const GemmEngine& eng, int m, int n, int k, const double2* A, int lda, long long sA,
+                  const double2* B, int ldb, long long sB, double2* C, int ldc, long long sC, int batch) {
+    if (eng.slices == 0)
+        return zgemm(st, m, n, k, make_double2(1.0, 0.0), A, lda, sA, B, ldb, sB, make_double2(0.0, 0.0), C, ldc, sC,
+                     batch);
+    GemmArgs g;
+    g.m = m;
+    g.n = n;
+    g.k = k;
+    g.A = A;
+    g.lda = lda;
+    g.sA = sA;
+    g.B = B;
+    g.ldb = ldb;
+    g.sB = sB;
+    g.C = C;
+    g.ldc = ldc;
+    g.sC = sC;
+    return eng.run(st, g, batch);
+}
+
 }  // namespace
+
+sc_status set_volume_precision(sc_context* ctx, int precision) {
+    int sl;
+    bool force;
+    if (!precision_slices(precision, &sl, &force)) {
+        set_error("sc_volume_precision: unknown precision %d", precision);
+        return SC_BADINPUT;
+    }
+    ctx->precision = precision;
+    return SC_OK;
+}
 
 // ---------------------------------------------------------------- the plan
 sc_status make_plan(const sc_volume_params* p, int Z, int S1, int S2, VolumePlan* plan) {
@@ -347,6 +394,16 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     Workspace& ws = ctx->ws;
     for (int i = 0; i < 7; ++i)
         if (!ctx->ev[i]) SC_CUDA_TRY(cudaEventCreate(&ctx->ev[i]));
+    // products of the transfer chain, the boundary block and Pz: FP64 tiles, or
+    // the int8 engine under a mixed precision setting (the FFT, assembly,
+    // Omega, the eigensolve, the eigenvectors and every LU stay FP64)
+    GemmEngine eng;
+    precision_slices(ctx->precision, &eng.slices, &eng.force_int8);
+    eng.ws = &ws;
+    if (eng.slices) {
+        SC_TRY(ws.get(&eng.err, 1, WS_OZ_ERR, st));
+        SC_CUDA_TRY(cudaMemsetAsync(eng.err, 0, sizeof(int), st));
+    }
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
 
     // small host-built arrays: lattice, S vectors, EF, z planes
@@ -464,8 +521,8 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
                 scale_rows_batched_kernel<<<g, 256, 0, st>>>(Inv + i0 * s4, s4, cG + (long long)i0 * n4, n4, n4,
                                                             n4, scaled, s4);
                 count_launch();
-                SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), V + i0 * s4, n4, s4, scaled, n4, s4,
-                             make_double2(0.0, 0.0), tree + i0 * s4, n4, s4, cnt));
+                SC_TRY(product(st, eng, n4, n4, n4, V + i0 * s4, n4, s4, scaled, n4, s4, tree + i0 * s4, n4, s4,
+                               cnt));
             }
         }
         // pairwise products M_{2j+1} M_{2j}, level by level (order preserved)
@@ -474,8 +531,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         int cnt = nt;
         while (cnt > 1) {
             const int pairs = cnt / 2;
-            SC_TRY(zgemm(st, n4, n4, n4, make_double2(1.0, 0.0), cur + s4, n4, 2 * s4, cur, n4, 2 * s4,
-                         make_double2(0.0, 0.0), nxt, n4, s4, pairs));
+            SC_TRY(product(st, eng, n4, n4, n4, cur + s4, n4, 2 * s4, cur, n4, 2 * s4, nxt, n4, s4, pairs));
             if (cnt & 1)
                 SC_CUDA_TRY(cudaMemcpyAsync(nxt + pairs * s4, cur + (cnt - 1) * s4, sizeof(double2) * s4,
                                             cudaMemcpyDeviceToDevice, st));
@@ -502,8 +558,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, dG, n4, n4, n4, X, s4);
     count_launch();
     SC_TRY(boundary_system(st, MF, svec, 0, d_kz0, A6, 0, b6, 0, 1));
-    SC_TRY(zgemm(st, n4, 3 * MF, n4, make_double2(1.0, 0.0), X, n4, s4, F, n4, 0, make_double2(0.0, 0.0),
-                 A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0, 1));
+    SC_TRY(product(st, eng, n4, 3 * MF, n4, X, n4, s4, F, n4, 0, A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0, 1));
     SC_TRY(getrf(st, A6, n6, 0, n6, 1, piv6, dinfo + Z));
     SC_TRY(getrs(st, A6, n6, 0, n6, piv6, b6, n6, 0, 1, 1));
     if (x_out) SC_CUDA_TRY(cudaMemcpyAsync(x_out, b6, sizeof(double2) * n6, cudaMemcpyDeviceToDevice, st));
@@ -546,10 +601,10 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
             dim3 g(grid_for((long long)MF * MF), Z);
             kp_kernel<<<g, 256, 0, st>>>(Nif, Mx, My, k, KP);
             count_launch();
-            SC_TRY(zgemm(st, MF, n2, MF, make_double2(1.0, 0.0), KP, MF, (long long)MF * MF, Gc, MF,
-                         (long long)MF * n2, make_double2(0.0, 0.0), Qc + n2, 3 * MF, sq, Z));
-            SC_TRY(zgemm(st, MF, n2, MF, make_double2(1.0, 0.0), KP, MF, (long long)MF * MF, Gh, MF,
-                         (long long)MF * n2, make_double2(0.0, 0.0), Qh + n2, 3 * MF, sq, Z));
+            SC_TRY(product(st, eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gc, MF, (long long)MF * n2, Qc + n2,
+                           3 * MF, sq, Z));
+            SC_TRY(product(st, eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gh, MF, (long long)MF * n2, Qh + n2,
+                           3 * MF, sq, Z));
         } else {
             for (int z = 0; z < Z; ++z) {
                 SC_CUDA_TRY(cudaMemset2DAsync(Qc + z * sq + n2, sizeof(double2) * 3 * MF, 0, sizeof(double2) * MF,
@@ -577,6 +632,14 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         ctx->stage_ms[6] = ms;
         SC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]));
         ctx->stage_ms[7] = ms;
+    }
+    if (eng.slices) {
+        int herr = 0;
+        SC_CUDA_TRY(cudaMemcpy(&herr, eng.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) {
+            set_error("volume solve: tensor-core pipeline wait timed out (stage %d)", herr);
+            return SC_CUDA_ERROR;
+        }
     }
     int first = 0;
     for (int i = 0; i < Z && !first; ++i) first = hinfo[i];

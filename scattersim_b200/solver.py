@@ -64,6 +64,10 @@ class Context:
         keys = ("sweeps", "shifts", "chase", "far_right", "far_rows", "small", "unused", "total")
         return [dict(zip(keys, out[8 * i:8 * i + 8])) for i in range(count)]
 
+    def set_precision(self, precision: int):
+        """Precision code (SC_SWEEP_*) of the products of later solve() calls."""
+        check(self.lib.sc_volume_precision(self.handle, int(precision)))
+
     def kernel_timing(self, on: bool = True):
         """Start (clearing the record) or stop per-launch timing of the engine's GEMM kernels."""
         check(self.lib.sc_kernel_timing(self.handle, int(on)))

@@ -145,3 +145,17 @@ def test_energy_balance(ctx):
     R = (np.abs(x[0:3 * MF].reshape(3, MF)) ** 2).sum(0) @ Sz0.real
     T = (np.abs(x[3 * MF:].reshape(3, MF)) ** 2).sum(0) @ Sz1.real
     assert abs(R + T - 1.0) < 1e-10
+
+
+def test_mixed_precision_solve_matches_oracle(ctx):
+    """Transfer-chain, boundary and Pz products on the int8 tensor cores (7 digit
+    slices, forced): R/T and fields within 1e-8 of the FP64 oracle."""
+    from scattersim_b200 import _lib
+    smp = samples.sphere_volume(2, nxy=32, nz=6, size=(20.0, 20.0, 8.0))
+    kw = dict(lambda_=0.6, size=(20, 20, 8), coef=(7, 7),
+              direction=(np.sin(np.radians(10)), 0, np.cos(np.radians(10))), ex=(1, 0), ey=(0, 0))
+    ctx.set_precision(_lib.SC_SWEEP_SLICES(7))
+    try:
+        run_case(ctx, smp, kw, tol=1e-8)
+    finally:
+        ctx.set_precision(_lib.SC_SWEEP_FP64)
