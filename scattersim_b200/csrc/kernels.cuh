@@ -219,6 +219,14 @@ sc_status boundary_f3(cudaStream_t st, int MF, const double2* svec, long long sv
                       int count);
 sc_status boundary_system(cudaStream_t st, int MF, const double2* svec, long long sv_stride, const double* kz0,
                           double2* A6, long long sA, double2* b6, long long sb, int count);
+// the boundary system with R eliminated order by order: 3MF x 3MF in T (needs
+// Sz0 != 0 at every order), and x = [R; T] recovered from its solution
+sc_status boundary_reduced(cudaStream_t st, int MF, const double2* svec, long long sv_stride, const double* kz0,
+                           const double2* const* Y, int ldy, double2* A3, long long sA, double2* b3, long long sb,
+                           int count);
+sc_status boundary_recover(cudaStream_t st, int MF, const double2* svec, long long sv_stride, const double* kz0,
+                           const double2* const* Y, int ldy, const double2* T, long long sT, double2* const* x,
+                           int count);
 sc_status copy_blocks(cudaStream_t st, int rows, int cols, const double2* const* src, int lds, double2* const* dst,
                       int ldd, int count);
 

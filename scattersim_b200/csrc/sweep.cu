@@ -13,8 +13,11 @@
 //   4. the chain X <- T_l^-1 X from f3 up through the stack, one batched GEMM
 //      per depth step over all instances still inside their stack (instances
 //      are sorted by depth, so the active ones are a prefix);
-//   5. the 6M x 6M boundary systems (ScatterVolume.cpp:398-466) and their LU
-//      solves, batched over instances.
+//   5. the boundary systems (ScatterVolume.cpp:398-466), batched over
+//      instances: the reflected amplitudes enter only through per-order 3 x 3
+//      blocks, so they are eliminated order by order and a 3M x 3M system in
+//      the transmitted amplitudes is LU-solved (8x fewer flops than the 6M
+//      system, which remains the path when an order grazes the top interface).
 // A group larger than the memory budget is processed in chunks of instances.
 #include <algorithm>
 #include <cmath>
@@ -149,6 +152,11 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
         std::copy(P.Sz1.begin(), P.Sz1.end(), sv + 3 * MF);
         std::copy(P.EF.begin(), P.EF.end(), sv + 4 * MF);
     }
+    // the reduced boundary system divides by Sz0 at every order
+    bool reduced = true;
+    for (int a = 0; a < nI && reduced; ++a)
+        for (const cplx& z : items[a]->plan.Sz0)
+            if (std::abs(z) < 1e-9) reduced = false;
     std::vector<const void*> hptr(nptr);
     for (int j = 0; j < maxZ; ++j) {
         const void** row = hptr.data() + (size_t)j * nI * 3;
@@ -226,15 +234,27 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
         SC_TRY(eng.run(st, g, act));
     }
     SC_CUDA_TRY(cudaEventRecord(ev[4], st));
-    // 5. boundary systems and their solves
+    // 5. boundary systems and their solves: with R eliminated order by order
+    // (3MF unknowns) when no order grazes the top interface, else the full
+    // 6MF system of ScatterVolume.cpp:398-466
     void** tl = dptr + (size_t)maxZ * nI * 3;
-    SC_TRY(copy_blocks(st, n4, 3 * MF, reinterpret_cast<const double2* const*>(tl), n4,
-                       reinterpret_cast<double2* const*>(tl + nI), n6, nI));
-    SC_TRY(boundary_system(st, MF, b.svec, 7LL * MF, b.kz0, b.A6, s6, b.b6, n6, nI));
-    SC_TRY(getrf(st, b.A6, n6, s6, n6, nI, b.piv, b.info));
-    SC_TRY(getrs(st, b.A6, n6, s6, n6, b.piv, b.b6, n6, n6, 1, nI));
-    SC_TRY(copy_blocks(st, n6, 1, reinterpret_cast<const double2* const*>(tl + 2 * nI), n6,
-                       reinterpret_cast<double2* const*>(tl + 3 * nI), n6, nI));
+    const auto* Yp = reinterpret_cast<const double2* const*>(tl);
+    if (reduced) {
+        const int n3 = 3 * MF;
+        const long long s3 = (long long)n3 * n3;
+        SC_TRY(boundary_reduced(st, MF, b.svec, 7LL * MF, b.kz0, Yp, n4, b.A6, s3, b.b6, n3, nI));
+        SC_TRY(getrf(st, b.A6, n3, s3, n3, nI, b.piv, b.info));
+        SC_TRY(getrs(st, b.A6, n3, s3, n3, b.piv, b.b6, n3, n3, 1, nI));
+        SC_TRY(boundary_recover(st, MF, b.svec, 7LL * MF, b.kz0, Yp, n4, b.b6, n3,
+                                reinterpret_cast<double2* const*>(tl + 3 * nI), nI));
+    } else {
+        SC_TRY(copy_blocks(st, n4, 3 * MF, Yp, n4, reinterpret_cast<double2* const*>(tl + nI), n6, nI));
+        SC_TRY(boundary_system(st, MF, b.svec, 7LL * MF, b.kz0, b.A6, s6, b.b6, n6, nI));
+        SC_TRY(getrf(st, b.A6, n6, s6, n6, nI, b.piv, b.info));
+        SC_TRY(getrs(st, b.A6, n6, s6, n6, b.piv, b.b6, n6, n6, 1, nI));
+        SC_TRY(copy_blocks(st, n6, 1, reinterpret_cast<const double2* const*>(tl + 2 * nI), n6,
+                           reinterpret_cast<double2* const*>(tl + 3 * nI), n6, nI));
+    }
     SC_CUDA_TRY(cudaEventRecord(ev[5], st));
     std::vector<int> hinfo(nI);
     SC_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), b.info, sizeof(int) * nI, cudaMemcpyDeviceToHost, st));
