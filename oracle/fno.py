@@ -2,7 +2,7 @@
 
 The reference has no learned component; this file is the oracle for the
 project's own Fourier neural operator (scattersim_b200/csrc/fno.cu): the same
-parameter layout, the same dense DFT operators, and the same arithmetic
+parameter layout, the same separable DFT operators, and the same arithmetic
 points -- every GEMM rounds its two operands to BF16 (round to nearest even)
 and accumulates in float64 here (float32 on the GPU), and every stored
 intermediate is float32.  With ``bf16=False`` the network runs in float64
@@ -67,32 +67,37 @@ def kx_of(r):
 
 
 def operators():
-    """F (NP x NF), Gi (NF x NP), R (NP x 2 NORD) as in fno.cu::build_operators."""
-    x = np.arange(G)[:, None]
-    y = np.arange(G)[None, :]
-    F = np.zeros((NP, NF))
-    Gi = np.zeros((NF, NP))
-    R = np.zeros((NP, 2 * NORD))
+    """Separable DFT operators and the readout, as fno.cu::build_operators.
+
+    Fy (64 x 32), Ex (64 x 64), Er (64 x 64), Ei (64 x 64), Gy (32 x 64), R (NP x 2 NORD).
+    """
     tp = 2 * np.pi / G
-    for r in range(2 * MX):
-        for ky in range(MY):
-            md = r * MY + ky
-            ph = ((kx_of(r) * x + ky * y) % G + G) % G
-            th = (tp * ph).ravel()
-            c, s = np.cos(th), np.sin(th)
-            F[:, md] = c
-            F[:, NM + md] = -s
-            cw = (1.0 if ky == 0 else 2.0) / NP
-            Gi[md] = cw * c
-            Gi[NM + md] = -cw * s
+
+    def trig(ph):
+        th = tp * ((np.asarray(ph) % G + G) % G)
+        return np.cos(th), np.sin(th)
+    y = np.arange(G)
+    ky = np.arange(MY)
+    c, s_ = trig(np.outer(y, ky))                       # (y, ky)
+    Fy = np.concatenate([c, -s_], axis=1)
+    cw = np.where(ky == 0, 1.0, 2.0)[:, None] / NP
+    Gy = np.concatenate([cw * c.T, -cw * s_.T], axis=0)   # (32, y)
+    kx = np.array([kx_of(r) for r in range(2 * MX)])
+    x = np.arange(G)
+    c, s_ = trig(np.outer(kx, x))                         # (r, x)
+    Ex = np.concatenate([c, s_], axis=0)                  # (64 rows, x)
+    Er = np.concatenate([c.T, -s_.T], axis=1)             # (x, 64)
+    Ei = np.concatenate([s_.T, c.T], axis=1)
+    R = np.zeros((NP, 2 * NORD))
+    xx = np.repeat(np.arange(G), G)
+    yy = np.tile(np.arange(G), G)
     for j in range(NORD):
         qq = j % NO - NO // 2
         pp = j // NO - NO // 2
-        ph = ((pp * x + qq * y) % G + G) % G
-        th = (tp * ph).ravel()
-        R[:, j] = np.cos(th) / NP
-        R[:, NORD + j] = np.sin(th) / NP
-    return F.astype(np.float32), Gi.astype(np.float32), R.astype(np.float32)
+        cc, ss = trig(pp * xx + qq * yy)
+        R[:, j] = cc / NP
+        R[:, NORD + j] = ss / NP
+    return tuple(a.astype(np.float32) for a in (Fy, Ex, Er, Ei, Gy, R))
 
 
 class Net:
@@ -100,11 +105,12 @@ class Net:
         self.lay = Layout()
         self.w = np.asarray(params, dtype=np.float32)
         self.q = bf16_ops
-        self.F, self.Gi, self.R = operators()
+        self.Fy, self.Ex, self.Er, self.Ei, self.Gy, self.R = operators()
         self.dt = np.float32 if bf16_ops else np.float64
         if not bf16_ops:
             self.w = self.w.astype(np.float64)
-            self.F, self.Gi, self.R = (a.astype(np.float64) for a in (self.F, self.Gi, self.R))
+            self.Fy, self.Ex, self.Er, self.Ei, self.Gy, self.R = (
+                a.astype(np.float64) for a in (self.Fy, self.Ex, self.Er, self.Ei, self.Gy, self.R))
 
     # a GEMM the way the GPU does it: BF16 operands, wide accumulation, stored as float32
     def mm(self, A, B):
@@ -112,6 +118,51 @@ class Net:
             out = bf16(A).astype(np.float64) @ bf16(B).astype(np.float64)
             return out.astype(np.float32)
         return A @ B
+
+    def bmm(self, A, B):
+        """Batched GEMM (broadcast leading dims), same arithmetic as mm."""
+        if self.q:
+            return np.matmul(bf16(A).astype(np.float64), bf16(B).astype(np.float64)).astype(np.float32)
+        return np.matmul(A, B)
+
+    def fwd_dft(self, v):
+        """v (B, W, NP) -> X (B, W, NF): along y, then x, combined (fno.cu)."""
+        B = v.shape[0]
+        A1 = self.mm(v.reshape(-1, G), self.Fy).reshape(B * W, G, 2 * MY)
+        U = self.bmm(self.Ex[None], A1)                                     # (nch, 64, 32)
+        X = np.zeros((B * W, NF), self.dt)
+        r, ky = np.divmod(np.arange(NM), MY)
+        X[:, :NM] = (U[:, r, ky] + U[:, 2 * MX + r, MY + ky]).astype(self.dt)
+        X[:, NM:] = (U[:, r, MY + ky] - U[:, 2 * MX + r, ky]).astype(self.dt)
+        return X.reshape(B, W, NF)
+
+    def inv_dft(self, Y):
+        """Y (B, W, NF) -> the spectral branch of u (B, W, NP)."""
+        B = Y.shape[0]
+        Yc = Y.reshape(B * W, G, MY)                                          # rows: [re r | im r]
+        Z = np.concatenate([self.bmm(self.Er[None], Yc), self.bmm(self.Ei[None], Yc)], axis=2)   # (nch, 64, 32)
+        return self.mm(Z.reshape(-1, 2 * MY), self.Gy).reshape(B, W, NP)
+
+    def fwd_dft_adj(self, dX):
+        """Adjoint of fwd_dft: dX (B, W, NF) -> dv (B, W, NP)."""
+        B = dX.shape[0]
+        dXc = dX.reshape(B * W, NF)
+        dU = np.zeros((B * W, G, 2 * MY), self.dt)
+        r, ky = np.divmod(np.arange(NM), MY)
+        dU[:, r, ky] = dXc[:, :NM]
+        dU[:, 2 * MX + r, MY + ky] = dXc[:, :NM]
+        dU[:, r, MY + ky] = dXc[:, NM:]
+        dU[:, 2 * MX + r, ky] = -dXc[:, NM:]
+        dA1 = self.bmm(self.Ex.T[None], dU)
+        return self.mm(dA1.reshape(-1, 2 * MY), self.Fy.T).reshape(B, W, NP)
+
+    def inv_dft_adj(self, du):
+        """Adjoint of inv_dft: du (B, W, NP) -> dY (B, W, NF)."""
+        B = du.shape[0]
+        dZ = self.mm(du.reshape(-1, G), self.Gy.T).reshape(B * W, G, 2 * MY)
+        dY = (self.bmm(self.Er.T[None], dZ[:, :, :MY]).astype(np.float64)
+              + self.bmm(self.Ei.T[None], dZ[:, :, MY:]).astype(np.float64)).astype(self.dt)
+        return dY.reshape(B, W, NF)
 
     def par(self, off, shape):
         n = int(np.prod(shape))
@@ -146,7 +197,7 @@ class Net:
         v = v.astype(self.dt)
         acts, pres, Xs = [v], [], []
         for l in range(L):
-            X = np.stack([self.mm(v[b], self.F) for b in range(B)])          # B x W x NF
+            X = self.fwd_dft(v)                                                   # B x W x NF
             Xs.append(X)
             Wr = self.par(Ly.SWr[l], (NM, W, W))
             Wi = self.par(Ly.SWi[l], (NM, W, W))
@@ -157,8 +208,8 @@ class Net:
                 Y[:, :, md] = (self.mm(a, Wr[md]).astype(np.float64) - self.mm(bm, Wi[md]).astype(np.float64)).astype(self.dt)
                 Y[:, :, NM + md] = (self.mm(a, Wi[md]).astype(np.float64) + self.mm(bm, Wr[md]).astype(np.float64)).astype(self.dt)
             Wl = self.par(Ly.Wl[l], (W, W))
-            u = np.stack([(self.mm(Wl, v[b]).astype(np.float64) + self.mm(Y[b], self.Gi).astype(np.float64))
-                          for b in range(B)]).astype(self.dt)
+            u = np.stack([self.mm(Wl, v[b]) for b in range(B)])
+            u = (u.astype(np.float64) + self.inv_dft(Y).astype(np.float64)).astype(self.dt)
             u = (u + self.par(Ly.bl[l], (W,))[None, :, None]).astype(self.dt)
             pres.append(u)
             v = self.gelu(u) if l < L - 1 else u
@@ -217,7 +268,7 @@ class Net:
             acc(Ly.Wl[l], sum(self.mm(du[b], vin[b].T).astype(np.float64) for b in range(B)))
             Wl = self.par(Ly.Wl[l], (W, W))
             dvn = np.stack([self.mm(Wl.T, du[b]) for b in range(B)])
-            dY = np.stack([self.mm(du[b], self.Gi.T) for b in range(B)])
+            dY = self.inv_dft_adj(du)
             X = c["Xs"][l]
             Xr, Xi = X[:, :, :NM], X[:, :, NM:]
             dYr, dYi = dY[:, :, :NM], dY[:, :, NM:]
@@ -235,7 +286,7 @@ class Net:
                 gWi[md] = -self.mm(xi.T, r).astype(np.float64) + self.mm(xr.T, i).astype(np.float64)
             acc(Ly.SWr[l], gWr)
             acc(Ly.SWi[l], gWi)
-            dv = (dvn.astype(np.float64) + np.stack([self.mm(dX[b], self.F.T) for b in range(B)]).astype(np.float64)).astype(self.dt)
+            dv = (dvn.astype(np.float64) + self.fwd_dft_adj(dX).astype(np.float64)).astype(self.dt)
         acc(Ly.P, sum(self.mm(dv[b], c["in"][b].T).astype(np.float64) for b in range(B)))
         acc(Ly.bP, dv.astype(np.float64).sum((0, 2)))
         return loss, g

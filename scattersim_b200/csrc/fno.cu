@@ -16,9 +16,9 @@
 //   h   = GELU(Q1 v4 + bQ1) (128 channels), o = Q2 h + bQ2 (12 channels)
 //   amplitudes of channel pair c: sum_xy (o_2c + i o_2c+1) e^-i theta / 4096
 //         at the 121 orders, theta = 2 pi (p x + q y) / 64, p, q in [-5, 5]
-// Every linear map (lift, pointwise, the forward and inverse DFT as dense
-// 4096 x 1024 operators, the per-mode mixing, projections, readout) is one
-// hand-written tensor-core GEMM: operands rounded to BF16 as they are staged,
+// Every linear map (lift, pointwise, the truncated DFT and its real inverse
+// as separable partial DFTs -- along y, then x; back along x, then y -- the
+// per-mode mixing, projections, readout) is one hand-written tensor-core GEMM: operands rounded to BF16 as they are staged,
 // mma.sync m16n8k16 with FP32 accumulation, FP32 in global memory, arbitrary
 // strides and batches.  Training: relative squared error per sample, Adam on
 // FP32 master weights.
@@ -44,11 +44,15 @@ constexpr int L = 4;                  // spectral layers
 constexpr int MX = 16, MY = 16;       // retained modes: kx in [-MX, MX), ky in [0, MY)
 constexpr int NM = 2 * MX * MY;       // 512 complex modes
 constexpr int NF = 2 * NM;            // 1024 real columns: [re | im]
+constexpr int SEP = G * 2 * MY;       // 2048: one channel after the y transform (64 x [re 16 | im 16])
 constexpr int HID = 128;              // projection hidden channels
 constexpr int COUT = 12;              // 6 complex output fields
 constexpr int NO = 11;                // orders per axis
 constexpr int NORD = NO * NO;         // 121
 constexpr int NOUT = 6 * NORD * 2;    // 1452 reals per sample
+// separable-transform operators, packed in one buffer
+constexpr int OP_FY = 0, OP_EX = OP_FY + G * 2 * MY, OP_ER = OP_EX + G * G, OP_EI = OP_ER + G * G,
+              OP_GY = OP_EI + G * G, OP_TOTAL = OP_GY + 2 * MY * G;
 
 // ------------------------------------------------------------------ BF16 GEMM
 // C_b[m, n] = alpha * sum_k A_b[m, k] B_b[k, n] + beta * C_b[m, n], element
@@ -245,12 +249,15 @@ __global__ void gelu_back_kernel(float* __restrict__ g, const float* __restrict_
         g[t] *= gelu_grad(pre[t]);
 }
 
-// db[c] += sum_{b, p} g[b][c][p]  (one CTA per channel, fixed order)
-__global__ void bias_grad_kernel(const float* __restrict__ g, int C, int Bn, float* __restrict__ db) {
+// bias gradient in two deterministic passes: partial[c][s] = sum over the
+// samples b = s, s + NSPL, ... and all pixels of g[b][c][p] (one CTA each),
+// then db[c] += sum_s partial[c][s] in order
+constexpr int NSPL = 32;
+__global__ void bias_grad_part_kernel(const float* __restrict__ g, int C, int Bn, float* __restrict__ part) {
     __shared__ float red[8];
-    const int c = blockIdx.x;
+    const int c = blockIdx.x, sp = blockIdx.y;
     float s = 0.f;
-    for (int b = 0; b < Bn; ++b)
+    for (int b = sp; b < Bn; b += NSPL)
         for (int p = threadIdx.x; p < NP; p += blockDim.x) s += g[((long long)b * C + c) * NP + p];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -258,8 +265,16 @@ __global__ void bias_grad_kernel(const float* __restrict__ g, int C, int Bn, flo
     if (threadIdx.x == 0) {
         float t = 0.f;
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
-        db[c] += t;
+        part[c * NSPL + sp] = t;
     }
+}
+
+__global__ void bias_grad_sum_kernel(const float* __restrict__ part, int C, float* __restrict__ db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    float t = 0.f;
+    for (int sp = 0; sp < NSPL; ++sp) t += part[c * NSPL + sp];
+    db[c] += t;
 }
 
 // out[i] += sum_b part[b][i]
@@ -296,6 +311,38 @@ __global__ void readout_back_kernel(const float* __restrict__ dpred, int Bn, flo
         pi[NORD + j] = d[0];
         pi[j] = d[1];
         pr[NORD + j] = -d[1];
+    }
+}
+
+// x transform output U ([q][channel][32]: rows q = [cos kx; sin kx], columns
+// [re ky | im ky] of the y transform) -> X (mode-major: X[md][channel] for the
+// real parts md < 512, X[512 + md][channel] for the imaginary parts, mode md =
+// r * 16 + ky):  Re = U[r][ky] + U[32+r][16+ky],  Im = U[r][16+ky] - U[32+r][ky]
+__global__ void xcombine_kernel(const float* __restrict__ U, long long nch, float* __restrict__ X) {
+    const long long tot = nch * NM;
+    const long long qs = nch * 2 * MY;   // stride of q in U
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long c = t % nch;
+        const int md = (int)(t / nch), r = md / MY, ky = md % MY;
+        const float* u = U + c * 2 * MY;
+        X[(long long)md * nch + c] = u[r * qs + ky] + u[(2 * MX + r) * qs + MY + ky];
+        X[(long long)(NM + md) * nch + c] = u[r * qs + MY + ky] - u[(2 * MX + r) * qs + ky];
+    }
+}
+
+// adjoint of xcombine_kernel
+__global__ void xcombine_back_kernel(const float* __restrict__ dX, long long nch, float* __restrict__ dU) {
+    const long long tot = nch * NM;
+    const long long qs = nch * 2 * MY;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long c = t % nch;
+        const int md = (int)(t / nch), r = md / MY, ky = md % MY;
+        float* u = dU + c * 2 * MY;
+        const float dr = dX[(long long)md * nch + c], di = dX[(long long)(NM + md) * nch + c];
+        u[r * qs + ky] = dr;
+        u[(2 * MX + r) * qs + MY + ky] = dr;
+        u[r * qs + MY + ky] = di;
+        u[(2 * MX + r) * qs + ky] = -di;
     }
 }
 
@@ -352,6 +399,13 @@ unsigned blocks(long long tot) {
     return (unsigned)b;
 }
 
+sc_status bias_grad(cudaStream_t st, const float* g, int C, int Bn, float* db, float* part) {
+    bias_grad_part_kernel<<<dim3(C, NSPL), 256, 0, st>>>(g, C, Bn, part);
+    bias_grad_sum_kernel<<<(C + 127) / 128, 128, 0, st>>>(part, C, db);
+    count_launch(2);
+    return SC_OK;
+}
+
 // ------------------------------------------------------------------ parameters
 struct Layout {
     long long P, bP, Wl[L], bl[L], SWr[L], SWi[L], Q1, bQ1, Q2, bQ2, total;
@@ -389,11 +443,12 @@ struct sc_fno {
     int max_batch = 0;
     Layout lay;
     float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // params, grads, Adam moments
-    float *F = nullptr, *Gi = nullptr, *R = nullptr;                 // DFT operators
+    float *ops = nullptr, *R = nullptr;                               // DFT operators
+    float *S1 = nullptr, *S2 = nullptr;                               // separable-transform scratch
     float *in = nullptr, *act[L + 1] = {}, *pre[L] = {}, *X[L] = {}, *Y = nullptr;
     float *hpre = nullptr, *h = nullptr, *o12 = nullptr, *P = nullptr, *pred = nullptr;
     float *dact = nullptr, *dv = nullptr, *dX = nullptr, *dY = nullptr, *dh = nullptr, *do12 = nullptr,
-          *dP = nullptr, *dpred = nullptr, *part = nullptr, *loss = nullptr;
+          *dP = nullptr, *dpred = nullptr, *part = nullptr, *loss = nullptr, *bpart = nullptr;
     long long step = 0;
 };
 
@@ -450,24 +505,40 @@ sc_status forward(sc_fno* f, const float* maps, const float* lam, int Bn, cudaSt
     count_launch();
     for (int l = 0; l < L; ++l) {
         float* vin = f->act[l];
-        // X_b (W x NF) = v_b (W x NP) F (NP x NF)
-        SC_TRY(gemm(st, mk(W, NF, NP, Bn, 1.f, 0.f, vin, NP, 1, sv, f->F, NF, 1, 0, f->X[l], NF, 1, (long long)W * NF)));
-        // per mode md: Y[b, o] = sum_i X[b, i] M[md][i][o] (complex, as four real products)
+        // truncated DFT: along y (batched over x: rows = channels, 64 y -> [re | im] 16),
+        // then along x (one GEMM: [cos; sin] (64 x 64) times x by (channel, 32)),
+        // combined into mode-major X
+        const long long nch = (long long)Bn * W;
+        SC_TRY(gemm(st, mk((int)nch, 2 * MY, G, G, 1.f, 0.f, vin, NP, 1, G, f->ops + OP_FY, 2 * MY, 1, 0, f->S1, 2 * MY,
+                           1, nch * 2 * MY)));
+        SC_TRY(gemm(st, mk(G, (int)(nch * 2 * MY), G, 1, 1.f, 0.f, f->ops + OP_EX, G, 1, 0, f->S1, nch * 2 * MY, 1, 0,
+                           f->S2, nch * 2 * MY, 1, 0)));
+        xcombine_kernel<<<blocks(nch * NM), 256, 0, st>>>(f->S2, nch, f->X[l]);
+        count_launch();
+        // per mode md: Y[md] (B x W) = X[md] (B x W) M[md] (W x W), complex as four real products
         const float* Xr = f->X[l];
-        const float* Xi = f->X[l] + NM;
+        const float* Xi = f->X[l] + NM * nch;
         const float* Wr = w + Ly.SWr[l];
         const float* Wi = w + Ly.SWi[l];
         float* Yr = f->Y;
-        float* Yi = f->Y + NM;
-        const long long sb = (long long)W * NF;
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, sb, NF, 1, Wr, W, 1, (long long)W * W, Yr, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 1.f, Xi, sb, NF, 1, Wi, W, 1, (long long)W * W, Yr, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, sb, NF, 1, Wi, W, 1, (long long)W * W, Yi, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, Xi, sb, NF, 1, Wr, W, 1, (long long)W * W, Yi, sb, NF, 1)));
+        float* Yi = f->Y + NM * nch;
+        const long long ww = (long long)W * W;
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, W, 1, nch, Wr, W, 1, ww, Yr, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 1.f, Xi, W, 1, nch, Wi, W, 1, ww, Yr, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, Xr, W, 1, nch, Wi, W, 1, ww, Yi, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, Xi, W, 1, nch, Wr, W, 1, ww, Yi, W, 1, nch)));
         // u_b = W_l v_b + Y_b G + b_l
         float* u = f->pre[l];
         SC_TRY(gemm(st, mk(W, NP, W, Bn, 1.f, 0.f, w + Ly.Wl[l], W, 1, 0, vin, NP, 1, sv, u, NP, 1, sv)));
-        SC_TRY(gemm(st, mk(W, NP, NF, Bn, 1.f, 1.f, f->Y, NF, 1, sb, f->Gi, NP, 1, 0, u, NP, 1, sv)));
+        // inverse: along x (Z[x][ky][channel] = [cos | -sin] Y and [sin | cos] Y,
+        // one GEMM each over (ky, channel)), then along y into u (batched over x,
+        // accumulated)
+        SC_TRY(gemm(st, mk(G, (int)(MY * nch), G, 1, 1.f, 0.f, f->ops + OP_ER, G, 1, 0, f->Y, MY * nch, 1, 0, f->S1,
+                           2 * MY * nch, 1, 0)));
+        SC_TRY(gemm(st, mk(G, (int)(MY * nch), G, 1, 1.f, 0.f, f->ops + OP_EI, G, 1, 0, f->Y, MY * nch, 1, 0,
+                           f->S1 + MY * nch, 2 * MY * nch, 1, 0)));
+        SC_TRY(gemm(st, mk((int)nch, G, 2 * MY, G, 1.f, 1.f, f->S1, 1, nch, 2 * MY * nch, f->ops + OP_GY, G, 1, 0, u,
+                           NP, 1, G)));
         const int act = (l < L - 1);
         bias_act_kernel<<<blocks((long long)Bn * sv), 256, 0, st>>>(u, w + Ly.bl[l], W, Bn, act, f->act[l + 1]);
         count_launch();
@@ -498,7 +569,6 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     const float* w = f->w;
     float* g = f->g;
     const long long sv = (long long)W * NP, sh = (long long)HID * NP, so = (long long)COUT * NP;
-    const long long sb = (long long)W * NF;
     SC_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(float) * Ly.total, st));
     loss_kernel<<<Bn, 256, 0, st>>>(f->pred, tgt, Bn, f->dpred, f->loss);
     readout_back_kernel<<<blocks((long long)Bn * 6 * NORD), 256, 0, st>>>(f->dpred, Bn, f->dP);
@@ -510,8 +580,8 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     SC_TRY(gemm(st, mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
                        (long long)COUT * HID)));
     batch_sum_kernel<<<blocks((long long)COUT * HID), 256, 0, st>>>(f->part, Bn, (long long)COUT * HID, g + Ly.Q2);
-    bias_grad_kernel<<<COUT, 256, 0, st>>>(f->do12, COUT, Bn, g + Ly.bQ2);
-    count_launch(2);
+    bias_grad(st, f->do12, COUT, Bn, g + Ly.bQ2, f->bpart);
+    count_launch();   // batch_sum_kernel
     // dh_b = Q2^T do12_b, through GELU
     SC_TRY(gemm(st, mk(HID, NP, COUT, Bn, 1.f, 0.f, w + Ly.Q2, 1, HID, 0, f->do12, NP, 1, so, f->dh, NP, 1, sh)));
     gelu_back_kernel<<<blocks((long long)Bn * sh), 256, 0, st>>>(f->dh, f->hpre, (long long)Bn * sh);
@@ -519,8 +589,8 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     SC_TRY(gemm(st, mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
                        (long long)HID * W)));
     batch_sum_kernel<<<blocks((long long)HID * W), 256, 0, st>>>(f->part, Bn, (long long)HID * W, g + Ly.Q1);
-    bias_grad_kernel<<<HID, 256, 0, st>>>(f->dh, HID, Bn, g + Ly.bQ1);
-    count_launch(2);
+    bias_grad(st, f->dh, HID, Bn, g + Ly.bQ1, f->bpart);
+    count_launch();   // batch_sum_kernel
     // dv4 = Q1^T dh
     SC_TRY(gemm(st, mk(W, NP, HID, Bn, 1.f, 0.f, w + Ly.Q1, 1, W, 0, f->dh, NP, 1, sh, f->dact, NP, 1, sv)));
     for (int l = L - 1; l >= 0; --l) {
@@ -530,8 +600,7 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
             gelu_back_kernel<<<blocks((long long)Bn * sv), 256, 0, st>>>(du, f->pre[l], (long long)Bn * sv);
             count_launch();
         }
-        bias_grad_kernel<<<W, 256, 0, st>>>(du, W, Bn, g + Ly.bl[l]);
-        count_launch();
+        bias_grad(st, du, W, Bn, g + Ly.bl[l], f->bpart);
         const float* vin = f->act[l];
         // W_l
         SC_TRY(gemm(st, mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1, (long long)W * W)));
@@ -539,38 +608,51 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
         count_launch();
         // dv_l = W_l^T du
         SC_TRY(gemm(st, mk(W, NP, W, Bn, 1.f, 0.f, w + Ly.Wl[l], 1, W, 0, du, NP, 1, sv, f->dv, NP, 1, sv)));
-        // dY_b = du_b G^T
-        SC_TRY(gemm(st, mk(W, NF, NP, Bn, 1.f, 0.f, du, NP, 1, sv, f->Gi, 1, NP, 0, f->dY, NF, 1, sb)));
+        // adjoint of the inverse transform: dZ[x][ky'][channel] = du Gy^T (batched over
+        // x), dY = Er^T dZr + Ei^T dZi (mode-major)
+        const long long nch = (long long)Bn * W;
+        SC_TRY(gemm(st, mk((int)nch, 2 * MY, G, G, 1.f, 0.f, du, NP, 1, G, f->ops + OP_GY, 1, G, 0, f->S1, 1, nch,
+                           2 * MY * nch)));
+        SC_TRY(gemm(st, mk(G, (int)(MY * nch), G, 1, 1.f, 0.f, f->ops + OP_ER, 1, G, 0, f->S1, 2 * MY * nch, 1, 0, f->dY,
+                           MY * nch, 1, 0)));
+        SC_TRY(gemm(st, mk(G, (int)(MY * nch), G, 1, 1.f, 1.f, f->ops + OP_EI, 1, G, 0, f->S1 + MY * nch, 2 * MY * nch,
+                           1, 0, f->dY, MY * nch, 1, 0)));
         // mode mixing: dX = dY M^H, dM = X^H dY (complex, per mode)
         const float* Xr = f->X[l];
-        const float* Xi = f->X[l] + NM;
+        const float* Xi = f->X[l] + NM * nch;
         const float* Wr = w + Ly.SWr[l];
         const float* Wi = w + Ly.SWi[l];
         const float* dYr = f->dY;
-        const float* dYi = f->dY + NM;
+        const float* dYi = f->dY + NM * nch;
         float* dXr = f->dX;
-        float* dXi = f->dX + NM;
+        float* dXi = f->dX + NM * nch;
         const long long ww = (long long)W * W;
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, dYr, sb, NF, 1, Wr, 1, W, ww, dXr, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, sb, NF, 1, Wi, 1, W, ww, dXr, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 0.f, dYr, sb, NF, 1, Wi, 1, W, ww, dXi, sb, NF, 1)));
-        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, sb, NF, 1, Wr, 1, W, ww, dXi, sb, NF, 1)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 0.f, dYr, W, 1, nch, Wr, 1, W, ww, dXr, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, W, 1, nch, Wi, 1, W, ww, dXr, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, -1.f, 0.f, dYr, W, 1, nch, Wi, 1, W, ww, dXi, W, 1, nch)));
+        SC_TRY(gemm(st, mk(Bn, W, W, NM, 1.f, 1.f, dYi, W, 1, nch, Wr, 1, W, ww, dXi, W, 1, nch)));
         float* gWr = g + Ly.SWr[l];
         float* gWi = g + Ly.SWi[l];
-        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 0.f, Xr, NF, sb, 1, dYr, sb, NF, 1, gWr, W, 1, ww)));
-        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xi, NF, sb, 1, dYi, sb, NF, 1, gWr, W, 1, ww)));
-        SC_TRY(gemm(st, mk(W, W, Bn, NM, -1.f, 0.f, Xi, NF, sb, 1, dYr, sb, NF, 1, gWi, W, 1, ww)));
-        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xr, NF, sb, 1, dYi, sb, NF, 1, gWi, W, 1, ww)));
-        // dv_l += dX_b F^T
-        SC_TRY(gemm(st, mk(W, NP, NF, Bn, 1.f, 1.f, f->dX, NF, 1, sb, f->F, 1, NF, 0, f->dv, NP, 1, sv)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 0.f, Xr, 1, W, nch, dYr, W, 1, nch, gWr, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xi, 1, W, nch, dYi, W, 1, nch, gWr, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, -1.f, 0.f, Xi, 1, W, nch, dYr, W, 1, nch, gWi, W, 1, ww)));
+        SC_TRY(gemm(st, mk(W, W, Bn, NM, 1.f, 1.f, Xr, 1, W, nch, dYi, W, 1, nch, gWi, W, 1, ww)));
+        // adjoint of the forward transform: dU from dX, dA1 = Ex^T dU (one GEMM),
+        // dv += dA1 Fy^T (batched over x)
+        xcombine_back_kernel<<<blocks(nch * NM), 256, 0, st>>>(f->dX, nch, f->S2);
+        count_launch();
+        SC_TRY(gemm(st, mk(G, (int)(nch * 2 * MY), G, 1, 1.f, 0.f, f->ops + OP_EX, 1, G, 0, f->S2, nch * 2 * MY, 1, 0,
+                           f->S1, nch * 2 * MY, 1, 0)));
+        SC_TRY(gemm(st, mk((int)nch, G, 2 * MY, G, 1.f, 1.f, f->S1, 2 * MY, 1, nch * 2 * MY, f->ops + OP_FY, 1, 2 * MY,
+                           0, f->dv, NP, 1, G)));
         std::swap(f->dact, f->dv);
     }
     // lift
     SC_TRY(gemm(st, mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part, CIN,
                        1, (long long)W * CIN)));
     batch_sum_kernel<<<blocks((long long)W * CIN), 256, 0, st>>>(f->part, Bn, (long long)W * CIN, g + Ly.P);
-    bias_grad_kernel<<<W, 256, 0, st>>>(f->dact, W, Bn, g + Ly.bP);
-    count_launch(2);
+    bias_grad(st, f->dact, W, Bn, g + Ly.bP, f->bpart);
+    count_launch();   // batch_sum_kernel
     SC_CHECK_LAUNCH("fno backward");
     return SC_OK;
 }
@@ -596,36 +678,50 @@ void init_params(const Layout& Ly, uint64_t seed, std::vector<float>& w) {
     unif(Ly.bQ2, COUT, 1.0 / std::sqrt((double)HID));
 }
 
-// dense DFT operators: F (NP x NF) = [cos | -sin] of the retained modes,
-// Gi (NF x NP) = [c cos; -c sin] / NP (real inverse of the half spectrum,
-// c = 1 for ky = 0 else 2), R (NP x 242) = [cos | sin] / NP at the orders
-void build_operators(std::vector<float>& F, std::vector<float>& Gi, std::vector<float>& R) {
-    F.assign((size_t)NP * NF, 0.f);
-    Gi.assign((size_t)NF * NP, 0.f);
+// separable DFT operators (phases reduced mod 64 before the trigonometric call):
+//   Fy (64 y x 32): [cos(2 pi ky y / 64) | -sin]                  forward along y
+//   Ex (64 x 64 x): rows q < 32 cos(2 pi kx(q) x / 64), q >= 32 sin  forward along x
+//   Er, Ei (64 x x 64): [cos | -sin], [sin | cos] of kx(k) x           inverse along x
+//   Gy (32 x 64 y): [c cos; -c sin] / 4096, c = 1 for ky = 0 else 2   real inverse along y
+// and R (NP x 242) = [cos | sin] / NP at the 121 orders (readout)
+void build_operators(std::vector<float>& ops, std::vector<float>& R) {
+    ops.assign(OP_TOTAL, 0.f);
     R.assign((size_t)NP * 2 * NORD, 0.f);
     const double tp = 2.0 * M_PI / G;
+    auto trig = [&](long long ph, double* c, double* s) {
+        const double th = tp * (double)(((ph % G) + G) % G);
+        *c = std::cos(th);
+        *s = std::sin(th);
+    };
+    double c, sn;
+    for (int y = 0; y < G; ++y)
+        for (int ky = 0; ky < MY; ++ky) {
+            trig((long long)ky * y, &c, &sn);
+            ops[OP_FY + y * 2 * MY + ky] = (float)c;
+            ops[OP_FY + y * 2 * MY + MY + ky] = (float)(-sn);
+            const double cw = (ky == 0 ? 1.0 : 2.0) / NP;
+            ops[OP_GY + ky * G + y] = (float)(cw * c);
+            ops[OP_GY + (MY + ky) * G + y] = (float)(-cw * sn);
+        }
+    for (int x = 0; x < G; ++x)
+        for (int r = 0; r < 2 * MX; ++r) {
+            trig((long long)kx_of(r) * x, &c, &sn);
+            ops[OP_EX + r * G + x] = (float)c;
+            ops[OP_EX + (2 * MX + r) * G + x] = (float)sn;
+            ops[OP_ER + x * G + r] = (float)c;
+            ops[OP_ER + x * G + 2 * MX + r] = (float)(-sn);
+            ops[OP_EI + x * G + r] = (float)sn;
+            ops[OP_EI + x * G + 2 * MX + r] = (float)c;
+        }
     for (int x = 0; x < G; ++x)
         for (int y = 0; y < G; ++y) {
             const int p = x * G + y;
-            for (int r = 0; r < 2 * MX; ++r)
-                for (int ky = 0; ky < MY; ++ky) {
-                    const int md = r * MY + ky;
-                    const long long ph = ((long long)kx_of(r) * x + (long long)ky * y) % G;
-                    const double th = tp * (double)((ph + G) % G);
-                    const double c = std::cos(th), s = std::sin(th);
-                    F[(size_t)p * NF + md] = (float)c;
-                    F[(size_t)p * NF + NM + md] = (float)(-s);
-                    const double cw = (ky == 0 ? 1.0 : 2.0) / NP;
-                    Gi[(size_t)md * NP + p] = (float)(cw * c);
-                    Gi[(size_t)(NM + md) * NP + p] = (float)(-cw * s);
-                }
             for (int j = 0; j < NORD; ++j) {
                 int pp, qq;
                 order_pq(j, &pp, &qq);
-                const long long ph = ((long long)pp * x + (long long)qq * y) % G;
-                const double th = tp * (double)((ph + G) % G);
-                R[(size_t)p * 2 * NORD + j] = (float)(std::cos(th) / NP);
-                R[(size_t)p * 2 * NORD + NORD + j] = (float)(std::sin(th) / NP);
+                trig((long long)pp * x + (long long)qq * y, &c, &sn);
+                R[(size_t)p * 2 * NORD + j] = (float)(c / NP);
+                R[(size_t)p * 2 * NORD + NORD + j] = (float)(sn / NP);
             }
         }
 }
@@ -673,8 +769,9 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->g, Ly.total);
     A(&f->m, Ly.total);
     A(&f->v, Ly.total);
-    A(&f->F, (long long)NP * NF);
-    A(&f->Gi, (long long)NF * NP);
+    A(&f->ops, OP_TOTAL);
+    A(&f->S1, B * W * SEP);
+    A(&f->S2, B * W * SEP);
     A(&f->R, (long long)NP * 2 * NORD);
     A(&f->in, B * CIN * NP);
     for (int l = 0; l <= L; ++l) A(&f->act[l], B * sv);
@@ -698,13 +795,13 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->dpred, B * NOUT);
     A(&f->part, B * (long long)HID * W);
     A(&f->loss, B);
+    A(&f->bpart, (long long)HID * NSPL);
     if (s == SC_OK) {
-        std::vector<float> w, F, Gi, R;
+        std::vector<float> w, ops, R;
         init_params(Ly, seed, w);
-        build_operators(F, Gi, R);
+        build_operators(ops, R);
         cudaError_t e = cudaMemcpy(f->w, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(f->F, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(f->Gi, Gi.data(), sizeof(float) * Gi.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(f->ops, ops.data(), sizeof(float) * ops.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(f->R, R.data(), sizeof(float) * R.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(f->m, 0, sizeof(float) * Ly.total);
         if (e == cudaSuccess) e = cudaMemset(f->v, 0, sizeof(float) * Ly.total);
@@ -721,8 +818,8 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
 sc_status sc_fno_destroy(sc_fno* f) {
     if (!f) return SC_OK;
     Guard gd(f->device);
-    float* ptrs[] = {f->w, f->g, f->m, f->v, f->F, f->Gi, f->R, f->in, f->Y, f->hpre, f->h, f->o12, f->P, f->pred,
-                     f->dact, f->dv, f->dX, f->dY, f->dh, f->do12, f->dP, f->dpred, f->part, f->loss};
+    float* ptrs[] = {f->w, f->g, f->m, f->v, f->ops, f->S1, f->S2, f->R, f->in, f->Y, f->hpre, f->h, f->o12, f->P, f->pred,
+                     f->dact, f->dv, f->dX, f->dY, f->dh, f->do12, f->dP, f->dpred, f->part, f->loss, f->bpart};
     for (float* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l <= L; ++l)
