@@ -18,6 +18,8 @@ Cases (seeded synthetic samples, see samples.py):
   volume31      the sphere volume at 31x31 orders (M = 961, 3844 x 3844 layer
                 matrices), solved in FP64 and in mixed precision; prints times
                 and the mixed path's error per stage against the FP64 path
+  fno_train     20 surrogate training steps (batch 64, random maps and targets):
+                samples/s and the launch mix of the network's kernels
   gemm          batched complex GEMM throughput at the shapes of the solves
   gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
                 twice each (the profiling case of the tcgen05 MMA kernel)
@@ -60,6 +62,8 @@ def main(argv):
         return gemm_case()
     if name == "volume31":
         return volume31_case()
+    if name == "fno_train":
+        return fno_train_case()
     if name == "gemm_int8":
         return gemm_int8_case()
     if name in ("sweep", "sweep_plain", "sweep_mixed"):
@@ -121,6 +125,28 @@ def gemm_case():
             err = (C[0] - ref).abs().max().item() / ref.abs().max().item()
             print(f"   int8 x{slices}: {ms:.3f} ms, {tf:.1f} FP64-equivalent TFLOP/s, err {err:.1e}")
     ctx.close()
+    return 0
+
+
+def fno_train_case(steps=20, batch=64):
+    import time
+    import numpy as np
+    import torch
+    from . import surrogate as sg
+    rng = np.random.default_rng(0)
+    sur = sg.Surrogate(0, max_batch=batch, seed=1)
+    maps = torch.from_numpy(rng.uniform(1.0, 1.6, (batch, 64, 64)).astype(np.float32)).cuda()
+    lams = torch.from_numpy(rng.uniform(0.4, 0.8, batch).astype(np.float32)).cuda()
+    tgt = torch.from_numpy(rng.standard_normal((batch, sg.NOUT)).astype(np.float32)).cuda()
+    sur.train_step(maps, lams, tgt, 1e-4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sur.train_step(maps, lams, tgt, 1e-4)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    print(f"fno_train: {steps * batch / dt:.0f} samples/s ({1e3 * dt / steps:.2f} ms per step of {batch})")
+    sur.close()
     return 0
 
 

@@ -72,6 +72,11 @@ constexpr int TM = 64, TN = 64, TK = 32, GT = 128, PADK = 8;
 
 __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
+// operand load modes: 0 scalar (any strides), 1 float4 along k (stride_k == 1),
+// 2 float4 along m / n (stride_m or stride_n == 1); the host picks a vector
+// mode only when the base is 16-byte aligned, the other stride is a multiple
+// of 4 and the contiguous extent is a multiple of 4
+template <int VA, int VB>
 __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
     __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PADK];
     __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PADK];
@@ -83,45 +88,100 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int gq = lane >> 2, tq = lane & 3;
-    const bool a_kfast = (g.sAk == 1), b_kfast = (g.sBk == 1);
     float ra[TM * TK / GT], rb[TN * TK / GT];
 
     auto load = [&](int k0) {
+        if constexpr (VA == 0) {
+            const bool kf = (g.sAk == 1);
 #pragma unroll
-        for (int i = 0; i < TM * TK / GT; ++i) {
-            const int e = tid + GT * i;
-            int r, kk;
-            if (a_kfast) { r = e / TK; kk = e % TK; }
-            else { r = e % TM; kk = e / TM; }
-            const int gm = m0 + r, gk = k0 + kk;
-            ra[i] = (gm < g.m && gk < g.k) ? A[gm * g.sAm + gk * g.sAk] : 0.f;
+            for (int i = 0; i < TM * TK / GT; ++i) {
+                const int e = tid + GT * i;
+                const int r = kf ? e / TK : e % TM, kk = kf ? e % TK : e / TM;
+                const int gm = m0 + r, gk = k0 + kk;
+                ra[i] = (gm < g.m && gk < g.k) ? A[gm * g.sAm + gk * g.sAk] : 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < TM * TK / GT / 4; ++i) {
+                const int e = tid + GT * i;
+                const int r = (VA == 1) ? e / (TK / 4) : (e % (TM / 4)) * 4;
+                const int kk = (VA == 1) ? (e % (TK / 4)) * 4 : e / (TM / 4);
+                const int gm = m0 + r, gk = k0 + kk;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gm < g.m && gk < g.k) v = *reinterpret_cast<const float4*>(A + gm * g.sAm + gk * g.sAk);
+                ra[4 * i] = v.x;
+                ra[4 * i + 1] = v.y;
+                ra[4 * i + 2] = v.z;
+                ra[4 * i + 3] = v.w;
+            }
         }
+        if constexpr (VB == 0) {
+            const bool kf = (g.sBk == 1);
 #pragma unroll
-        for (int i = 0; i < TN * TK / GT; ++i) {
-            const int e = tid + GT * i;
-            int c, kk;
-            if (b_kfast) { c = e / TK; kk = e % TK; }
-            else { c = e % TN; kk = e / TN; }
-            const int gn = n0 + c, gk = k0 + kk;
-            rb[i] = (gn < g.n && gk < g.k) ? B[gk * g.sBk + gn * g.sBn] : 0.f;
+            for (int i = 0; i < TN * TK / GT; ++i) {
+                const int e = tid + GT * i;
+                const int c = kf ? e / TK : e % TN, kk = kf ? e % TK : e / TN;
+                const int gn = n0 + c, gk = k0 + kk;
+                rb[i] = (gn < g.n && gk < g.k) ? B[gk * g.sBk + gn * g.sBn] : 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < TN * TK / GT / 4; ++i) {
+                const int e = tid + GT * i;
+                const int c = (VB == 1) ? e / (TK / 4) : (e % (TN / 4)) * 4;
+                const int kk = (VB == 1) ? (e % (TK / 4)) * 4 : e / (TN / 4);
+                const int gn = n0 + c, gk = k0 + kk;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gn < g.n && gk < g.k) v = *reinterpret_cast<const float4*>(B + gk * g.sBk + gn * g.sBn);
+                rb[4 * i] = v.x;
+                rb[4 * i + 1] = v.y;
+                rb[4 * i + 2] = v.z;
+                rb[4 * i + 3] = v.w;
+            }
         }
     };
     auto store = [&]() {
+        if constexpr (VA == 0) {
+            const bool kf = (g.sAk == 1);
 #pragma unroll
-        for (int i = 0; i < TM * TK / GT; ++i) {
-            const int e = tid + GT * i;
-            int r, kk;
-            if (a_kfast) { r = e / TK; kk = e % TK; }
-            else { r = e % TM; kk = e / TM; }
-            As[r][kk] = __float2bfloat16_rn(ra[i]);
+            for (int i = 0; i < TM * TK / GT; ++i) {
+                const int e = tid + GT * i;
+                const int r = kf ? e / TK : e % TM, kk = kf ? e % TK : e / TM;
+                As[r][kk] = __float2bfloat16_rn(ra[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < TM * TK / GT / 4; ++i) {
+                const int e = tid + GT * i;
+                const int r = (VA == 1) ? e / (TK / 4) : (e % (TM / 4)) * 4;
+                const int kk = (VA == 1) ? (e % (TK / 4)) * 4 : e / (TM / 4);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (VA == 1) As[r][kk + q] = __float2bfloat16_rn(ra[4 * i + q]);
+                    else As[r + q][kk] = __float2bfloat16_rn(ra[4 * i + q]);
+                }
+            }
         }
+        if constexpr (VB == 0) {
+            const bool kf = (g.sBk == 1);
 #pragma unroll
-        for (int i = 0; i < TN * TK / GT; ++i) {
-            const int e = tid + GT * i;
-            int c, kk;
-            if (b_kfast) { c = e / TK; kk = e % TK; }
-            else { c = e % TN; kk = e / TN; }
-            Bs[c][kk] = __float2bfloat16_rn(rb[i]);
+            for (int i = 0; i < TN * TK / GT; ++i) {
+                const int e = tid + GT * i;
+                const int c = kf ? e / TK : e % TN, kk = kf ? e % TK : e / TN;
+                Bs[c][kk] = __float2bfloat16_rn(rb[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < TN * TK / GT / 4; ++i) {
+                const int e = tid + GT * i;
+                const int c = (VB == 1) ? e / (TK / 4) : (e % (TN / 4)) * 4;
+                const int kk = (VB == 1) ? (e % (TK / 4)) * 4 : e / (TN / 4);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (VB == 1) Bs[c][kk + q] = __float2bfloat16_rn(rb[4 * i + q]);
+                    else Bs[c + q][kk] = __float2bfloat16_rn(rb[4 * i + q]);
+                }
+            }
         }
     };
 
@@ -190,6 +250,22 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
             }
 }
 
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// vector mode of an operand with rows x cols = (mrows, k): 1 when k is
+// contiguous, 2 when the row index is, 0 otherwise (see bf16_gemm_kernel)
+int vec_mode(const float* base, long long s_row, long long s_k, long long s_batch, int rows, int k) {
+    if (!aligned16(base) || s_batch % 4 != 0) return 0;
+    if (s_k == 1 && s_row % 4 == 0 && k % 4 == 0) return 1;
+    if (s_row == 1 && s_k % 4 == 0 && rows % 4 == 0) return 2;
+    return 0;
+}
+
+template <int VA, int VB>
+void launch_gemm(dim3 grid, cudaStream_t st, const Gemm& g) {
+    bf16_gemm_kernel<VA, VB><<<grid, GT, 0, st>>>(g);
+}
+
 sc_status gemm(cudaStream_t st, const Gemm& g) {
     if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return SC_OK;
     if (g.batch > 65535 || (g.n + TN - 1) / TN > 65535) {
@@ -197,7 +273,19 @@ sc_status gemm(cudaStream_t st, const Gemm& g) {
         return SC_BADINPUT;
     }
     dim3 grid((g.m + TM - 1) / TM, (g.n + TN - 1) / TN, g.batch);
-    bf16_gemm_kernel<<<grid, GT, 0, st>>>(g);
+    const int va = vec_mode(g.A, g.sAm, g.sAk, g.batch > 1 ? g.sAb : 0, g.m, g.k);
+    const int vb = vec_mode(g.B, g.sBn, g.sBk, g.batch > 1 ? g.sBb : 0, g.n, g.k);
+    switch (va * 3 + vb) {
+        case 0: launch_gemm<0, 0>(grid, st, g); break;
+        case 1: launch_gemm<0, 1>(grid, st, g); break;
+        case 2: launch_gemm<0, 2>(grid, st, g); break;
+        case 3: launch_gemm<1, 0>(grid, st, g); break;
+        case 4: launch_gemm<1, 1>(grid, st, g); break;
+        case 5: launch_gemm<1, 2>(grid, st, g); break;
+        case 6: launch_gemm<2, 0>(grid, st, g); break;
+        case 7: launch_gemm<2, 1>(grid, st, g); break;
+        default: launch_gemm<2, 2>(grid, st, g); break;
+    }
     count_launch();
     SC_CHECK_LAUNCH("fno gemm");
     return SC_OK;

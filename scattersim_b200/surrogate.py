@@ -95,9 +95,13 @@ def solve_plain(ctx, maps: np.ndarray, lams, chunk: int = 1024, precision: int =
 def generate(ctx, seeds):
     """Maps and wavelengths of the seeded instances (float32, as the network reads
     them) and the plain solve's R/T vectors of exactly those float32 inputs."""
-    maps, lams = zip(*(instance(int(s)) for s in seeds))
-    maps = np.stack(maps).astype(np.float32)
-    lams = np.array(lams, dtype=np.float32)
+    seeds = list(seeds)
+    maps = np.empty((len(seeds), 64, 64), dtype=np.float32)
+    lams = np.empty(len(seeds), dtype=np.float32)
+    for i, s in enumerate(seeds):
+        m, lam = instance(int(s))
+        maps[i] = m
+        lams[i] = lam
     x = solve_plain(ctx, maps, lams)
     return maps, lams, x
 
