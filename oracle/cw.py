@@ -5,6 +5,9 @@
   files the reference ships (``data/psf.cw``, ``x64/a.cw``): one record is
   ``sizeof(tira::planewave<double>)`` = 80 bytes = {E0x, E0y, kx, ky, kz}
   complex128.  E0z is not stored.
+* ``get_e0_tira``/``put_e0_tira``: the storage frame of a record's E pair
+  (tira's planewave keeps E in a frame rotated to the real k direction),
+  pinned by reproducing both shipped files from their incident waves.
 * ``unpack`` restates ``cw_allocate``/``cw_unpack`` (cpuEvaluator.cpp:34-102):
   region 0 = Pi + Pr_0, region l = Pt_{l-1} + Pr_l, last = Pt_last.
 * ``evaluate`` restates the GPU ``evaluate`` device function
@@ -89,33 +92,53 @@ def get_e0(E2, k):
     return E
 
 
-def _rotation_z_to(kh):
-    """Rodrigues rotation taking z-hat to the unit vector kh (complex kh with kh.kh = 1 allowed)."""
-    z = np.array([0.0, 0.0, 1.0])
-    a = np.cross(z, kh)
-    c = kh[2]
-    s2 = a @ a
-    if abs(s2) < 1e-30:
-        return np.eye(3, dtype=np.complex128) if np.real(c) > 0 else np.diag([1.0, -1.0, -1.0]).astype(np.complex128)
-    sn = np.sqrt(s2)
-    ah = a / sn
-    K = np.array([[0, -ah[2], ah[1]], [ah[2], 0, -ah[0]], [-ah[1], ah[0], 0]])
-    return np.eye(3) + sn * K + (1 - c) * (K @ K)
+def tira_frame(k):
+    """Rotation R whose third column is the real propagation direction Re(k)/|Re(k)|.
 
-
-def get_e0_local(E2, k):
-    """Alternative reading of a record: (E0x, E0y) as components in a k-aligned frame.
-
-    The two files the reference ships are continuous across their boundaries
-    only under this reading (psf.cw to ~1e-4): E_world = R (E0x, E0y, 0) with R
-    the rotation taking z-hat to k / sqrt(k.k).  The azimuthal gauge of that
-    frame for oblique waves is not pinned by the data (tira is not available).
+    R is the minimal (Rodrigues) rotation taking z-hat to that direction: about
+    the axis z-hat x k-hat by the angle between them.  Straight down (-z-hat)
+    has no minimal rotation; a half turn about x is used there (no shipped
+    record is exactly vertical downwards, so that case is unpinned).
     """
+    kr = np.real(np.asarray(k, dtype=np.complex128))
+    kh = kr / np.linalg.norm(kr)
+    ax = np.array([-kh[1], kh[0], 0.0])           # z-hat x k-hat
+    s2 = ax @ ax
+    if s2 < 1e-30:
+        return np.eye(3) if kh[2] > 0 else np.diag([1.0, -1.0, -1.0])
+    K = np.array([[0.0, -ax[2], ax[1]], [ax[2], 0.0, -ax[0]], [-ax[1], ax[0], 0.0]])
+    return np.eye(3) + K + (1.0 - kh[2]) / s2 * (K @ K)
+
+
+def get_e0_tira(E2, k):
+    """A record's E0 as tira::planewave::getE0() rebuilds it (pinned by the shipped files).
+
+    A record stores (E0x, E0y) = the first two components of R^T E in the
+    frame of ``tira_frame(k)``; the third local component is rebuilt from
+    k . E = 0 in that frame (k' = R^T k, complex for absorbing media).  Under
+    this reading every wave of data/psf.cw (scatterplane, 4096 incident,
+    reflected and transmitted records) and every transmitted wave of x64/a.cw
+    (scatterlayer, three boundaries) is reproduced to ~1e-15 by the layer
+    solve of ScatterLayer.cpp:152-266 fed with the file's own incident waves.
+    """
+    E2 = np.asarray(E2, dtype=np.complex128).reshape(-1, 2)
+    k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
     out = np.zeros((len(E2), 3), dtype=np.complex128)
     for i in range(len(E2)):
-        kv = np.asarray(k[i], dtype=np.complex128)
-        R = _rotation_z_to(kv / np.sqrt(kv @ kv))
-        out[i] = R @ np.array([E2[i, 0], E2[i, 1], 0.0])
+        R = tira_frame(k[i])
+        kp = R.T @ k[i]
+        ez = -(kp[0] * E2[i, 0] + kp[1] * E2[i, 1]) / kp[2] if kp[2] != 0 else 0.0
+        out[i] = R @ np.array([E2[i, 0], E2[i, 1], ez])
+    return out
+
+
+def put_e0_tira(E, k):
+    """The (E0x, E0y) pair a record stores for a Cartesian E0 (inverse of get_e0_tira)."""
+    E = np.asarray(E, dtype=np.complex128).reshape(-1, 3)
+    k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
+    out = np.zeros((len(E), 2), dtype=np.complex128)
+    for i in range(len(E)):
+        out[i] = (tira_frame(k[i]).T @ E[i])[:2]
     return out
 
 

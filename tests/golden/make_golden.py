@@ -62,9 +62,9 @@ def cw_entry(path, tag, out):
         out[f"{tag}_L{l}_Pr_k"] = Prk[sel]
         out[f"{tag}_L{l}_Pt_E"] = PtE[sel]
         out[f"{tag}_L{l}_Pt_k"] = Ptk[sel]
-    # field of the full file (E_z rebuilt by transversality, as the viewer does)
-    full = [(z, ocw.get_e0(PrE, Prk), Prk, ocw.get_e0(PtE, Ptk), Ptk) for (z, PrE, Prk, PtE, Ptk) in layers]
-    zl, b, e, WE, Wk = ocw.unpack(ocw.get_e0(PiE, Pik), Pik, full)
+    # field of the full file, records read in tira's frame as the viewer's getE0() does
+    full = [(z, ocw.get_e0_tira(PrE, Prk), Prk, ocw.get_e0_tira(PtE, Ptk), Ptk) for (z, PrE, Prk, PtE, Ptk) in layers]
+    zl, b, e, WE, Wk = ocw.unpack(ocw.get_e0_tira(PiE, Pik), Pik, full)
     pts = grid_points(out[f"{tag}_z"])
     out[f"{tag}_pts"] = pts
     out[f"{tag}_E_full"] = ocw.evaluate(pts, zl, b, e, WE, Wk)

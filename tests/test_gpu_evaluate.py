@@ -23,10 +23,10 @@ def fixture_table(tag):
     fx = np.load(os.path.join(GOLD, "cw_fixtures.npz"))
     layers = []
     for l in range(len(fx[f"{tag}_z"])):
-        layers.append((float(fx[f"{tag}_z"][l]), ocw.get_e0_local(fx[f"{tag}_L{l}_Pr_E"], fx[f"{tag}_L{l}_Pr_k"]),
-                       fx[f"{tag}_L{l}_Pr_k"], ocw.get_e0_local(fx[f"{tag}_L{l}_Pt_E"], fx[f"{tag}_L{l}_Pt_k"]),
+        layers.append((float(fx[f"{tag}_z"][l]), ocw.get_e0_tira(fx[f"{tag}_L{l}_Pr_E"], fx[f"{tag}_L{l}_Pr_k"]),
+                       fx[f"{tag}_L{l}_Pr_k"], ocw.get_e0_tira(fx[f"{tag}_L{l}_Pt_E"], fx[f"{tag}_L{l}_Pt_k"]),
                        fx[f"{tag}_L{l}_Pt_k"]))
-    return ocw.unpack(ocw.get_e0_local(fx[f"{tag}_Pi_E"], fx[f"{tag}_Pi_k"]), fx[f"{tag}_Pi_k"], layers)
+    return ocw.unpack(ocw.get_e0_tira(fx[f"{tag}_Pi_E"], fx[f"{tag}_Pi_k"]), fx[f"{tag}_Pi_k"], layers)
 
 
 @pytest.mark.parametrize("tag", ["psf", "acw"])

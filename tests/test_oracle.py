@@ -4,7 +4,10 @@
   byte (when the reference tree is mounted) and matches the committed
   fixtures (always).
 * The stored E pair of a record is not a Cartesian (E_x, E_y): read that way
-  psf.cw jumps at its interface; read in a k-aligned frame it is continuous.
+  psf.cw jumps at its interface.  It is the pair in tira's frame rotated to
+  Re k: read that way psf.cw is continuous, and the restated focused beams
+  and layer solves reproduce psf.cw and the incident/transmitted records of
+  a.cw to rounding.
 * scattervolume at one Fourier order on layers.npy equals the closed-form
   scatterlayer solve (the consistency data/generate_layer_volume.py states).
 * Literal-restatement details: fftshift, the column-major reinterpretation,
@@ -101,9 +104,70 @@ def test_cw_records_are_not_cartesian_pairs(cwfix):
     assert _jump(cwfix, "psf", ocw.get_e0) > 1e-2
 
 
-def test_cw_records_in_k_aligned_frame_are_continuous(cwfix):
-    """Read in the k-aligned frame, psf.cw is continuous to 2e-4 (the frame's gauge is unpinned)."""
-    assert _jump(cwfix, "psf", ocw.get_e0_local) < 2e-4
+def test_cw_records_in_tira_frame_are_continuous(cwfix):
+    """Read in tira's frame (rotated to Re k), psf.cw is continuous across its interface
+    (to the phase change over the 2e-9 um between the two evaluation planes)."""
+    assert _jump(cwfix, "psf", ocw.get_e0_tira) < 1e-7
+
+
+def test_tira_frame_roundtrip():
+    rng = np.random.default_rng(3)
+    k = rng.normal(size=(50, 3)) + 1j * np.concatenate([np.zeros((50, 2)), rng.uniform(0, 0.5, (50, 1))], 1)
+    k[:, 2] = np.abs(k[:, 2].real) * np.sign(rng.normal(size=50)) + 1j * k[:, 2].imag
+    E = rng.normal(size=(50, 3)) + 1j * rng.normal(size=(50, 3))
+    E -= ((E * k).sum(1) / (k * k).sum(1))[:, None] * k          # transverse: k . E = 0
+    assert np.allclose(ocw.get_e0_tira(ocw.put_e0_tira(E, k), k), E, atol=1e-12)
+    R = ocw.tira_frame(np.array([1.0, 0.0, 1.0]))
+    assert np.allclose(R @ R.T, np.eye(3)) and np.allclose(R[:, 2], np.array([1, 0, 1]) / np.sqrt(2))
+
+
+def _beam_at(fx, tag, ks, Es):
+    sel = fx[f"{tag}_sel"]
+    return ks[sel], Es[sel]
+
+
+@pytest.fixture(scope="module")
+def psf_restated():
+    return osl.scatterplane()
+
+
+@pytest.fixture(scope="module")
+def acw_restated():
+    return osl.scatterlayer(z=(-3.0, 0.0, 3.0))
+
+
+def test_scatterplane_beam_and_solve_reproduce_psf(cwfix, psf_restated):
+    """data/psf.cw = scatterplane defaults: polar beam (alpha 0.5, 64 x 64 about (1, 0, 1)),
+    one interface n 1 | 1.4 + 0.05i at z = 0; every record agrees to rounding."""
+    ks, Es, layers = psf_restated
+    sel = cwfix["psf_sel"]
+    scale = np.abs(cwfix["psf_Pi_E"]).max()
+    assert np.abs(ks[sel] - cwfix["psf_Pi_k"]).max() < 1e-13
+    assert np.abs(ocw.put_e0_tira(Es[sel], ks[sel]) - cwfix["psf_Pi_E"]).max() < 1e-13 * scale
+    z, PrE, Prk, PtE, Ptk = layers[0]
+    assert z == float(cwfix["psf_z"][0])
+    assert np.abs(Prk[sel] - cwfix["psf_L0_Pr_k"]).max() < 1e-13
+    assert np.abs(Ptk[sel] - cwfix["psf_L0_Pt_k"]).max() < 1e-13
+    assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel]) - cwfix["psf_L0_Pr_E"]).max() < 1e-13 * scale
+    assert np.abs(ocw.put_e0_tira(PtE[sel], Ptk[sel]) - cwfix["psf_L0_Pt_E"]).max() < 1e-13 * scale
+
+
+def test_scatterlayer_beam_and_solve_reproduce_acw(cwfix, acw_restated):
+    """x64/a.cw = scatterlayer's default stack (n 1, 1.4 + 0.05i, 1.4, 1; z -3, 0, 3) under a
+    polar beam (alpha 1, 64 x 64 about z): incident and transmitted records agree to rounding
+    at every boundary; the reflected records do not match any solve of the stated system."""
+    ks, Es, layers = acw_restated
+    sel = cwfix["acw_sel"]
+    scale = np.abs(cwfix["acw_Pi_E"]).max()
+    assert np.abs(ks[sel] - cwfix["acw_Pi_k"]).max() < 1e-13
+    assert np.abs(ocw.put_e0_tira(Es[sel], ks[sel]) - cwfix["acw_Pi_E"]).max() < 1e-13 * scale
+    for l in range(3):
+        z, PrE, Prk, PtE, Ptk = layers[l]
+        assert z == float(cwfix["acw_z"][l])
+        assert np.abs(Prk[sel] - cwfix[f"acw_L{l}_Pr_k"]).max() < 1e-13
+        assert np.abs(Ptk[sel] - cwfix[f"acw_L{l}_Pt_k"]).max() < 1e-13
+        assert np.abs(ocw.put_e0_tira(PtE[sel], Ptk[sel]) - cwfix[f"acw_L{l}_Pt_E"]).max() < 1e-13 * scale
+        assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel]) - cwfix[f"acw_L{l}_Pr_E"]).max() > 1e-2 * scale
 
 
 def test_cw_fixture_field_matches_reference_file(cwfix):
@@ -112,8 +176,8 @@ def test_cw_fixture_field_matches_reference_file(cwfix):
     if not os.path.exists(path):
         pytest.skip("reference tree not mounted")
     PiE, Pik, layers = ocw.load(path)
-    full = [(z, ocw.get_e0(a, b), b, ocw.get_e0(c, d), d) for (z, a, b, c, d) in layers]
-    zl, b, e, WE, Wk = ocw.unpack(ocw.get_e0(PiE, Pik), Pik, full)
+    full = [(z, ocw.get_e0_tira(a, b), b, ocw.get_e0_tira(c, d), d) for (z, a, b, c, d) in layers]
+    zl, b, e, WE, Wk = ocw.unpack(ocw.get_e0_tira(PiE, Pik), Pik, full)
     E = ocw.evaluate(cwfix["acw_pts"], zl, b, e, WE, Wk)
     assert np.allclose(E, cwfix["acw_E_full"], rtol=0, atol=1e-12 * np.abs(E).max())
 
