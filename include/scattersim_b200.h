@@ -21,6 +21,9 @@
  *                           cw_allocate / cw_unpack          cpuEvaluator.cpp:34-102
  *   sc_cw_evaluate          gpu_cw_evaluate / evaluate       gpuEvaluator.cu:28-165
  *   sc_mkl_eigensolve       host-buffer MKL_eigensolve       third_Lapack.h:37-44
+ *   sc_beam_polar           planewave::SolidAnglePolar       ScatterLayer.cpp:355-385, ScatterPlane.cpp:154-171,236-242
+ *   sc_layer_solve          scatterlayer / scatterplane      ScatterLayer.cpp:110-266,390-420,
+ *                           per-wave solves                  ScatterPlane.cpp:175,243-256
  *   sc_gpu_initialize /
  *   sc_gpu_cw_evaluate      host-buffer gpu_initialize /     gpuEvaluator.cu:15-26,131-165
  *                           gpu_cw_evaluate
@@ -261,6 +264,39 @@ sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw,
                          const double* z_layers, const int* begin, const int* end, int layers,
                          double zeps, const double* points, long long np, void* out,
                          int precision, void* stream);
+
+/* ----------------------------------------- homogeneous layers, focused beams */
+
+/* tira::planewave::SolidAnglePolar as scatterlayer and scatterplane call it
+ * (ScatterLayer.cpp:384, ScatterPlane.cpp:240): N0 x N1 waves about
+ * the centre wave (k_center: 3 doubles, E_center: 3 complex128, host; E is
+ * expected orthogonal to k as the callers' orthogonalize() leaves it).  Wave
+ * t = j N0 + i has polar angle beta + i (alpha - beta) / N0 and azimuth
+ * j 2 pi / N1 about the centre direction (in the centre wave's record frame),
+ * and E0 = sin(theta) dtheta dphi times the centre wave's record pair in its
+ * own frame; each is then wound to the focal point (E0 exp(-i k.focus);
+ * focus may be NULL).  alpha = 0 or N0 N1 = 1 gives the centre wave alone.
+ * k_out: N0 N1 x 3 doubles, E_out: N0 N1 x 3 complex128 (device);
+ * *count = the number of waves written.  Replaces the beam set-up of
+ * ScatterLayer.cpp:355-385 and ScatterPlane.cpp:154-171, 236-242. */
+sc_status sc_beam_polar(sc_context* ctx, double alpha, double beta, int N0, int N1,
+                        const double* k_center, const double* E_center, const double* focus,
+                        double* k_out, void* E_out, int* count, void* stream);
+
+/* scatterlayer's per-wave solve (ScatterLayer.cpp:110-266, 390-420) for
+ * `count` incident plane waves at once: layers L (1..15) with refractive
+ * indices n[0..L-1] and absorbances kappa[0..L-2] of layers 1..L-1, boundary
+ * planes z[0..L-2] (host arrays, the padded lists of ScatterLayer.cpp:321-343),
+ * vacuum wavelength lambda.  k_in: count x 3 doubles (only the direction is
+ * used), E_in: count x 3 complex128 (device).  Outputs per wave and boundary
+ * l (count x (L-1) x 3 complex128 each, device): the reflected and
+ * transmitted E0 and k of mat2waves, wound by -z_l as the .cw file stores
+ * them.  status (device, count ints, may be NULL): SC_OK or SC_SINGULAR per
+ * wave.  scatterplane's interface solve is the case L = 2. */
+sc_status sc_layer_solve(sc_context* ctx, int layers, const double* n, const double* kappa,
+                         const double* z, double lambda, int count, const double* k_in,
+                         const void* E_in, void* r_E, void* r_k, void* t_E, void* t_k,
+                         int* status, void* stream);
 
 /* ----------------------------------------- reference-signature shims (host) */
 

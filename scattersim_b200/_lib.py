@@ -100,6 +100,11 @@ _SIGS = {
     "sc_cw_evaluate": (c_int, [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_double), POINTER(c_int),
                                POINTER(c_int), c_int, c_double, c_void_p, c_longlong, c_void_p, c_int, c_void_p]),
     "sc_mkl_eigensolve": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "sc_beam_polar": (c_int, [c_void_p, c_double, c_double, c_int, c_int, POINTER(c_double), POINTER(c_double),
+                              POINTER(c_double), c_void_p, c_void_p, POINTER(c_int), c_void_p]),
+    "sc_layer_solve": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double), c_double,
+                               c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                               c_void_p]),
     "sc_gpu_initialize": (c_int, [c_int, POINTER(ctypes.c_float), POINTER(c_int), POINTER(c_int), c_void_p,
                                   c_longlong, c_int]),
     "sc_gpu_cw_evaluate": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,

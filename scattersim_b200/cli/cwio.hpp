@@ -4,6 +4,7 @@
 // read/write, and the coupled-wave (.cw) file of CoupledWaveStructure.h:63-125.
 #pragma once
 
+#include <cmath>
 #include <complex>
 #include <cstdint>
 #include <cstdio>
@@ -137,8 +138,19 @@ inline void write_npy(const std::string& path, const std::string& descr, const s
 
 // ------------------------------------------------------------------ .cw
 // One record = {E0x, E0y, kx, ky, kz} complex128 (80 bytes); E0z is not stored.
+//
+// Record frame (Frame::tira, the default): tira's planewave keeps E0 in a
+// frame whose z axis is the real propagation direction Re(k)/|Re(k)| (the
+// minimal rotation taking z-hat there) and the file holds the first two
+// components in that frame; the reader rebuilds the third from k . E = 0 in
+// the same frame.  This is the reading under which every record of the
+// reference's data/psf.cw, and the incident and transmitted records of
+// x64/a.cw, equal the restated solves of their runs, so files written here
+// read correctly in the reference's viewer and vice versa.  Frame::cartesian
+// stores (E_x, E_y) and rebuilds E_z from k . E = 0 (not the reference's
+// convention; kept for files written that way).
 struct Wave {
-    cplx E[3];
+    cplx E[3];   // Cartesian E0
     cplx k[3];
 };
 struct Boundary {
@@ -150,63 +162,120 @@ struct CoupledWave {
     std::vector<Boundary> layers;
 };
 
-inline void put_records(std::ofstream& f, const std::vector<Wave>& w) {
+enum class Frame { tira, cartesian };
+
+inline Frame parse_frame(const std::string& s) {
+    if (s == "tira") return Frame::tira;
+    if (s == "cartesian") return Frame::cartesian;
+    throw std::runtime_error("unknown --cw-frame '" + s + "' (tira or cartesian)");
+}
+
+// R (row-major) with third column Re(k)/|Re(k)|: minimal rotation from z-hat;
+// straight down is a half turn about x
+inline void record_frame(const cplx k[3], double R[3][3]) {
+    double kh[3] = {k[0].real(), k[1].real(), k[2].real()};
+    const double nk = std::sqrt(kh[0] * kh[0] + kh[1] * kh[1] + kh[2] * kh[2]);
+    for (double& v : kh) v = nk > 0 ? v / nk : 0.0;
+    const double ax0 = -kh[1], ax1 = kh[0], s2 = ax0 * ax0 + ax1 * ax1;
+    if (s2 < 1e-30) {
+        const double sg = kh[2] >= 0 ? 1.0 : -1.0;
+        const double I[3][3] = {{1, 0, 0}, {0, sg, 0}, {0, 0, sg}};
+        std::memcpy(R, I, sizeof(I));
+        return;
+    }
+    const double f = (1.0 - kh[2]) / s2;
+    const double M[3][3] = {{1.0 - f * ax1 * ax1, f * ax0 * ax1, ax1},
+                            {f * ax0 * ax1, 1.0 - f * ax0 * ax0, -ax0},
+                            {-ax1, ax0, kh[2]}};
+    std::memcpy(R, M, sizeof(M));
+}
+
+inline void to_record(const Wave& w, Frame fr, cplx out[2]) {
+    if (fr == Frame::cartesian) {
+        out[0] = w.E[0];
+        out[1] = w.E[1];
+        return;
+    }
+    double R[3][3];
+    record_frame(w.k, R);
+    for (int c = 0; c < 2; ++c) out[c] = R[0][c] * w.E[0] + R[1][c] * w.E[1] + R[2][c] * w.E[2];
+}
+
+inline void from_record(const cplx p[2], Wave& w, Frame fr) {
+    if (fr == Frame::cartesian) {
+        w.E[0] = p[0];
+        w.E[1] = p[1];
+        w.E[2] = (w.k[2] == cplx(0.0)) ? cplx(0.0) : -(w.k[0] * p[0] + w.k[1] * p[1]) / w.k[2];
+        return;
+    }
+    double R[3][3];
+    record_frame(w.k, R);
+    cplx kp[3];
+    for (int c = 0; c < 3; ++c) kp[c] = R[0][c] * w.k[0] + R[1][c] * w.k[1] + R[2][c] * w.k[2];
+    const cplx e2 = (kp[2] == cplx(0.0)) ? cplx(0.0) : -(kp[0] * p[0] + kp[1] * p[1]) / kp[2];
+    for (int r = 0; r < 3; ++r) w.E[r] = R[r][0] * p[0] + R[r][1] * p[1] + R[r][2] * e2;
+}
+
+inline void put_records(std::ofstream& f, const std::vector<Wave>& w, Frame fr) {
     uint64_t n = w.size();
     f.write((const char*)&n, 8);
     for (auto& x : w) {
-        cplx rec[5] = {x.E[0], x.E[1], x.k[0], x.k[1], x.k[2]};
+        cplx rec[5];
+        to_record(x, fr, rec);
+        rec[2] = x.k[0];
+        rec[3] = x.k[1];
+        rec[4] = x.k[2];
         f.write((const char*)rec, sizeof(rec));
     }
 }
 
-inline void save_cw(const std::string& path, const CoupledWave& cw) {
+inline void save_cw(const std::string& path, const CoupledWave& cw, Frame fr = Frame::tira) {
     std::ofstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("cannot write " + path);
     uint64_t sz = 8;
     f.write((const char*)&sz, 8);
-    put_records(f, cw.Pi);
+    put_records(f, cw.Pi, fr);
     uint64_t nl = cw.layers.size();
     f.write((const char*)&nl, 8);
     for (auto& L : cw.layers) {
         f.write((const char*)&L.z, 8);
-        put_records(f, L.Pr);
-        put_records(f, L.Pt);
+        put_records(f, L.Pr, fr);
+        put_records(f, L.Pt, fr);
     }
 }
 
-inline std::vector<Wave> get_records(std::ifstream& f) {
+inline std::vector<Wave> get_records(std::ifstream& f, Frame fr) {
     uint64_t n = 0;
     f.read((char*)&n, 8);
+    if (!f || n > (uint64_t(1) << 40)) throw std::runtime_error("corrupt record count");
     std::vector<Wave> w(n);
     for (auto& x : w) {
         cplx rec[5];
         f.read((char*)rec, sizeof(rec));
-        x.E[0] = rec[0];
-        x.E[1] = rec[1];
         x.k[0] = rec[2];
         x.k[1] = rec[3];
         x.k[2] = rec[4];
-        // E_z by transversality (k . E = 0)
-        x.E[2] = (x.k[2] == cplx(0.0)) ? cplx(0.0) : -(x.k[0] * x.E[0] + x.k[1] * x.E[1]) / x.k[2];
+        from_record(rec, x, fr);
     }
     return w;
 }
 
-inline CoupledWave load_cw(const std::string& path) {
+inline CoupledWave load_cw(const std::string& path, Frame fr = Frame::tira) {
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("file " + path + " not found");
     uint64_t sz = 0;
     f.read((char*)&sz, 8);
     if (sz != 8) throw std::runtime_error(path + ": only double-precision .cw files are supported");
     CoupledWave cw;
-    cw.Pi = get_records(f);
+    cw.Pi = get_records(f, fr);
     uint64_t nl = 0;
     f.read((char*)&nl, 8);
+    if (!f || nl > (uint64_t(1) << 20)) throw std::runtime_error(path + ": corrupt layer count");
     cw.layers.resize(nl);
     for (auto& L : cw.layers) {
         f.read((char*)&L.z, 8);
-        L.Pr = get_records(f);
-        L.Pt = get_records(f);
+        L.Pr = get_records(f, fr);
+        L.Pt = get_records(f, fr);
     }
     if (!f) throw std::runtime_error(path + ": truncated");
     return cw;

@@ -4,8 +4,9 @@
 //   scattereval --input c.cw [--cuda 0] [--size 100] [--resolution 8]
 //               [--axis 1] [--center x y z] [--slice s] [--output xz.npy]
 //
-// Loads the coupled-wave structure, unpacks it in cw_unpack order
-// (cpuEvaluator.cpp:34-102; E_z rebuilt by transversality), evaluates the x-y,
+// Loads the coupled-wave structure (records read in the reference's record
+// frame, E0 rebuilt as tira's getE0() does), unpacks it in cw_unpack order
+// (cpuEvaluator.cpp:34-102), evaluates the x-y,
 // x-z and y-z slices of N = 2^resolution points with step extent / (N - 1)
 // starting at center - extent / 2 (ScatterView.cpp:354-370), and saves the
 // slice of --axis (0: y-z at x, 1: x-z at y, 2: x-y at z; the slice
@@ -20,7 +21,7 @@
 
 int main(int argc, char** argv) {
     const std::vector<std::string> known = {"input", "help", "cuda", "nogui", "verbose", "size", "resolution",
-                                            "output", "axis", "center", "slice"};
+                                            "output", "axis", "center", "slice", "cw-frame"};
     cwio::Options o;
     try {
         o = cwio::parse(argc, argv, known, "input");
@@ -31,7 +32,8 @@ int main(int argc, char** argv) {
     if (o.has("help")) {
         std::cout << "Allowed options:\n  --input arg (=c.cw)\n  --cuda arg (=0)\n  --size arg (=100)\n"
                      "  --resolution arg (=8)\n  --output arg (=xz.npy)\n  --axis arg (=1)\n"
-                     "  --center arg (={0, 0, 0})\n  --slice arg (=0)\n";
+                     "  --center arg (={0, 0, 0})\n  --slice arg (=0)\n"
+                     "  --cw-frame arg (=tira) record frame of the file ('tira' or 'cartesian')\n";
         return 1;
     }
     const std::string in = o.str("input", "c.cw"), out = o.str("output", "xz.npy");
@@ -46,7 +48,7 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     cwio::CoupledWave cw;
     try {
-        cw = cwio::load_cw(in);
+        cw = cwio::load_cw(in, cwio::parse_frame(o.str("cw-frame", "tira")));
     } catch (const std::exception& e) {
         std::cout << "ERROR: " << e.what() << std::endl;
         return 1;

@@ -8,10 +8,9 @@
 // ScatterVolume.cpp:995-1002.  scatterthinvolume is the same program (a 2-D
 // sample is one layer, FourierWave.h:291-299).
 //
-// --cw-frame cartesian (default) stores each wave's (E_x, E_y) as the
-// reference's solver passes them to the plane-wave constructor; --cw-frame
-// local stores them in the k-aligned frame under which the reference's shipped
-// .cw files are continuous (E = R(z -> k) (E0x, E0y, 0)).
+// Records are stored in the reference's record frame (--cw-frame tira, the
+// default: the E0 pair in the frame rotated to Re k, which the reference's
+// viewer reads back); --cw-frame cartesian stores (E_x, E_y).
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -25,34 +24,6 @@
 using cwio::cplx;
 
 namespace {
-
-void to_local_frame(cwio::Wave& w) {
-    // R(z -> khat) with khat = k / sqrt(k.k); store (R^T E)_{x,y}
-    cplx kk = std::sqrt(w.k[0] * w.k[0] + w.k[1] * w.k[1] + w.k[2] * w.k[2]);
-    cplx kh[3] = {w.k[0] / kk, w.k[1] / kk, w.k[2] / kk};
-    cplx a[3] = {-kh[1], kh[0], 0.0};   // z x khat
-    cplx s2 = a[0] * a[0] + a[1] * a[1];
-    cplx c = kh[2];
-    cplx R[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-    if (std::abs(s2) > 1e-30) {
-        cplx sn = std::sqrt(s2);
-        cplx ah[3] = {a[0] / sn, a[1] / sn, 0.0};
-        cplx K[3][3] = {{0, -ah[2], ah[1]}, {ah[2], 0, -ah[0]}, {-ah[1], ah[0], 0}};
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) {
-                cplx kk2 = 0;
-                for (int l = 0; l < 3; ++l) kk2 += K[i][l] * K[l][j];
-                R[i][j] = (i == j ? 1.0 : 0.0) + sn * K[i][j] + (1.0 - c) * kk2;
-            }
-    } else if (c.real() < 0) {
-        R[1][1] = -1.0;
-        R[2][2] = -1.0;
-    }
-    cplx loc[2];
-    for (int i = 0; i < 2; ++i) loc[i] = R[0][i] * w.E[0] + R[1][i] * w.E[1] + R[2][i] * w.E[2];
-    w.E[0] = loc[0];
-    w.E[1] = loc[1];
-}
 
 int fail(const char* what, sc_status s) {
     std::cerr << "ERROR: " << what << " failed (status " << (int)s << "): " << sc_last_error_string() << std::endl;
@@ -91,7 +62,7 @@ int main(int argc, char** argv) {
                      "  --external             save waves for the external field only\n"
                      "  --log                  produce a log file\n"
                      "  --npz                  calculate Px and Py only\n"
-                     "  --cw-frame arg (=cartesian) E pair stored as 'cartesian' or 'local'\n"
+                     "  --cw-frame arg (=tira)  E pair stored in the record frame ('tira') or as (E_x, E_y) ('cartesian')\n"
                      "  --cuda arg (=0)        CUDA device\n";
         return 1;
     }
@@ -124,7 +95,13 @@ int main(int argc, char** argv) {
     p.external = o.has("external");
     p.npz = o.has("npz");
     const std::string out = o.str("output", "c.cw");
-    const bool local = o.str("cw-frame", "cartesian") == "local";
+    cwio::Frame frame;
+    try {
+        frame = cwio::parse_frame(o.str("cw-frame", "tira"));
+    } catch (const std::exception& e) {
+        std::cerr << "ERROR: " << e.what() << std::endl;
+        return 1;
+    }
     if (!o.has("sample")) {
         std::cerr << "ERROR: no --sample given" << std::endl;
         return 1;
@@ -192,7 +169,6 @@ int main(int argc, char** argv) {
                 w[i - b0].E[c] = hE[3 * i + c];
                 w[i - b0].k[c] = hk[3 * i + c];
             }
-            if (local) to_local_frame(w[i - b0]);
         }
         return w;
     };
@@ -216,7 +192,7 @@ int main(int argc, char** argv) {
         return 1;
     }
     try {
-        if (!out.empty()) cwio::save_cw(out, cw);
+        if (!out.empty()) cwio::save_cw(out, cw, frame);
     } catch (const std::exception& e) {
         std::cerr << "ERROR: " << e.what() << std::endl;
         return 1;

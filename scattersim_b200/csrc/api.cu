@@ -607,6 +607,31 @@ sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw,
     return SC_OK;
 }
 
+// ------------------------------------------------- layers and focused beams
+sc_status sc_beam_polar(sc_context* ctx, double alpha, double beta, int N0, int N1, const double* k_center,
+                        const double* E_center, const double* focus, double* k_out, void* E_out, int* count,
+                        void* stream) {
+    if (!ctx) {
+        set_error("sc_beam_polar: null context");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return beam_polar((cudaStream_t)stream, alpha, beta, N0, N1, k_center, (const double2*)E_center, focus, k_out,
+                      (double2*)E_out, count);
+}
+
+sc_status sc_layer_solve(sc_context* ctx, int layers, const double* n, const double* kappa, const double* z,
+                         double lambda, int count, const double* k_in, const void* E_in, void* r_E, void* r_k,
+                         void* t_E, void* t_k, int* status, void* stream) {
+    if (!ctx) {
+        set_error("sc_layer_solve: null context");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return layer_solve(ctx, layers, n, kappa, z, lambda, count, k_in, (const double2*)E_in, (double2*)r_E,
+                       (double2*)r_k, (double2*)t_E, (double2*)t_k, status, (cudaStream_t)stream);
+}
+
 // ------------------------------------------------------------ host shims
 sc_status sc_mkl_eigensolve(void* A, void* evl, void* evt, int N) {
     if (!A || !evl || !evt || N <= 0) {

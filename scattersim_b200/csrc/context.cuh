@@ -38,3 +38,15 @@ struct VolumePlan {
 sc_status make_plan(const sc_volume_params* p, int Z, int S1, int S2, VolumePlan* plan);
 
 }  // namespace sc
+
+namespace sc {
+
+// Focused beam of tira::planewave::SolidAnglePolar and the batched
+// homogeneous-layer solve (layer.cu).
+sc_status beam_polar(cudaStream_t st, double alpha, double beta, int N0, int N1, const double* kc,
+                     const double2* ec, const double* focus, double* kout, double2* Eout, int* count);
+sc_status layer_solve(sc_context* ctx, int L, const double* n, const double* kappa, const double* z, double lambda,
+                      int count, const double* kin, const double2* Ein, double2* rE, double2* rk, double2* tE,
+                      double2* tk, int* status, cudaStream_t st);
+
+}  // namespace sc

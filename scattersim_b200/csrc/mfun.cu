@@ -13,18 +13,22 @@
 //   F = cosh(t sqrt Omega), G = sinh(t sqrt Omega) / (t sqrt Omega),
 //   H = (cosh(t sqrt Omega) - I) Omega^-1
 // (all three are power series in t^2 Omega, so no square root or inverse is
-// formed).  They are evaluated by scaling and double-angle squaring:
-//   y = (t / 2^s)^2 Omega with ||y||_1 <= 4;
+// formed).  They are evaluated by scaling and double-angle squaring, with the
+// scaling s_l chosen per layer:
+//   y = (t / 2^s_l)^2 Omega with ||y||_1 <= 4;
 //   F = sum_{j<=12} y^j / (2j)!,  G = sum_{j<=12} y^j / (2j+1)!
 //   (Paterson-Stockmeyer in y^4: 3 powers + 2 products per series; the
 //   truncation error is below 4^13/26! ~ 2e-19 in the 1-norm);
-//   s - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
-//   sinh 2a / 2a = (sinh a / a) cosh a);
+//   s_l - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
+//   sinh 2a / 2a = (sinh a / a) cosh a), step j batched over the layers with
+//   s_l > j (pointer tables follow each layer's current F and G buffers);
 //   the last step also forms H_t = (t^2 / 2) G_{t/2}^2 (cosh 2a - 1 = 2 sinh^2 a).
 // Every product is a batched complex GEMM over all layers of the batch with
 // per-layer scalars, run by the caller's GEMM engine (FP64 tensor-pipe tiles,
 // or int8 digit slices on the tcgen05 tensor cores).
+#include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -61,6 +65,13 @@ __global__ void set_diag_kernel(int n, int ld, long long stride, double val, dou
         const int r = (int)(t % n), c = (int)(t / n);
         p[(long long)c * ld + r] = make_double2(r == c ? val : 0.0, 0.0);
     }
+}
+
+// P[b](i, i) += val for the n x n blocks of a pointer table (leading dimension n)
+__global__ void add_diag_ptr_kernel(int n, double val, double2* const* __restrict__ P) {
+    double2* p = P[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        p[(long long)i * n + i].x += val;
 }
 
 // A_l *= s_l (real per-layer scale, stored in .x)
@@ -129,28 +140,30 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     double2* P1 = scr + 5LL * count * nn;
     double2* P2 = scr + 6LL * count * nn;
 
-    // 1. scaling: s = max over layers so that (kdz/2^s)^2 ||Omega||_1 <= 4, s >= 1
+    // 1. scaling per layer: the least s_l >= 1 with (kdz / 2^s_l)^2 ||Omega_l||_1 <= 4
     norm1_kernel<<<count, 256, 0, st>>>(n2, Om, dnorm);
     count_launch();
     SC_CHECK_LAUNCH("norm1");
     std::vector<double> hn(count);
     SC_CUDA_TRY(cudaMemcpyAsync(hn.data(), dnorm, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
     SC_CUDA_TRY(cudaStreamSynchronize(st));
-    int s = 1;
+    std::vector<int> sl(count, 1);
+    int smax = 1;
     for (int l = 0; l < count; ++l) {
         const double v = kdz[l] * kdz[l] * hn[l];
         if (!std::isfinite(v)) {
             set_error("transfer_inv_batched: non-finite layer matrix norm (layer %d)", l);
             return SC_BADINPUT;
         }
-        while (s < 60 && v / std::ldexp(1.0, 2 * s) > 4.0) ++s;
+        while (sl[l] < 60 && v / std::ldexp(1.0, 2 * sl[l]) > 4.0) ++sl[l];
+        smax = std::max(smax, sl[l]);
     }
-    if (squarings) *squarings = s;
+    if (squarings) *squarings = smax;
 
     // per-layer scalars: y scale, H factor t^2/2 = -(kdz)^2/2, off-diagonal factor -t = -i kdz
     std::vector<double2> hc(3 * (size_t)count);
     for (int l = 0; l < count; ++l) {
-        const double h = std::ldexp(kdz[l], -s);
+        const double h = std::ldexp(kdz[l], -sl[l]);
         hc[l] = make_double2(-h * h, 0.0);
         hc[count + l] = make_double2(-0.5 * kdz[l] * kdz[l], 0.0);
         hc[2 * count + l] = make_double2(0.0, -kdz[l]);
@@ -184,7 +197,7 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     };
     const dim3 ge(nblocks(nn), count);
 
-    // 2. y = (kdz/2^s)^2 * (-1) * Omega, in place
+    // 2. y = (kdz / 2^s_l)^2 * (-1) * Omega, in place
     scale_layers_kernel<<<ge, 256, 0, st>>>(nn, a_y, Om);
     count_launch();
     const double2* y = Om;
@@ -206,30 +219,91 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         SC_TRY(mm(Y4, n2, nn, P2, n2, nn, out, n2, nn, one, one, nullptr));
     }
 
-    // 4. s - 1 double-angle steps
-    for (int step = 1; step < s; ++step) {
-        SC_TRY(mm(G, n2, nn, F, n2, nn, P1, n2, nn, one, zero, nullptr));
-        set_diag_kernel<<<ge, 256, 0, st>>>(n2, n2, nn, -1.0, P2);
+    // 4. s_l - 1 double-angle steps per layer.  Each layer's current F and G
+    // live in F or P2 and in G or P1; step j runs over the layers with s_l > j.
+    std::vector<double2*> Fc(count), Fo(count), Gc(count), Go(count);
+    for (int l = 0; l < count; ++l) {
+        Fc[l] = F + (long long)l * nn;
+        Fo[l] = P2 + (long long)l * nn;
+        Gc[l] = G + (long long)l * nn;
+        Go[l] = P1 + (long long)l * nn;
+    }
+    std::vector<void*> tab;
+    std::vector<std::pair<size_t, int>> steps;   // (table offset, active layers)
+    for (int j = 1; j < smax; ++j) {
+        std::vector<int> act;
+        for (int l = 0; l < count; ++l)
+            if (sl[l] > j) act.push_back(l);
+        steps.emplace_back(tab.size(), (int)act.size());
+        for (int l : act) tab.push_back(Gc[l]);
+        for (int l : act) tab.push_back(Fc[l]);
+        for (int l : act) tab.push_back(Go[l]);
+        for (int l : act) tab.push_back(Fo[l]);
+        for (int l : act) {
+            std::swap(Fc[l], Fo[l]);
+            std::swap(Gc[l], Go[l]);
+        }
+    }
+    const size_t last = tab.size();
+    for (int l = 0; l < count; ++l) tab.push_back(Gc[l]);
+    for (int l = 0; l < count; ++l) tab.push_back(Fc[l]);
+    for (int l = 0; l < count; ++l) tab.push_back(Go[l]);
+    void** dtab = nullptr;
+    SC_TRY(eng.ws->get(&dtab, tab.size(), WS_MFUN_PTR, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(void*) * tab.size(), cudaMemcpyHostToDevice, st));
+    auto cp = [&](size_t o) { return reinterpret_cast<const double2* const*>(dtab + o); };
+    auto mp = [&](size_t o) { return reinterpret_cast<double2* const*>(dtab + o); };
+    // one batched product with any operand given by a pointer table (Ap/Bp/Cp) or by base + stride
+    auto mmp = [&](const double2* const* Ap, const double2* A, long long sA, const double2* const* Bp,
+                   const double2* Bm, long long sB, double2* const* Cp, double2* Cm, int ldc, long long sC,
+                   double2 alpha, double2 beta, const double2* alphas, int batch) {
+        GemmArgs g;
+        g.m = n2;
+        g.n = n2;
+        g.k = n2;
+        g.alpha = alpha;
+        g.beta = beta;
+        g.alphas = alphas;
+        g.Ap = Ap;
+        g.A = A;
+        g.lda = n2;
+        g.sA = sA;
+        g.Bp = Bp;
+        g.B = Bm;
+        g.ldb = n2;
+        g.sB = sB;
+        g.Cp = Cp;
+        g.C = Cm;
+        g.ldc = ldc;
+        g.sC = sC;
+        return eng.run(st, g, batch);
+    };
+    const double2 two = make_double2(2.0, 0.0);
+    for (const auto& sp : steps) {
+        const int na = sp.second;
+        const size_t gc = sp.first, fc = gc + na, go = fc + na, fo = go + na;
+        SC_TRY(mmp(cp(gc), nullptr, 0, cp(fc), nullptr, 0, mp(go), nullptr, n2, 0, one, zero, nullptr, na));  // G F
+        SC_TRY(mmp(cp(fc), nullptr, 0, cp(fc), nullptr, 0, mp(fo), nullptr, n2, 0, two, zero, nullptr, na));  // 2 F^2
+        add_diag_ptr_kernel<<<dim3((n2 + 255) / 256, na), 256, 0, st>>>(n2, -1.0, mp(fo));                     // - I
         count_launch();
-        SC_TRY(mm(F, n2, nn, F, n2, nn, P2, n2, nn, make_double2(2.0, 0.0), one, nullptr));
-        std::swap(G, P1);
-        std::swap(F, P2);
+        SC_CHECK_LAUNCH("add_diag_ptr");
     }
 
     // 5. last step straight into the quadrants of T (n4 x n4 per layer)
+    const size_t lg = last, lf = last + count, lgo = last + 2 * (size_t)count;
     double2* T11 = T;
     double2* T21 = T + n2;
     double2* T12 = T + (long long)n2 * n4;
     double2* T22 = T + (long long)n2 * n4 + n2;
-    SC_TRY(mm(G, n2, nn, G, n2, nn, Y2, n2, nn, one, zero, a_h));          // H = (t^2/2) G^2
-    SC_TRY(mm(G, n2, nn, F, n2, nn, P1, n2, nn, one, zero, nullptr));     // G_t = G F
+    SC_TRY(mmp(cp(lg), nullptr, 0, cp(lg), nullptr, 0, nullptr, Y2, n2, nn, one, zero, a_h, count));  // H = (t^2/2) G^2
+    SC_TRY(mmp(cp(lg), nullptr, 0, cp(lf), nullptr, 0, mp(lgo), nullptr, n2, 0, one, zero, nullptr, count));  // G_t
     set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, -1.0, T11);
     set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, 1.0, T22);
     count_launch(2);
     SC_CHECK_LAUNCH("set_diag");
-    SC_TRY(mm(F, n2, nn, F, n2, nn, T11, n4, s4, make_double2(2.0, 0.0), one, nullptr));   // F_t = 2F^2 - I
-    SC_TRY(mm(P1, n2, nn, B, n2, nn, T12, n4, s4, one, zero, a_off));      // -t G_t B
-    SC_TRY(mm(C, n2, nn, P1, n2, nn, T21, n4, s4, one, zero, a_off));      // -t C G_t
+    SC_TRY(mmp(cp(lf), nullptr, 0, cp(lf), nullptr, 0, nullptr, T11, n4, s4, two, one, nullptr, count));  // 2F^2 - I
+    SC_TRY(mmp(cp(lgo), nullptr, 0, nullptr, B, nn, nullptr, T12, n4, s4, one, zero, a_off, count));      // -t G_t B
+    SC_TRY(mmp(nullptr, C, nn, cp(lgo), nullptr, 0, nullptr, T21, n4, s4, one, zero, a_off, count));      // -t C G_t
     SC_TRY(mm(Y2, n2, nn, B, n2, nn, Y3, n2, nn, one, zero, nullptr));     // H B
     SC_TRY(mm(C, n2, nn, Y3, n2, nn, T22, n4, s4, one, one, nullptr));     // I + C H B
     return SC_OK;

@@ -1,0 +1,113 @@
+"""Coupled-wave (.cw) files in the reference's byte layout and record frame.
+
+Layout (CoupledWaveStructure.h:63-125): u64 sizeof(double) = 8; u64 #Pi, the
+incident records; u64 #layers; per layer: f64 z, u64 #Pr, records, u64 #Pt,
+records.  One record = sizeof(tira::planewave<double>) = 80 bytes =
+{E0x, E0y, kx, ky, kz} complex128.
+
+Record frame: tira's planewave keeps E0 in a frame whose z axis is the real
+propagation direction Re(k)/|Re(k)| (the minimal rotation taking z-hat
+there), and the file stores the first two components of E0 in that frame.
+getE0() rebuilds the third from k . E = 0 in the same frame.  This reading
+reproduces every record of the reference's shipped data/psf.cw and the
+incident and transmitted records of x64/a.cw from their restated solves.
+"""
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+
+def frames(k):
+    """(N, 3, 3) rotations whose third column is Re(k)/|Re(k)| (minimal rotation from z-hat)."""
+    kr = np.real(np.asarray(k, dtype=np.complex128)).reshape(-1, 3)
+    kh = kr / np.linalg.norm(kr, axis=1, keepdims=True)
+    ax0, ax1, c = -kh[:, 1], kh[:, 0], kh[:, 2]
+    s2 = ax0 * ax0 + ax1 * ax1
+    small = s2 < 1e-30
+    f = np.where(small, 0.0, (1.0 - c) / np.where(small, 1.0, s2))
+    R = np.zeros((len(kh), 3, 3))
+    R[:, 0, 0] = 1.0 - f * ax1 * ax1
+    R[:, 0, 1] = f * ax0 * ax1
+    R[:, 0, 2] = ax1
+    R[:, 1, 0] = f * ax0 * ax1
+    R[:, 1, 1] = 1.0 - f * ax0 * ax0
+    R[:, 1, 2] = -ax0
+    R[:, 2, 0] = -ax1
+    R[:, 2, 1] = ax0
+    R[:, 2, 2] = c
+    down = small & (c < 0)                       # straight down: half turn about x
+    R[small] = np.eye(3)
+    R[down] = np.diag([1.0, -1.0, -1.0])
+    return R
+
+
+def to_record(E, k):
+    """Cartesian E0 (N, 3) -> the stored pair (N, 2)."""
+    R = frames(k)
+    return np.einsum("nij,ni->nj", R, np.asarray(E, dtype=np.complex128).reshape(-1, 3))[:, :2]
+
+
+def from_record(E2, k):
+    """Stored pair (N, 2) -> Cartesian E0 (N, 3), the third local component from k . E = 0."""
+    k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
+    E2 = np.asarray(E2, dtype=np.complex128).reshape(-1, 2)
+    R = frames(k)
+    kp = np.einsum("nij,ni->nj", R, k)
+    ez = np.where(kp[:, 2] != 0, -(kp[:, 0] * E2[:, 0] + kp[:, 1] * E2[:, 1]) / np.where(kp[:, 2] != 0, kp[:, 2], 1),
+                  0)
+    loc = np.stack([E2[:, 0], E2[:, 1], ez], 1)
+    return np.einsum("nij,nj->ni", R, loc)
+
+
+def _records(E, k):
+    E = np.asarray(E, dtype=np.complex128).reshape(-1, 3)
+    rec = np.empty((len(E), 5), dtype=np.complex128)
+    if len(E):
+        rec[:, 0:2] = to_record(E, k)
+        rec[:, 2:5] = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
+    return rec.tobytes()
+
+
+def save(path, Pi_E, Pi_k, layers):
+    """Write a .cw file.  E arguments are Cartesian E0 (N, 3); layers = [(z, Pr_E, Pr_k, Pt_E, Pt_k)]."""
+    with open(path, "wb") as f:
+        f.write(struct.pack("<QQ", 8, len(Pi_E)))
+        f.write(_records(Pi_E, Pi_k))
+        f.write(struct.pack("<Q", len(layers)))
+        for z, PrE, Prk, PtE, Ptk in layers:
+            f.write(struct.pack("<dQ", float(z), len(PrE)))
+            f.write(_records(PrE, Prk))
+            f.write(struct.pack("<Q", len(PtE)))
+            f.write(_records(PtE, Ptk))
+
+
+def load(path):
+    """Read a .cw file: (Pi_E, Pi_k, layers) with Cartesian E0 (N, 3) as getE0() rebuilds it."""
+    b = open(path, "rb").read()
+    sz, npi = struct.unpack_from("<QQ", b, 0)
+    if sz != 8:
+        raise ValueError("only double-precision .cw files are supported")
+    o = 16
+
+    def recs(count):
+        nonlocal o
+        r = np.frombuffer(b, dtype=np.complex128, count=5 * count, offset=o).reshape(count, 5)
+        o += 80 * count
+        k = r[:, 2:5].copy()
+        return from_record(r[:, 0:2], k) if count else np.zeros((0, 3), np.complex128), k
+
+    PiE, Pik = recs(npi)
+    (nl,) = struct.unpack_from("<Q", b, o)
+    o += 8
+    layers = []
+    for _ in range(nl):
+        z, npr = struct.unpack_from("<dQ", b, o)
+        o += 16
+        PrE, Prk = recs(npr)
+        (npt,) = struct.unpack_from("<Q", b, o)
+        o += 8
+        PtE, Ptk = recs(npt)
+        layers.append((z, PrE, Prk, PtE, Ptk))
+    return PiE, Pik, layers
