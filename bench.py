@@ -15,7 +15,13 @@ the line also carries the batched FP64 path, the plain per-instance FP64 path
 20x20x8 um (seeded), 32 layers, lambda 0.6 um, 10 deg, x-polarised, 21x21
 orders, FP64 with interior fields; one step = one solve.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume]
+--workload layer: scatterlayer's focused-beam solve -- the reference's default
+stack (n 1, 1.4 + 0.05i, 1.4, 1; boundaries -3, 0, 3 um; lambda 1 um) under a
+1024 x 1024 polar beam (alpha 1 rad about z, y-polarised): 1,048,576 incident
+plane waves, one 24 x 24 complex system each; one step = the batched layer
+solve of the whole beam (incident waves resident in HBM), in plane waves/s.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume|layer]
 
 Under torchrun each rank solves its own seeded sweep / instance (weak scaling,
 no data-path collective); timing is on the device, max over ranks.
@@ -49,6 +55,12 @@ N_2M = 2 * 441
 SWEEP_NAME = ("uneven sweep: 256 instances = 64 seeded wavelengths in [0.4, 0.8] um x 0/10/20/30 deg incidence; "
               "each a seeded 4-16 layer stack of 64x64 random-disk maps (n 1.0-1.6, 25x25 um period, 0.1-0.5 um "
               "layers); orders drawn from {7,11,15,21,25}^2; x-pol; R/T only")
+LAYER_METRIC = "plane waves/s through a homogeneous multilayer stack (scatterlayer focused-beam solve)"
+LAYER_UNIT = "waves/s"
+LAYER_BEAM = 1024
+LAYER_STACK = dict(n=(1.0, 1.4, 1.4, 1.0), kappa=(0.05,), z=(-3.0, 0.0, 3.0))
+LAYER_NAME = ("scatterlayer default stack (n 1, 1.4+0.05i, 1.4, 1; boundaries -3, 0, 3 um; lambda 1 um) under a "
+              "1024x1024 polar beam (alpha 1 rad about z, y-pol): 1,048,576 plane waves, 24x24 complex system each")
 MIXED = 1          # SC_SWEEP_MIXED: int8 tcgen05 digit-sliced products, 7 slices
 PLAIN_EVERY = 8    # the per-instance FP64 path is timed on every 8th instance
 
@@ -169,6 +181,8 @@ def run_reference(args):
         return 0
     if args.workload == "sweep":
         return run_sweep_reference(args)
+    if args.workload == "layer":
+        return run_layer_reference(args)
     for _ in range(args.warmup):
         cpu_layer_sample(0)
     ts = [cpu_layer_sample(0) for _ in range(args.steps)]
@@ -568,6 +582,161 @@ def run_sweep_ours(args):
         dist.destroy_process_group()
     return 0
 
+def cpu_layer_waves(k, E, count):
+    """The oracle's per-wave solve (ScatterLayer.cpp:110-266 restated, scipy LAPACK) on `count` waves."""
+    from oracle import scatterlayer as osl
+    L, n, kappa, z, ri = osl.fill_layers(LAYER_STACK["n"], LAYER_STACK["kappa"], LAYER_STACK["z"])
+    t0 = time.perf_counter()
+    for w in range(count):
+        osl.solve_wave(k[w], E[w], ri, z, 2 * math.pi, n[0])
+    return count / (time.perf_counter() - t0)
+
+
+def run_layer_reference(args):
+    from oracle import scatterlayer as osl
+    kc, e = osl.incident(1.0, (0, 0, 1), (0, 0), (1, 0), (0, 0), LAYER_STACK["n"][0])
+    ks, Es = osl.beam_polar(1.0, kc, e, 64, 64)            # a 4096-wave sample of the same beam law
+    per = 2000
+    for _ in range(args.warmup):
+        cpu_layer_waves(ks, Es, 200)
+    vals = [cpu_layer_waves(ks, Es, per) for _ in range(args.steps)]
+    value = statistics.median(vals)
+    sample = (f"{per} waves per step of a 64x64 beam with the workload's beam law and stack; one 24x24 complex "
+              "solve per wave (numpy/scipy restatement of ScatterLayer.cpp, 1 thread like the reference's loop)")
+    line = {"impl": "reference", "metric": LAYER_METRIC, "value": value, "unit": LAYER_UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": LAYER_NAME},
+            "cpu_baseline": {"value": value, "unit": LAYER_UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": LAYER_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_layer_ours(args):
+    import torch
+    from scattersim_b200 import layers, solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = solver.Context(local)
+    L, n, kappa, z = layers.fill_layers(LAYER_STACK["n"], LAYER_STACK["kappa"], LAYER_STACK["z"])
+    kc, e = layers._centre(1.0, (0, 0, 1), (0, 0), (1, 0), (0, 0), n[0])
+    ks, Es = layers.beam(ctx, 1.0, kc, e, 1.0, 0.0, (LAYER_BEAM, LAYER_BEAM))
+    W = int(ks.shape[0])
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(fn):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        layers.layer_solve(ctx, ks, Es, n, kappa, z, 1.0)
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    l0 = ctx.launches()
+    step_ms = []
+    for _ in range(args.steps):
+        out, ms = timed(lambda: layers.layer_solve(ctx, ks, Es, n, kappa, z, 1.0))
+        step_ms.append(ms)
+    launches = ctx.launches() - l0
+    barrier()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * W * args.steps / (total_ms / 1e3)
+
+    # end to end: incident waves from pinned host memory, every output back to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        hk = ks.cpu().pin_memory()
+        hE = Es.cpu().pin_memory()
+        dk, dE = torch.empty_like(ks), torch.empty_like(Es)
+        houts = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in out]
+        barrier()
+        e2e_ms = []
+        for _ in range(max(1, min(3, args.steps))):
+            def step():
+                dk.copy_(hk, non_blocking=True)
+                dE.copy_(hE, non_blocking=True)
+                r = layers.layer_solve(ctx, dk, dE, n, kappa, z, 1.0)
+                for h, o in zip(houts, r):
+                    h.copy_(o, non_blocking=True)
+                return r
+            _, ms = timed(step)
+            e2e_ms.append(ms)
+        e2e = {"value": world * W * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) / 1e3), "unit": LAYER_UNIT,
+               "h2d_bytes_per_step": int(hk.numel() * 8 + hE.numel() * 16),
+               "d2h_bytes_per_step": int(sum(h.numel() for h in houts) * 16)}
+
+    # roofline: FP64 LU of one 6L x 6L complex system per wave against the measured FP64 FMA rate
+    fp64_peak = ctx.fp64_peak_tflops()
+    per_ms = statistics.median(step_ms)
+    flops = W * (8.0 / 3.0) * (6 * L) ** 3
+    achieved = flops / (per_ms / 1e3) / 1e12
+    algo_bytes = W * (24 + 48 + 4 * 3 * (L - 1) * 16)
+    tr = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "layer_solve_traffic.json")) as f:
+            tr = json.load(f)["bytes_per_wave"] * W
+    except Exception:
+        pass
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": tr,
+                "kernel": "layer_solve_kernel (one warp per wave, LU with partial pivoting in shared memory)",
+                "peak_source": "FP64 FMA pipe probe measured in this run",
+                "flops_per_wave": (8.0 / 3.0) * (6 * L) ** 3, "algorithmic_bytes_per_wave": algo_bytes / W,
+                "hbm_gbs_achieved": algo_bytes / (per_ms / 1e3) / 1e9,
+                "hbm_peak_gbs": float(_peaks().get("hbm_gbs", 6650.0))}
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            hk_np, hE_np = ks[:2000].cpu().numpy(), Es[:2000].cpu().numpy()
+            v = cpu_layer_waves(hk_np, hE_np, 2000)
+            cpu = {"value": v, "unit": LAYER_UNIT, "cores": 1, "kind": "port",
+                   "sample": "the first 2000 waves of the workload's beam through the oracle's per-wave solve "
+                             "(numpy/scipy restatement of ScatterLayer.cpp, 1 thread like the reference's loop)"}
+        line = {"metric": LAYER_METRIC, "value": value, "unit": LAYER_UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": LAYER_NAME, "l2": "flushed between steps (256 MB write, untimed); "
+                           "outputs 604 MB > L2", "parallelism": f"independent beam per rank x{world}"},
+                "clocks": clocks, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -577,12 +746,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "volume"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "volume", "layer"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "sweep":
         return run_sweep_ours(args)
+    if args.workload == "layer":
+        return run_layer_ours(args)
     return run_volume_ours(args)
 
 

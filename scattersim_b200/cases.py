@@ -23,6 +23,10 @@ Cases (seeded synthetic samples, see samples.py):
   gemm          batched complex GEMM throughput at the shapes of the solves
   gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
                 twice each (the profiling case of the tcgen05 MMA kernel)
+  layer [N]     scatterlayer's default stack (4 layers) under an N x N polar beam
+                (default 1024: 1,048,576 waves) and a 15-layer stack under a
+                256 x 256 beam: waves/s of the beam and of the batched layer
+                solve (bench.py --workload layer adds the host baseline)
 Prints the per-stage device milliseconds of the last repeat.
 """
 from __future__ import annotations
@@ -66,6 +70,8 @@ def main(argv):
         return fno_train_case()
     if name == "gemm_int8":
         return gemm_int8_case()
+    if name == "layer":
+        return layer_case(int(argv[2]) if len(argv) > 2 else 1024)
     if name in ("sweep", "sweep_plain", "sweep_mixed"):
         count = int(argv[2]) if len(argv) > 2 and not argv[2].startswith("--") else 256
         opt = dict(zip(argv[3::2], argv[4::2])) if len(argv) > 3 else {}
@@ -259,6 +265,42 @@ def sweep_case(name, count, choices_in=None, choices_out=None):
         import json
         with open(choices_out, "w") as f:
             json.dump(ctx.gemm_choices(), f)
+    ctx.close()
+    return 0
+
+
+
+
+def layer_case(N=1024, reps=5):
+    """Batched homogeneous-layer solves: device time per call (CUDA events), waves/s."""
+    import numpy as np
+    import torch
+
+    from . import layers, solver
+    ctx = solver.Context(0)
+    stacks = [("scatterlayer defaults (4 layers)", dict(n=(1, 1.4, 1.4, 1.0), kappa=(0.05,), z=(-3.0, 0.0, 3.0)), N),
+              ("15 layers", dict(n=[1.0] + [1.2 + 0.05 * i for i in range(14)], kappa=[0.01] * 14,
+                                 z=[-3.0 + 0.4 * i for i in range(14)]), 256)]
+    for label, st, nb in stacks:
+        L, n, kappa, z = layers.fill_layers(st["n"], st["kappa"], st["z"])
+        kc, e = layers._centre(1.0, (0, 0, 1), (0, 0), (1, 0), (0, 0), n[0])
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        tb, ts = [], []
+        for r in range(reps + 2):
+            ev[0].record()
+            ks, Es = layers.beam(ctx, 1.0, kc, e, 1.0, 0.0, (nb, nb))
+            ev[1].record()
+            out = layers.layer_solve(ctx, ks, Es, n, kappa, z, 1.0)
+            ev[2].record()
+            torch.cuda.synchronize()
+            if r >= 2:
+                tb.append(ev[0].elapsed_time(ev[1]))
+                ts.append(ev[1].elapsed_time(ev[2]))
+        W = nb * nb
+        tbm, tsm = float(np.median(tb)), float(np.median(ts))
+        flops = W * (8.0 / 3.0) * (6 * L) ** 3          # LU of the 6L x 6L complex system
+        print(f"{label}: {W} waves; beam {tbm:.3f} ms ({W / tbm * 1e3:.3e} waves/s); "
+              f"layer solve {tsm:.3f} ms ({W / tsm * 1e3:.3e} waves/s, {flops / tsm / 1e9:.2f} TFLOP/s FP64 LU)")
     ctx.close()
     return 0
 
