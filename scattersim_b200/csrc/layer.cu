@@ -16,10 +16,10 @@
 // layer_solve_kernel: one warp per wave.  The warp builds the system in its
 // own slice of shared memory (row stride n + 1 so that a quarter warp's
 // 16-byte column accesses fall in distinct banks), factors it by LU with
-// partial pivoting (pivot search by warp arg-max, trailing update spread over
-// the lanes), back-substitutes and writes the wound waves.  The reference
-// uses colPivHouseholderQr; both are backward stable on this square system
-// and agree to rounding.  A wave whose system has an exact zero pivot gets
+// partial pivoting (pivot search by warp arg-max; in the trailing update each
+// lane owns a column and walks rows), back-substitutes and writes the wound
+// waves.  The reference uses colPivHouseholderQr; both are backward stable on
+// this square system and agree to rounding.  A wave whose system has an exact zero pivot gets
 // SC_SINGULAR in its status word.
 #include <cmath>
 #include <vector>
@@ -176,7 +176,7 @@ __global__ void layer_solve_kernel(LayerArgs p, const double* __restrict__ kin, 
         double bv = -1.0;
         int bi = n;
         for (int i = j + lane; i < n; i += 32) {
-            const double v = cabs1(A[(size_t)i * ld + j]);
+            const double v = cabs1(A[i * ld + j]);
             if (v > bv) { bv = v; bi = i; }
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -190,9 +190,9 @@ __global__ void layer_solve_kernel(LayerArgs p, const double* __restrict__ kin, 
         }
         if (bi != j) {
             for (int c = lane; c < n; c += 32) {
-                const double2 t = A[(size_t)j * ld + c];
-                A[(size_t)j * ld + c] = A[(size_t)bi * ld + c];
-                A[(size_t)bi * ld + c] = t;
+                const double2 t = A[j * ld + c];
+                A[j * ld + c] = A[bi * ld + c];
+                A[bi * ld + c] = t;
             }
             if (lane == 0) {
                 const double2 t = b[j];
@@ -201,23 +201,40 @@ __global__ void layer_solve_kernel(LayerArgs p, const double* __restrict__ kin, 
             }
         }
         __syncwarp();
-        const double2 piv = A[(size_t)j * ld + j];
-        for (int i = j + 1 + lane; i < n; i += 32) A[(size_t)i * ld + j] = cdiv(A[(size_t)i * ld + j], piv);
+        // multipliers: one reciprocal of the pivot per step
+        const double2 rpiv = cdiv(make_double2(1.0, 0.0), A[j * ld + j]);
+        for (int i = j + 1 + lane; i < n; i += 32) A[i * ld + j] = cmul(A[i * ld + j], rpiv);
         __syncwarp();
+        // trailing update A(i, c) -= A(i, j) A(j, c), i, c > j: a lane keeps its column's
+        // pivot-row entry in registers and walks rows; with m <= 32 columns the warp
+        // is split into 32 / m row groups (one division per step, none per element)
         const int m = n - j - 1;
-        for (int t = lane; t < m * m; t += 32) {
-            const int i = j + 1 + t / m, c = j + 1 + t % m;
-            A[(size_t)i * ld + c] = csub(A[(size_t)i * ld + c], cmul(A[(size_t)i * ld + j], A[(size_t)j * ld + c]));
+        if (m > 0 && m <= 32) {
+            const int groups = 32 / m, cl = lane % m, r0 = lane / m;
+            if (r0 < groups) {
+                const int c = j + 1 + cl;
+                const double2 ajc = A[j * ld + c];
+#pragma unroll 4
+                for (int i = j + 1 + r0; i < n; i += groups)
+                    A[i * ld + c] = csub(A[i * ld + c], cmul(A[i * ld + j], ajc));
+            }
+        } else if (m > 32) {
+            for (int c = j + 1 + lane; c < n; c += 32) {
+                const double2 ajc = A[j * ld + c];
+#pragma unroll 4
+                for (int i = j + 1; i < n; ++i)
+                    A[i * ld + c] = csub(A[i * ld + c], cmul(A[i * ld + j], ajc));
+            }
         }
-        for (int i = j + 1 + lane; i < n; i += 32) b[i] = csub(b[i], cmul(A[(size_t)i * ld + j], b[j]));
+        for (int i = j + 1 + lane; i < n; i += 32) b[i] = csub(b[i], cmul(A[i * ld + j], b[j]));
         __syncwarp();
     }
     if (!singular) {
         for (int j = n - 1; j >= 0; --j) {
-            const double2 xj = cdiv(b[j], A[(size_t)j * ld + j]);
+            const double2 xj = cdiv(b[j], A[j * ld + j]);
             __syncwarp();
             if (lane == 0) b[j] = xj;
-            for (int i = lane; i < j; i += 32) b[i] = csub(b[i], cmul(A[(size_t)i * ld + j], xj));
+            for (int i = lane; i < j; i += 32) b[i] = csub(b[i], cmul(A[i * ld + j], xj));
             __syncwarp();
         }
     }
