@@ -213,17 +213,15 @@ __global__ void layer_solve_kernel(LayerArgs p, const double* __restrict__ kin, 
             const int groups = 32 / m, cl = lane % m, r0 = lane / m;
             if (r0 < groups) {
                 const int c = j + 1 + cl;
-                const double2 ajc = A[j * ld + c];
+                const double2 najc = cneg(A[j * ld + c]);
 #pragma unroll 4
-                for (int i = j + 1 + r0; i < n; i += groups)
-                    A[i * ld + c] = csub(A[i * ld + c], cmul(A[i * ld + j], ajc));
+                for (int i = j + 1 + r0; i < n; i += groups) A[i * ld + c] = cfma(A[i * ld + j], najc, A[i * ld + c]);
             }
         } else if (m > 32) {
             for (int c = j + 1 + lane; c < n; c += 32) {
-                const double2 ajc = A[j * ld + c];
+                const double2 najc = cneg(A[j * ld + c]);
 #pragma unroll 4
-                for (int i = j + 1; i < n; ++i)
-                    A[i * ld + c] = csub(A[i * ld + c], cmul(A[i * ld + j], ajc));
+                for (int i = j + 1; i < n; ++i) A[i * ld + c] = cfma(A[i * ld + j], najc, A[i * ld + c]);
             }
         }
         for (int i = j + 1 + lane; i < n; i += 32) b[i] = csub(b[i], cmul(A[i * ld + j], b[j]));

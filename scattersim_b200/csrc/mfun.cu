@@ -22,7 +22,9 @@
 //   s_l - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
 //   sinh 2a / 2a = (sinh a / a) cosh a), step j batched over the layers with
 //   s_l > j (pointer tables follow each layer's current F and G buffers);
-//   the last step also forms H_t = (t^2 / 2) G_{t/2}^2 (cosh 2a - 1 = 2 sinh^2 a).
+//   the last step forms the blocks from the half-angle F and G with
+//   G_t = G F and H_t = (t^2 / 2) G^2 (cosh 2a - 1 = 2 sinh^2 a): six products,
+//   since F and G commute (F (G B), (C G) F, (C G)(G B)).
 // Every product is a batched complex GEMM over all layers of the batch with
 // per-layer scalars, run by the caller's GEMM engine (FP64 tensor-pipe tiles,
 // or int8 digit slices on the tcgen05 tensor cores).
@@ -247,7 +249,6 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     const size_t last = tab.size();
     for (int l = 0; l < count; ++l) tab.push_back(Gc[l]);
     for (int l = 0; l < count; ++l) tab.push_back(Fc[l]);
-    for (int l = 0; l < count; ++l) tab.push_back(Go[l]);
     void** dtab = nullptr;
     SC_TRY(eng.ws->get(&dtab, tab.size(), WS_MFUN_PTR, st));
     SC_CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(void*) * tab.size(), cudaMemcpyHostToDevice, st));
@@ -289,23 +290,27 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         SC_CHECK_LAUNCH("add_diag_ptr");
     }
 
-    // 5. last step straight into the quadrants of T (n4 x n4 per layer)
-    const size_t lg = last, lf = last + count, lgo = last + 2 * (size_t)count;
+    // 5. last step straight into the quadrants of T (n4 x n4 per layer), from F and
+    // G at the half angle.  F and G commute (both are functions of Omega), so
+    //   G_t B = G F B = F (G B),  C G_t = (C G) F,  C H_t B = (t^2 / 2) (C G)(G B):
+    // six products, with G B and C G shared.
+    const size_t lg = last, lf = last + count;
     double2* T11 = T;
     double2* T21 = T + n2;
     double2* T12 = T + (long long)n2 * n4;
     double2* T22 = T + (long long)n2 * n4 + n2;
-    SC_TRY(mmp(cp(lg), nullptr, 0, cp(lg), nullptr, 0, nullptr, Y2, n2, nn, one, zero, a_h, count));  // H = (t^2/2) G^2
-    SC_TRY(mmp(cp(lg), nullptr, 0, cp(lf), nullptr, 0, mp(lgo), nullptr, n2, 0, one, zero, nullptr, count));  // G_t
+    double2* GB = Y2;
+    double2* CG = Y3;
+    SC_TRY(mmp(cp(lg), nullptr, 0, nullptr, B, nn, nullptr, GB, n2, nn, one, zero, nullptr, count));     // G B
+    SC_TRY(mmp(nullptr, C, nn, cp(lg), nullptr, 0, nullptr, CG, n2, nn, one, zero, nullptr, count));     // C G
     set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, -1.0, T11);
     set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, 1.0, T22);
     count_launch(2);
     SC_CHECK_LAUNCH("set_diag");
     SC_TRY(mmp(cp(lf), nullptr, 0, cp(lf), nullptr, 0, nullptr, T11, n4, s4, two, one, nullptr, count));  // 2F^2 - I
-    SC_TRY(mmp(cp(lgo), nullptr, 0, nullptr, B, nn, nullptr, T12, n4, s4, one, zero, a_off, count));      // -t G_t B
-    SC_TRY(mmp(nullptr, C, nn, cp(lgo), nullptr, 0, nullptr, T21, n4, s4, one, zero, a_off, count));      // -t C G_t
-    SC_TRY(mm(Y2, n2, nn, B, n2, nn, Y3, n2, nn, one, zero, nullptr));     // H B
-    SC_TRY(mm(C, n2, nn, Y3, n2, nn, T22, n4, s4, one, one, nullptr));     // I + C H B
+    SC_TRY(mmp(cp(lf), nullptr, 0, nullptr, GB, nn, nullptr, T12, n4, s4, one, zero, a_off, count));     // -t F (G B)
+    SC_TRY(mmp(nullptr, CG, nn, cp(lf), nullptr, 0, nullptr, T21, n4, s4, one, zero, a_off, count));     // -t (C G) F
+    SC_TRY(mm(CG, n2, nn, GB, n2, nn, T22, n4, s4, one, one, a_h));        // I + (t^2/2) (C G)(G B)
     return SC_OK;
 }
 
