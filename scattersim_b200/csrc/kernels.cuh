@@ -19,7 +19,7 @@ enum WsSlot {
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
     WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR, WS_TUNE_C, WS_TUNE_P,
-    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR,
+    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR, WS_MFUN_OUT, WS_CHAIN_T,
     WS_COUNT
 };
 
@@ -205,9 +205,11 @@ sc_status assemble_bc(cudaStream_t st, const double2* Nf, const double2* Nif, in
 sc_status assemble_bc_layers(cudaStream_t st, const double2* Nf, const double2* Nif, int L, int Mx, int My,
                              const double* lat, const int* inst, const double* kinv, double2* Bm, double2* Cm);
 
-// mfun.cu: T_l = exp(-i kdz_l Phi_l) (n4 x n4, n4 = 2 n2) for a batch of layers
-// from B, C and Omega = B C (destroyed).  scr: transfer_scratch_blocks() * count
-// * n2^2 entries; dnorm: count doubles; dcoef: 3 * count entries.
+// mfun.cu: the inverse layer factor exp(-t_l Phi_l), t_l = i kdz_l, of a batch of
+// layers from B, C and Omega = B C (destroyed), in factored form: block l of T
+// (stride 4 n2^2) holds F, G B and C G of the half angle (n2 x n2 each, leading
+// dimension n2, at offsets 0, n2^2, 2 n2^2).  scr: transfer_scratch_blocks() *
+// count * n2^2 entries; dnorm: count doubles; dcoef: count entries.
 size_t transfer_scratch_blocks();
 sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, int count, const double2* B,
                                const double2* C, double2* Om, const std::vector<double>& kdz, double2* T,

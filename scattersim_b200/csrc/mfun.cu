@@ -22,9 +22,17 @@
 //   s_l - 1 steps of F <- 2 F^2 - I, G <- G F (cosh 2a = 2 cosh^2 a - 1,
 //   sinh 2a / 2a = (sinh a / a) cosh a), step j batched over the layers with
 //   s_l > j (pointer tables follow each layer's current F and G buffers);
-//   the last step forms the blocks from the half-angle F and G with
-//   G_t = G F and H_t = (t^2 / 2) G^2 (cosh 2a - 1 = 2 sinh^2 a): six products,
-//   since F and G commute (F (G B), (C G) F, (C G)(G B)).
+//   the factor is returned at the half angle, in factored form: with F, G of
+//   t / 2 (G_t = G F, H_t = (t^2 / 2) G^2 since cosh 2a - 1 = 2 sinh^2 a, and F,
+//   G commute as functions of Omega)
+//     exp(-t Phi) = [[ 2 F^2 - I,    -t F (G B)             ],
+//                    [ -t (C G) F,   I + (t^2/2) (C G)(G B) ]],
+//   so a layer is stored as F, G B and C G (three 2M x 2M blocks) and applied
+//   to a 4M x 3M vector block X = [X1; X2] by four products:
+//     U = (G B) X2, V = F X1, X1' = F (2 V - t U) - X1,
+//     X2' = X2 + (C G) ((t^2/2) U - t V)
+//   (sweep.cu), which is 32 M^3 fewer multiply-adds per layer than forming the
+//   4M x 4M factor and multiplying by it.
 // Every product is a batched complex GEMM over all layers of the batch with
 // per-layer scalars, run by the caller's GEMM engine (FP64 tensor-pipe tiles,
 // or int8 digit slices on the tcgen05 tensor cores).
@@ -55,17 +63,6 @@ __global__ void poly_block_kernel(int n, const double2* __restrict__ y, const do
         if (c4 != 0.0) v = cadd(v, cscale(Y4[i], c4));
         if (t % (n + 1) == 0) v.x += c0;
         out[i] = v;
-    }
-}
-
-// block_l (n x n at base + l * stride, leading dimension ld) = val * I
-__global__ void set_diag_kernel(int n, int ld, long long stride, double val, double2* __restrict__ base) {
-    double2* p = base + (long long)blockIdx.y * stride;
-    const long long nn = (long long)n * n;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t % n), c = (int)(t / n);
-        p[(long long)c * ld + r] = make_double2(r == c ? val : 0.0, 0.0);
     }
 }
 
@@ -132,8 +129,7 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         return SC_BADINPUT;
     }
     const long long nn = (long long)n2 * n2;
-    const int n4 = 2 * n2;
-    const long long s4 = (long long)n4 * n4;
+    const long long sT = 4 * nn;   // per-layer block of T (F, G B, C G in its first three quarters)
     double2* Y2 = scr;
     double2* Y3 = scr + (long long)count * nn;
     double2* Y4 = scr + 2LL * count * nn;
@@ -162,19 +158,15 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     }
     if (squarings) *squarings = smax;
 
-    // per-layer scalars: y scale, H factor t^2/2 = -(kdz)^2/2, off-diagonal factor -t = -i kdz
-    std::vector<double2> hc(3 * (size_t)count);
+    // per-layer y scale -(kdz / 2^s_l)^2
+    std::vector<double2> hc(count);
     for (int l = 0; l < count; ++l) {
         const double h = std::ldexp(kdz[l], -sl[l]);
         hc[l] = make_double2(-h * h, 0.0);
-        hc[count + l] = make_double2(-0.5 * kdz[l] * kdz[l], 0.0);
-        hc[2 * count + l] = make_double2(0.0, -kdz[l]);
     }
     SC_CUDA_TRY(cudaMemcpyAsync(dcoef, hc.data(), sizeof(double2) * hc.size(), cudaMemcpyHostToDevice, st));
     SC_CUDA_TRY(cudaStreamSynchronize(st));
     const double2* a_y = dcoef;
-    const double2* a_h = dcoef + count;
-    const double2* a_off = dcoef + 2 * count;
 
     const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
     auto mm = [&](const double2* A, int lda, long long sA, const double2* Bm, int ldb, long long sB, double2* Cm,
@@ -290,27 +282,16 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         SC_CHECK_LAUNCH("add_diag_ptr");
     }
 
-    // 5. last step straight into the quadrants of T (n4 x n4 per layer), from F and
-    // G at the half angle.  F and G commute (both are functions of Omega), so
-    //   G_t B = G F B = F (G B),  C G_t = (C G) F,  C H_t B = (t^2 / 2) (C G)(G B):
-    // six products, with G B and C G shared.
+    // 5. the factored layer: F, G B and C G (half angle) into the layer's block of T
     const size_t lg = last, lf = last + count;
-    double2* T11 = T;
-    double2* T21 = T + n2;
-    double2* T12 = T + (long long)n2 * n4;
-    double2* T22 = T + (long long)n2 * n4 + n2;
-    double2* GB = Y2;
-    double2* CG = Y3;
-    SC_TRY(mmp(cp(lg), nullptr, 0, nullptr, B, nn, nullptr, GB, n2, nn, one, zero, nullptr, count));     // G B
-    SC_TRY(mmp(nullptr, C, nn, cp(lg), nullptr, 0, nullptr, CG, n2, nn, one, zero, nullptr, count));     // C G
-    set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, -1.0, T11);
-    set_diag_kernel<<<ge, 256, 0, st>>>(n2, n4, s4, 1.0, T22);
-    count_launch(2);
-    SC_CHECK_LAUNCH("set_diag");
-    SC_TRY(mmp(cp(lf), nullptr, 0, cp(lf), nullptr, 0, nullptr, T11, n4, s4, two, one, nullptr, count));  // 2F^2 - I
-    SC_TRY(mmp(cp(lf), nullptr, 0, nullptr, GB, nn, nullptr, T12, n4, s4, one, zero, a_off, count));     // -t F (G B)
-    SC_TRY(mmp(nullptr, CG, nn, cp(lf), nullptr, 0, nullptr, T21, n4, s4, one, zero, a_off, count));     // -t (C G) F
-    SC_TRY(mm(CG, n2, nn, GB, n2, nn, T22, n4, s4, one, one, a_h));        // I + (t^2/2) (C G)(G B)
+    std::vector<void*> outp(count);
+    for (int l = 0; l < count; ++l) outp[l] = T + (long long)l * sT;
+    void** dout = nullptr;
+    SC_TRY(eng.ws->get(&dout, outp.size(), WS_MFUN_OUT, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(dout, outp.data(), sizeof(void*) * outp.size(), cudaMemcpyHostToDevice, st));
+    SC_TRY(copy_blocks(st, n2, n2, cp(lf), n2, reinterpret_cast<double2* const*>(dout), n2, count));        // F
+    SC_TRY(mmp(cp(lg), nullptr, 0, nullptr, B, nn, nullptr, T + nn, n2, sT, one, zero, nullptr, count));   // G B
+    SC_TRY(mmp(nullptr, C, nn, cp(lg), nullptr, 0, nullptr, T + 2 * nn, n2, sT, one, zero, nullptr, count));  // C G
     return SC_OK;
 }
 

@@ -9,10 +9,13 @@
 //   1. fft2_crop per instance into the group's coefficient arrays;
 //   2. B, C of every layer (per-layer lattice and k), Omega = B C;
 //   3. the inverse layer factors exp(-i k dz Phi) as matrix functions of Omega
-//      (mfun.cu) -- no eigendecomposition is needed for R/T;
-//   4. the chain X <- T_l^-1 X from f3 up through the stack, one batched GEMM
-//      per depth step over all instances still inside their stack (instances
-//      are sorted by depth, so the active ones are a prefix);
+//      (mfun.cu), kept in factored form (F, G B, C G) -- no eigendecomposition
+//      is needed for R/T;
+//   4. the chain X <- T_l^-1 X from f3 up through the stack, four batched
+//      GEMMs per depth step over all instances still inside their stack
+//      (instances are sorted by depth, so the active ones are a prefix):
+//      U = (G B) X2, V = F X1, X1' = F (2 V - t U) - X1,
+//      X2' = X2 + (C G) ((t^2/2) U - t V);
 //   5. the boundary systems (ScatterVolume.cpp:398-466), batched over
 //      instances: the reflected amplitudes enter only through per-order 3 x 3
 //      blocks, so they are eliminated order by order and a 3M x 3M system in
@@ -50,6 +53,33 @@ struct Carve {
         return p;
     }
 };
+
+// Between the products of one chain step, per instance b (U, V: n2 x ncol, leading
+// dimension n2; X: n4 x ncol, leading dimension n4 = 2 n2):
+//   V <- 2 V - t U,  U <- (t^2 / 2) U - t V (both from the old U, V),
+//   Xn <- Xc (the X1' product then runs with beta = -1, the X2' product with beta = +1)
+__global__ void chain_mix_kernel(int n2, int ncol, const double2* __restrict__ tv, double2* const* __restrict__ Up,
+                                 double2* const* __restrict__ Vp, const double2* const* __restrict__ Xc,
+                                 double2* const* __restrict__ Xn) {
+    const int b = blockIdx.y;
+    const double2 t = tv[b];
+    const double2 t2h = cscale(cmul(t, t), 0.5);
+    double2* U = Up[b];
+    double2* V = Vp[b];
+    const double2* xc = Xc[b];
+    double2* xn = Xn[b];
+    const long long tot = (long long)n2 * ncol;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e % n2), c = (int)(e / n2);
+        const double2 u = U[e], v = V[e];
+        V[e] = csub(cscale(v, 2.0), cmul(t, u));
+        U[e] = csub(cmul(t2h, u), cmul(t, v));
+        const long long x = (long long)c * (2 * n2) + r;
+        xn[x] = xc[x];
+        xn[x + n2] = xc[x + n2];
+    }
+}
 
 struct ChunkBufs {
     double *lat, *kinv, *kz0, *dnorm;
@@ -121,8 +151,9 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
     Carve real;
     real.base = base;
     ChunkBufs b = carve_chunk(real, nI, Ltot, maxZS1, Mx, My);
-    // device pointer tables: chain (maxZ * nI * 3), final copies (2 nI), outputs (2 nI)
-    const size_t nptr = (size_t)maxZ * nI * 3 + 4 * (size_t)nI;
+    // device pointer tables: chain (maxZ * nI * CHAIN_PTRS), final copies (2 nI), outputs (2 nI)
+    constexpr int CHAIN_PTRS = 9;
+    const size_t nptr = (size_t)maxZ * nI * CHAIN_PTRS + 4 * (size_t)nI;
     void** dptr = nullptr;
     SC_TRY(ws.get(&dptr, nptr, WS_SWEEP_PTR, st));
 
@@ -157,19 +188,39 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
     for (int a = 0; a < nI && reduced; ++a)
         for (const cplx& z : items[a]->plan.Sz0)
             if (std::abs(z) < 1e-9) reduced = false;
+    // chain step j for instance a (layer l, counted from the bottom of its stack):
+    // operands of the four products and the mix in between, and t = i kdz_l.
+    // U and V live in the transfer scratch, free once the layer factors exist.
+    const long long n2sq = (long long)n2 * n2, suv = 2LL * n2 * 3 * MF;
     std::vector<const void*> hptr(nptr);
+    std::vector<double2> htv((size_t)maxZ * nI, make_double2(0.0, 0.0));
     for (int j = 0; j < maxZ; ++j) {
-        const void** row = hptr.data() + (size_t)j * nI * 3;
+        const void** row = hptr.data() + (size_t)j * nI * CHAIN_PTRS;
         int act = 0;
         while (act < nI && items[act]->Z > j) ++act;
         for (int a = 0; a < act; ++a) {
             const int l = off[a] + items[a]->Z - 1 - j;
-            row[a] = b.T + l * s4;
-            row[nI + a] = ((j & 1) ? b.X1 : b.X0) + a * sX;
-            row[2 * nI + a] = ((j & 1) ? b.X0 : b.X1) + a * sX;
+            const double2* Tl = b.T + l * s4;                 // F | G B | C G
+            double2* Xc = ((j & 1) ? b.X1 : b.X0) + a * sX;
+            double2* Xn = ((j & 1) ? b.X0 : b.X1) + a * sX;
+            double2* U = b.scr + a * suv;
+            double2* V = U + (long long)n2 * 3 * MF;
+            row[0 * nI + a] = Tl + n2sq;          // G B
+            row[1 * nI + a] = Xc + n2;            // X2
+            row[2 * nI + a] = U;
+            row[3 * nI + a] = Tl;                 // F
+            row[4 * nI + a] = Xc;                 // X1 (and the whole of X for the mix)
+            row[5 * nI + a] = V;
+            row[6 * nI + a] = Xn;                 // X1'
+            row[7 * nI + a] = Tl + 2 * n2sq;      // C G
+            row[8 * nI + a] = Xn + n2;            // X2'
+            htv[(size_t)j * nI + a] = make_double2(0.0, kdz[l]);
         }
     }
-    const void** tail = hptr.data() + (size_t)maxZ * nI * 3;
+    double2* dtv = nullptr;
+    SC_TRY(ws.get(&dtv, htv.size(), WS_CHAIN_T, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(dtv, htv.data(), sizeof(double2) * htv.size(), cudaMemcpyHostToDevice, st));
+    const void** tail = hptr.data() + (size_t)maxZ * nI * CHAIN_PTRS;
     for (int a = 0; a < nI; ++a) {
         tail[a] = ((items[a]->Z & 1) ? b.X1 : b.X0) + a * sX;
         tail[nI + a] = b.A6 + a * s6 + (long long)3 * MF * n6 + 2 * MF;
@@ -217,27 +268,41 @@ sc_status solve_chunk(sc_context* ctx, std::vector<Item*> items, int Mx, int My,
     SC_CUDA_TRY(cudaEventRecord(ev[3], st));
     // 4. chain from f3 up through each stack
     SC_TRY(boundary_f3(st, MF, b.svec, 7LL * MF, b.X0, sX, nI));
+    const unsigned chain_blocks = (unsigned)std::min<long long>(1024, ((long long)n2 * 3 * MF + 255) / 256);
     for (int j = 0; j < maxZ; ++j) {
         int act = 0;
         while (act < nI && items[act]->Z > j) ++act;
-        void** row = dptr + (size_t)j * nI * 3;
-        GemmArgs g;
-        g.m = n4;
-        g.n = 3 * MF;
-        g.k = n4;
-        g.Ap = reinterpret_cast<const double2* const*>(row);
-        g.lda = n4;
-        g.Bp = reinterpret_cast<const double2* const*>(row + nI);
-        g.ldb = n4;
-        g.Cp = reinterpret_cast<double2* const*>(row + 2 * nI);
-        g.ldc = n4;
-        SC_TRY(eng.run(st, g, act));
+        void** row = dptr + (size_t)j * nI * CHAIN_PTRS;
+        auto cpt = [&](int k) { return reinterpret_cast<const double2* const*>(row + (size_t)k * nI); };
+        auto mpt = [&](int k) { return reinterpret_cast<double2* const*>(row + (size_t)k * nI); };
+        auto prod = [&](int a, int lda, int bb, int ldb, int c, int ldc, double beta) {
+            GemmArgs g;
+            g.m = n2;
+            g.n = 3 * MF;
+            g.k = n2;
+            g.beta = make_double2(beta, 0.0);
+            g.Ap = cpt(a);
+            g.lda = lda;
+            g.Bp = cpt(bb);
+            g.ldb = ldb;
+            g.Cp = mpt(c);
+            g.ldc = ldc;
+            return eng.run(st, g, act);
+        };
+        SC_TRY(prod(0, n2, 1, n4, 2, n2, 0.0));                 // U = (G B) X2
+        SC_TRY(prod(3, n2, 4, n4, 5, n2, 0.0));                 // V = F X1
+        chain_mix_kernel<<<dim3(chain_blocks, act), 256, 0, st>>>(n2, 3 * MF, dtv + (size_t)j * nI, mpt(2), mpt(5),
+                                                                  cpt(4), mpt(6));
+        count_launch();
+        SC_CHECK_LAUNCH("chain_mix");
+        SC_TRY(prod(3, n2, 5, n2, 6, n4, -1.0));                // X1' = F (2 V - t U) - X1
+        SC_TRY(prod(7, n2, 2, n2, 8, n4, 1.0));                 // X2' = X2 + (C G)((t^2/2) U - t V)
     }
     SC_CUDA_TRY(cudaEventRecord(ev[4], st));
     // 5. boundary systems and their solves: with R eliminated order by order
     // (3MF unknowns) when no order grazes the top interface, else the full
     // 6MF system of ScatterVolume.cpp:398-466
-    void** tl = dptr + (size_t)maxZ * nI * 3;
+    void** tl = dptr + (size_t)maxZ * nI * CHAIN_PTRS;
     const auto* Yp = reinterpret_cast<const double2* const*>(tl);
     if (reduced) {
         const int n3 = 3 * MF;
