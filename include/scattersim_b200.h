@@ -89,17 +89,21 @@ sc_status sc_linearsolve_batched(sc_context* ctx, void* A, int n, void* B, int n
                                  int batch, int* info, void* stream);
 
 /* Allocation-free variant of sc_linearsolve_batched (no counterpart in the
- * reference).  Same arguments and results, no context, runs on the current
- * device, and allocates no device memory: for callers that cannot call
- * cudaMalloc -- solves recorded into a CUDA graph under stream capture,
- * real-time loops that must not take cudaMalloc's implicit synchronisation,
- * frameworks that forbid device allocations after start-up.  Its scratch
- * (pivots and status words) is a fixed 260 KiB array in the library's device
- * memory, held by every GPU that loads the library until exit; limits:
- * n * batch <= 65536 and batch <= 1024, larger sizes return SC_BADINPUT.
- * The first call on a device looks the array up for that device (make it
- * before any stream capture).  All calls share the array: calls whose work
- * overlaps on the GPU race. */
+ * reference).  Same arguments and results, no context, and no device memory
+ * allocated: for callers that cannot call cudaMalloc -- real-time loops that
+ * must not take the implicit device-wide synchronisation of cudaMalloc and
+ * cudaFree, and host programs whose framework reserves the GPU's memory up
+ * front and forbids later allocations (a late cudaMalloc would stall other
+ * work or run out of memory mid-run).  Its scratch (pivots and status words)
+ * is a fixed 260 KiB array in the library's device memory, held by every GPU
+ * that loads the library until exit; limits: n * batch <= 65536 and
+ * batch <= 1024, larger sizes return SC_BADINPUT.  It runs on the current
+ * device; a stream of another device returns SC_BADINPUT.  The first call on
+ * a device looks the array's device address up for that device and keeps it
+ * (make that call before any stream capture, and none after cudaDeviceReset).
+ * Like the allocating entry, each call copies the status words back into the
+ * host array info and synchronises the stream.  All calls share the array:
+ * calls whose work overlaps on the GPU race. */
 sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int nrhs, int batch, int* info,
                                          void* stream);
 

@@ -2,12 +2,13 @@
 //
 // sc_linearsolve_batched_noalloc solves A X = B exactly like
 // sc_linearsolve_batched (same LU kernels, same results) but allocates no
-// device memory.  It exists for callers that cannot call cudaMalloc: code
-// that records the solve into a CUDA graph under stream capture (where an
-// allocation would break or invalidate the capture), real-time loops that
-// must not take the implicit device synchronisation of cudaMalloc/cudaFree,
-// and host frameworks that hand the library pre-allocated buffers and forbid
-// further device allocations.
+// device memory.  It is for callers that cannot call cudaMalloc: real-time
+// loops that must not take the implicit device-wide synchronisation of
+// cudaMalloc/cudaFree, and host programs (a solver plugin inside a larger
+// application, say) whose framework reserves the GPU's memory up front and
+// forbids further device allocations, so that a late cudaMalloc would stall
+// other work or fail with out-of-memory in the middle of a run.  Those callers
+// pass in A, B and info and get the same solve without a context.
 //
 // Its only scratch -- the pivot indices and one status word per system --
 // lives in g_noalloc_scratch, a fixed array in this library's device memory
@@ -19,7 +20,13 @@
 // can reach host memory, silently address the wrong memory.  The device
 // address is therefore looked up with cudaGetSymbolAddress once per device,
 // with that device current, on the first call made on that device; that first
-// call should come before any stream capture starts.
+// call should come before any stream capture starts.  The looked-up address is
+// kept for the life of the process: after cudaDeviceReset the library's
+// module is reloaded and the kept address is stale, so do not call this entry
+// point after resetting the device.
+//
+// Each call ends by copying the status words back to the host and
+// synchronising `stream` (info is a host array, as in the allocating entry).
 //
 // All calls share the one array and keep the last call's contents: the status
 // words are cleared on the stream at the start of every call, and calls whose
@@ -59,6 +66,15 @@ extern "C" sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int
     if (dev < 0 || dev >= MAX_DEVICES) {
         set_error("sc_linearsolve_batched_noalloc: device %d out of range", dev);
         return SC_BADINPUT;
+    }
+    if (stream) {
+        int sdev = dev;
+        SC_CUDA_TRY(cudaStreamGetDevice((cudaStream_t)stream, &sdev));
+        if (sdev != dev) {
+            set_error("sc_linearsolve_batched_noalloc: the stream belongs to device %d, the current device is %d",
+                      sdev, dev);
+            return SC_BADINPUT;
+        }
     }
     int* base = nullptr;
     {
