@@ -1,6 +1,7 @@
 """Generates the golden fixtures in this directory from the reference's shipped data.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    SCATTERSIM_REFERENCE=/path/to/reference python tests/golden/make_golden.py
+    python tests/golden/make_golden.py /path/to/reference
 
 Inputs (read-only, from the reference tree):
   data/psf.cw      scatterplane output: 4096 incident waves, one boundary at z=0
@@ -88,4 +89,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SCATTERSIM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_TREE  (or set SCATTERSIM_REFERENCE)")
+    main(ref)

@@ -27,7 +27,8 @@ from scattersim_b200 import samples
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
-REF = "/root/reference"
+# the reference tree, when mounted (its shipped .cw files); tests that need it skip otherwise
+REF = os.environ.get("SCATTERSIM_REFERENCE", "")
 
 
 @pytest.fixture(scope="module")
