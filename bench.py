@@ -9,7 +9,10 @@ solved for R/T.  One step = the whole 256-instance sweep, samples resident in
 HBM.  The headline value is the batched mixed-precision path (int8 tcgen05
 digit-sliced products, 7 slices, where the GEMM autotuner finds them faster);
 the line also carries the batched FP64 path, the plain per-instance FP64 path
-(timed on every 8th instance) and the R/T error of the mixed path against FP64.
+(timed on a sample stratified over every incidence angle and order count) and
+the R/T error of the mixed path against FP64.  Under torchrun the one sweep is
+split over the ranks (LPT by cost) and the R/T vectors are all-gathered inside
+every timed step (strong scaling).
 
 --workload volume: the plain 3-D volume -- a 128x128x32-voxel sphere volume over
 20x20x8 um (seeded), 32 layers, lambda 0.6 um, 10 deg, x-polarised, 21x21
@@ -23,8 +26,9 @@ solve of the whole beam (incident waves resident in HBM), in plane waves/s.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume|layer]
 
-Under torchrun each rank solves its own seeded sweep / instance (weak scaling,
-no data-path collective); timing is on the device, max over ranks.
+Timing is on the device (CUDA events), max over ranks.  --workload volume and
+layer run one independent instance / beam per rank under torchrun (weak
+scaling).  --case NAME runs one of the named profiling cases listed below.
 """
 from __future__ import annotations
 
@@ -62,7 +66,6 @@ LAYER_STACK = dict(n=(1.0, 1.4, 1.4, 1.0), kappa=(0.05,), z=(-3.0, 0.0, 3.0))
 LAYER_NAME = ("scatterlayer default stack (n 1, 1.4+0.05i, 1.4, 1; boundaries -3, 0, 3 um; lambda 1 um) under a "
               "1024x1024 polar beam (alpha 1 rad about z, y-pol): 1,048,576 plane waves, 24x24 complex system each")
 MIXED = 1          # SC_SWEEP_MIXED: int8 tcgen05 digit-sliced products, 7 slices
-PLAIN_EVERY = 8    # the per-instance FP64 path is timed on every 8th instance
 
 
 def _peaks():
@@ -338,60 +341,109 @@ def run_volume_ours(args):
 
 
 # --------------------------------------------------------------------------- sweep
-def sweep_instances(seed):
+SWEEP_SEED = 1000
+ANGLES = (0.0, 10.0, 20.0, 30.0)
+ORDERS = (7, 11, 15, 21, 25)
+# work of the layer-independent part of a CPU solve (the boundary zgesv of order 6M,
+# Gc_static^-1 and its products) in units of one layer's work (Phi, zgeev of order
+# 4M, the sort and one transfer step), from their LAPACK flop counts
+FIXED_LAYERS = 0.2
+PLAIN_PER_STRATUM = 2
+
+
+def sweep_instances(seed=SWEEP_SEED):
     from scattersim_b200 import samples
     return samples.sweep_instances(seed, count=256)
 
 
-def cpu_sweep_sample(inst):
-    """The reference CPU path on a bounded sample of the sweep (the oracle port).
+def representatives(inst):
+    """One instance per order count (the shallowest stack), the incidence angle rotating."""
+    out = []
+    for j, m in enumerate(ORDERS):
+        cand = [it for it in inst if it.orders == m and it.angle_deg == ANGLES[j % 4]]
+        out.append(min(cand, key=lambda it: (it.maps.shape[0], it.index)))
+    return out
 
-    For each order count one layer of one instance is timed -- phi assembly,
-    zgeev of the 4M x 4M layer matrix, the eigen sort and one T-matrix step
-    (ScatterVolume.cpp:235-336); the sweep's time is the sum over instances of
-    layers x that per-layer time (boundary solves excluded, a lower bound).
-    Returns (solves/s, description, seconds spent).
-    """
+
+def cpu_instance_seconds(it, layers=None):
+    """One whole instance through the oracle (the reference's CPU path, --external):
+    Phi, zgeev of every 4M x 4M layer matrix, the sort, the transfer chain and the
+    boundary zgesv (ScatterVolume.cpp:654-739).  layers: solve only the first ones."""
     from oracle import scattervolume as osv
-    per_layer, spent = {}, 0.0
-    for m in sorted({it.orders for it in inst}):
-        it = next(i for i in inst if i.orders == m)
-        p = osv.Params(**it.params_kw())
-        d, e, dirv, k, ni, slices, num_pixels, z, M, msgs = osv.setup(it.maps, p)
-        lat = osv.upwq_cal(M, p.size, dirv, k, ni)
-        t0 = time.perf_counter()
-        P, _, _ = osv.phi(slices[0], M, lat, k)
-        w, v = osv.mkl_eigensolve(P)
-        sl, sv = osv.eigen_sort(w, v)
-        dz = z[1] - z[0]
-        odd = (np.arange(sl.size) % 2) != 0
-        Gd = sv * np.where(odd, np.exp(1j * k * sl * (-dz)), 1.0)[None, :]
-        Gc = sv * np.where(odd, 1.0, np.exp(1j * k * sl * dz))[None, :]
-        _ = (Gc @ osv.mkl_inverse(Gd)) @ Gc
-        per_layer[m] = time.perf_counter() - t0
-        spent += per_layer[m]
-    total = sum(it.maps.shape[0] * per_layer[it.orders] for it in inst)
-    desc = ("one layer per order count timed (phi, zgeev n=4M, sort, one T-matrix step: "
-            + ", ".join(f"M={m}x{m}: {t:.2f} s" for m, t in per_layer.items())
-            + f"), times the sweep's {sum(i.maps.shape[0] for i in inst)} layers; numpy/scipy OpenBLAS "
-              "restatement of ScatterVolume.cpp")
+    maps = it.maps if layers is None else it.maps[:layers]
+    kw = it.params_kw()
+    if layers is not None:
+        kw["size"] = (it.period, it.period, it.thickness * maps.shape[0])
+    t0 = time.perf_counter()
+    osv.solve(maps, osv.Params(**kw), keep=False)
+    return time.perf_counter() - t0
+
+
+def cpu_sweep_estimate(inst, per_order):
+    """Seconds of the whole sweep from per-order timings {orders: (seconds, layers solved)}:
+    t_i = t_rep (L_i + FIXED_LAYERS) / (L_rep + FIXED_LAYERS)."""
+    total = 0.0
+    for it in inst:
+        t, L = per_order[it.orders]
+        total += t * (it.maps.shape[0] + FIXED_LAYERS) / (L + FIXED_LAYERS)
+    return total
+
+
+def cpu_sweep_baseline(inst, budget_s=25.0):
+    """The GPU arm's host baseline: whole representative instances while the budget lasts,
+    then one-layer instances of the remaining (larger) order counts."""
+    per, spent, parts = {}, 0.0, []
+    for it in representatives(inst):
+        L = it.maps.shape[0] if spent < budget_s / 3 else 1
+        t = cpu_instance_seconds(it, None if L == it.maps.shape[0] else L)
+        per[it.orders] = (t, L)
+        spent += t
+        parts.append(f"{it.orders}x{it.orders}: {L} layer{'s' if L > 1 else ''} {t:.2f} s")
+    total = cpu_sweep_estimate(inst, per)
+    desc = ("whole scattervolume --external solves through the oracle (Phi, zgeev 4M, sort, chain, boundary "
+            "zgesv), one instance per order count (" + "; ".join(parts) + f"), scaled to the sweep's "
+            f"{sum(i.maps.shape[0] for i in inst)} layers by (L + {FIXED_LAYERS}) per instance")
     return len(inst) / total, desc, spent
 
 
 def run_sweep_reference(args):
-    inst = sweep_instances(1000)
+    """The reference's CPU path on whole instances: step j solves representative j mod 5
+    (one per order count, 7..25, the shallowest stack, angles rotating) end to end."""
+    inst = sweep_instances()
+    reps = representatives(inst)
+    warm = reps[0]
     for _ in range(args.warmup):
-        cpu_sweep_sample([i for i in inst if i.orders == 7][:1])
-    vals, desc = [], ""
-    for _ in range(args.steps):
-        v, desc, _ = cpu_sweep_sample(inst)
-        vals.append(v)
-    value = statistics.mean(vals)
+        cpu_instance_seconds(warm)
+    times = {m: [] for m in ORDERS}
+    step_s = []
+    for j in range(args.steps):
+        it = reps[j % len(reps)]
+        t = cpu_instance_seconds(it)
+        times[it.orders].append(t)
+        step_s.append(t)
+    per = {}
+    timed = [m for m in ORDERS if times[m]]
+    for m in ORDERS:
+        it = reps[ORDERS.index(m)]
+        if times[m]:
+            per[m] = (statistics.mean(times[m]), it.maps.shape[0])
+        else:   # not reached with so few steps: scale the largest timed order by (4M)^3
+            mt = max(timed)
+            per[m] = (statistics.mean(times[mt]) * (m / mt) ** 6, reps[ORDERS.index(mt)].maps.shape[0])
+    value = len(inst) / cpu_sweep_estimate(inst, per)
+    sample = ("step j = one whole instance end to end through the oracle (numpy/scipy OpenBLAS restatement of "
+              "ScatterVolume.cpp: Phi, zgeev of every 4M x 4M layer matrix, sort, transfer chain, boundary zgesv, "
+              "--external), cycling over one instance per order count (" +
+              ", ".join(f"#{it.index}: {it.orders}x{it.orders} orders, {it.maps.shape[0]} layers, "
+                        f"{it.angle_deg:g} deg" for it in reps) +
+              f"); value = 256 / sum over the sweep of t(orders) (L + {FIXED_LAYERS}) / (L_rep + {FIXED_LAYERS})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 256e3 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": SWEEP_NAME, "seed": 1000},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": blas_threads(), "kind": "port", "sample": desc},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(step_s),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": SWEEP_NAME, "seed": SWEEP_SEED},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": blas_threads(), "kind": "port", "sample": sample,
+                             "per_order_s": {str(m): round(per[m][0], 3) for m in ORDERS},
+                             "sample_solves_per_s": len(step_s) / sum(step_s)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -401,20 +453,31 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+def plain_strata(inst):
+    """PLAIN_PER_STRATUM instances of every (angle, orders) stratum, by index."""
+    out = {}
+    for it in inst:
+        key = (it.angle_deg, it.orders)
+        out.setdefault(key, [])
+        if len(out[key]) < PLAIN_PER_STRATUM:
+            out[key].append(it.index)
+    return out
+
+
 def run_sweep_ours(args):
     import torch
-    from scattersim_b200 import solver
+    from scattersim_b200 import solver, sweep
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    dev_t = torch.device("cuda", local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
-                                device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=dev_t)
 
     def barrier():
         if dist is not None:
@@ -422,19 +485,26 @@ def run_sweep_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return sweep.max_over_ranks(v, dist, dev_t)
 
     ctx = solver.Context(local)
-    inst = sweep_instances(1000 + rank)
-    params = [solver.make_params(**it.params_kw()) for it in inst]
-    dev = [torch.from_numpy(it.maps).cuda() for it in inst]
-    stream = torch.cuda.current_stream()
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+    inst = sweep_instances()                       # one sweep, split across the ranks
     n = len(inst)
+    params = [solver.make_params(**it.params_kw()) for it in inst]
+    dims = [solver.plan(p, it.maps.shape) for p, it in zip(params, inst)]
+    sizes = [6 * d.MF for d in dims]
+    costs = [sweep.solve_cost(it.maps.shape[0], d.MF) for it, d in zip(inst, dims)]
+    parts = sweep.assign_lpt(costs, world)
+    mine = parts[rank]
+    dev = {i: torch.from_numpy(inst[i].maps).to(dev_t) for i in mine}
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev_t)   # 256 MB > 126 MB L2
+
+    def solve_share(precision, samples=None):
+        def fn(idx):
+            smp = [samples[i] if samples is not None else dev[i] for i in idx]
+            return solver.sweep(ctx, [params[i] for i in idx], smp, precision=precision).x
+        return sweep.shard_solve(costs, sizes, fn, dist, dev_t)
 
     def timed(fn):
         flush.zero_()
@@ -447,80 +517,107 @@ def run_sweep_ours(args):
         return out, e0.elapsed_time(e1)
 
     for _ in range(args.warmup):          # the first call also autotunes every GEMM shape
-        solver.sweep(ctx, params, dev, precision=MIXED)
+        solve_share(MIXED)
 
     # ---- headline: batched mixed precision, device-timed, samples resident in HBM
     sampler = ClockSampler(local)
     barrier()
     sampler.start()
-    ctx.kernel_timing(True)
     l0 = ctx.launches()
     step_ms = []
     res_mixed = None
     for _ in range(args.steps):
-        res_mixed, ms = timed(lambda: solver.sweep(ctx, params, dev, precision=MIXED))
+        res_mixed, ms = timed(lambda: solve_share(MIXED))
         step_ms.append(ms)
     launches = ctx.launches() - l0
-    kst = ctx.kernel_stats()
-    ctx.kernel_timing(False)
     stages = ctx.stage_ms()
     barrier()
     clocks = sampler.stop()
     total_ms = max_over_ranks(sum(step_ms))
-    value = world * n * args.steps / (total_ms / 1e3)
+    value = n * args.steps / (total_ms / 1e3)
 
-    # ---- batched FP64 (one warm-up for its own GEMM shapes, then timed)
-    solver.sweep(ctx, params, dev, precision=0)
-    fp_steps = max(1, min(2, args.steps))
+    # ---- one instrumented step: per-launch GEMM timing for the roofline (not in the headline)
+    ctx.kernel_timing(True)
+    _, instr_ms = timed(lambda: solve_share(MIXED))
+    kst = ctx.kernel_stats()
+    ctx.kernel_timing(False)
+
+    # ---- batched FP64, same step count (one warm-up for its own GEMM shapes)
+    solve_share(0)
+    barrier()
     fp_ms = []
     res_fp = None
-    for _ in range(fp_steps):
-        res_fp, ms = timed(lambda: solver.sweep(ctx, params, dev, precision=0))
+    for _ in range(args.steps):
+        res_fp, ms = timed(lambda: solve_share(0))
         fp_ms.append(ms)
-    fp_value = world * n * fp_steps / (max_over_ranks(sum(fp_ms)) / 1e3)
-    errs = [_rel(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(res_mixed.x, res_fp.x)]
+    fp_value = n * args.steps / (max_over_ranks(sum(fp_ms)) / 1e3)
+    errs = [_rel(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(res_mixed, res_fp)]
 
-    # ---- plain per-instance FP64 path on every 8th instance
-    sub = list(range(0, n, PLAIN_EVERY))
-    solver.solve(ctx, params[sub[0]], dev[sub[0]], fields=False)
-    plain_ms = 0.0
-    for i in sub:
-        _, ms = timed(lambda: solver.solve(ctx, params[i], dev[i], fields=False))
-        plain_ms += ms
-    plain_value = world * len(sub) / (max_over_ranks(plain_ms) / 1e3)
+    # ---- plain per-instance FP64 path on a stratified sample (every angle x order count)
+    strata = plain_strata(inst)
+    my_strata = [key for j, key in enumerate(sorted(strata)) if j % world == rank]
+    warmed = set()
+    for key in my_strata:                  # one untimed solve per order count (workspace growth)
+        i = strata[key][0]
+        if inst[i].orders not in warmed:
+            solver.solve(ctx, params[i], torch.from_numpy(inst[i].maps).to(dev_t), fields=False)
+            warmed.add(inst[i].orders)
+    plain_est_ms = 0.0
+    plain_count = 0
+    for key in my_strata:
+        ms_k = []
+        for i in strata[key]:
+            d_i = torch.from_numpy(inst[i].maps).to(dev_t)
+            _, ms = timed(lambda: solver.solve(ctx, params[i], d_i, fields=False))
+            ms_k.append(ms)
+            plain_count += 1
+        pop = sum(1 for it in inst if (it.angle_deg, it.orders) == key)
+        plain_est_ms += pop * statistics.mean(ms_k)
+    if dist is not None:       # the strata are split over the ranks: sum their estimates
+        t = torch.tensor([plain_est_ms], dtype=torch.float64, device=dev_t)
+        dist.all_reduce(t)
+        plain_est_ms = float(t.item())
+    plain_value = world * n / (plain_est_ms / 1e3)
 
-    # ---- end to end through the public API with host buffers
+    # ---- end to end through the public API with host buffers (same step count)
     e2e = None
     if not args.no_e2e:
-        sizes = [it.maps.size for it in inst]
-        offs = np.concatenate([[0], np.cumsum(sizes)])
+        sz = [inst[i].maps.size for i in mine]
+        offs = np.concatenate([[0], np.cumsum(sz)]).astype(np.int64)
         pin_in = torch.empty(int(offs[-1]), dtype=torch.complex128).pin_memory()
-        for it, o in zip(inst, offs[:-1]):
-            pin_in[int(o):int(o) + it.maps.size].copy_(torch.from_numpy(it.maps.ravel()))
-        outs = [torch.empty(x.numel(), dtype=torch.complex128).pin_memory() for x in res_mixed.x]
-        d_in = torch.empty_like(pin_in, device="cuda")
+        for i, o in zip(mine, offs[:-1]):
+            pin_in[int(o):int(o) + inst[i].maps.size].copy_(torch.from_numpy(inst[i].maps.ravel()))
+        outs = [torch.empty(s, dtype=torch.complex128).pin_memory() for s in sizes]
+        d_in = torch.empty_like(pin_in, device=dev_t)
         barrier()
         e2e_ms = []
-        for _ in range(max(1, min(2, args.steps))):
+        for _ in range(args.steps):
             def step():
                 d_in.copy_(pin_in, non_blocking=True)
-                views = [d_in[int(o):int(o) + it.maps.size].view(it.maps.shape) for it, o in zip(inst, offs[:-1])]
-                r = solver.sweep(ctx, params, views, precision=MIXED)
-                for o, x in zip(outs, r.x):
+                views = {i: d_in[int(o):int(o) + inst[i].maps.size].view(inst[i].maps.shape)
+                         for i, o in zip(mine, offs[:-1])}
+                r = solve_share(MIXED, views)
+                for o, x in zip(outs, r):
                     o.copy_(x, non_blocking=True)
                 return r
             _, ms = timed(step)
             e2e_ms.append(ms)
-        e2e_value = world * n * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) / 1e3)
+        e2e_value = n * args.steps / (max_over_ranks(sum(e2e_ms)) / 1e3)
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(offs[-1]) * 16,
-               "d2h_bytes_per_step": int(sum(x.numel() for x in outs)) * 16}
+               "d2h_bytes_per_step": int(sum(sizes)) * 16}
 
-    # ---- roofline of the dominant kernel (by device time over the timed steps)
+    # ---- roofline of the dominant kernel (by device time over the instrumented step)
     peaks = _peaks()
     fp64_peak = ctx.fp64_peak_tflops()
+    int8_peak_meas = ctx.int8_peak_tops() if hasattr(ctx, "int8_peak_tops") else None
     d8, dd = kst["int8"], kst["dmma"]
     if d8["ms"] >= dd["ms"]:
-        int8_peak = 2.0 * float(peaks.get("bf16_tflops", 1590.0))
+        if int8_peak_meas:
+            int8_peak, src = int8_peak_meas, ("int8 tcgen05 MMA probe measured in this run (operands resident in "
+                                              "shared memory, no loads): the device's dense int8 rate")
+        else:
+            int8_peak = 2.0 * float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1590.0)))
+            src = "2 x measured bf16 dense sustained peak (MEASURED_PEAKS.json)"
         achieved = d8["int8_ops"] / (d8["ms"] / 1e3) / 1e12
         tr = None
         try:
@@ -532,8 +629,7 @@ def run_sweep_ours(args):
         roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS (int8)",
                     "frac": achieved / int8_peak, "traffic": tr,
                     "kernel": "oz_mma_kernel (int8 tcgen05 MMA, 7 digit slices, TMEM accumulators)",
-                    "peak_source": "2 x measured bf16 dense burst peak (MEASURED_PEAKS.json): int8 dense "
-                                   "is twice bf16 dense on B200",
+                    "peak_source": src,
                     "launches": int(d8["launches"]), "avg_launch_ms": d8["ms"] / max(d8["launches"], 1),
                     "fp64_equivalent_tflops": d8["flops"] / (d8["ms"] / 1e3) / 1e12,
                     "fp64_peak_tflops": fp64_peak,
@@ -546,27 +642,30 @@ def run_sweep_ours(args):
                     "kernel": "zgemm_kernel (FP64 mma.sync m8n8k4 complex GEMM)",
                     "peak_source": "FP64 FMA probe measured in this run",
                     "launches": int(dd["launches"]), "avg_launch_ms": dd["ms"] / max(dd["launches"], 1)}
-    roofline["gemm_time_share"] = (d8["ms"] + dd["ms"]) / (sum(step_ms) or 1.0)
-    roofline["int8_ms_per_step"] = d8["ms"] / args.steps
-    roofline["fp64_tile_ms_per_step"] = dd["ms"] / args.steps
+    roofline["instrumented_step_ms"] = instr_ms
+    roofline["gemm_time_share"] = (d8["ms"] + dd["ms"]) / (instr_ms or 1.0)
+    roofline["int8_ms_per_step"] = d8["ms"]
+    roofline["fp64_tile_ms_per_step"] = dd["ms"]
 
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            v, desc, spent = cpu_sweep_sample(inst)
+            v, desc, spent = cpu_sweep_baseline(inst)
             cpu = {"value": v, "unit": UNIT, "cores": blas_threads(), "kind": "port",
                    "sample": desc + f"; {spent:.1f} s of host work"}
+        strata_desc = (f"stratified: {PLAIN_PER_STRATUM} instances of each of the {len(strata)} (angle, orders) "
+                       f"strata ({plain_count * world if world > 1 else plain_count} timed), one "
+                       "sc_volume_solve (--external) each; sweep time = sum over strata of population x mean time")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "int8 tensor products (7 digit slices) + f64",
+                "scaling": "strong", "vs_baseline": None, "dtype": "int8 tensor products (7 digit slices) + f64",
                 "data": "synthetic",
-                "config": {"workload": SWEEP_NAME, "seed": "1000+rank", "path": "batched mixed precision",
+                "config": {"workload": SWEEP_NAME, "seed": SWEEP_SEED, "path": "batched mixed precision",
                            "l2": "flushed between steps (256 MB write, untimed); working set >> L2",
-                           "parallelism": f"independent sweep per rank x{world}"},
+                           "parallelism": (f"one sweep split over {world} ranks (LPT by batched-path cost), R/T "
+                                           "all-gathered inside each step" if world > 1 else "one GPU")},
                 "paths": {"batched_mixed": value, "batched_fp64": fp_value,
-                          "plain_fp64_per_instance": plain_value,
-                          "plain_sample": f"every {PLAIN_EVERY}th instance ({len(sub)} of {n}), one "
-                                          "sc_volume_solve (--external) each",
+                          "plain_fp64_per_instance": plain_value, "plain_sample": strata_desc,
                           "mixed_rt_rel_err_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
                           "speedup_mixed_vs_plain": value / plain_value,
                           "speedup_fp64_batched_vs_plain": fp_value / plain_value},
@@ -581,6 +680,7 @@ def run_sweep_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
 
 def cpu_layer_waves(k, E, count):
     """The oracle's per-wave solve (ScatterLayer.cpp:110-266 restated, scipy LAPACK) on `count` waves."""
