@@ -27,6 +27,7 @@
  *   sc_gpu_initialize /
  *   sc_gpu_cw_evaluate      host-buffer gpu_initialize /     gpuEvaluator.cu:15-26,131-165
  *                           gpu_cw_evaluate
+ *   sc_scatterio_write/read write_file / read_file           ScatterIO.h:18-117
  */
 #ifndef SCATTERSIM_B200_H
 #define SCATTERSIM_B200_H
@@ -129,6 +130,20 @@ sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, i
                                     long long strideB, const double* beta, void* C, int ldc,
                                     long long strideC, int batch, void* stream);
 
+/* The product of sc_zgemm_batched on the int8 tensor cores (tcgen05) by
+ * modular arithmetic: the operands, scaled per row (A) and column (B) by
+ * powers of two and rounded to integers of about 47 bits, are reduced modulo
+ * 14 pairwise coprime moduli (<= 255); one exact int8 product per modulus,
+ * and the integer result is rebuilt in FP64 by the Chinese remainder theorem.
+ * Error about 2^-47 times the row scale x column scale x k per element for
+ * k <= 1250 (one bit less per doubling of k beyond).  No reference
+ * counterpart: it is the arithmetic of the mixed-precision sweep (14 int8
+ * products where the digit-sliced form needs 28).  Synchronises the stream;
+ * SC_CUDA_ERROR if a tensor-core pipeline wait timed out. */
+sc_status sc_zgemm_crt_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
+                               long long strideA, const void* B, int ldb, long long strideB, const double* beta,
+                               void* C, int ldc, long long strideC, int batch, void* stream);
+
 /* --------------------------------------------------------- volume solve */
 
 typedef struct {
@@ -181,11 +196,15 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
  * on the int8 tensor cores with 7 digit slices per operand
  * (sc_zgemm_emulated_batched; about 1e-13 relative per product) wherever the
  * context's GEMM autotuner measured that faster than the FP64 tile, which on
- * the sweep workload keeps R/T within 2e-9 of FP64; SC_SWEEP_SLICES(s) runs
- * every such product on the int8 engine with s = 1..7 slices.  FFT, assembly,
+ * the sweep workload keeps R/T within 2e-9 of FP64; the candidates are the
+ * digit-sliced engine (7 slices) and the modular engine of
+ * sc_zgemm_crt_batched.  SC_SWEEP_CRT runs every such product on the modular
+ * engine; SC_SWEEP_SLICES(s) every such product on the digit-sliced engine
+ * with s = 1..7 slices.  FFT, assembly,
  * the boundary systems and their LU stay in FP64. */
 #define SC_SWEEP_FP64 0
 #define SC_SWEEP_MIXED 1
+#define SC_SWEEP_CRT 2
 #define SC_SWEEP_SLICES(s) (0x100 | (s))
 
 /* A batched sweep of independent scattervolume solves, R/T only (the
@@ -228,6 +247,10 @@ sc_status sc_qr_stats(sc_context* ctx, long long* out, int count);
  * FP64-equivalent flops, int8 ops} for the int8 tcgen05 MMA kernel. */
 sc_status sc_kernel_timing(sc_context* ctx, int on);
 sc_status sc_kernel_stats(sc_context* ctx, double* out8);
+/* The same record for `classes` kernel classes, 4 values each: 0 FP64 tiles,
+ * 1 digit-sliced int8 MMA kernel, 2 modular (CRT) int8 MMA kernel, 3 whole
+ * modular-engine products (exponents, packing, MMA kernel and reconstruction). */
+sc_status sc_kernel_stats_ex(sc_context* ctx, double* out, int classes);
 
 /* The GEMM autotuner's choices on this context, as 6-int records (m, n, k,
  * batch, slices, variant: 0/1 FP64 tile of 64/128 rows, 2 int8 engine).
@@ -242,6 +265,9 @@ sc_status sc_gemm_choices_set(sc_context* ctx, const int* rec, int count);
 sc_status sc_fp64_peak_probe(sc_context* ctx, double* tflops);
 /* Measured FP64 tensor-core (mma.sync m8n8k4 f64) throughput (TFLOP/s). */
 sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops);
+/* Measured int8 tensor-core (tcgen05.mma kind::i8, 128 x 256 x 32, operands in
+ * shared memory) throughput (TOPS): a roofline denominator of the int8 engines. */
+sc_status sc_int8_peak_probe(sc_context* ctx, double* tops);
 
 /* Wave table of a solved volume in cw_unpack order: Pi, then per boundary l
  * its reflected and transmitted lists (ScatterVolume.cpp:907-987,
@@ -301,6 +327,28 @@ sc_status sc_layer_solve(sc_context* ctx, int layers, const double* n, const dou
                          const double* z, double lambda, int count, const double* k_in,
                          const void* E_in, void* r_E, void* r_k, void* t_E, void* t_k,
                          int* status, void* stream);
+
+/* ------------------------------------------------- ScatterIO files (host) */
+
+/* ScatterIO.h write_file (:18-42; the single-beam and single-event overloads
+ * :89-117 are beams = 1): the plane normal and a point on the plane (3 doubles
+ * each), then per beam its count of scattering events and their incident,
+ * reflected and transmitted plane waves.  Records are tira planewave<double>
+ * bytes, 80 per wave ({E0x, E0y, kx, ky, kz} complex128, as in the .cw file);
+ * incident / reflected / transmitted hold sum(counts) records each, the beams
+ * back to back. */
+sc_status sc_scatterio_write(const char* path, const double* normal, const double* position, int beams,
+                             const long long* counts, const void* incident, const void* reflected,
+                             const void* transmitted);
+
+/* ScatterIO.h read_file (:44-87): reads beams until a zero or missing count.
+ * Writes the plane, *beams, *events (total records per list) and, when the
+ * buffers are given, counts (beams_cap entries) and the records (events_cap
+ * each).  Call with NULL buffers to size them; SC_BADINPUT if the file holds
+ * more than the buffers or ends inside a beam. */
+sc_status sc_scatterio_read(const char* path, double* normal, double* position, int* beams, long long* counts,
+                            int beams_cap, void* incident, void* reflected, void* transmitted,
+                            long long events_cap, long long* events);
 
 /* ----------------------------------------- reference-signature shims (host) */
 

@@ -2,7 +2,7 @@
 
 This package is a numpy/scipy restatement of the reference's CPU algorithm
 (ScatterVolume.cpp, FourierWave.h, third_Lapack.h, CoupledWaveStructure.h,
-cpuEvaluator.cpp, gpuEvaluator.cu).  It is the checker for the CUDA path and
+ScatterIO.h, cpuEvaluator.cpp, gpuEvaluator.cu).  It is the checker for the CUDA path and
 the timed CPU baseline; nothing in the product package imports it.
 
 Parity pin status

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "SC_OK", 1: "SC_BADINPUT", 2: "SC_NOCONVERGE", 3: "SC_SINGULA
 
 SC_SWEEP_FP64 = 0
 SC_SWEEP_MIXED = 1
+SC_SWEEP_CRT = 2
 
 
 def SC_SWEEP_SLICES(s):
@@ -68,15 +69,24 @@ _SIGS = {
     "sc_zgemm_emulated_batched": (c_int, [c_void_p, c_int, c_int, c_int, c_int, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_void_p, c_int, c_longlong, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_int, c_void_p]),
+    "sc_zgemm_crt_batched": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double), c_void_p, c_int, c_longlong,
+                                     c_void_p, c_int, c_longlong, POINTER(c_double), c_void_p, c_int, c_longlong,
+                                     c_int, c_void_p]),
     "sc_zgemm_batched": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_void_p, c_int, c_longlong, POINTER(c_double), c_void_p, c_int, c_longlong,
                                  c_int, c_void_p]),
+    "sc_scatterio_write": (c_int, [ctypes.c_char_p, POINTER(c_double), POINTER(c_double), c_int, POINTER(c_longlong),
+                                   c_void_p, c_void_p, c_void_p]),
+    "sc_scatterio_read": (c_int, [ctypes.c_char_p, POINTER(c_double), POINTER(c_double), POINTER(c_int),
+                                  POINTER(c_longlong), c_int, c_void_p, c_void_p, c_void_p, c_longlong,
+                                  POINTER(c_longlong)]),
     "sc_volume_params_default": (None, [POINTER(VolumeParams)]),
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
     "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),
                                POINTER(c_int), POINTER(c_int), POINTER(c_void_p), c_int, POINTER(c_int), c_void_p]),
     "sc_kernel_timing": (c_int, [c_void_p, c_int]),
     "sc_kernel_stats": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_kernel_stats_ex": (c_int, [c_void_p, POINTER(c_double), c_int]),
     "sc_gemm_choices_get": (c_int, [c_void_p, POINTER(c_int), c_int, POINTER(c_int)]),
     "sc_gemm_choices_set": (c_int, [c_void_p, POINTER(c_int), c_int]),
     "sc_fno_create": (c_int, [POINTER(c_void_p), c_int, c_int, ctypes.c_ulonglong]),
@@ -93,6 +103,7 @@ _SIGS = {
     "sc_volume_stage_ms": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_fp64_peak_probe": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_fp64_dmma_probe": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_int8_peak_probe": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_qr_stats": (c_int, [c_void_p, POINTER(c_longlong), c_int]),
     "sc_volume_waves": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_int, POINTER(c_longlong), POINTER(c_int), POINTER(c_int),

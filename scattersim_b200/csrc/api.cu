@@ -236,13 +236,15 @@ sc_status sc_inverse_batched(sc_context* ctx, const void* A, int n, int batch, v
     return sc_linearsolve_batched(ctx, LU, n, Ainv, n, batch, info, stream);
 }
 
-sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, int k, const double* alpha,
-                                    const void* A, int lda, long long strideA, const void* B, int ldb,
-                                    long long strideB, const double* beta, void* C, int ldc, long long strideC,
-                                    int batch, void* stream) {
-    if (!ctx || !alpha || !beta || !A || !B || !C || m < 0 || n < 0 || k < 0 || lda < (m > 1 ? m : 1) ||
-        ldb < (k > 1 ? k : 1) || ldc < (m > 1 ? m : 1)) {
-        set_error("sc_zgemm_emulated_batched: bad argument");
+namespace {
+// the int8 tensor-core engines behind one C entry each: slices 1..7 = digit
+// slices, 0 = modular (CRT)
+sc_status int8_gemm_entry(const char* name, sc_context* ctx, int slices, int m, int n, int k, const double* alpha,
+                          const void* A, int lda, long long strideA, const void* B, int ldb, long long strideB,
+                          const double* beta, void* C, int ldc, long long strideC, int batch, void* stream) {
+    if (!ctx || !alpha || !beta || !A || !B || !C || m < 0 || n < 0 || k < 0 || batch < 0 ||
+        lda < (m > 1 ? m : 1) || ldb < (k > 1 ? k : 1) || ldc < (m > 1 ? m : 1)) {
+        set_error("%s: bad argument", name);
         return SC_BADINPUT;
     }
     DeviceGuard g(ctx->device);
@@ -265,15 +267,38 @@ sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, i
     a.C = (double2*)C;
     a.ldc = ldc;
     a.sC = strideC;
-    SC_TRY(zgemm_ozaki(st, slices, a, batch, ctx->ws, err));
+    if (slices > 0)
+        SC_TRY(zgemm_ozaki(st, slices, a, batch, ctx->ws, err));
+    else
+        SC_TRY(zgemm_crt(st, a, batch, ctx->ws, err));
     int herr = 0;
     SC_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SC_CUDA_TRY(cudaStreamSynchronize(st));
     if (herr) {
-        set_error("sc_zgemm_emulated_batched: tensor-core pipeline wait timed out (stage %d)", herr);
+        set_error("%s: tensor-core pipeline wait timed out (stage %d)", name, herr);
         return SC_CUDA_ERROR;
     }
     return SC_OK;
+}
+}  // namespace
+
+sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, int k, const double* alpha,
+                                    const void* A, int lda, long long strideA, const void* B, int ldb,
+                                    long long strideB, const double* beta, void* C, int ldc, long long strideC,
+                                    int batch, void* stream) {
+    if (slices < 1 || slices > 7) {
+        set_error("sc_zgemm_emulated_batched: slices must be 1..7");
+        return SC_BADINPUT;
+    }
+    return int8_gemm_entry("sc_zgemm_emulated_batched", ctx, slices, m, n, k, alpha, A, lda, strideA, B, ldb,
+                           strideB, beta, C, ldc, strideC, batch, stream);
+}
+
+sc_status sc_zgemm_crt_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
+                               long long strideA, const void* B, int ldb, long long strideB, const double* beta,
+                               void* C, int ldc, long long strideC, int batch, void* stream) {
+    return int8_gemm_entry("sc_zgemm_crt_batched", ctx, 0, m, n, k, alpha, A, lda, strideA, B, ldb, strideB, beta, C,
+                           ldc, strideC, batch, stream);
 }
 
 sc_status sc_zgemm_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
@@ -361,9 +386,31 @@ sc_status sc_kernel_stats(sc_context* ctx, double* out8) {
     SC_CUDA_TRY(cudaDeviceSynchronize());
     for (int i = 0; i < 8; ++i) out8[i] = 0.0;
     for (auto& m : ctx->ws.marks) {
+        if (m.cls > 1) continue;
         float ms = 0.f;
         SC_CUDA_TRY(cudaEventElapsedTime(&ms, m.e0, m.e1));
         double* o = out8 + 4 * m.cls;
+        o[0] += 1.0;
+        o[1] += ms;
+        o[2] += m.flops;
+        o[3] += m.int8_ops;
+    }
+    return SC_OK;
+}
+
+sc_status sc_kernel_stats_ex(sc_context* ctx, double* out, int classes) {
+    if (!ctx || !out || classes < 0) {
+        set_error("sc_kernel_stats_ex: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    SC_CUDA_TRY(cudaDeviceSynchronize());
+    for (int i = 0; i < 4 * classes; ++i) out[i] = 0.0;
+    for (auto& m : ctx->ws.marks) {
+        if (m.cls >= classes) continue;
+        float ms = 0.f;
+        SC_CUDA_TRY(cudaEventElapsedTime(&ms, m.e0, m.e1));
+        double* o = out + 4 * m.cls;
         o[0] += 1.0;
         o[1] += ms;
         o[2] += m.flops;
@@ -514,6 +561,15 @@ sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops) {
         return SC_BADINPUT;
     }
     return fp64_probe(ctx, true, tflops);
+}
+
+sc_status sc_int8_peak_probe(sc_context* ctx, double* tops) {
+    if (!ctx || !tops) {
+        set_error("sc_int8_peak_probe: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return int8_peak_probe(ctx->device, ctx->ws, tops);
 }
 
 sc_status sc_qr_stats(sc_context* ctx, long long* out, int count) {

@@ -1,0 +1,603 @@
+// Complex128 GEMM on the int8 tensor cores by modular arithmetic (the
+// Chinese remainder theorem): C_b = alpha * A_b B_b + beta * C_b with about
+// 2^-47 relative error per product for K up to ~1300 (fewer bits beyond).
+//
+// Method (the modular integer emulation published as "Ozaki scheme II",
+// Ozaki, Uchino and Imamura, 2025, restated here for complex operands):
+//   * Each complex row i of A is scaled by 2^(al - e_i), each column c of B by
+//     2^(be - f_c) (e_i, f_c: exponents bounding the row / column), and
+//     rounded to integers, |a| <= 2^al, |b| <= 2^be.  The complex product is
+//     the real product A' B' of the interleaved embedding used by the
+//     digit-sliced engine (rows 2i / 2i+1 of C' are Re / Im of row i), so the
+//     exact integer result C'_int = A'_int B'_int satisfies
+//     |C'_int| <= 2k 2^(al+be) < P / 4 with P the product of the moduli.
+//   * For each of NMOD pairwise coprime moduli p (odd, <= 255) the operands
+//     are reduced to symmetric residues (|r| <= 127, int8) and one int8 GEMM
+//     on the tensor cores gives A'_p B'_p exactly in int32; its residue mod p
+//     is C'_int mod p.
+//   * C'_int is rebuilt from its NMOD residues r_p as S = sum_p r_p w_p minus
+//     the nearest multiple of P, w_p = (P/p) ((P/p)^-1 mod p) mod P.  The
+//     110-bit constants are held as three 37-bit limbs in doubles, so the three
+//     limb sums and the reduction by q = round(S / P) are exact in FP64 and
+//     only the final limb combination rounds (absolute error ~2^34 on values
+//     needing ~2^58).  C = 2^(e_i + f_c - al - be) C'_int.
+// NMOD = 14 moduli -> P ~ 2^109.8: al = be = 47 for k <= 1250 (2^-47 per
+// element relative to row x column scale x k, on par with 7 digit slices of
+// the digit-sliced engine) at 14 int8 products instead of 28.
+//
+// Data path: pack kernels write, per modulus, the A' and B' residue tiles in
+// the UMMA K-major core-matrix layout (as the digit-sliced engine does for its
+// digit planes).  The MMA kernel is persistent (one CTA per SM); a CTA owns
+// output tiles of 128 rows of C' (64 complex rows) x 256 complex columns and
+// for each tile runs NMOD passes of the K loop: warp 0 streams 12 KB stages
+// (A 4 KB + B 8 KB) through a 16-slot ring with cp.async.bulk, warp 1 issues
+// one 128 x 256 x 32 MMA per stage into one of two 256-column TMEM
+// accumulators, and eight epilogue warps turn a finished accumulator into
+// int8 residues (written to a per-CTA scratch slot that stays in L2) while the
+// MMAs of the next modulus run in the other accumulator.  After the last
+// modulus the epilogue warps rebuild the tile from the residues in FP64 and
+// write C.  All waits are bounded; a timeout sets the error word and the CTA
+// drains its copies, frees its TMEM and returns.
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "tcgen05.cuh"
+
+namespace sc {
+
+namespace {
+
+constexpr int CRT_NMOD = 14;
+constexpr int CRT_BM = 128;                  // rows of C' per tile (TMEM lanes)
+constexpr int CRT_BN = 256;                  // complex columns per tile
+constexpr int CRT_BK = 32;                   // K' bytes per stage
+constexpr int CRT_ATILE = CRT_BM * CRT_BK;   // 4 KB
+constexpr int CRT_BTILE = CRT_BN * CRT_BK;   // 8 KB
+constexpr int CRT_STAGE = CRT_ATILE + CRT_BTILE;
+constexpr int CRT_NS = 16;                   // ring slots (192 KB)
+constexpr int CRT_EPI_WARPS = 8;
+constexpr int CRT_THREADS = 32 * (2 + CRT_EPI_WARPS);
+constexpr int CRT_SCRATCH = CRT_NMOD * CRT_BM * CRT_BN;   // residue bytes per CTA (448 KB)
+constexpr uint32_t CRT_IDESC = tc::idesc_i8(CRT_BM, CRT_BN);
+constexpr int CRT_MODS[CRT_NMOD] = {255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197};
+
+// moduli, 1/p, the three limbs of w_p and of P, 1/P (filled once per device)
+struct CrtConst {
+    double p[CRT_NMOD];
+    double inv_p[CRT_NMOD];
+    double wh[CRT_NMOD], wm[CRT_NMOD], wl[CRT_NMOD];
+    double Ph, Pm, Pl, invP;
+    double log2P;
+};
+__constant__ CrtConst c_crt;
+
+// ---------------------------------------------------------------- host constants
+// 128-bit unsigned arithmetic for the limbs (P < 2^110)
+typedef unsigned __int128 u128;
+
+CrtConst make_constants() {
+    CrtConst k{};
+    u128 P = 1;
+    for (int i = 0; i < CRT_NMOD; ++i) P *= (u128)CRT_MODS[i];
+    const u128 mask = ((u128)1 << 37) - 1;
+    auto limb = [&](u128 x, double* h, double* m, double* l) {
+        *h = (double)(uint64_t)(x >> 74);
+        *m = (double)(uint64_t)((x >> 37) & mask);
+        *l = (double)(uint64_t)(x & mask);
+    };
+    for (int i = 0; i < CRT_NMOD; ++i) {
+        const uint64_t p = (uint64_t)CRT_MODS[i];
+        const u128 Mp = P / p;
+        const uint64_t mr = (uint64_t)(Mp % p);
+        uint64_t y = 0;   // Mp^-1 mod p by search (p < 256)
+        for (uint64_t t = 1; t < p; ++t)
+            if ((mr * t) % p == 1) {
+                y = t;
+                break;
+            }
+        const u128 w = (Mp * (u128)y) % P;
+        k.p[i] = (double)p;
+        k.inv_p[i] = 1.0 / (double)p;
+        limb(w, &k.wh[i], &k.wm[i], &k.wl[i]);
+    }
+    limb(P, &k.Ph, &k.Pm, &k.Pl);
+    const double Pd = std::ldexp(k.Ph, 74) + std::ldexp(k.Pm, 37) + k.Pl;
+    k.invP = 1.0 / Pd;
+    k.log2P = std::log2(Pd);
+    return k;
+}
+
+// scale exponents: al = be = floor((log2 P - 3 - log2 K') / 2), K' = 2k
+int crt_bits(int k, double log2P) {
+    const double kp = 2.0 * (double)(k > 0 ? k : 1);
+    int b = (int)std::floor((log2P - 3.0 - std::log2(kp)) / 2.0);
+    return b > 52 ? 52 : b;
+}
+
+// symmetric residue of an integer-valued double (|x| <= 2^52) mod p
+__device__ __forceinline__ int sym_mod(double x, double p, double inv_p) {
+    const double q = rint(x * inv_p);
+    return (int)fma(-q, p, x);
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+    return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
+           ((uint32_t)(uint8_t)d << 24);
+}
+
+// ---------------------------------------------------------------- packing
+// A' residue tiles: [b][p][rb][kb][4 KB]; a thread takes one complex row i and
+// 8 complex columns (16 K' bytes) and writes one 16-byte core-matrix row per
+// modulus for each of A' rows 2i (Re, -Im pairs) and 2i+1 (Im, Re pairs)
+__global__ void __launch_bounds__(128) crt_pack_a_kernel(int m, int k, const double2* __restrict__ A,
+                                                         const double2* const* Ap, int lda, long long sA,
+                                                         const int* __restrict__ rowexp, int al, int RB, int KB,
+                                                         int8_t* __restrict__ out) {
+    const int b = blockIdx.z;
+    const int rb = blockIdx.x, kb = blockIdx.y;
+    const double2* a = Ap ? Ap[b] : A + b * sA;
+    const int il = threadIdx.x & 63, jc = threadIdx.x >> 6;
+    const int i = rb * (CRT_BM / 2) + il, j0 = kb * (CRT_BK / 2) + 8 * jc;
+    double xr[8], xi[8];
+    const int ex = (i < m) ? rowexp[(long long)b * m + i] : 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double2 v = make_double2(0.0, 0.0);
+        if (i < m && j0 + q < k) v = a[(long long)(j0 + q) * lda + i];
+        xr[q] = rint(ldexp(v.x, al - ex));
+        xi[q] = rint(ldexp(v.y, al - ex));
+    }
+    const int o0 = tc::tile_off(2 * il, 16 * jc), o1 = tc::tile_off(2 * il + 1, 16 * jc);
+    const long long plane = (long long)RB * KB * CRT_ATILE;
+    int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)rb * KB + kb) * CRT_ATILE;
+#pragma unroll 1
+    for (int t = 0; t < CRT_NMOD; ++t) {
+        const double p = c_crt.p[t], ip = c_crt.inv_p[t];
+        int dr[8], di[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            dr[q] = sym_mod(xr[q], p, ip);
+            di[q] = sym_mod(xi[q], p, ip);
+        }
+        const uint4 w0 = make_uint4(pack4(dr[0], -di[0], dr[1], -di[1]), pack4(dr[2], -di[2], dr[3], -di[3]),
+                                    pack4(dr[4], -di[4], dr[5], -di[5]), pack4(dr[6], -di[6], dr[7], -di[7]));
+        const uint4 w1 = make_uint4(pack4(di[0], dr[0], di[1], dr[1]), pack4(di[2], dr[2], di[3], dr[3]),
+                                    pack4(di[4], dr[4], di[5], dr[5]), pack4(di[6], dr[6], di[7], dr[7]));
+        int8_t* pl = base + (long long)t * plane;
+        *reinterpret_cast<uint4*>(pl + o0) = w0;
+        *reinterpret_cast<uint4*>(pl + o1) = w1;
+    }
+}
+
+// B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB]; a thread takes one
+// column c and 16 complex rows (32 K' bytes: both core matrices along K)
+__global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const double2* __restrict__ B,
+                                                         const double2* const* Bp, int ldb, long long sB,
+                                                         const int* __restrict__ colexp, int be, int CB, int KB,
+                                                         int8_t* __restrict__ out) {
+    const int b = blockIdx.z;
+    const int cb = blockIdx.x, kb = blockIdx.y;
+    const double2* bb = Bp ? Bp[b] : B + b * sB;
+    const int cl = threadIdx.x;
+    const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2);
+    double xr[16], xi[16];
+    const int ex = (c < n) ? colexp[(long long)b * n + c] : 0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        double2 v = make_double2(0.0, 0.0);
+        if (c < n && j0 + q < k) v = bb[(long long)c * ldb + j0 + q];
+        xr[q] = rint(ldexp(v.x, be - ex));
+        xi[q] = rint(ldexp(v.y, be - ex));
+    }
+    const int o0 = tc::tile_off(cl, 0), o1 = tc::tile_off(cl, 16);
+    const long long plane = (long long)CB * KB * CRT_BTILE;
+    int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)cb * KB + kb) * CRT_BTILE;
+#pragma unroll 1
+    for (int t = 0; t < CRT_NMOD; ++t) {
+        const double p = c_crt.p[t], ip = c_crt.inv_p[t];
+        int d[32];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            d[2 * q] = sym_mod(xr[q], p, ip);
+            d[2 * q + 1] = sym_mod(xi[q], p, ip);
+        }
+        int8_t* pl = base + (long long)t * plane;
+        *reinterpret_cast<uint4*>(pl + o0) = make_uint4(pack4(d[0], d[1], d[2], d[3]), pack4(d[4], d[5], d[6], d[7]),
+                                                       pack4(d[8], d[9], d[10], d[11]),
+                                                       pack4(d[12], d[13], d[14], d[15]));
+        *reinterpret_cast<uint4*>(pl + o1) =
+            make_uint4(pack4(d[16], d[17], d[18], d[19]), pack4(d[20], d[21], d[22], d[23]),
+                       pack4(d[24], d[25], d[26], d[27]), pack4(d[28], d[29], d[30], d[31]));
+    }
+}
+
+// ---------------------------------------------------------------- MMA kernel
+struct CrtArgs {
+    int m, n, k, RB, CB, KB, batch, ntiles;
+    int shift;               // al + be
+    const int8_t* Aq;
+    const int8_t* Bq;
+    const int* rowexp;
+    const int* colexp;
+    double2 alpha, beta;
+    const double2* alphas;
+    double2* C;
+    double2* const* Cp;
+    int ldc;
+    long long sC;
+    int8_t* scratch;         // CRT_SCRATCH bytes per CTA
+    int* err;
+};
+
+// C'_int from its residues (one value): exact limb sums, exact reduction, one rounding
+__device__ __forceinline__ double crt_value(const int (&r)[CRT_NMOD]) {
+    double sh = 0.0, sm = 0.0, sl = 0.0;
+#pragma unroll
+    for (int t = 0; t < CRT_NMOD; ++t) {
+        const double rv = (double)r[t];
+        sh = fma(rv, c_crt.wh[t], sh);
+        sm = fma(rv, c_crt.wm[t], sm);
+        sl = fma(rv, c_crt.wl[t], sl);
+    }
+    const double s = fma(sh, 0x1p74, fma(sm, 0x1p37, sl));
+    const double q = rint(s * c_crt.invP);
+    const double dh = fma(-q, c_crt.Ph, sh);
+    const double dm = fma(-q, c_crt.Pm, sm);
+    const double dl = fma(-q, c_crt.Pl, sl);
+    return fma(dh, 0x1p74, fma(dm, 0x1p37, dl));
+}
+
+__global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[CRT_NS], empty[CRT_NS], accfull[2], accempty[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    volatile int* aborted = &abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int KB = g.KB;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < CRT_NS; ++q) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&empty[q], 1);
+        }
+        for (int q = 0; q < 2; ++q) {
+            tc::mbar_init(&accfull[q], 1);
+            tc::mbar_init(&accempty[q], CRT_EPI_WARPS);
+        }
+        *aborted = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 512u);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    const long long planeA = (long long)g.RB * KB * CRT_ATILE;
+    const long long planeB = (long long)g.CB * KB * CRT_BTILE;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: for each tile, modulus and K step, one A and one B tile
+            long long stage = 0;
+            for (int tile = blockIdx.x; tile < g.ntiles && !*aborted; tile += gridDim.x) {
+                const int cb = tile % g.CB, rb = (tile / g.CB) % g.RB, b = tile / (g.CB * g.RB);
+                for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
+                    const int8_t* Ab = g.Aq + ((long long)b * CRT_NMOD + t) * planeA + (long long)rb * KB * CRT_ATILE;
+                    const int8_t* Bb = g.Bq + ((long long)b * CRT_NMOD + t) * planeB + (long long)cb * KB * CRT_BTILE;
+                    for (int kb = 0; kb < KB; ++kb, ++stage) {
+                        const int slot = (int)(stage % CRT_NS);
+                        if (stage >= CRT_NS && !tc::mbar_wait(&empty[slot], (uint32_t)(((stage / CRT_NS) - 1) & 1))) {
+                            atomicExch(g.err, 11);
+                            *aborted = 1;
+                            break;
+                        }
+                        if (*aborted) break;
+                        unsigned char* sa = smem_raw + (size_t)slot * CRT_STAGE;
+                        tc::mbar_expect_tx(&full[slot], (uint32_t)CRT_STAGE);
+                        tc::bulk_g2s(sa, Ab + (long long)kb * CRT_ATILE, (uint32_t)CRT_ATILE, &full[slot]);
+                        tc::bulk_g2s(sa + CRT_ATILE, Bb + (long long)kb * CRT_BTILE, (uint32_t)CRT_BTILE, &full[slot]);
+                    }
+                }
+            }
+            // drain: the last CRT_NS stages' copies must have landed before the CTA exits
+            for (long long s2 = (stage > CRT_NS ? stage - CRT_NS : 0); s2 < stage; ++s2)
+                tc::mbar_wait(&full[s2 % CRT_NS], (uint32_t)((s2 / CRT_NS) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: accumulator unit u (tile, modulus) in buffer u & 1
+            const uint64_t desc0 = tc::smem_desc(smem_raw);
+            const uint64_t slot_step = (uint64_t)(CRT_STAGE >> 4);
+            long long stage = 0, u = 0;
+            for (int tile = blockIdx.x; tile < g.ntiles && !*aborted; tile += gridDim.x) {
+                for (int t = 0; t < CRT_NMOD && !*aborted; ++t, ++u) {
+                    const int buf = (int)(u & 1);
+                    if (u >= 2 && !tc::mbar_wait(&accempty[buf], (uint32_t)(((u >> 1) - 1) & 1))) {
+                        atomicExch(g.err, 12);
+                        *aborted = 1;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t acc = tmem + (uint32_t)(buf * CRT_BN);
+                    for (int kb = 0; kb < KB; ++kb, ++stage) {
+                        const int slot = (int)(stage % CRT_NS);
+                        if (!tc::mbar_wait(&full[slot], (uint32_t)((stage / CRT_NS) & 1))) {
+                            atomicExch(g.err, 13);
+                            *aborted = 1;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        const uint64_t da = desc0 + (uint64_t)slot * slot_step;
+                        const uint64_t db = da + (uint64_t)(CRT_ATILE >> 4);
+                        tc::mma_i8<CRT_IDESC>(acc, da, db, kb > 0 ? 1u : 0u);
+                        tc::mma_commit(&empty[slot]);
+                    }
+                    if (*aborted) break;
+                    tc::mma_commit(&accfull[buf]);
+                }
+            }
+        }
+    } else {
+        // epilogue warps: TMEM lane quarter (hardware: warp % 4) and column half
+        const int ew = warp - 2;
+        const int quarter = warp & 3;
+        const int half = ew >> 2;
+        const int row = quarter * 32 + lane;                 // row of C' in the tile
+        int8_t* scr = g.scratch + (long long)blockIdx.x * CRT_SCRATCH;
+        long long u = 0;
+        for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+            const int cb = tile % g.CB, rb = (tile / g.CB) % g.RB, b = tile / (g.CB * g.RB);
+            bool ok = true;
+            for (int t = 0; t < CRT_NMOD; ++t, ++u) {
+                const int buf = (int)(u & 1);
+                bool ready = !*aborted && tc::mbar_wait(&accfull[buf], (uint32_t)((u >> 1) & 1));
+                ready = __all_sync(0xffffffffu, ready);
+                if (!ready) {
+                    if (lane == 0 && !*aborted) atomicExch(g.err, 14);
+                    *aborted = 1;
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const double p = c_crt.p[t], ip = c_crt.inv_p[t];
+                int8_t* dst = scr + ((long long)t * CRT_BM + row) * CRT_BN;
+#pragma unroll 1
+                for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+                    uint32_t r[32];
+                    tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * CRT_BN + c0), r);
+                    uint32_t w[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        w[q] = pack4(sym_mod((double)(int)r[4 * q], p, ip), sym_mod((double)(int)r[4 * q + 1], p, ip),
+                                     sym_mod((double)(int)r[4 * q + 2], p, ip),
+                                     sym_mod((double)(int)r[4 * q + 3], p, ip));
+                    *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
+                    *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&accempty[buf]);
+            }
+            if (!ok) break;
+            __syncwarp();
+            // rebuild this warp's rows x columns from the residues (this thread wrote them)
+            const int rowp = rb * CRT_BM + row;
+            const int i = rowp >> 1;
+            const bool im = rowp & 1;
+            double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
+            const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
+            const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
+            const int ex = (i < g.m) ? g.rowexp[(long long)b * g.m + i] : 0;
+#pragma unroll 1
+            for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
+                uint4 rv[CRT_NMOD];
+#pragma unroll
+                for (int t = 0; t < CRT_NMOD; ++t)
+                    rv[t] = *reinterpret_cast<const uint4*>(scr + ((long long)t * CRT_BM + row) * CRT_BN + c0);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    int r[CRT_NMOD];
+#pragma unroll
+                    for (int t = 0; t < CRT_NMOD; ++t) {
+                        const uint32_t word = (q < 4) ? rv[t].x : (q < 8) ? rv[t].y : (q < 12) ? rv[t].z : rv[t].w;
+                        r[t] = (int)(int8_t)(word >> (8 * (q & 3)));
+                    }
+                    const int c = cb * CRT_BN + c0 + q;
+                    const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
+                    const double v = ldexp(crt_value(r), ex + fx - g.shift);
+                    const double o = __shfl_xor_sync(0xffffffffu, v, 1);
+                    if (!im && i < g.m && c < g.n) {
+                        double2* pc = C + (long long)c * g.ldc + i;
+                        double2 val = cmul(alpha, make_double2(v, o));
+                        if (!beta_zero) val = cfma(g.beta, *pc, val);
+                        *pc = val;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 512u);
+}
+
+bool g_crt_const_ready[64] = {};
+
+// int8 tensor-core throughput probe: one CTA per SM issues `iters` MMAs of
+// 128 x 256 x 32 (the modular engine's shape) on operands resident in shared
+// memory into one TMEM accumulator, then waits (bounded) for them
+__global__ void __launch_bounds__(128, 1) int8_probe_kernel(int iters, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t done;
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < CRT_STAGE / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(smem_raw)[i] = make_uint4(0x01010101u, 0u, 0x01010101u, 0u);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 256u);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    if (threadIdx.x == 32) {
+        const uint64_t da = tc::smem_desc(smem_raw);
+        const uint64_t db = da + (uint64_t)(CRT_ATILE >> 4);
+        for (int it = 0; it < iters; ++it) tc::mma_i8<CRT_IDESC>(tmem, da, db, it > 0 ? 1u : 0u);
+        tc::mma_commit(&done);
+    }
+    bool ok = tc::mbar_wait(&done, 0);
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 256u);
+}
+
+}  // namespace
+
+sc_status int8_peak_probe(int device, Workspace& ws, double* tops) {
+    int sms = 148;
+    SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    int* err;
+    SC_TRY(ws.get(&err, 1, WS_OZ_ERR, 0));
+    SC_CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
+    SC_CUDA_TRY(cudaFuncSetAttribute(int8_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CRT_STAGE + 1024));
+    const int iters = 8192;
+    cudaEvent_t e0, e1;
+    SC_CUDA_TRY(cudaEventCreate(&e0));
+    SC_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(e0, 0);
+        int8_probe_kernel<<<sms, 128, CRT_STAGE + 1024>>>(iters, err);
+        count_launch();
+        cudaEventRecord(e1, 0);
+        SC_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int herr = 0;
+    SC_CUDA_TRY(cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        set_error("int8 probe: tensor-core wait timed out");
+        return SC_CUDA_ERROR;
+    }
+    const double ops = 2.0 * CRT_BM * CRT_BN * CRT_BK * (double)iters * sms;
+    *tops = ops / (best * 1e-3) / 1e12;
+    return SC_OK;
+}
+
+// packed bytes of the residue operands per batch entry
+size_t crt_packed_bytes(int m, int n, int k) {
+    const long long RB = (2LL * m + CRT_BM - 1) / CRT_BM, CB = ((long long)n + CRT_BN - 1) / CRT_BN,
+                    KB = (2LL * k + CRT_BK - 1) / CRT_BK;
+    return (size_t)CRT_NMOD * (size_t)KB * ((size_t)RB * CRT_ATILE + (size_t)CB * CRT_BTILE);
+}
+
+sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws, int* err) {
+    if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
+    if (!err) {
+        set_error("zgemm_crt: no error word");
+        return SC_BADINPUT;
+    }
+    if (2LL * g.k * 128 * 128 >= (1LL << 31)) {
+        set_error("zgemm_crt: K = %d too deep for exact int32 accumulation", g.k);
+        return SC_BADINPUT;
+    }
+    int dev = 0;
+    SC_CUDA_TRY(cudaGetDevice(&dev));
+    static CrtConst host_const = make_constants();
+    if (dev >= 0 && dev < 64 && !g_crt_const_ready[dev]) {
+        SC_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &host_const, sizeof(CrtConst)));
+        SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         CRT_NS * CRT_STAGE + 1024));
+        g_crt_const_ready[dev] = true;
+    }
+    int sms = 148;
+    SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int bits = crt_bits(g.k, host_const.log2P);
+    const int RB = (2 * g.m + CRT_BM - 1) / CRT_BM, CB = (g.n + CRT_BN - 1) / CRT_BN,
+              KB = (2 * g.k + CRT_BK - 1) / CRT_BK;
+    if (RB > 65535 || KB > 65535) {
+        set_error("zgemm_crt: grid too large");
+        return SC_BADINPUT;
+    }
+    // sub-batches so that the packed operands stay within 8 GiB
+    const size_t per = crt_packed_bytes(g.m, g.n, g.k);
+    int sub = (int)std::max<size_t>(1, std::min<size_t>((size_t)batch, (8ULL << 30) / std::max<size_t>(per, 1)));
+    if (sub > 65535) sub = 65535;
+    int8_t *Aq, *Bq, *scratch;
+    int* ex;
+    const size_t aq = (size_t)sub * CRT_NMOD * RB * KB * CRT_ATILE;
+    const size_t bq = (size_t)sub * CRT_NMOD * CB * KB * CRT_BTILE;
+    SC_TRY(ws.get(&Aq, aq, WS_OZ_A, st));
+    SC_TRY(ws.get(&Bq, bq, WS_OZ_B, st));
+    SC_TRY(ws.get(&ex, (size_t)batch * (g.m + g.n), WS_OZ_E, st));
+    SC_TRY(ws.get(&scratch, (size_t)sms * CRT_SCRATCH, WS_CRT_SCRATCH, st));
+    int* rowexp = ex;
+    int* colexp = ex + (size_t)batch * g.m;
+    size_t mark_all = 0;
+    if (ws.time_kernels)
+        SC_TRY(ws.mark_begin(st, 3, 8.0 * g.m * (double)g.n * g.k * batch, 0.0, &mark_all));
+    SC_CUDA_TRY(cudaMemsetAsync(rowexp, 0x80, sizeof(int) * (size_t)batch * g.m, st));
+    SC_TRY(oz_exponents(st, g, batch, rowexp, colexp));
+    for (int b0 = 0; b0 < batch; b0 += sub) {
+        const int nb = std::min(sub, batch - b0);
+        GemmArgs h = g;
+        if (g.Ap) h.Ap = g.Ap + b0; else h.A = g.A + (long long)b0 * g.sA;
+        if (g.Bp) h.Bp = g.Bp + b0; else h.B = g.B + (long long)b0 * g.sB;
+        crt_pack_a_kernel<<<dim3(RB, KB, nb), 128, 0, st>>>(g.m, g.k, h.A, h.Ap, g.lda, g.sA,
+                                                           rowexp + (size_t)b0 * g.m, bits, RB, KB, Aq);
+        crt_pack_b_kernel<<<dim3(CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
+                                                           colexp + (size_t)b0 * g.n, bits, CB, KB, Bq);
+        count_launch(2);
+        SC_CHECK_LAUNCH("crt pack");
+        CrtArgs a;
+        a.m = g.m;
+        a.n = g.n;
+        a.k = g.k;
+        a.RB = RB;
+        a.CB = CB;
+        a.KB = KB;
+        a.batch = nb;
+        a.ntiles = nb * RB * CB;
+        a.shift = 2 * bits;
+        a.Aq = Aq;
+        a.Bq = Bq;
+        a.rowexp = rowexp + (size_t)b0 * g.m;
+        a.colexp = colexp + (size_t)b0 * g.n;
+        a.alpha = g.alpha;
+        a.beta = g.beta;
+        a.alphas = g.alphas ? g.alphas + b0 : nullptr;
+        a.C = g.Cp ? nullptr : g.C + (long long)b0 * g.sC;
+        a.Cp = g.Cp ? g.Cp + b0 : nullptr;
+        a.ldc = g.ldc;
+        a.sC = g.sC;
+        a.scratch = scratch;
+        a.err = err;
+        const int grid = std::min(a.ntiles, sms);
+        size_t mark = 0;
+        if (ws.time_kernels) {
+            const double macs = (double)CRT_NMOD * nb * (double)RB * CRT_BM * (double)CB * CRT_BN * (double)KB * CRT_BK;
+            SC_TRY(ws.mark_begin(st, 2, 8.0 * g.m * (double)g.n * g.k * nb, 2.0 * macs, &mark));
+        }
+        crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_STAGE + 1024, st>>>(a);
+        count_launch();
+        if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark));
+        SC_CHECK_LAUNCH("crt mma");
+    }
+    if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark_all));
+    return SC_OK;
+}
+
+}  // namespace sc

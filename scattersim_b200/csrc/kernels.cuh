@@ -19,7 +19,7 @@ enum WsSlot {
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
     WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR, WS_TUNE_C, WS_TUNE_P,
-    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR, WS_MFUN_OUT, WS_CHAIN_T,
+    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR, WS_MFUN_OUT, WS_CHAIN_T, WS_CRT_SCRATCH,
     WS_COUNT
 };
 
@@ -155,15 +155,30 @@ sc_status zgemm_op(cudaStream_t st, bool conjA, bool conjB, int m, int n, int k,
 // `slices` 7-bit digits per operand (1..7); err: device word set nonzero if a
 // pipeline wait timed out (never cleared here)
 sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch, Workspace& ws, int* err);
+// power-of-two row exponents of A (rowexp, batch x m) and column exponents of
+// B (colexp, batch x n): max |Re|, |Im| of the row / column < 2^e
+sc_status oz_exponents(cudaStream_t st, const GemmArgs& g, int batch, int* rowexp, int* colexp);
+
+// crt.cu: the same product on the int8 tensor cores by modular arithmetic
+// (14 moduli, Chinese-remainder reconstruction in FP64); about 2^-47 relative
+// to row scale x column scale x k per element for k <= 1250
+sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws, int* err);
+size_t crt_packed_bytes(int m, int n, int k);
+// measured int8 tcgen05 throughput (TOPS) at the modular engine's MMA shape,
+// operands resident in shared memory
+sc_status int8_peak_probe(int device, Workspace& ws, double* tops);
 
 // A GEMM engine for op = N products: FP64 tensor-pipe tiles, and with
 // slices > 0 also int8 digit slices on the tcgen05 tensor cores.  The first
 // product of each shape times every candidate once (into scratch output) and
 // caches the fastest in the workspace; later products of that shape reuse it.
-// force_int8 skips the tuning and runs every product on the int8 engine.
+// force_int8 skips the tuning and runs every product on the digit-slice
+// engine; force_crt every product on the modular (CRT) engine.  With
+// slices == 7 and neither forced, the modular engine is a tuning candidate too.
 struct GemmEngine {
     int slices = 0;
     bool force_int8 = false;
+    bool force_crt = false;
     Workspace* ws = nullptr;
     int* err = nullptr;
     sc_status run(cudaStream_t st, const GemmArgs& g, int batch) const;

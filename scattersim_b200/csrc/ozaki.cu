@@ -32,6 +32,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace sc {
 
@@ -46,14 +47,8 @@ constexpr int OZ_MAXS = 7;
 constexpr int OZ_MAXST = 8;      // pipeline slots
 constexpr int OZ_SMEM_BUDGET = 200 * 1024;
 constexpr int OZ_THREADS = 128;
-constexpr long long OZ_SPIN = 1LL << 24;
 
-// byte offset of (row, kk) inside one K-major core-matrix tile of 32 K bytes:
-// core matrices of 8 rows x 16 bytes, the two along K 128 B apart (LBO), the
-// 8-row groups 256 B apart (SBO)
-__device__ __forceinline__ int tile_off(int r, int kk) {
-    return (r >> 3) * 256 + (kk >> 4) * 128 + (r & 7) * 16 + (kk & 15);
-}
+using tc::tile_off;
 
 // stages of the ring for s digit planes
 __host__ __device__ __forceinline__ int oz_stages(int s) {
@@ -195,61 +190,14 @@ __global__ void __launch_bounds__(128) oz_pack_b_kernel(int k, int n, const doub
     }
 }
 
-// ------------------------------------------------------------------ tcgen05 plumbing
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait: false after OZ_SPIN polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (long long it = 0; it < OZ_SPIN; ++it)
-        if (mbar_try(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ uint64_t smem_desc(const void* p) {
-    // K-major, no swizzle: LBO = 128 B (next core matrix along K), SBO = 256 B
-    // (next 8-row group), descriptor version 1
-    return (uint64_t)((smem_u32(p) >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
-           (1ULL << 46);
-}
-// kind::i8: D s32 (bits 4-5 = 2), A and B signed (bits 7-9, 10-12 = 1), K-major,
-// N >> 3 at bits 17-22, M >> 4 at bits 24-28
-constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
-                              ((uint32_t)(OZ_BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
-                 : "memory");
-}
+constexpr uint32_t OZ_IDESC = tc::idesc_i8(OZ_BM, OZ_BN);
+using tc::bulk_g2s;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::mma_commit;
+using tc::smem_desc;
+using tc::smem_u32;
 
 struct OzArgs {
     int m, n, k, s, RB, CB, KB;
@@ -342,7 +290,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
             for (int t = 0; t < S; ++t)
 #pragma unroll
                 for (int u = 0; u < S - t; ++u)
-                    mma_i8(tmem + (uint32_t)((t + u) * OZ_BN), da + (uint64_t)(t * (OZ_ATILE >> 4)),
+                    tc::mma_i8<OZ_IDESC>(tmem + (uint32_t)((t + u) * OZ_BN), da + (uint64_t)(t * (OZ_ATILE >> 4)),
                            db + (uint64_t)(u * (OZ_BTILE >> 4)), (t > 0) ? 1u : later);
             mma_commit(&empty[slot]);
         }
@@ -430,6 +378,17 @@ sc_status launch_mma(int s, dim3 grid, size_t smem, cudaStream_t st, const OzArg
 }
 }  // namespace
 
+sc_status oz_exponents(cudaStream_t st, const GemmArgs& g, int batch, int* rowexp, int* colexp) {
+    // row exponents start at the smallest exponent (all-zero rows pack to zeros)
+    SC_CUDA_TRY(cudaMemsetAsync(rowexp, 0x80, sizeof(int) * (size_t)batch * g.m, st));
+    oz_rowexp_kernel<<<dim3((g.m + 127) / 128, (g.k + 255) / 256, batch), 128, 0, st>>>(g.m, g.k, g.A, g.Ap, g.lda,
+                                                                                       g.sA, rowexp);
+    oz_colexp_kernel<<<dim3((g.n + 7) / 8, batch), 256, 0, st>>>(g.k, g.n, g.B, g.Bp, g.ldb, g.sB, colexp);
+    count_launch(2);
+    SC_CHECK_LAUNCH("int8 engine exponents");
+    return SC_OK;
+}
+
 size_t ozaki_smem_bytes(int s) { return (size_t)oz_stages(s) * s * (OZ_ATILE + OZ_BTILE) + 1024; }
 
 sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch, Workspace& ws, int* err) {
@@ -461,14 +420,10 @@ sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch,
         set_error("zgemm_ozaki: no error word");
         return SC_BADINPUT;
     }
-    // row exponents start at the smallest exponent (all-zero rows pack to zeros)
-    SC_CUDA_TRY(cudaMemsetAsync(rowexp, 0x80, sizeof(int) * (size_t)batch * g.m, st));
-    oz_rowexp_kernel<<<dim3((g.m + 127) / 128, (g.k + 255) / 256, batch), 128, 0, st>>>(g.m, g.k, g.A, g.Ap, g.lda,
-                                                                                       g.sA, rowexp);
-    oz_colexp_kernel<<<dim3((g.n + 7) / 8, batch), 256, 0, st>>>(g.k, g.n, g.B, g.Bp, g.ldb, g.sB, colexp);
+    SC_TRY(oz_exponents(st, g, batch, rowexp, colexp));
     oz_pack_a_kernel<<<dim3(RB, KB, batch), 128, 0, st>>>(g.m, g.k, g.A, g.Ap, g.lda, g.sA, rowexp, s, RB, KB, Aq);
     oz_pack_b_kernel<<<dim3(CB, KB, batch), 128, 0, st>>>(g.k, g.n, g.B, g.Bp, g.ldb, g.sB, colexp, s, CB, KB, Bq);
-    count_launch(4);
+    count_launch(2);
     SC_CHECK_LAUNCH("ozaki pack");
     OzArgs a;
     a.m = g.m;
@@ -506,16 +461,18 @@ sc_status zgemm_ozaki(cudaStream_t st, int slices, const GemmArgs& g, int batch,
 
 // ------------------------------------------------------------------ engine
 namespace {
-enum { VAR_TILE64 = 0, VAR_TILE128 = 1, VAR_INT8 = 2 };
+enum { VAR_TILE64 = 0, VAR_TILE128 = 1, VAR_INT8 = 2, VAR_CRT = 3 };
 
 sc_status run_variant(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, int batch, int v) {
     if (v == VAR_INT8) return zgemm_ozaki(st, e.slices, g, batch, *e.ws, e.err);
+    if (v == VAR_CRT) return zgemm_crt(st, g, batch, *e.ws, e.err);
     return zgemm_tile(st, false, false, g, batch, v == VAR_TILE128 ? 128 : 64);
 }
 // the chosen variant; FP64 tiles are bracketed by timing marks here, the int8
-// MMA kernel marks itself (its pack kernels stay outside the mark)
+// engines mark themselves (the digit-slice engine its MMA kernel; the modular
+// engine its MMA kernel and, separately, the whole product with its packing)
 sc_status run_timed(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, int batch, int v) {
-    if (!e.ws->time_kernels || v == VAR_INT8) return run_variant(st, e, g, batch, v);
+    if (!e.ws->time_kernels || v == VAR_INT8 || v == VAR_CRT) return run_variant(st, e, g, batch, v);
     size_t mark = 0;
     SC_TRY(e.ws->mark_begin(st, 0, 8.0 * g.m * (double)g.n * g.k * batch, 0.0, &mark));
     SC_TRY(run_variant(st, e, g, batch, v));
@@ -525,6 +482,7 @@ sc_status run_timed(cudaStream_t st, const GemmEngine& e, const GemmArgs& g, int
 
 sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
     if (g.m <= 0 || g.n <= 0 || batch <= 0) return SC_OK;
+    if (force_crt) return zgemm_crt(st, g, batch, *ws, err);
     if (force_int8 && slices > 0) return zgemm_ozaki(st, slices, g, batch, *ws, err);
     const auto key = std::make_tuple(g.m, g.n, g.k, batch, slices);
     auto it = ws->gemm_choice.find(key);
@@ -532,6 +490,7 @@ sc_status GemmEngine::run(cudaStream_t st, const GemmArgs& g, int batch) const {
     std::vector<int> cand{VAR_TILE64};
     if (g.m > 64) cand.push_back(VAR_TILE128);
     if (slices > 0 && 2LL * g.k * (slices + 1) <= (1LL << 16)) cand.push_back(VAR_INT8);
+    if (slices == 7 && g.k <= 4096) cand.push_back(VAR_CRT);
     int best = cand[0];
     if (cand.size() > 1) {
         // candidates write a compact scratch output (ldc = m, at most 1 GiB: the

@@ -203,12 +203,16 @@ sc_status upload(cudaStream_t st, T* dst, const std::vector<T>& src) {
     return SC_OK;
 }
 
-// slices / forcing of a precision code (SC_SWEEP_FP64, _MIXED, _SLICES(s))
-bool precision_slices(int precision, int* slices, bool* force) {
+// slices / forcing of a precision code (SC_SWEEP_FP64, _MIXED, _CRT, _SLICES(s))
+bool precision_slices(int precision, int* slices, bool* force, bool* crt) {
     *force = false;
+    *crt = false;
     if (precision == SC_SWEEP_FP64) *slices = 0;
     else if (precision == SC_SWEEP_MIXED) *slices = 7;
-    else if ((precision & ~0xFF) == 0x100 && (precision & 0xFF) >= 1 && (precision & 0xFF) <= 7) {
+    else if (precision == SC_SWEEP_CRT) {
+        *slices = 7;
+        *crt = true;
+    } else if ((precision & ~0xFF) == 0x100 && (precision & 0xFF) >= 1 && (precision & 0xFF) <= 7) {
         *slices = precision & 0xFF;
         *force = true;
     } else
@@ -243,8 +247,8 @@ sc_status product(cudaStream_t st, const GemmEngine& eng, int m, int n, int k, c
 
 sc_status set_volume_precision(sc_context* ctx, int precision) {
     int sl;
-    bool force;
-    if (!precision_slices(precision, &sl, &force)) {
+    bool force, crt;
+    if (!precision_slices(precision, &sl, &force, &crt)) {
         set_error("sc_volume_precision: unknown precision %d", precision);
         return SC_BADINPUT;
     }
@@ -398,7 +402,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     // the int8 engine under a mixed precision setting (the FFT, assembly,
     // Omega, the eigensolve, the eigenvectors and every LU stay FP64)
     GemmEngine eng;
-    precision_slices(ctx->precision, &eng.slices, &eng.force_int8);
+    precision_slices(ctx->precision, &eng.slices, &eng.force_int8, &eng.force_crt);
     eng.ws = &ws;
     if (eng.slices) {
         SC_TRY(ws.get(&eng.err, 1, WS_OZ_ERR, st));

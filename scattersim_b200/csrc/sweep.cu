@@ -343,11 +343,14 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
         return SC_BADINPUT;
     }
     int slices = -1;
-    bool force = false;
+    bool force = false, crt = false;
     if (precision == SC_SWEEP_FP64) {
         slices = 0;
     } else if (precision == SC_SWEEP_MIXED) {
         slices = 7;
+    } else if (precision == SC_SWEEP_CRT) {
+        slices = 7;
+        crt = true;
     } else if ((precision & ~0xFF) == 0x100 && (precision & 0xFF) >= 1 && (precision & 0xFF) <= 7) {
         slices = precision & 0xFF;
         force = true;
@@ -386,13 +389,15 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
     size_t freeb = 0, totalb = 0;
     SC_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
     const size_t held = ctx->ws.bytes[WS_SWEEP];
-    // the digit-slice engine keeps its packed operands in its own workspace
+    // the int8 engines keep their packed operands in their own workspace
+    // (the modular engine caps them at 8 GiB per product)
     size_t budget = (size_t)((slices ? 0.45 : 0.6) * (double)(freeb + held));
     const size_t cap = (size_t)48 << 30;
     if (budget > cap) budget = cap;
     GemmEngine eng;
     eng.slices = slices;
     eng.force_int8 = force;
+    eng.force_crt = crt;
     eng.ws = &ctx->ws;
     SC_TRY(ctx->ws.get(&eng.err, 1, WS_OZ_ERR, st));
     SC_CUDA_TRY(cudaMemsetAsync(eng.err, 0, sizeof(int), st));

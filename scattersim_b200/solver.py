@@ -79,6 +79,15 @@ class Context:
         keys = ("launches", "ms", "flops", "int8_ops")
         return {"dmma": dict(zip(keys, out[0:4])), "int8": dict(zip(keys, out[4:8]))}
 
+    def kernel_stats_ex(self):
+        """Per kernel class: 'dmma' FP64 tiles, 'int8' digit-sliced MMA kernel, 'crt' modular MMA kernel,
+        'crt_gemm' whole modular-engine products; each {launches, ms, flops, int8_ops}."""
+        out = (ctypes.c_double * 16)()
+        check(self.lib.sc_kernel_stats_ex(self.handle, out, 4))
+        keys = ("launches", "ms", "flops", "int8_ops")
+        return {name: dict(zip(keys, out[4 * i:4 * i + 4])) for i, name in
+                enumerate(("dmma", "int8", "crt", "crt_gemm"))}
+
     def gemm_choices(self):
         """The autotuner's table: list of (m, n, k, batch, slices, variant)."""
         n = ctypes.c_int(0)
@@ -91,6 +100,12 @@ class Context:
         flat = [int(v) for rec in table for v in rec]
         buf = (ctypes.c_int * max(len(flat), 1))(*flat)
         check(self.lib.sc_gemm_choices_set(self.handle, buf, len(table)))
+
+    def int8_peak_tops(self) -> float:
+        """Measured int8 tcgen05 MMA throughput (TOPS), operands resident in shared memory."""
+        v = ctypes.c_double(0.0)
+        check(self.lib.sc_int8_peak_probe(self.handle, ctypes.byref(v)))
+        return v.value
 
     def fp64_peak_tflops(self, tensor: bool = False) -> float:
         """Measured FP64 throughput: FMA pipe, or mma.sync f64 with tensor=True."""
