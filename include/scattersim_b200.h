@@ -191,6 +191,26 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
                           int Z, int S1, int S2, void* x, void* evl, void* Qc, void* Qh,
                           int* info, void* stream);
 
+/* One rank's share of a volume solve split by layers over several GPUs
+ * (contiguous layer blocks, one exchange, ScatterVolume.cpp:282-336): for
+ * layers [layer_begin, layer_end) of the (Z, S1, S2) sample (the whole
+ * sample is passed; only the block's slices are read), the ordered product of
+ * the block's transfer matrices
+ *     P = T_{end-1} ... T_{begin},  T_i = GC_i GD_i^-1,
+ * in which the block starting at layer 0 has GC_0 in place of T_0, as one
+ * 4MF x 4MF column-major matrix.  The blocks' products, multiplied in layer
+ * order (P_last ... P_1 P_0), are Gc_static of ScatterVolume.cpp:326-335.
+ * GD0 (may be NULL; only for the block starting at layer 0) receives GD_0.
+ * info (host, may be NULL): first nonzero per-layer eigensolve status. */
+sc_status sc_volume_chain_block(sc_context* ctx, const sc_volume_params* p, const void* sample, int Z, int S1,
+                                int S2, int layer_begin, int layer_end, void* P, void* GD0, int* info, void* stream);
+
+/* The boundary system and its solve (ScatterVolume.cpp:339-466, 739) from
+ * the whole chain Gc_static and GD_0 (4MF x 4MF each, device): x = [R; T]
+ * (6 MF complex128), as sc_volume_solve with --external writes it. */
+sc_status sc_volume_boundary_solve(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
+                                   const void* Gc_static, const void* GD0, void* x, int* info, void* stream);
+
 /* Precision of sc_sweep_solve.  SC_SWEEP_FP64 runs every product on the FP64
  * tensor pipe.  SC_SWEEP_MIXED lets the layer-factor and chain products run
  * on the int8 tensor cores with 7 digit slices per operand

@@ -522,6 +522,103 @@ def solve(sample: np.ndarray, p: Params, keep=True) -> Solution:
 
 
 # --------------------------------------------------------------------------
+# the chain split by layer blocks (ScatterVolume.cpp:282-336 over a layer
+# range) and the boundary step from a given chain (:339-466, 739)
+# --------------------------------------------------------------------------
+def chain_block(sample: np.ndarray, p: Params, lb: int, le: int):
+    """Ordered product of the transfer matrices of layers [lb, le) and, for lb == 0, GD_0.
+
+    Gc_static <- Gc_i inv(Gd_i) Gc_static (:326-335) restricted to the block:
+    P = T_{le-1} ... T_{lb} with T_i = Gc_i inv(Gd_i), and Gc_0 in place of T_0
+    when the block starts at layer 0 (Gc_static starts as Gc_0, :321-324).
+    """
+    d, e, dirv, k, ni, slices, num_pixels, z, M, msgs = setup(sample, p)
+    Mx, My = M
+    MF = Mx * My
+    Z = num_pixels[0]
+    ZL = Z + 1
+    kc = complex(k, 0.0)
+    lat = upwq_cal(M, p.size, dirv, k, ni)
+    P = None
+    Gd0 = None
+    for i in range(lb, le):
+        Phi, _, _ = phi(slices[i], M, lat, k)
+        lam, V = eigen_sort(*mkl_eigensolve(Phi))
+        if Z == 1:                                                      # :298-301
+            dz_c, dz_d = z[ZL - 1] - z[0], z[0] - z[ZL - 1]
+        else:                                                           # :303-306
+            dz_c, dz_d = z[i + 1] - z[i], z[i] - z[i + 1]
+        odd = (np.arange(4 * MF) % 2) != 0
+        Gd = V * np.where(odd, np.exp(1j * kc * lam * dz_d), 1.0)[None, :]
+        Gc = V * np.where(odd, 1.0, np.exp(1j * kc * lam * dz_c))[None, :]
+        if i == 0:
+            Gd0 = Gd
+            T = Gc
+        else:
+            T = Gc @ mkl_inverse(Gd)
+        P = T if P is None else T @ P
+    return P, Gd0
+
+
+def boundary_from_chain(sample: np.ndarray, p: Params, Gc_static, Gd_static):
+    """x = [R; T] from the whole chain: MatTransfer, SetBoundaryConditions and zgesv (:339-466, 739)."""
+    d, e, dirv, k, ni, slices, num_pixels, z, M, msgs = setup(sample, p)
+    Mx, My = M
+    MF = Mx * My
+    kc = complex(k, 0.0)
+    lat = upwq_cal(M, p.size, dirv, k, ni)
+    E0 = e
+    Ef = []
+    for c in range(3):
+        if p.psf:
+            Ef.append(E0[c] * np.ones((Mx, My), dtype=np.complex128))
+        else:
+            Ef.append(fftw_fft2(E0[c] * np.ones((num_pixels[1], num_pixels[2]), dtype=np.complex128), My, Mx))
+    EF = np.concatenate([f.ravel(order="F") for f in Ef])
+    Sx = lat.meshS0.ravel(order="F")
+    Sy = lat.meshS1.ravel(order="F")
+    Sz0 = lat.Sz[0].ravel(order="F")
+    Sz1 = lat.Sz[1].ravel(order="F")
+    A = np.zeros((6 * MF, 6 * MF), dtype=np.complex128)
+    b = np.zeros(6 * MF, dtype=np.complex128)
+    m = np.arange(MF)
+    A[m, m] = Sx
+    A[m, MF + m] = Sy
+    A[m, 2 * MF + m] = -Sz0
+    A[MF + m, 3 * MF + m] = Sx
+    A[MF + m, 4 * MF + m] = Sy
+    A[MF + m, 5 * MF + m] = Sz1
+    phase = np.exp(1j * kc * z[0] * Sz0)
+    I = np.eye(MF, dtype=np.complex128)
+    dg = np.diag
+    f1 = np.zeros((4 * MF, 3 * MF), dtype=np.complex128)
+    f2 = np.zeros_like(f1)
+    f3 = np.zeros_like(f1)
+    f1[0:MF, 0:MF] = dg(phase)
+    f1[MF:2 * MF, MF:2 * MF] = dg(phase)
+    f1[2 * MF:3 * MF, MF:2 * MF] = -dg(phase * Sz0)
+    f1[2 * MF:3 * MF, 2 * MF:3 * MF] = dg(phase * Sy)
+    f1[3 * MF:4 * MF, 0:MF] = dg(phase * Sz0)
+    f1[3 * MF:4 * MF, 2 * MF:3 * MF] = -dg(phase * Sx)
+    f2[0:MF, 0:MF] = I
+    f2[MF:2 * MF, MF:2 * MF] = I
+    f2[2 * MF:3 * MF, MF:2 * MF] = dg(Sz0)
+    f2[2 * MF:3 * MF, 2 * MF:3 * MF] = dg(Sy)
+    f2[3 * MF:4 * MF, 0:MF] = -dg(Sz0)
+    f2[3 * MF:4 * MF, 2 * MF:3 * MF] = -dg(Sx)
+    f3[0:MF, 0:MF] = -I
+    f3[MF:2 * MF, MF:2 * MF] = -I
+    f3[2 * MF:3 * MF, MF:2 * MF] = dg(Sz1)
+    f3[2 * MF:3 * MF, 2 * MF:3 * MF] = -dg(Sy)
+    f3[3 * MF:4 * MF, 0:MF] = -dg(Sz1)
+    f3[3 * MF:4 * MF, 2 * MF:3 * MF] = dg(Sx)
+    A[2 * MF:6 * MF, 0:3 * MF] = f2
+    A[2 * MF:6 * MF, 3 * MF:6 * MF] = (Gd_static @ mkl_inverse(Gc_static)) @ f3
+    b[2 * MF:6 * MF] = -(f1 @ EF)
+    return sla.solve(A, b, check_finite=False)
+
+
+# --------------------------------------------------------------------------
 # a16/a17: wave lists of the coupled-wave structure (ScatterVolume.cpp:469-493, 907-987)
 # --------------------------------------------------------------------------
 def wind(E, kvec, dz):

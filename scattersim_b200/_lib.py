@@ -80,6 +80,10 @@ _SIGS = {
     "sc_scatterio_read": (c_int, [ctypes.c_char_p, POINTER(c_double), POINTER(c_double), POINTER(c_int),
                                   POINTER(c_longlong), c_int, c_void_p, c_void_p, c_void_p, c_longlong,
                                   POINTER(c_longlong)]),
+    "sc_volume_chain_block": (c_int, [c_void_p, POINTER(VolumeParams), c_void_p, c_int, c_int, c_int, c_int, c_int,
+                                      c_void_p, c_void_p, POINTER(c_int), c_void_p]),
+    "sc_volume_boundary_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
+                                         c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_params_default": (None, [POINTER(VolumeParams)]),
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
     "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),

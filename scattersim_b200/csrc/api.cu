@@ -40,6 +40,12 @@ sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params
 sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
                        int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
                        int* info_host, cudaStream_t st);
+sc_status volume_chain_block(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
+                             int S2, int lb, int le, double2* P_out, double2* GD0_out, int* info_host,
+                             cudaStream_t st);
+sc_status volume_boundary_solve(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
+                                const double2* Gcs_in, const double2* GD0, double2* x_out, int* info_host,
+                                cudaStream_t st);
 sc_status volume_waves_launch(cudaStream_t st, int MF, int Z, const double2* svec, const double2* x,
                               const double2* evl, const double2* Qc, const double2* Qh, const double* zpl,
                               double k, double ntop, double nbot, int external, int ez_mode, long long nw,
@@ -347,6 +353,28 @@ sc_status sc_volume_solve(sc_context* ctx, const sc_volume_params* p, const void
     DeviceGuard g(ctx->device);
     return volume_solve(ctx, p, (const double2*)sample, Z, S1, S2, (double2*)x, (double2*)evl, (double2*)Qc,
                         (double2*)Qh, info, (cudaStream_t)stream);
+}
+
+sc_status sc_volume_chain_block(sc_context* ctx, const sc_volume_params* p, const void* sample, int Z, int S1,
+                                int S2, int layer_begin, int layer_end, void* P, void* GD0, int* info, void* stream) {
+    if (!ctx || !p || !sample || !P) {
+        set_error("sc_volume_chain_block: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return volume_chain_block(ctx, p, (const double2*)sample, Z, S1, S2, layer_begin, layer_end, (double2*)P,
+                              (double2*)GD0, info, (cudaStream_t)stream);
+}
+
+sc_status sc_volume_boundary_solve(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
+                                   const void* Gc_static, const void* GD0, void* x, int* info, void* stream) {
+    if (!ctx || !p || !Gc_static || !GD0 || !x) {
+        set_error("sc_volume_boundary_solve: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return volume_boundary_solve(ctx, p, Z, S1, S2, (const double2*)Gc_static, (const double2*)GD0, (double2*)x,
+                                 info, (cudaStream_t)stream);
 }
 
 sc_status sc_sweep_solve(sc_context* ctx, int count, const sc_volume_params* params, const void* const* samples,

@@ -386,31 +386,48 @@ sc_status make_plan(const sc_volume_params* p, int Z, int S1, int S2, VolumePlan
 }
 
 // ---------------------------------------------------------------- the solve
-sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
-                       int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
-                       int* info_host, cudaStream_t st) {
+namespace {
+
+// per-solve state shared by the stages: plan, product engine and the small
+// host-built device arrays (lattice, z planes, S vectors, EF)
+struct VolumeRun {
     VolumePlan P;
-    SC_TRY(make_plan(p, Z, S1, S2, &P));
-    const int Mx = P.dims.Mx, My = P.dims.My, MF = P.dims.MF;
-    const int n2 = 2 * MF, n4 = 4 * MF, n6 = 6 * MF;
-    const long long s2 = (long long)n2 * n2, s4 = (long long)n4 * n4;
-    const double k = P.dims.k;
+    int Mx = 0, My = 0, MF = 0, n2 = 0, n4 = 0, n6 = 0, Z = 0;
+    long long s2 = 0, s4 = 0;
+    double k = 0.0;
+    GemmEngine eng;
+    const double *d_up = nullptr, *d_upk = nullptr, *d_wqk = nullptr, *d_z = nullptr, *d_kz0 = nullptr;
+    double2* svec = nullptr;   // Sx, Sy, Sz0, Sz1, EF (7 MF)
+};
+
+sc_status volume_setup(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2, cudaStream_t st,
+                       VolumeRun& v) {
+    SC_TRY(make_plan(p, Z, S1, S2, &v.P));
+    const VolumePlan& P = v.P;
+    v.Mx = P.dims.Mx;
+    v.My = P.dims.My;
+    v.MF = P.dims.MF;
+    v.n2 = 2 * v.MF;
+    v.n4 = 4 * v.MF;
+    v.n6 = 6 * v.MF;
+    v.Z = Z;
+    v.s2 = (long long)v.n2 * v.n2;
+    v.s4 = (long long)v.n4 * v.n4;
+    v.k = P.dims.k;
+    const int Mx = v.Mx, My = v.My, MF = v.MF;
+    const double k = v.k;
     Workspace& ws = ctx->ws;
     for (int i = 0; i < 7; ++i)
         if (!ctx->ev[i]) SC_CUDA_TRY(cudaEventCreate(&ctx->ev[i]));
     // products of the transfer chain, the boundary block and Pz: FP64 tiles, or
-    // the int8 engine under a mixed precision setting (the FFT, assembly,
+    // the int8 engines under a mixed precision setting (the FFT, assembly,
     // Omega, the eigensolve, the eigenvectors and every LU stay FP64)
-    GemmEngine eng;
-    precision_slices(ctx->precision, &eng.slices, &eng.force_int8, &eng.force_crt);
-    eng.ws = &ws;
-    if (eng.slices) {
-        SC_TRY(ws.get(&eng.err, 1, WS_OZ_ERR, st));
-        SC_CUDA_TRY(cudaMemsetAsync(eng.err, 0, sizeof(int), st));
+    precision_slices(ctx->precision, &v.eng.slices, &v.eng.force_int8, &v.eng.force_crt);
+    v.eng.ws = &ws;
+    if (v.eng.slices) {
+        SC_TRY(ws.get(&v.eng.err, 1, WS_OZ_ERR, st));
+        SC_CUDA_TRY(cudaMemsetAsync(v.eng.err, 0, sizeof(int), st));
     }
-    SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
-
-    // small host-built arrays: lattice, S vectors, EF, z planes
     double* lat = nullptr;     // up (Mx), wq (My), UPk (Mx), WQk (My), z (Z+1), k, z0
     const size_t nlat = (size_t)2 * (Mx + My) + Z + 3;
     SC_TRY(ws.get(&lat, nlat, WS_LAT, st));
@@ -423,109 +440,122 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     hl[2 * (Mx + My) + Z + 1] = k;
     hl[2 * (Mx + My) + Z + 2] = P.z[0];
     SC_TRY(upload(st, lat, hl));
-    const double* d_up = lat;
-    const double* d_upk = lat + Mx + My;
-    const double* d_wqk = lat + 2 * Mx + My;
-    const double* d_z = lat + 2 * (Mx + My);
-    const double* d_kz0 = d_z + Z + 1;
-    double2* svec = nullptr;   // Sx, Sy, Sz0, Sz1, EF (7 MF)
-    SC_TRY(ws.get(&svec, (size_t)7 * MF, WS_EVAL_W, st));
-    {
-        std::vector<cplx> hv;
-        hv.reserve(7 * MF);
-        hv.insert(hv.end(), P.Sx.begin(), P.Sx.end());
-        hv.insert(hv.end(), P.Sy.begin(), P.Sy.end());
-        hv.insert(hv.end(), P.Sz0.begin(), P.Sz0.end());
-        hv.insert(hv.end(), P.Sz1.begin(), P.Sz1.end());
-        hv.insert(hv.end(), P.EF.begin(), P.EF.end());
-        SC_CUDA_TRY(cudaMemcpyAsync(svec, hv.data(), hv.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));
-    }
-    const double2 *dSx = svec, *dSy = svec + MF, *dSz0 = svec + 2 * MF, *dEF = svec + 4 * MF;
+    v.d_up = lat;
+    v.d_upk = lat + Mx + My;
+    v.d_wqk = lat + 2 * Mx + My;
+    v.d_z = lat + 2 * (Mx + My);
+    v.d_kz0 = v.d_z + Z + 1;
+    SC_TRY(ws.get(&v.svec, (size_t)7 * MF, WS_EVAL_W, st));
+    std::vector<cplx> hv;
+    hv.reserve(7 * MF);
+    hv.insert(hv.end(), P.Sx.begin(), P.Sx.end());
+    hv.insert(hv.end(), P.Sy.begin(), P.Sy.end());
+    hv.insert(hv.end(), P.Sz0.begin(), P.Sz0.end());
+    hv.insert(hv.end(), P.Sz1.begin(), P.Sz1.end());
+    hv.insert(hv.end(), P.EF.begin(), P.EF.end());
+    SC_CUDA_TRY(cudaMemcpyAsync(v.svec, hv.data(), hv.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));
+    return SC_OK;
+}
 
+// device buffers of the layer stages, kept for the interior stage
+struct LayerBufs {
+    double2 *Nif = nullptr, *V = nullptr, *evl = nullptr, *dG = nullptr, *cG = nullptr, *Inv = nullptr;
+    double2* Gcs = nullptr;     // the ordered chain product of the layers
+    int* dinfo = nullptr;       // per-layer eigensolve status, then boundary LU status at [Zb]
+};
+
+// a3-a9 for layers [lb, le) of the sample: Fourier coefficients, B, C and
+// Omega, eigenpairs, GD/GC and all GD_i^-1, and the ordered chain product
+//   Gcs = T_{le-1} ... T_{lb},  T_i = GC_i GD_i^-1 = V_i diag(cG_i) GD_i^-1,
+// in which layer 0 (when lb == 0) contributes GC_0 itself (ScatterVolume.cpp:
+// 282-336 multiplies the same factors in sequence; here a pairwise tree).
+// Events ev[1..4] mark the stage boundaries.
+sc_status volume_layers(sc_context* ctx, VolumeRun& v, const double2* sample, int S1, int S2, int lb, int le,
+                        cudaStream_t st, LayerBufs& b) {
+    const int Zb = le - lb, MF = v.MF, n2 = v.n2, n4 = v.n4;
+    const long long s2 = v.s2, s4 = v.s4;
+    Workspace& ws = ctx->ws;
     // ---- a3: Fourier coefficients
-    double2 *Nf, *Nif, *R2, *Ri2;
-    SC_TRY(ws.get(&Nf, (size_t)Z * MF, WS_NF, st));
-    SC_TRY(ws.get(&Nif, (size_t)Z * MF, WS_NIF, st));
-    SC_TRY(ws.get(&R2, (size_t)Z * S1 * Mx, WS_TMP, st));
-    SC_TRY(ws.get(&Ri2, (size_t)Z * S1 * Mx, WS_TMP2, st));
+    double2 *Nf, *R2, *Ri2;
+    SC_TRY(ws.get(&Nf, (size_t)Zb * MF, WS_NF, st));
+    SC_TRY(ws.get(&b.Nif, (size_t)Zb * MF, WS_NIF, st));
+    SC_TRY(ws.get(&R2, (size_t)Zb * S1 * v.Mx, WS_TMP, st));
+    SC_TRY(ws.get(&Ri2, (size_t)Zb * S1 * v.Mx, WS_TMP2, st));
     int* bins;
-    SC_TRY(ws.get(&bins, (size_t)Mx + My, WS_BINS, st));
-    SC_TRY(fft2_crop(st, sample, Z, S1, S2, Mx, My, Nf, Nif, R2, Ri2, bins));
+    SC_TRY(ws.get(&bins, (size_t)v.Mx + v.My, WS_BINS, st));
+    SC_TRY(fft2_crop(st, sample + (long long)lb * S1 * S2, Zb, S1, S2, v.Mx, v.My, Nf, b.Nif, R2, Ri2, bins));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
 
     // ---- a5: B, C blocks and Omega = B C
     double2 *Bm, *Cm, *Om;
-    SC_TRY(ws.get(&Bm, (size_t)Z * s2, WS_BMAT, st));
-    SC_TRY(ws.get(&Cm, (size_t)Z * s2, WS_CMAT, st));
-    SC_TRY(ws.get(&Om, (size_t)Z * s2, WS_OMEGA, st));
-    SC_TRY(assemble_bc(st, Nf, Nif, Z, Mx, My, d_up, k, Bm, Cm));
+    SC_TRY(ws.get(&Bm, (size_t)Zb * s2, WS_BMAT, st));
+    SC_TRY(ws.get(&Cm, (size_t)Zb * s2, WS_CMAT, st));
+    SC_TRY(ws.get(&Om, (size_t)Zb * s2, WS_OMEGA, st));
+    SC_TRY(assemble_bc(st, Nf, b.Nif, Zb, v.Mx, v.My, v.d_up, v.k, Bm, Cm));
     SC_TRY(zgemm(st, n2, n2, n2, make_double2(1.0, 0.0), Bm, n2, s2, Cm, n2, s2, make_double2(0.0, 0.0), Om, n2,
-                 s2, Z));
+                 s2, Zb));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
 
     // ---- a7/a8: eigenpairs
-    double2 *mu, *Wm, *CW, *V, *evl;
-    int* dinfo;
-    SC_TRY(ws.get(&mu, (size_t)Z * n2, WS_MU, st));
-    SC_TRY(ws.get(&Wm, (size_t)Z * s2, WS_W, st));
-    SC_TRY(ws.get(&CW, (size_t)Z * s2, WS_CW, st));
-    SC_TRY(ws.get(&V, (size_t)Z * s4, WS_V, st));
-    SC_TRY(ws.get(&evl, (size_t)Z * n4, WS_EVL, st));
-    SC_TRY(ws.get(&dinfo, (size_t)Z + 4, WS_INFO, st));
-    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * (Z + 4), st));
-    SC_TRY(eig_batched(st, Om, n2, Z, mu, Wm, dinfo, ws));
+    double2 *mu, *Wm, *CW;
+    SC_TRY(ws.get(&mu, (size_t)Zb * n2, WS_MU, st));
+    SC_TRY(ws.get(&Wm, (size_t)Zb * s2, WS_W, st));
+    SC_TRY(ws.get(&CW, (size_t)Zb * s2, WS_CW, st));
+    SC_TRY(ws.get(&b.V, (size_t)Zb * s4, WS_V, st));
+    SC_TRY(ws.get(&b.evl, (size_t)Zb * n4, WS_EVL, st));
+    SC_TRY(ws.get(&b.dinfo, (size_t)Zb + 4, WS_INFO, st));
+    SC_CUDA_TRY(cudaMemsetAsync(b.dinfo, 0, sizeof(int) * (Zb + 4), st));
+    SC_TRY(eig_batched(st, Om, n2, Zb, mu, Wm, b.dinfo, ws));
     SC_TRY(zgemm(st, n2, n2, n2, make_double2(1.0, 0.0), Cm, n2, s2, Wm, n2, s2, make_double2(0.0, 0.0), CW, n2,
-                 s2, Z));
+                 s2, Zb));
     {
-        dim3 g(grid_for(s4), Z);
-        build_v_kernel<<<g, 256, 0, st>>>(mu, Wm, CW, n2, V, evl);
+        dim3 g(grid_for(s4), Zb);
+        build_v_kernel<<<g, 256, 0, st>>>(mu, Wm, CW, n2, b.V, b.evl);
         count_launch();
     }
-    SC_TRY(normalize_columns(st, V, n4, n4, n4, s4, Z));
+    SC_TRY(normalize_columns(st, b.V, n4, n4, n4, s4, Zb));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
 
-    // ---- a9: GD/GC, explicit GD_i^-1 for all layers, and the chain
-    //   Gc_static = T_{Z-1} ... T_1 GC_0,  T_i = GC_i GD_i^-1 = V_i diag(cG_i) GD_i^-1
-    // computed as one batched inverse, one batched product and a pairwise
-    // product tree (ScatterVolume.cpp:326-335 multiplies the same factors in
-    // sequence).
-    double2 *dG, *cG, *LU, *Inv, *Gcs, *X, *tree, *gpart;
+    // ---- a9: GD/GC, explicit GD_i^-1 for all layers, and the chain product
+    double2 *LU, *tree;
     int* piv;
-    SC_TRY(ws.get(&dG, (size_t)Z * n4, WS_TMP, st));
-    SC_TRY(ws.get(&cG, (size_t)Z * n4, WS_TMP2, st));
-    SC_TRY(ws.get(&LU, (size_t)Z * s4, WS_GD, st));
-    SC_TRY(ws.get(&Inv, (size_t)Z * s4, WS_INV, st));
-    SC_TRY(ws.get(&piv, (size_t)Z * n4, WS_PIV, st));
-    SC_TRY(ws.get(&Gcs, (size_t)s4, WS_T, st));
-    SC_TRY(ws.get(&X, (size_t)s4, WS_T2, st));
-    SC_TRY(ws.get(&gpart, zgemv_part_size(n4, n4, 1) + 2 * (size_t)n4, WS_GEMV, st));
+    SC_TRY(ws.get(&b.dG, (size_t)Zb * n4, WS_TMP, st));
+    SC_TRY(ws.get(&b.cG, (size_t)Zb * n4, WS_TMP2, st));
+    SC_TRY(ws.get(&LU, (size_t)Zb * s4, WS_GD, st));
+    SC_TRY(ws.get(&b.Inv, (size_t)Zb * s4, WS_INV, st));
+    SC_TRY(ws.get(&piv, (size_t)Zb * n4, WS_PIV, st));
+    SC_TRY(ws.get(&b.Gcs, (size_t)s4, WS_T, st));
     {
-        dim3 g((n4 + 255) / 256, Z);
-        gdgc_scale_kernel<<<g, 256, 0, st>>>(evl, n4, Z, d_z, k, dG, cG);
+        dim3 g((n4 + 255) / 256, Zb);
+        gdgc_scale_kernel<<<g, 256, 0, st>>>(b.evl, n4, Zb, v.d_z + lb, v.k, b.dG, b.cG);
         count_launch();
-        dim3 g2(grid_for(s4), Z);
-        scale_cols_kernel<<<g2, 256, 0, st>>>(V, s4, dG, n4, n4, n4, LU, s4);
+        dim3 g2(grid_for(s4), Zb);
+        scale_cols_kernel<<<g2, 256, 0, st>>>(b.V, s4, b.dG, n4, n4, n4, LU, s4);
         count_launch();
     }
-    SC_TRY(getrf(st, LU, n4, s4, n4, Z, piv, nullptr));
-    SC_TRY(set_identity(st, Inv, n4, s4, n4, Z));
-    SC_TRY(getrs(st, LU, n4, s4, n4, piv, Inv, n4, s4, n4, Z));
+    SC_TRY(getrf(st, LU, n4, s4, n4, Zb, piv, nullptr));
+    SC_TRY(set_identity(st, b.Inv, n4, s4, n4, Zb));
+    SC_TRY(getrs(st, LU, n4, s4, n4, piv, b.Inv, n4, s4, n4, Zb));
     {
-        // level 0 of the tree: M_0 = GC_0 = V_0 diag(cG_0), M_i = T_i (i >= 1)
-        const int nt = Z;
+        // level 0 of the tree: M_i = T_{lb+i}; with lb == 0 the first is GC_0 = V_0 diag(cG_0)
+        const int nt = Zb;
         SC_TRY(ws.get(&tree, (size_t)(nt + (nt + 1) / 2) * s4, WS_TREE, st));
-        scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, cG, n4, n4, n4, tree, s4);
-        count_launch();
-        if (Z > 1) {
+        int first = 0;
+        if (lb == 0) {
+            scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(b.V, s4, b.cG, n4, n4, n4, tree, s4);
+            count_launch();
+            first = 1;
+        }
+        if (first < Zb) {
             // rows of GD_i^-1 scaled by cG_i, into the spare half of the tree buffer, then T_i = V_i (.)
             double2* scaled = tree + (long long)nt * s4;
-            for (int i0 = 1; i0 < Z; i0 += (nt + 1) / 2) {
-                const int cnt = (Z - i0) < (nt + 1) / 2 ? (Z - i0) : (nt + 1) / 2;
+            for (int i0 = first; i0 < Zb; i0 += (nt + 1) / 2) {
+                const int cnt = (Zb - i0) < (nt + 1) / 2 ? (Zb - i0) : (nt + 1) / 2;
                 dim3 g(grid_for(s4), cnt);
-                scale_rows_batched_kernel<<<g, 256, 0, st>>>(Inv + i0 * s4, s4, cG + (long long)i0 * n4, n4, n4,
+                scale_rows_batched_kernel<<<g, 256, 0, st>>>(b.Inv + i0 * s4, s4, b.cG + (long long)i0 * n4, n4, n4,
                                                             n4, scaled, s4);
                 count_launch();
-                SC_TRY(product(st, eng, n4, n4, n4, V + i0 * s4, n4, s4, scaled, n4, s4, tree + i0 * s4, n4, s4,
+                SC_TRY(product(st, v.eng, n4, n4, n4, b.V + i0 * s4, n4, s4, scaled, n4, s4, tree + i0 * s4, n4, s4,
                                cnt));
             }
         }
@@ -535,7 +565,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         int cnt = nt;
         while (cnt > 1) {
             const int pairs = cnt / 2;
-            SC_TRY(product(st, eng, n4, n4, n4, cur + s4, n4, 2 * s4, cur, n4, 2 * s4, nxt, n4, s4, pairs));
+            SC_TRY(product(st, v.eng, n4, n4, n4, cur + s4, n4, 2 * s4, cur, n4, 2 * s4, nxt, n4, s4, pairs));
             if (cnt & 1)
                 SC_CUDA_TRY(cudaMemcpyAsync(nxt + pairs * s4, cur + (cnt - 1) * s4, sizeof(double2) * s4,
                                             cudaMemcpyDeviceToDevice, st));
@@ -544,49 +574,96 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
             cur = nxt;
             nxt = t;
         }
-        SC_CUDA_TRY(cudaMemcpyAsync(Gcs, cur, sizeof(double2) * s4, cudaMemcpyDeviceToDevice, st));
+        SC_CUDA_TRY(cudaMemcpyAsync(b.Gcs, cur, sizeof(double2) * s4, cudaMemcpyDeviceToDevice, st));
     }
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[4], st));
+    return SC_OK;
+}
 
-    // ---- a10-a13: boundary system and its solve
+// a10-a13 (ScatterVolume.cpp:339-466, 739): f3, Gc_static^-1 f3 (Gcs is
+// factored in place), A6[2MF:, 3MF:] = GD_0 (.), the Gaussian rows, the
+// incident right-hand side, and the LU solve; returns b6 = [R; T] (6 MF) and
+// the boundary LU status word in *dinfo_lu
+sc_status volume_boundary(sc_context* ctx, VolumeRun& v, double2* Gcs, const double2* GD0, int* dinfo_lu,
+                          cudaStream_t st, double2** b6_out) {
+    const int MF = v.MF, n4 = v.n4, n6 = v.n6;
+    const long long s4 = v.s4;
+    Workspace& ws = ctx->ws;
     double2 *F, *A6, *b6;
     int* piv6;
     SC_TRY(ws.get(&F, (size_t)n4 * 3 * MF, WS_F, st));
     SC_TRY(ws.get(&A6, (size_t)n6 * n6, WS_A6, st));
     SC_TRY(ws.get(&b6, (size_t)n6, WS_B6, st));
     SC_TRY(ws.get(&piv6, (size_t)n6 + n4, WS_PIV6, st));
-    SC_TRY(boundary_f3(st, MF, svec, 0, F, 0, 1));
+    SC_TRY(boundary_f3(st, MF, v.svec, 0, F, 0, 1));
     SC_TRY(getrf(st, Gcs, n4, s4, n4, 1, piv6 + n6, nullptr));
     SC_TRY(getrs(st, Gcs, n4, s4, n4, piv6 + n6, F, n4, 0, 3 * MF, 1));
-    // GD_0 = V_0 diag(dG_0) into X, then A6[2MF:, 3MF:] = GD_0 * F
-    scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(V, s4, dG, n4, n4, n4, X, s4);
-    count_launch();
-    SC_TRY(boundary_system(st, MF, svec, 0, d_kz0, A6, 0, b6, 0, 1));
-    SC_TRY(product(st, eng, n4, 3 * MF, n4, X, n4, s4, F, n4, 0, A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0, 1));
-    SC_TRY(getrf(st, A6, n6, 0, n6, 1, piv6, dinfo + Z));
+    SC_TRY(boundary_system(st, MF, v.svec, 0, v.d_kz0, A6, 0, b6, 0, 1));
+    SC_TRY(product(st, v.eng, n4, 3 * MF, n4, GD0, n4, s4, F, n4, 0, A6 + (long long)3 * MF * n6 + 2 * MF, n6, 0,
+                   1));
+    SC_TRY(getrf(st, A6, n6, 0, n6, 1, piv6, dinfo_lu));
     SC_TRY(getrs(st, A6, n6, 0, n6, piv6, b6, n6, 0, 1, 1));
-    if (x_out) SC_CUDA_TRY(cudaMemcpyAsync(x_out, b6, sizeof(double2) * n6, cudaMemcpyDeviceToDevice, st));
+    *b6_out = b6;
+    return SC_OK;
+}
+
+sc_status volume_engine_status(VolumeRun& v) {
+    if (!v.eng.slices) return SC_OK;
+    int herr = 0;
+    SC_CUDA_TRY(cudaMemcpy(&herr, v.eng.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        set_error("volume solve: tensor-core pipeline wait timed out (stage %d)", herr);
+        return SC_CUDA_ERROR;
+    }
+    return SC_OK;
+}
+
+}  // namespace
+
+sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
+                       int S2, double2* x_out, double2* evl_out, double2* Qc_out, double2* Qh_out,
+                       int* info_host, cudaStream_t st) {
+    VolumeRun v;
+    SC_TRY(volume_setup(ctx, p, Z, S1, S2, st, v));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
+    const int Mx = v.Mx, My = v.My, MF = v.MF, n2 = v.n2, n4 = v.n4;
+    const long long s4 = v.s4;
+    const double k = v.k;
+    Workspace& ws = ctx->ws;
+    LayerBufs b;
+    SC_TRY(volume_layers(ctx, v, sample, S1, S2, 0, Z, st, b));
+
+    // ---- a10-a13: boundary system and its solve, with GD_0 = V_0 diag(dG_0)
+    double2* X;
+    SC_TRY(ws.get(&X, (size_t)s4, WS_T2, st));
+    scale_cols_kernel<<<dim3(grid_for(s4), 1), 256, 0, st>>>(b.V, s4, b.dG, n4, n4, n4, X, s4);
+    count_launch();
+    double2* b6;
+    SC_TRY(volume_boundary(ctx, v, b.Gcs, X, b.dinfo + Z, st, &b6));
+    if (x_out) SC_CUDA_TRY(cudaMemcpyAsync(x_out, b6, sizeof(double2) * v.n6, cudaMemcpyDeviceToDevice, st));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[5], st));
 
     // ---- a14/a15: beta chain, Q, Pz
+    const double2 *dSx = v.svec, *dSy = v.svec + MF, *dSz0 = v.svec + 2 * MF, *dEF = v.svec + 4 * MF;
     if (!p->external && (Qc_out || Qh_out)) {
-        double2 *beta, *tv;
+        double2 *beta, *tv, *gpart;
+        SC_TRY(ws.get(&gpart, zgemv_part_size(n4, n4, 1) + 2 * (size_t)n4, WS_GEMV, st));
         SC_TRY(ws.get(&beta, (size_t)Z * n4 + 2 * n4, WS_BETA, st));
         tv = beta + (long long)Z * n4;
         double2* rhs = tv + n4;
-        beta0_rhs_kernel<<<grid_for(n4), 256, 0, st>>>(MF, dSx, dSy, dSz0, dEF, b6, k, P.z[0], rhs);
+        beta0_rhs_kernel<<<grid_for(n4), 256, 0, st>>>(MF, dSx, dSy, dSz0, dEF, b6, k, v.P.z[0], rhs);
         count_launch();
         // beta_0 = GD_0^-1 (f1 EF + f2 R);  beta_i = GD_i^-1 V_{i-1} (cG_{i-1} .* beta_{i-1})
-        SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), Inv, n4, s4, rhs, 0, make_double2(0.0, 0.0), beta, 0, 1,
+        SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), b.Inv, n4, s4, rhs, 0, make_double2(0.0, 0.0), beta, 0, 1,
                      gpart));
         for (int i = 1; i < Z; ++i) {
             scale_cols_kernel<<<dim3(grid_for(n4), 1), 256, 0, st>>>(beta + (long long)(i - 1) * n4, 0,
-                                                                      cG + (long long)(i - 1) * n4, 0, 1, n4,
+                                                                      b.cG + (long long)(i - 1) * n4, 0, 1, n4,
                                                                       rhs, 0);
             count_launch();
-            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), V + (i - 1) * s4, n4, s4, rhs, 0,
+            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), b.V + (i - 1) * s4, n4, s4, rhs, 0,
                          make_double2(0.0, 0.0), tv, 0, 1, gpart));
-            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), Inv + i * s4, n4, s4, tv, 0, make_double2(0.0, 0.0),
+            SC_TRY(zgemv(st, n4, n4, make_double2(1.0, 0.0), b.Inv + i * s4, n4, s4, tv, 0, make_double2(0.0, 0.0),
                          beta + (long long)i * n4, 0, 1, gpart));
         }
         double2 *Gc, *Gh, *KP;
@@ -598,16 +675,16 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         const long long sq = (long long)3 * MF * n2;
         {
             dim3 g(grid_for((long long)n2 * n2), Z);
-            q_kernel<<<g, 256, 0, st>>>(V, beta, MF, d_upk, d_wqk, Mx, Qc, Qh, Gc, Gh);
+            q_kernel<<<g, 256, 0, st>>>(b.V, beta, MF, v.d_upk, v.d_wqk, Mx, Qc, Qh, Gc, Gh);
             count_launch();
         }
         if (!p->npz) {
             dim3 g(grid_for((long long)MF * MF), Z);
-            kp_kernel<<<g, 256, 0, st>>>(Nif, Mx, My, k, KP);
+            kp_kernel<<<g, 256, 0, st>>>(b.Nif, Mx, My, k, KP);
             count_launch();
-            SC_TRY(product(st, eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gc, MF, (long long)MF * n2, Qc + n2,
+            SC_TRY(product(st, v.eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gc, MF, (long long)MF * n2, Qc + n2,
                            3 * MF, sq, Z));
-            SC_TRY(product(st, eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gh, MF, (long long)MF * n2, Qh + n2,
+            SC_TRY(product(st, v.eng, MF, n2, MF, KP, MF, (long long)MF * MF, Gh, MF, (long long)MF * n2, Qh + n2,
                            3 * MF, sq, Z));
         } else {
             for (int z = 0; z < Z; ++z) {
@@ -618,12 +695,12 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
             }
         }
     }
-    if (evl_out) SC_CUDA_TRY(cudaMemcpyAsync(evl_out, evl, sizeof(double2) * Z * n4, cudaMemcpyDeviceToDevice, st));
+    if (evl_out) SC_CUDA_TRY(cudaMemcpyAsync(evl_out, b.evl, sizeof(double2) * Z * n4, cudaMemcpyDeviceToDevice, st));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[6], st));
 
     // ---- status: eig info per layer + boundary LU info
     std::vector<int> hinfo(Z + 4, 0);
-    SC_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * (Z + 4), cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), b.dinfo, sizeof(int) * (Z + 4), cudaMemcpyDeviceToHost, st));
     SC_CUDA_TRY(cudaStreamSynchronize(st));
     for (int i = 0; i < 6; ++i) {
         float ms = 0.f;
@@ -637,14 +714,7 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
         SC_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]));
         ctx->stage_ms[7] = ms;
     }
-    if (eng.slices) {
-        int herr = 0;
-        SC_CUDA_TRY(cudaMemcpy(&herr, eng.err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (herr) {
-            set_error("volume solve: tensor-core pipeline wait timed out (stage %d)", herr);
-            return SC_CUDA_ERROR;
-        }
-    }
+    SC_TRY(volume_engine_status(v));
     int first = 0;
     for (int i = 0; i < Z && !first; ++i) first = hinfo[i];
     if (info_host) *info_host = first ? first : hinfo[Z];
@@ -654,6 +724,70 @@ sc_status volume_solve(sc_context* ctx, const sc_volume_params* p, const double2
     }
     if (hinfo[Z]) {
         set_error("boundary system is singular (zero pivot in column %d)", hinfo[Z] - 1);
+        return SC_SINGULAR;
+    }
+    return SC_OK;
+}
+
+sc_status volume_chain_block(sc_context* ctx, const sc_volume_params* p, const double2* sample, int Z, int S1,
+                             int S2, int lb, int le, double2* P_out, double2* GD0_out, int* info_host,
+                             cudaStream_t st) {
+    if (lb < 0 || le > Z || lb >= le) {
+        set_error("sc_volume_chain_block: layer range [%d, %d) outside [0, %d)", lb, le, Z);
+        return SC_BADINPUT;
+    }
+    VolumeRun v;
+    SC_TRY(volume_setup(ctx, p, Z, S1, S2, st, v));
+    SC_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
+    LayerBufs b;
+    SC_TRY(volume_layers(ctx, v, sample, S1, S2, lb, le, st, b));
+    SC_CUDA_TRY(cudaMemcpyAsync(P_out, b.Gcs, sizeof(double2) * v.s4, cudaMemcpyDeviceToDevice, st));
+    if (GD0_out) {
+        if (lb != 0) {
+            set_error("sc_volume_chain_block: GD_0 belongs to the block that starts at layer 0");
+            return SC_BADINPUT;
+        }
+        scale_cols_kernel<<<dim3(grid_for(v.s4), 1), 256, 0, st>>>(b.V, v.s4, b.dG, v.n4, v.n4, v.n4, GD0_out,
+                                                                    v.s4);
+        count_launch();
+        SC_CHECK_LAUNCH("chain block GD_0");
+    }
+    const int Zb = le - lb;
+    std::vector<int> hinfo(Zb, 0);
+    SC_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), b.dinfo, sizeof(int) * Zb, cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    SC_TRY(volume_engine_status(v));
+    int first = 0;
+    for (int i = 0; i < Zb && !first; ++i) first = hinfo[i];
+    if (info_host) *info_host = first;
+    if (first) {
+        set_error("eigensolve did not converge (layer status %d)", first);
+        return SC_NOCONVERGE;
+    }
+    return SC_OK;
+}
+
+sc_status volume_boundary_solve(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
+                                const double2* Gcs_in, const double2* GD0, double2* x_out, int* info_host,
+                                cudaStream_t st) {
+    VolumeRun v;
+    SC_TRY(volume_setup(ctx, p, Z, S1, S2, st, v));
+    double2* Gcs;
+    int* dinfo;
+    SC_TRY(ctx->ws.get(&Gcs, (size_t)v.s4, WS_T, st));
+    SC_TRY(ctx->ws.get(&dinfo, 4, WS_INFO, st));
+    SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * 4, st));
+    SC_CUDA_TRY(cudaMemcpyAsync(Gcs, Gcs_in, sizeof(double2) * v.s4, cudaMemcpyDeviceToDevice, st));
+    double2* b6;
+    SC_TRY(volume_boundary(ctx, v, Gcs, GD0, dinfo, st, &b6));
+    SC_CUDA_TRY(cudaMemcpyAsync(x_out, b6, sizeof(double2) * v.n6, cudaMemcpyDeviceToDevice, st));
+    int h = 0;
+    SC_CUDA_TRY(cudaMemcpyAsync(&h, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SC_CUDA_TRY(cudaStreamSynchronize(st));
+    SC_TRY(volume_engine_status(v));
+    if (info_host) *info_host = h;
+    if (h) {
+        set_error("boundary system is singular (zero pivot in column %d)", h - 1);
         return SC_SINGULAR;
     }
     return SC_OK;

@@ -175,6 +175,59 @@ def solve(ctx: Context, params: VolumeParams, sample: torch.Tensor, fields: bool
     return VolumeSolution(d, shape, x, evl, Qc, Qh)
 
 
+def chain_block(ctx: Context, params: VolumeParams, sample: torch.Tensor, layer_begin: int, layer_end: int,
+                stream=None):
+    """(P, GD0): the ordered transfer product of layers [begin, end) (4MF x 4MF, column-major storage in a
+    (4MF, 4MF) tensor read as its transpose) and GD_0 for the block that starts at layer 0 (else None)."""
+    if sample.dim() == 2:
+        sample = sample.unsqueeze(0)
+    sample = sample.contiguous()
+    shape = tuple(sample.shape)
+    d = plan(params, shape)
+    n4 = 4 * d.MF
+    P = torch.empty((n4, n4), dtype=torch.complex128, device=sample.device)
+    GD0 = torch.empty((n4, n4), dtype=torch.complex128, device=sample.device) if layer_begin == 0 else None
+    info = ctypes.c_int(0)
+    check(ctx.lib.sc_volume_chain_block(ctx.handle, ctypes.byref(params), _ptr(sample), *shape, int(layer_begin),
+                                        int(layer_end), _ptr(P), _ptr(GD0), ctypes.byref(info), _stream_ptr(stream)))
+    return P, GD0
+
+
+def boundary_solve(ctx: Context, params: VolumeParams, shape, Gc_static: torch.Tensor, GD0: torch.Tensor,
+                   stream=None) -> torch.Tensor:
+    """x = [R; T] (6 MF) from the whole chain and GD_0 (storage as chain_block returns them)."""
+    d = plan(params, tuple(shape))
+    x = torch.empty(6 * d.MF, dtype=torch.complex128, device=Gc_static.device)
+    info = ctypes.c_int(0)
+    check(ctx.lib.sc_volume_boundary_solve(ctx.handle, ctypes.byref(params), *shape, _ptr(Gc_static.contiguous()),
+                                           _ptr(GD0.contiguous()), _ptr(x), ctypes.byref(info), _stream_ptr(stream)))
+    return x
+
+
+def colmajor_matmul(ctx: Context, A: torch.Tensor, B: torch.Tensor, stream=None) -> torch.Tensor:
+    """A B for square matrices held in column-major storage (as chain_block returns them), on the FP64 tile."""
+    n = A.shape[0]
+    C = torch.empty_like(A)
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    zero = (ctypes.c_double * 2)(0.0, 0.0)
+    check(ctx.lib.sc_zgemm_batched(ctx.handle, n, n, n, one, _ptr(A.contiguous()), n, n * n, _ptr(B.contiguous()),
+                                   n, n * n, zero, _ptr(C), n, n * n, 1, _stream_ptr(stream)))
+    return C
+
+
+def split_solve(ctx: Context, params: VolumeParams, sample: torch.Tensor, dist=None, stream=None) -> torch.Tensor:
+    """R/T of one volume solved with its layers split over the ranks of `dist` (one exchange of chain blocks)."""
+    from . import layersplit
+    if sample.dim() == 2:
+        sample = sample.unsqueeze(0)
+    shape = tuple(sample.shape)
+    d = plan(params, shape)
+    return layersplit.split_solve(
+        shape[0], lambda lb, le: chain_block(ctx, params, sample, lb, le, stream),
+        lambda a, b: colmajor_matmul(ctx, a, b, stream),
+        lambda g, gd: boundary_solve(ctx, params, shape, g, gd, stream), 6 * d.MF, dist, sample.device)
+
+
 @dataclass
 class WaveTable:
     E0: torch.Tensor         # (nw, 3) complex128

@@ -159,3 +159,25 @@ def test_mixed_precision_solve_matches_oracle(ctx):
         run_case(ctx, smp, kw, tol=1e-8)
     finally:
         ctx.set_precision(_lib.SC_SWEEP_FP64)
+
+
+def test_layer_split_blocks_on_one_gpu(ctx):
+    """sc_volume_chain_block on two layer blocks, their ordered product and sc_volume_boundary_solve: the same
+    R/T as the unsplit solve and the oracle (the exchange itself is covered by the gloo test)."""
+    smp = samples.sphere_volume(3, nxy=32, nz=6, size=(20.0, 20.0, 8.0))
+    kw = dict(lambda_=0.6, size=(20, 20, 8), coef=(7, 7),
+              direction=(np.sin(np.radians(10)), 0, np.cos(np.radians(10))), ex=(1, 0), ey=(0, 0), external=True)
+    p = solver.make_params(**kw)
+    d = torch.from_numpy(smp).cuda()
+    full = solver.solve(ctx, p, d, fields=False).x.cpu().numpy()
+    ref = osv.solve(smp, osv.Params(**kw), keep=False).x
+    for cut in (1, 3, 5):
+        P0, G0 = solver.chain_block(ctx, p, d, 0, cut)
+        P1, G1 = solver.chain_block(ctx, p, d, cut, 6)
+        assert G1 is None
+        x = solver.boundary_solve(ctx, p, smp.shape, solver.colmajor_matmul(ctx, P1, P0), G0).cpu().numpy()
+        assert rel(x, full) < 1e-11
+        assert rel(x, ref) < TOL
+    # a single block is the whole chain
+    P, G = solver.chain_block(ctx, p, d, 0, 6)
+    assert rel(solver.boundary_solve(ctx, p, smp.shape, P, G).cpu().numpy(), full) < 1e-12

@@ -111,3 +111,68 @@ def test_gather_rejects_a_result_of_the_wrong_length():
 
     with pytest.raises(ValueError):
         sweep.gather_results([0], [torch.zeros(3, dtype=torch.complex128)], [6, 6], [[0], [1]], FakeDist, "cpu")
+
+
+# ---------------------------------------------------------------- one volume split by layers
+LAYER_KW = dict(lambda_=0.6, size=(20.0, 20.0, 8.0), coef=(5, 5), ex=(1.0, 0.0), ey=(0.0, 0.0),
+                direction=(0.17, 0.0, 0.98), external=True)
+
+
+def layer_sample():
+    return samples.sphere_volume(3, nxy=24, nz=7, size=(20.0, 20.0, 8.0))
+
+
+def oracle_stages():
+    import torch
+    from oracle import scattervolume as osv
+    smp = layer_sample()
+    p = osv.Params(**LAYER_KW)
+
+    def block(lb, le):
+        P, G = osv.chain_block(smp, p, lb, le)
+        return torch.from_numpy(P), (torch.from_numpy(G) if G is not None else None)
+
+    def finish(g, gd):
+        return torch.from_numpy(osv.boundary_from_chain(smp, p, g.numpy(), gd.numpy()))
+
+    return block, (lambda a, b: a @ b), finish, 6 * 25, smp, p
+
+
+def _layer_worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    from scattersim_b200 import layersplit
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        block, mm, finish, n, smp, p = oracle_stages()
+        x = layersplit.split_solve(smp.shape[0], block, mm, finish, n, dist, "cpu")
+        q.put((rank, layersplit.layer_blocks(smp.shape[0], world)[rank], x.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_layer_blocks_partition_in_order():
+    from scattersim_b200 import layersplit
+    for Z, w in [(7, 2), (32, 8), (5, 5), (9, 4)]:
+        bl = layersplit.layer_blocks(Z, w)
+        assert bl[0][0] == 0 and bl[-1][1] == Z
+        assert all(a[1] == b[0] for a, b in zip(bl, bl[1:]))
+        sizes = [e - b for b, e in bl]
+        assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
+    with pytest.raises(ValueError):
+        layersplit.layer_blocks(2, 3)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_layer_split_equals_unsplit_chain(world):
+    """Blocks on 2 and 3 gloo ranks, one exchange, ordered product on rank 0: the oracle's unsplit R/T."""
+    from oracle import scattervolume as osv
+    res = run_ranks(_layer_worker, world)
+    _, _, _, _, smp, p = oracle_stages()
+    ref = osv.solve(smp, p, keep=False).x
+    for rank, blk, x in res:
+        assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-12, (rank, blk)
