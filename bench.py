@@ -24,7 +24,12 @@ stack (n 1, 1.4 + 0.05i, 1.4, 1; boundaries -3, 0, 3 um; lambda 1 um) under a
 plane waves, one 24 x 24 complex system each; one step = the batched layer
 solve of the whole beam (incident waves resident in HBM), in plane waves/s.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume|layer]
+--workload field: the field of the solved 3-D volume above on a 512x512x64 grid
+(the factorised grid evaluator, complex64 out), in plane-wave evaluations/s
+(the work of the direct sum), with the direct evaluator and the 64x64 triangle
+map's 256x256 x-z slice beside it.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume|layer|field]
 
 Timing is on the device (CUDA events), max over ranks.  --workload volume and
 layer run one independent instance / beam per rank under torchrun (weak
@@ -186,6 +191,8 @@ def run_reference(args):
         return run_sweep_reference(args)
     if args.workload == "layer":
         return run_layer_reference(args)
+    if args.workload == "field":
+        return run_field_reference(args)
     for _ in range(args.warmup):
         cpu_layer_sample(0)
     ts = [cpu_layer_sample(0) for _ in range(args.steps)]
@@ -838,6 +845,252 @@ def run_layer_ours(args):
     return 0
 
 
+# --------------------------------------------------------------------------- field
+FIELD_METRIC = "plane-wave evaluations/s of the coupled-wave field on a grid (gpuEvaluator sum)"
+FIELD_UNIT = "wave-evals/s"
+FIELD_NAME = ("field of the 128x128x32 sphere volume (seed 1000, 21x21 orders, 32 layers, fields on) on a "
+              "512x512x64 grid (x, y in [0, 20] um, z in [-6, 6] um), complex64 out; with the 64x64 triangle "
+              "map's 256x256 x-z slice (x in [0, 10], z in [-5, 5], y = 5) beside it")
+FIELD_GRID = dict(origin=(0.0, 0.0, -6.0), step=(20.0 / 511, 20.0 / 511, 12.0 / 63), counts=(512, 512, 64))
+THIN_GRID = dict(origin=(0.0, 5.0, -5.0), step=(10.0 / 255, 1.0, 10.0 / 255), counts=(256, 1, 256))
+THIN_KW = dict(lambda_=0.5, size=(10.0, 10.0, 1.0), coef=(11, 11), ex=(1.0, 0.0), ey=(0.0, 0.0))
+
+
+def wave_evals(wt, grid):
+    """Sum over the grid points of the number of waves in the point's region (the direct sum's work)."""
+    zl, b, e = wt.z_layers, wt.begin, wt.end
+    nx, ny, nz = grid["counts"]
+    total = 0
+    for i in range(nz):
+        z = grid["origin"][2] + grid["step"][2] * i
+        l = int(sum(1 for zz in zl if z >= zz - 0.001))
+        total += (int(e[l]) - int(b[l])) * nx * ny
+    return total
+
+
+def grid_points(grid, planes=None):
+    nx, ny, nz = grid["counts"]
+    o, s = grid["origin"], grid["step"]
+    zs = [o[2] + s[2] * i for i in (planes if planes is not None else range(nz))]
+    zz, yy, xx = np.meshgrid(np.array(zs), o[1] + s[1] * np.arange(ny), o[0] + s[0] * np.arange(nx), indexing="ij")
+    return np.stack([xx.ravel(), yy.ravel(), zz.ravel()], -1)
+
+
+def run_field_reference(args):
+    """The evaluator sum on the host (the oracle's float64 restatement of gpuEvaluator.cu:28-68), one x-z row
+    of the triangle slice's interior per step."""
+    from oracle import cw as ocw
+    from oracle import scattervolume as osv
+    from scattersim_b200 import samples
+    smp = samples.triangle_map(0)
+    p = osv.Params(**THIN_KW)
+    sol = osv.solve(smp, p)
+    W = osv.build_waves(sol, p)
+    layers = [(W.z[l], W.Pr_E[l], W.Pr_k[l], W.Pt_E[l], W.Pt_k[l]) for l in range(len(W.z))]
+    zl, b, e, WE, Wk = ocw.unpack(W.Pi_E, W.Pi_k, layers)
+    pts = grid_points(THIN_GRID)
+    inside = pts[(pts[:, 2] > -0.5) & (pts[:, 2] < 0.5)][:64]          # points in the slab's region
+    reg = ocw.region_of(inside[:, 2], zl)
+    evals = int(sum(int(e[r]) - int(b[r]) for r in reg))
+    for _ in range(args.warmup):
+        ocw.evaluate(inside[:8], zl, b, e, WE, Wk)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ocw.evaluate(inside, zl, b, e, WE, Wk)
+        ts.append(time.perf_counter() - t0)
+    value = evals / statistics.mean(ts)
+    sample = (f"{len(inside)} interior points of the 256x256 triangle-map slice ({evals} wave evaluations) per "
+              "step through the oracle's float64 restatement of the evaluator sum (numpy, vectorised)")
+    line = {"impl": "reference", "metric": FIELD_METRIC, "value": value, "unit": FIELD_UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(ts),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": FIELD_NAME},
+            "cpu_baseline": {"value": value, "unit": FIELD_UNIT, "cores": blas_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": FIELD_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_field_ours(args):
+    import torch
+    from scattersim_b200 import samples, solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = solver.Context(local)
+    stream = torch.cuda.current_stream()
+    params = solver.make_params(**WORKLOAD)
+    vol = torch.from_numpy(samples.sphere_volume(1000 + rank)).cuda()
+    sol = solver.solve(ctx, params, vol)
+    wt = solver.waves(ctx, params, sol)
+    evals = wave_evals(wt, FIELD_GRID)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(fn):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    def grid_step(s=sol):
+        return solver.field_grid(ctx, params, s, precision=1, **FIELD_GRID)
+
+    for _ in range(args.warmup):
+        grid_step()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    l0 = ctx.launches()
+    step_ms, stages = [], []
+    for _ in range(args.steps):
+        out, ms = timed(grid_step)
+        step_ms.append(ms)
+        stages.append(ctx.stage_ms())
+    launches = ctx.launches() - l0
+    barrier()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * evals * args.steps / (total_ms / 1e3)
+    out_bytes = out.numel() * 8
+    npts = int(np.prod(FIELD_GRID["counts"]))
+
+    # error of the complex64 grid against the FP64 direct sum on two interior planes, and the direct
+    # evaluator's own rate there (float32 with float64 phase reduction, and float64)
+    planes = [22, 41]
+    pts = torch.from_numpy(grid_points(FIELD_GRID, planes)).cuda()
+    direct64, t64 = timed(lambda: solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, pts, precision=0))
+    direct32, t32 = timed(lambda: solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, pts, precision=1))
+    g = out[planes].reshape(-1, 3).to(torch.complex128)
+    d64 = direct64.reshape(-1, 3)
+    err_grid = float((g - d64).norm() / d64.norm())
+    err_direct32 = float((direct32.reshape(-1, 3) - d64).norm() / d64.norm())
+    g64 = solver.field_grid(ctx, params, sol, precision=0, **FIELD_GRID)[planes].reshape(-1, 3)
+    err_grid64 = float((g64 - d64).norm() / d64.norm())
+    plane_evals = sum((int(wt.end[l]) - int(wt.begin[l])) for l in
+                      [int(sum(1 for zz in wt.z_layers if FIELD_GRID["origin"][2] + FIELD_GRID["step"][2] * i >=
+                               zz - 0.001)) for i in planes]) * FIELD_GRID["counts"][0] * FIELD_GRID["counts"][1]
+    direct_rate = {"float32_fp64_phase": plane_evals / (t32 / 1e3), "float64": plane_evals / (t64 / 1e3)}
+    nw_table = int(wt.E0.shape[0])
+    del wt
+
+    # the thin-volume slice (configs[0]-sized): factorised and direct
+    tsmp = torch.from_numpy(samples.triangle_map(0)).cuda()
+    tp = solver.make_params(**THIN_KW)
+    tsol = solver.solve(ctx, tp, tsmp)
+    twt = solver.waves(ctx, tp, tsol)
+    tev = wave_evals(twt, THIN_GRID)
+    solver.field_grid(ctx, tp, tsol, precision=1, **THIN_GRID)
+    _, t_thin = timed(lambda: solver.field_grid(ctx, tp, tsol, precision=1, **THIN_GRID))
+    tpts = torch.from_numpy(grid_points(THIN_GRID)).cuda()
+    solver.evaluate(ctx, twt.E0, twt.k, twt.z_layers, twt.begin, twt.end, tpts, precision=1)
+    _, t_thin_direct = timed(lambda: solver.evaluate(ctx, twt.E0, twt.k, twt.z_layers, twt.begin, twt.end, tpts,
+                                                     precision=1))
+
+    # end to end: the solution (x, eigenvalues, interior fields) from pinned host memory, the grid back
+    e2e = None
+    if not args.no_e2e:
+        hsol = [t.cpu().pin_memory() for t in (sol.x, sol.evl, sol.Qc, sol.Qh)]
+        dsol = [torch.empty_like(t) for t in (sol.x, sol.evl, sol.Qc, sol.Qh)]
+        hout = torch.empty(out.shape, dtype=out.dtype).pin_memory()
+        s2 = solver.VolumeSolution(sol.dims, sol.shape, *dsol)
+        barrier()
+        e2e_ms = []
+        for _ in range(args.steps):
+            def step():
+                for d, h in zip(dsol, hsol):
+                    d.copy_(h, non_blocking=True)
+                r = grid_step(s2)
+                hout.copy_(r, non_blocking=True)
+                return r
+            _, ms = timed(step)
+            e2e_ms.append(ms)
+        e2e = {"value": world * evals * args.steps / (max_over_ranks(sum(e2e_ms)) / 1e3), "unit": FIELD_UNIT,
+               "h2d_bytes_per_step": int(sum(h.numel() for h in hsol) * 16),
+               "d2h_bytes_per_step": int(hout.numel() * 8)}
+
+    # roofline: the dominant stage by device time
+    st = {k: statistics.mean(s[k] for s in stages) for k in ("fft", "assemble", "eig", "chain", "total")}
+    names = {"fft": "wave table (waves_kernel) + phase tables", "assemble": "order sums (field_h_kernel)",
+             "eig": "y transform (field_u_kernel)", "chain": "x transform + output (field_e_kernel)"}
+    MF, Mx, Ny = sol.dims.MF, sol.dims.Mx, FIELD_GRID["counts"][1]
+    dom = max(("fft", "assemble", "eig", "chain"), key=lambda k: st[k])
+    nz = FIELD_GRID["counts"][2]
+    peak = float(_peaks().get("hbm_gbs", 6650.0))
+    zb = sol.shape[0]
+    # algorithmic bytes per stage: table written + solution read; table read per plane's region (two
+    # internal lists); U written; output written + U read
+    bytes_dom = {"fft": nw_table * 96 + 2 * zb * 3 * MF * 2 * MF * 16,
+                 "assemble": nz * 2 * (2 * MF * MF) * 96,
+                 "eig": nz * 3 * Mx * Ny * 16,
+                 "chain": out_bytes + nz * 3 * Mx * Ny * 16}[dom]
+    roofline = {"bound": "hbm", "achieved": bytes_dom / (st[dom] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": bytes_dom / (st[dom] / 1e3) / 1e9 / peak, "traffic": None, "kernel": names[dom],
+                "algorithmic_bytes": bytes_dom, "stage_ms": {names[k]: round(st[k], 3) for k in names},
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if _peaks() else "fallback 6650 GB/s"}
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            from oracle import cw as ocw
+            E0h, Kh = twt.E0.cpu().numpy(), twt.k.cpu().numpy()
+            sub = grid_points(THIN_GRID)
+            sub = sub[(sub[:, 2] > -0.5) & (sub[:, 2] < 0.5)][:64]
+            reg = ocw.region_of(sub[:, 2], twt.z_layers)
+            ev = int(sum(int(twt.end[r]) - int(twt.begin[r]) for r in reg))
+            t0 = time.perf_counter()
+            ocw.evaluate(sub, twt.z_layers, twt.begin, twt.end, E0h, Kh)
+            cpu = {"value": ev / (time.perf_counter() - t0), "unit": FIELD_UNIT, "cores": blas_threads(),
+                   "kind": "port", "sample": f"{len(sub)} interior points of the triangle slice, {ev} wave "
+                                             "evaluations, oracle float64 sum (numpy)"}
+        line = {"metric": FIELD_METRIC, "value": value, "unit": FIELD_UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex64 output)", "data": "synthetic",
+                "config": {"workload": FIELD_NAME, "points": npts, "wave_evals_per_step": evals,
+                           "l2": "flushed between steps (256 MB write, untimed); output 403 MB > L2",
+                           "parallelism": f"independent volume per rank x{world}"},
+                "paths": {"grid_factorised_ms": total_ms / args.steps,
+                          "grid_error_vs_fp64_direct": {"complex64_out": err_grid, "complex128_out": err_grid64},
+                          "direct_evaluator_wave_evals_per_s": direct_rate,
+                          "direct_float32_error_vs_fp64": err_direct32,
+                          "thin_slice": {"points": 65536, "wave_evals": tev, "factorised_ms": t_thin,
+                                         "direct_float32_ms": t_thin_direct,
+                                         "factorised_wave_evals_per_s": tev / (t_thin / 1e3),
+                                         "direct_wave_evals_per_s": tev / (t_thin_direct / 1e3)}},
+                "clocks": clocks, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # --------------------------------------------------------------------------- named profiling cases
 # python bench.py --case <case> [args]: one configuration at a time, for timing
 # and for the ncu commands of the profile summaries.
@@ -1147,7 +1400,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "volume", "layer"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "volume", "layer", "field"])
     ap.add_argument("--case", nargs=argparse.REMAINDER, help="run one named profiling case instead")
     args = ap.parse_args()
     if args.case:
@@ -1158,6 +1411,8 @@ def main():
         return run_sweep_ours(args)
     if args.workload == "layer":
         return run_layer_ours(args)
+    if args.workload == "field":
+        return run_field_ours(args)
     return run_volume_ours(args)
 
 

@@ -315,6 +315,23 @@ sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw,
                          double zeps, const double* points, long long np, void* out,
                          int precision, void* stream);
 
+/* The field of a solved volume on a regular grid: points (x0 + i dx,
+ * y0 + j dy, z0 + b dz) for i < Nx, j < Ny, b < Nz (origin, step, counts: 3
+ * each, host); out[((b Ny + j) Nx + i) 3 + c] is E_c, complex128 (precision
+ * 0) or complex64 (precision 1), device.  The same sum as sc_cw_evaluate over
+ * the wave table of sc_volume_waves (ez_mode and zeps as there), evaluated in
+ * the coupled-wave factorised form: per z plane, the waves of each Fourier
+ * order are summed once, then two small separable transforms along y and x
+ * (all FP64).  Orders along x up to 64.  Replaces a whole-grid evaluation
+ * through gpu_cw_evaluate (gpuEvaluator.cu:131-165) / scatterview --nogui
+ * slices (ScatterView.cpp:713-795); an x-z slice is Ny = 1.  Synchronises the
+ * stream; sc_volume_stage_ms then holds [wave table, order sums, y transform,
+ * x transform, -, -, -, total] device milliseconds. */
+sc_status sc_volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2, const void* x,
+                               const void* evl, const void* Qc, const void* Qh, int ez_mode, const double* origin,
+                               const double* step, const int* counts, double zeps, void* out, int precision,
+                               void* stream);
+
 /* ----------------------------------------- homogeneous layers, focused beams */
 
 /* tira::planewave::SolidAnglePolar as scatterlayer and scatterplane call it

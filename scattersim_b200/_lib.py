@@ -84,6 +84,9 @@ _SIGS = {
                                       c_void_p, c_void_p, POINTER(c_int), c_void_p]),
     "sc_volume_boundary_solve": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
                                          c_void_p, POINTER(c_int), c_void_p]),
+    "sc_volume_field_grid": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int),
+                                     c_double, c_void_p, c_int, c_void_p]),
     "sc_volume_params_default": (None, [POINTER(VolumeParams)]),
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
     "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),

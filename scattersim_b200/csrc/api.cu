@@ -46,6 +46,10 @@ sc_status volume_chain_block(sc_context* ctx, const sc_volume_params* p, const d
 sc_status volume_boundary_solve(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2,
                                 const double2* Gcs_in, const double2* GD0, double2* x_out, int* info_host,
                                 cudaStream_t st);
+sc_status volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2, const double2* x,
+                            const double2* evl, const double2* Qc, const double2* Qh, int ez_mode,
+                            const double* origin, const double* step, const int* counts, double zeps, void* out,
+                            int precision, cudaStream_t st);
 sc_status volume_waves_launch(cudaStream_t st, int MF, int Z, const double2* svec, const double2* x,
                               const double2* evl, const double2* Qc, const double2* Qh, const double* zpl,
                               double k, double ntop, double nbot, int external, int ez_mode, long long nw,
@@ -68,6 +72,8 @@ struct DeviceGuard {
     }
 };
 
+}  // namespace
+
 // region index of a scattervolume wave table (cw_allocate, cpuEvaluator.cpp:34-53)
 void volume_regions(int MF, int Z, int external, long long* nw, int* begin, int* end) {
     const long long internal = 2LL * MF * MF;
@@ -84,7 +90,6 @@ void volume_regions(int MF, int Z, int external, long long* nw, int* begin, int*
     end[Z + 1] = (int)total;
     *nw = total;
 }
-}  // namespace
 
 }  // namespace sc
 
@@ -657,6 +662,21 @@ sc_status sc_volume_waves(sc_context* ctx, const sc_volume_params* p, int Z, int
                                (const double2*)Qh, zpl, P.dims.k, p->n[0], p->n[1], p->external, ez_mode, *nw,
                                (double2*)E0, (double2*)k));
     SC_CUDA_TRY(cudaStreamSynchronize(st));
+    return SC_OK;
+}
+
+sc_status sc_volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z, int S1, int S2, const void* x,
+                               const void* evl, const void* Qc, const void* Qh, int ez_mode, const double* origin,
+                               const double* step, const int* counts, double zeps, void* out, int precision,
+                               void* stream) {
+    if (!ctx || !p || !x || !evl || !origin || !step || !counts || !out) {
+        set_error("sc_volume_field_grid: null argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    SC_TRY(volume_field_grid(ctx, p, Z, S1, S2, (const double2*)x, (const double2*)evl, (const double2*)Qc,
+                             (const double2*)Qh, ez_mode, origin, step, counts, zeps, out, precision, st));
     return SC_OK;
 }
 

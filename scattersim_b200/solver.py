@@ -269,6 +269,23 @@ def evaluate(ctx: Context, E0: torch.Tensor, K: torch.Tensor, z_layers, begin, e
     return out
 
 
+def field_grid(ctx: Context, params: VolumeParams, sol: VolumeSolution, origin, step, counts, ez_mode: int = 0,
+               zeps: float = 0.001, precision: int = 0, stream=None) -> torch.Tensor:
+    """E on the grid origin + (i, j, b) * step, counts = (Nx, Ny, Nz): a (Nz, Ny, Nx, 3) complex tensor
+    (complex128, or complex64 with precision=1) -- the evaluator sum over the solution's waves, factorised."""
+    Z, S1, S2 = sol.shape
+    nx, ny, nz = (int(c) for c in counts)
+    dt = torch.complex128 if precision == 0 else torch.complex64
+    out = torch.empty((nz, ny, nx, 3), dtype=dt, device=sol.x.device)
+    o = (ctypes.c_double * 3)(*[float(v) for v in origin])
+    s = (ctypes.c_double * 3)(*[float(v) for v in step])
+    c = (ctypes.c_int * 3)(nx, ny, nz)
+    check(ctx.lib.sc_volume_field_grid(ctx.handle, ctypes.byref(params), Z, S1, S2, _ptr(sol.x), _ptr(sol.evl),
+                                       _ptr(sol.Qc), _ptr(sol.Qh), int(ez_mode), o, s, c, float(zeps), _ptr(out),
+                                       int(precision), _stream_ptr(stream)))
+    return out
+
+
 @dataclass
 class SweepResult:
     x: list                  # per instance: (6 MF,) complex128 device tensor [R; T]

@@ -13,6 +13,7 @@ import pytest
 import torch
 
 from oracle import cw as ocw
+from scattersim_b200 import samples, solver
 
 pytestmark = pytest.mark.gpu
 
@@ -72,3 +73,48 @@ def test_gpu_cw_evaluate_shim_matches_float32_sum(ctx):
                        W[:, 3:6].astype(np.complex128), eps=0.001)
     got = E_xz.reshape(-1, 3)
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+
+
+# ---------------------------------------------------------------- factorised grid evaluator
+def _grid_points(origin, step, counts):
+    nx, ny, nz = counts
+    zz, yy, xx = np.meshgrid(origin[2] + step[2] * np.arange(nz), origin[1] + step[1] * np.arange(ny),
+                             origin[0] + step[0] * np.arange(nx), indexing="ij")
+    return np.stack([xx.ravel(), yy.ravel(), zz.ravel()], -1)
+
+
+@pytest.mark.parametrize("kw,counts", [
+    (dict(lambda_=0.6, size=(20, 20, 8), coef=(7, 5), direction=(0.17, 0.05, 0.98), ex=(1, 0), ey=(0, 0)),
+     (17, 9, 23)),
+    (dict(lambda_=0.55, size=(20, 20, 8), coef=(5, 5), external=True), (12, 1, 31)),
+    (dict(lambda_=0.6, size=(20, 20, 8), coef=(9, 9), npz=True, kappa=0.02), (8, 6, 40)),
+])
+def test_field_grid_equals_direct_sum(ctx, kw, counts):
+    """sc_volume_field_grid against sc_cw_evaluate on the same wave table and points, and the oracle's
+    float64 sum: the factorised form regroups the same sum (FP64 both)."""
+    from oracle import scattervolume as osv
+    smp = samples.sphere_volume(4, nxy=24, nz=5, size=(20.0, 20.0, 8.0))
+    p = solver.make_params(**kw)
+    sol = solver.solve(ctx, p, torch.from_numpy(smp).cuda())
+    origin, step = (1.3, 2.1, -6.5), (1.1, 1.7, 13.0 / (counts[2] - 1))
+    grid = solver.field_grid(ctx, p, sol, origin, step, counts).cpu().numpy().reshape(-1, 3)
+    pts = _grid_points(origin, step, counts)
+    wt = solver.waves(ctx, p, sol)
+    direct = solver.evaluate(ctx, wt.E0, wt.k, wt.z_layers, wt.begin, wt.end, torch.from_numpy(pts).cuda())
+    direct = direct.cpu().numpy()
+    assert np.linalg.norm(grid - direct) / np.linalg.norm(direct) < 1e-12
+    okw = dict(kw)
+    if "kappa" in okw:
+        okw["kappa"] = (okw["kappa"],)
+    po = osv.Params(**okw)
+    ref = osv.solve(smp, po)
+    W = osv.build_waves(ref, po)
+    layers = [(W.z[l], W.Pr_E[l], W.Pr_k[l], W.Pt_E[l], W.Pt_k[l]) for l in range(len(W.z))]
+    zl, b, e, WE, Wk = ocw.unpack(W.Pi_E, W.Pi_k, layers)
+    if po.external:
+        zl = np.array([z if (l == 0 or l == len(zl) - 1) else 0.0 for l, z in enumerate(zl)])
+    E_ref = ocw.evaluate(pts, zl, b, e, WE, Wk)
+    assert np.linalg.norm(grid - E_ref) / np.linalg.norm(E_ref) < 1e-9
+    # complex64 output: the same values rounded
+    g32 = solver.field_grid(ctx, p, sol, origin, step, counts, precision=1).cpu().numpy().reshape(-1, 3)
+    assert np.linalg.norm(g32 - grid) / np.linalg.norm(grid) < 1e-7
