@@ -28,6 +28,7 @@
  *   sc_gpu_cw_evaluate      host-buffer gpu_initialize /     gpuEvaluator.cu:15-26,131-165
  *                           gpu_cw_evaluate
  *   sc_scatterio_write/read write_file / read_file           ScatterIO.h:18-117
+ *   sc_cw_write             CoupledWaveStructure::save       CoupledWaveStructure.h:63-125
  */
 #ifndef SCATTERSIM_B200_H
 #define SCATTERSIM_B200_H
@@ -300,6 +301,19 @@ sc_status sc_volume_waves(sc_context* ctx, const sc_volume_params* p, int Z, int
                           const void* x, const void* evl, const void* Qc, const void* Qh,
                           int ez_mode, long long* nw, int* begin, int* end, double* z_layers,
                           void* E0, void* k, void* stream);
+
+/* CoupledWaveStructure::save (CoupledWaveStructure.h:63-125) from a device
+ * wave table (E0, k: nw x 3 complex128 each, in file order -- the order
+ * sc_volume_waves writes): u64 8, u64 #Pi and the Pi records, u64 layers,
+ * then per layer its z (z_layers, host), u64 #Pr, records, u64 #Pt, records.
+ * counts (host, 1 + 2 layers): #Pi, then #Pr and #Pt per layer.  Records are
+ * 80 bytes {E0 pair, kx, ky, kz}; frame 0 stores the E0 pair in tira's record
+ * frame (the reference's own files), 1 the Cartesian (E_x, E_y).  Records are
+ * formed on the device and streamed through pinned buffers, the copy of one
+ * chunk overlapping the write of the previous (GB-scale files at disk speed).
+ * Synchronises the stream. */
+sc_status sc_cw_write(sc_context* ctx, const char* path, const void* E0, const void* k, long long nw, int layers,
+                      const double* z_layers, const long long* counts, int frame, void* stream);
 
 /* ------------------------------------------------------ field evaluation */
 

@@ -87,6 +87,8 @@ _SIGS = {
     "sc_volume_field_grid": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
                                      c_void_p, c_void_p, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int),
                                      c_double, c_void_p, c_int, c_void_p]),
+    "sc_cw_write": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_void_p, c_longlong, c_int, POINTER(c_double),
+                            POINTER(c_longlong), c_int, c_void_p]),
     "sc_volume_params_default": (None, [POINTER(VolumeParams)]),
     "sc_volume_plan": (c_int, [POINTER(VolumeParams), c_int, c_int, c_int, POINTER(VolumeDims)]),
     "sc_sweep_solve": (c_int, [c_void_p, c_int, POINTER(VolumeParams), POINTER(c_void_p), POINTER(c_int),

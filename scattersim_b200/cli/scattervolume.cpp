@@ -157,45 +157,27 @@ int main(int argc, char** argv) {
     if ((s = sc_volume_waves(ctx, &p, Z, S1, S2, d_x, d_evl, d_qc, d_qh, 0, &nw, begin.data(), end.data(), zl.data(),
                              d_E, d_k, nullptr)) != SC_OK)
         return fail("sc_volume_waves", s);
-    std::vector<cplx> hE(3 * nw), hk(3 * nw);
-    cudaMemcpy(hE.data(), d_E, sizeof(cplx) * 3 * nw, cudaMemcpyDeviceToHost);
-    cudaMemcpy(hk.data(), d_k, sizeof(cplx) * 3 * nw, cudaMemcpyDeviceToHost);
-    // table order = file order: Pi, then per boundary its Pr list and its Pt list
-    cwio::CoupledWave cw;
-    auto take = [&](long long b0, long long b1) {
-        std::vector<cwio::Wave> w((size_t)(b1 - b0));
-        for (long long i = b0; i < b1; ++i) {
-            for (int c = 0; c < 3; ++c) {
-                w[i - b0].E[c] = hE[3 * i + c];
-                w[i - b0].k[c] = hk[3 * i + c];
-            }
-        }
-        return w;
-    };
-    // list sizes of CoupledWaveStructure (ScatterVolume.cpp:907-987): boundary 0
-    // reflects MF waves, the last transmits MF, interior lists hold 2 MF^2 modes
+    // the file straight from the device table (table order = file order: Pi,
+    // then per boundary its Pr and its Pt list); list sizes of
+    // CoupledWaveStructure (ScatterVolume.cpp:907-987): boundary 0 reflects MF
+    // waves, the last transmits MF, interior lists hold 2 MF^2 modes
     const long long interior = p.external ? 0 : 2LL * MF * MF;
-    cw.Pi = take(0, MF);
-    cw.layers.resize(Z + 1);
+    std::vector<long long> counts(1 + 2 * (Z + 1));
+    counts[0] = MF;
     long long pos = MF;
     for (int l = 0; l <= Z; ++l) {
-        const long long npr = (l == 0) ? MF : interior;
-        const long long npt = (l == Z) ? MF : interior;
-        cw.layers[l].z = zl[l];
-        cw.layers[l].Pr = take(pos, pos + npr);
-        pos += npr;
-        cw.layers[l].Pt = take(pos, pos + npt);
-        pos += npt;
+        counts[1 + 2 * l] = (l == 0) ? MF : interior;
+        counts[2 + 2 * l] = (l == Z) ? MF : interior;
+        pos += counts[1 + 2 * l] + counts[2 + 2 * l];
     }
     if (pos != nw) {
         std::cerr << "ERROR: wave table size mismatch" << std::endl;
         return 1;
     }
-    try {
-        if (!out.empty()) cwio::save_cw(out, cw, frame);
-    } catch (const std::exception& e) {
-        std::cerr << "ERROR: " << e.what() << std::endl;
-        return 1;
+    if (!out.empty()) {
+        if ((s = sc_cw_write(ctx, out.c_str(), d_E, d_k, nw, Z + 1, zl.data(), counts.data(),
+                             frame == cwio::Frame::tira ? 0 : 1, nullptr)) != SC_OK)
+            return fail("sc_cw_write", s);
     }
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::cout << "Field saved in " << out << "." << std::endl;

@@ -50,6 +50,8 @@ sc_status volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z, i
                             const double2* evl, const double2* Qc, const double2* Qh, int ez_mode,
                             const double* origin, const double* step, const int* counts, double zeps, void* out,
                             int precision, cudaStream_t st);
+sc_status cw_write(sc_context* ctx, const char* path, const double2* E0, const double2* K, long long nw, int layers,
+                   const double* z_layers, const long long* counts, int frame, cudaStream_t st);
 sc_status volume_waves_launch(cudaStream_t st, int MF, int Z, const double2* svec, const double2* x,
                               const double2* evl, const double2* Qc, const double2* Qh, const double* zpl,
                               double k, double ntop, double nbot, int external, int ez_mode, long long nw,
@@ -678,6 +680,18 @@ sc_status sc_volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z
     SC_TRY(volume_field_grid(ctx, p, Z, S1, S2, (const double2*)x, (const double2*)evl, (const double2*)Qc,
                              (const double2*)Qh, ez_mode, origin, step, counts, zeps, out, precision, st));
     return SC_OK;
+}
+
+sc_status sc_cw_write(sc_context* ctx, const char* path, const void* E0, const void* k, long long nw, int layers,
+                      const double* z_layers, const long long* counts, int frame, void* stream) {
+    if (!ctx || !path || layers < 0 || nw < 0 || !counts || (layers > 0 && !z_layers) || (nw > 0 && (!E0 || !k)) ||
+        (frame != 0 && frame != 1)) {
+        set_error("sc_cw_write: bad argument");
+        return SC_BADINPUT;
+    }
+    DeviceGuard g(ctx->device);
+    return cw_write(ctx, path, (const double2*)E0, (const double2*)k, nw, layers, z_layers, counts, frame,
+                    (cudaStream_t)stream);
 }
 
 sc_status sc_cw_evaluate(sc_context* ctx, const void* E0, const void* k, int nw, const double* z_layers,
