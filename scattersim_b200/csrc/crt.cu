@@ -40,6 +40,7 @@
 // drains its copies, frees its TMEM and returns.
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -113,19 +114,79 @@ CrtConst make_constants() {
 int crt_bits(int k, double log2P) {
     const double kp = 2.0 * (double)(k > 0 ? k : 1);
     int b = (int)std::floor((log2P - 3.0 - std::log2(kp)) / 2.0);
-    return b > 52 ? 52 : b;
+    return b > 49 ? 49 : b;   // |scaled operand| <= 2^49 < 2^50, the range of the limb split
 }
 
-// symmetric residue of an integer-valued double (|x| <= 2^52) mod p
-__device__ __forceinline__ int sym_mod(double x, double p, double inv_p) {
-    const double q = rint(x * inv_p);
-    return (int)fma(-q, p, x);
+// The residue arithmetic runs in int32 with the moduli as compile-time
+// constants (the compiler turns x % p into multiply-high sequences on the
+// integer pipes); FP64 rounding and int<->double conversions would all go
+// through the conversion (XU) pipe, which then throttles the epilogue.
+__host__ __device__ constexpr int crt_mod(int t) {
+    return t == 0 ? 255 : t == 1 ? 253 : t == 2 ? 251 : t == 3 ? 247 : t == 4 ? 241 : t == 5 ? 239 : t == 6 ? 233
+         : t == 7 ? 229 : t == 8 ? 227 : t == 9 ? 223 : t == 10 ? 217 : t == 11 ? 211 : t == 12 ? 199 : 197;
+}
+// 2^e mod p for e = 17, 34, 50 (the limb weights of the operand split below)
+__host__ __device__ constexpr int pow2_mod(int e, int p) { return e == 0 ? 1 % p : (2 * pow2_mod(e - 1, p)) % p; }
+
+// symmetric residue of a 32-bit integer: |r| <= (p - 1) / 2
+template <int P>
+__device__ __forceinline__ int sym_res(int x) {
+    int r = x % P;
+    if (r > P / 2) r -= P;
+    if (r < -(P / 2)) r += P;
+    return r;
+}
+// symmetric residue of an integer u with |u| < 2^50, given as U = u + 2^50
+// split into 17-bit limbs U0 + 2^17 U1 + 2^34 U2
+template <int P>
+__device__ __forceinline__ int sym_res_wide(int U0, int U1, int U2) {
+    constexpr int c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
+    return sym_res<P>(U2 * c34 + U1 * c17 + U0 - c50);
+}
+
+// x (|x| < 2^50, any double) rounded to the nearest integer and returned as
+// the three 17-bit limbs of x + 2^50: 1.5 2^52 + x places the rounded integer
+// in the low mantissa bits (no FP64 rounding or conversion instruction)
+__device__ __forceinline__ void round_limbs(double x, int& U0, int& U1, int& U2) {
+    const double y = x + 6755399441055744.0;                                 // 1.5 * 2^52
+    const long long bits = __double_as_longlong(y) & ((1LL << 52) - 1);      // rounded x + 2^51
+    const long long U = bits + (1LL << 50) - (1LL << 51);                    // rounded x + 2^50
+    U0 = (int)(U & 0x1FFFF);
+    U1 = (int)((U >> 17) & 0x1FFFF);
+    U2 = (int)(U >> 34);
+}
+
+// x * 2^e exactly (a power-of-two multiply when 2^e is a normal double)
+__device__ __forceinline__ double scale2(double x, int e) {
+    if (e >= -1022 && e <= 1023) return x * __hiloint2double((e + 1023) << 20, 0);
+    return ldexp(x, e);
 }
 
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
     return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
            ((uint32_t)(uint8_t)d << 24);
 }
+
+// f(std::integral_constant<int, t>) for t = 0 .. NMOD-1 (the modulus a compile-time constant in each call)
+template <int T, typename F>
+__device__ __forceinline__ void for_each_mod_from(F& f) {
+    if constexpr (T < CRT_NMOD) {
+        f(std::integral_constant<int, T>());
+        for_each_mod_from<T + 1>(f);
+    }
+}
+template <typename F>
+__device__ __forceinline__ void for_each_mod(F& f) { for_each_mod_from<0>(f); }
+// f(std::integral_constant<int, t>) for one runtime t
+template <int T, typename F>
+__device__ __forceinline__ void with_mod_from(int t, F& f) {
+    if constexpr (T < CRT_NMOD) {
+        if (t == T) f(std::integral_constant<int, T>());
+        else with_mod_from<T + 1>(t, f);
+    }
+}
+template <typename F>
+__device__ __forceinline__ void with_mod(int t, F& f) { with_mod_from<0>(t, f); }
 
 // ---------------------------------------------------------------- packing
 // A' residue tiles: [b][p][rb][kb][4 KB]; a thread takes one complex row i and
@@ -140,35 +201,36 @@ __global__ void __launch_bounds__(128) crt_pack_a_kernel(int m, int k, const dou
     const double2* a = Ap ? Ap[b] : A + b * sA;
     const int il = threadIdx.x & 63, jc = threadIdx.x >> 6;
     const int i = rb * (CRT_BM / 2) + il, j0 = kb * (CRT_BK / 2) + 8 * jc;
-    double xr[8], xi[8];
+    int lr[8][3], li[8][3];
     const int ex = (i < m) ? rowexp[(long long)b * m + i] : 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         double2 v = make_double2(0.0, 0.0);
         if (i < m && j0 + q < k) v = a[(long long)(j0 + q) * lda + i];
-        xr[q] = rint(ldexp(v.x, al - ex));
-        xi[q] = rint(ldexp(v.y, al - ex));
+        round_limbs(scale2(v.x, al - ex), lr[q][0], lr[q][1], lr[q][2]);
+        round_limbs(scale2(v.y, al - ex), li[q][0], li[q][1], li[q][2]);
     }
     const int o0 = tc::tile_off(2 * il, 16 * jc), o1 = tc::tile_off(2 * il + 1, 16 * jc);
     const long long plane = (long long)RB * KB * CRT_ATILE;
     int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)rb * KB + kb) * CRT_ATILE;
-#pragma unroll 1
-    for (int t = 0; t < CRT_NMOD; ++t) {
-        const double p = c_crt.p[t], ip = c_crt.inv_p[t];
+    auto one = [&](auto tag) {
+        constexpr int T = decltype(tag)::value;
+        constexpr int P = crt_mod(T);
         int dr[8], di[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            dr[q] = sym_mod(xr[q], p, ip);
-            di[q] = sym_mod(xi[q], p, ip);
+            dr[q] = sym_res_wide<P>(lr[q][0], lr[q][1], lr[q][2]);
+            di[q] = sym_res_wide<P>(li[q][0], li[q][1], li[q][2]);
         }
         const uint4 w0 = make_uint4(pack4(dr[0], -di[0], dr[1], -di[1]), pack4(dr[2], -di[2], dr[3], -di[3]),
                                     pack4(dr[4], -di[4], dr[5], -di[5]), pack4(dr[6], -di[6], dr[7], -di[7]));
         const uint4 w1 = make_uint4(pack4(di[0], dr[0], di[1], dr[1]), pack4(di[2], dr[2], di[3], dr[3]),
                                     pack4(di[4], dr[4], di[5], dr[5]), pack4(di[6], dr[6], di[7], dr[7]));
-        int8_t* pl = base + (long long)t * plane;
+        int8_t* pl = base + (long long)T * plane;
         *reinterpret_cast<uint4*>(pl + o0) = w0;
         *reinterpret_cast<uint4*>(pl + o1) = w1;
-    }
+    };
+    for_each_mod(one);
 }
 
 // B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB]; a thread takes one
@@ -182,35 +244,33 @@ __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const dou
     const double2* bb = Bp ? Bp[b] : B + b * sB;
     const int cl = threadIdx.x;
     const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2);
-    double xr[16], xi[16];
+    int lx[32][3];
     const int ex = (c < n) ? colexp[(long long)b * n + c] : 0;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         double2 v = make_double2(0.0, 0.0);
         if (c < n && j0 + q < k) v = bb[(long long)c * ldb + j0 + q];
-        xr[q] = rint(ldexp(v.x, be - ex));
-        xi[q] = rint(ldexp(v.y, be - ex));
+        round_limbs(scale2(v.x, be - ex), lx[2 * q][0], lx[2 * q][1], lx[2 * q][2]);
+        round_limbs(scale2(v.y, be - ex), lx[2 * q + 1][0], lx[2 * q + 1][1], lx[2 * q + 1][2]);
     }
     const int o0 = tc::tile_off(cl, 0), o1 = tc::tile_off(cl, 16);
     const long long plane = (long long)CB * KB * CRT_BTILE;
     int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)cb * KB + kb) * CRT_BTILE;
-#pragma unroll 1
-    for (int t = 0; t < CRT_NMOD; ++t) {
-        const double p = c_crt.p[t], ip = c_crt.inv_p[t];
+    auto one = [&](auto tag) {
+        constexpr int T = decltype(tag)::value;
+        constexpr int P = crt_mod(T);
         int d[32];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            d[2 * q] = sym_mod(xr[q], p, ip);
-            d[2 * q + 1] = sym_mod(xi[q], p, ip);
-        }
-        int8_t* pl = base + (long long)t * plane;
+        for (int q = 0; q < 32; ++q) d[q] = sym_res_wide<P>(lx[q][0], lx[q][1], lx[q][2]);
+        int8_t* pl = base + (long long)T * plane;
         *reinterpret_cast<uint4*>(pl + o0) = make_uint4(pack4(d[0], d[1], d[2], d[3]), pack4(d[4], d[5], d[6], d[7]),
                                                        pack4(d[8], d[9], d[10], d[11]),
                                                        pack4(d[12], d[13], d[14], d[15]));
         *reinterpret_cast<uint4*>(pl + o1) =
             make_uint4(pack4(d[16], d[17], d[18], d[19]), pack4(d[20], d[21], d[22], d[23]),
                        pack4(d[24], d[25], d[26], d[27]), pack4(d[28], d[29], d[30], d[31]));
-    }
+    };
+    for_each_mod(one);
 }
 
 // ---------------------------------------------------------------- MMA kernel
@@ -236,13 +296,14 @@ __device__ __forceinline__ double crt_value(const int (&r)[CRT_NMOD]) {
     double sh = 0.0, sm = 0.0, sl = 0.0;
 #pragma unroll
     for (int t = 0; t < CRT_NMOD; ++t) {
-        const double rv = (double)r[t];
+        // r + 128 in the low bits of 2^52: an exact int8 -> double without a conversion instruction
+        const double rv = __hiloint2double(0x43300000, r[t] + 128) - 4503599627370624.0;   // 2^52 + 128
         sh = fma(rv, c_crt.wh[t], sh);
         sm = fma(rv, c_crt.wm[t], sm);
         sl = fma(rv, c_crt.wl[t], sl);
     }
     const double s = fma(sh, 0x1p74, fma(sm, 0x1p37, sl));
-    const double q = rint(s * c_crt.invP);
+    const double q = (s * c_crt.invP + 6755399441055744.0) - 6755399441055744.0;     // round to nearest
     const double dh = fma(-q, c_crt.Ph, sh);
     const double dm = fma(-q, c_crt.Pm, sm);
     const double dl = fma(-q, c_crt.Pl, sl);
@@ -362,21 +423,23 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                     break;
                 }
                 tc::fence_after_sync();
-                const double p = c_crt.p[t], ip = c_crt.inv_p[t];
                 int8_t* dst = scr + ((long long)t * CRT_BM + row) * CRT_BN;
+                auto extract = [&](auto tag) {
+                    constexpr int P = crt_mod(decltype(tag)::value);
 #pragma unroll 1
-                for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
-                    uint32_t r[32];
-                    tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * CRT_BN + c0), r);
-                    uint32_t w[8];
+                    for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+                        uint32_t r[32];
+                        tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * CRT_BN + c0), r);
+                        uint32_t w[8];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        w[q] = pack4(sym_mod((double)(int)r[4 * q], p, ip), sym_mod((double)(int)r[4 * q + 1], p, ip),
-                                     sym_mod((double)(int)r[4 * q + 2], p, ip),
-                                     sym_mod((double)(int)r[4 * q + 3], p, ip));
-                    *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
-                    *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
-                }
+                        for (int q = 0; q < 8; ++q)
+                            w[q] = pack4(sym_res<P>((int)r[4 * q]), sym_res<P>((int)r[4 * q + 1]),
+                                         sym_res<P>((int)r[4 * q + 2]), sym_res<P>((int)r[4 * q + 3]));
+                        *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
+                        *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
+                };
+                with_mod(t, extract);
                 tc::fence_before_sync();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&accempty[buf]);
@@ -407,7 +470,7 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                     }
                     const int c = cb * CRT_BN + c0 + q;
                     const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
-                    const double v = ldexp(crt_value(r), ex + fx - g.shift);
+                    const double v = scale2(crt_value(r), ex + fx - g.shift);
                     const double o = __shfl_xor_sync(0xffffffffu, v, 1);
                     if (!im && i < g.m && c < g.n) {
                         double2* pc = C + (long long)c * g.ldc + i;

@@ -14,6 +14,7 @@
 // region test with zeps) is the one sc_volume_waves builds; the transverse
 // wave numbers are read from it.  All arithmetic is FP64; the output is
 // complex128 or complex64.
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -158,8 +159,13 @@ __global__ void __launch_bounds__(FE_THREADS) field_e_kernel(FieldGeom g, const 
     for (int px = 0; px < MAXM; ++px)
         ex[px] = (active && px < Mx) ? Ex[i + (long long)g.Nx * px] : make_double2(0.0, 0.0);
     const long long per = (long long)Mx * g.Ny;
-    for (int j0 = 0; j0 < g.Ny; j0 += FE_YCHUNK) {
-        const int nj = min(FE_YCHUNK, g.Ny - j0);
+    // this CTA's share of the y rows (blockIdx.z of gridDim.z, in whole chunks)
+    const int chunks = (g.Ny + FE_YCHUNK - 1) / FE_YCHUNK;
+    const int cper = (chunks + gridDim.z - 1) / gridDim.z;
+    const int jbeg = blockIdx.z * cper * FE_YCHUNK;
+    const int jend = min(g.Ny, jbeg + cper * FE_YCHUNK);
+    for (int j0 = jbeg; j0 < jend; j0 += FE_YCHUNK) {
+        const int nj = min(FE_YCHUNK, jend - j0);
         __syncthreads();
         for (int t = threadIdx.x; t < nj * 3 * Mx; t += FE_THREADS) {
             const int px = t % Mx, c = (t / Mx) % 3, jj = t / (3 * Mx);
@@ -290,7 +296,12 @@ sc_status volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z, i
     const long long per = (long long)g.Mx * g.Ny;
     field_u_kernel<<<dim3((unsigned)((per + 255) / 256), g.Nz * 3), 256, 0, st>>>(g, H, Ey, U);
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
-    const dim3 ge((g.Nx + FE_THREADS - 1) / FE_THREADS, g.Nz);
+    // y split so that the grid holds about eight CTAs per SM
+    const int xblocks = (g.Nx + FE_THREADS - 1) / FE_THREADS;
+    const int chunks = (g.Ny + FE_YCHUNK - 1) / FE_YCHUNK;
+    int ysplit = (int)std::min<long long>(chunks, std::max<long long>(1, (148LL * 8) / ((long long)xblocks * g.Nz)));
+    if (ysplit > 65535) ysplit = 65535;
+    const dim3 ge(xblocks, g.Nz, ysplit);
     SC_TRY(launch_e(g, ge, st, Ex, U, out, precision));
     SC_CUDA_TRY(cudaEventRecord(ctx->ev[4], st));
     count_launch(5);

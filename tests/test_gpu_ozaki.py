@@ -95,7 +95,7 @@ def crt_bits(k):
     """The engine's scale bits: floor((log2 P - 3 - log2 2k) / 2) with P the product of its 14 moduli."""
     import math
     P = math.prod([255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197])
-    return min(52, int((math.log2(P) - 3 - math.log2(2 * max(k, 1))) // 2))
+    return min(49, int((math.log2(P) - 3 - math.log2(2 * max(k, 1))) // 2))
 
 
 @pytest.mark.parametrize("m,n,k,batch", [(1, 1, 1, 1), (5, 3, 7, 2), (64, 256, 16, 1), (130, 70, 97, 3),
