@@ -428,12 +428,16 @@ sc_status sc_gpu_cw_evaluate(void* E_xy, void* E_xz, void* E_yz, float x_start, 
  * its error.  Inputs per pixel: n, the scaled wavelength, the coordinates and
  * the thin-element slab phase 2 pi n (1 um) / lambda as cos and sin (the
  * workload's slab is 1 um).  Width 64, 4 spectral layers, 16 x 16 modes; every linear map is
- * a BF16 tensor-core GEMM with FP32 accumulation; training is Adam on FP32
+ * a BF16 tensor-core GEMM (tcgen05) with FP32 accumulation; training is Adam on FP32
  * master weights.  All buffers are device pointers; batch <= max_batch. */
 typedef struct sc_fno sc_fno;
 sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long long seed);
 sc_status sc_fno_destroy(sc_fno* f);
 sc_status sc_fno_param_count(const sc_fno* f, long long* n);
+/* Synchronises the network's device and reports SC_CUDA_ERROR if any of its
+ * tensor-core GEMMs gave up on a pipeline wait since the last call (their
+ * results are then not valid); the other sc_fno_* calls are asynchronous. */
+sc_status sc_fno_status(sc_fno* f);
 /* direction 0: copy the parameters out to dev_params; 1: load them from it */
 sc_status sc_fno_params(sc_fno* f, void* dev_params, int direction, void* stream);
 /* maps: batch x 64 x 64 floats; lambdas: batch floats (um); out: batch x 1452 */

@@ -101,6 +101,7 @@ _SIGS = {
     "sc_fno_create": (c_int, [POINTER(c_void_p), c_int, c_int, ctypes.c_ulonglong]),
     "sc_fno_destroy": (c_int, [c_void_p]),
     "sc_fno_param_count": (c_int, [c_void_p, POINTER(c_longlong)]),
+    "sc_fno_status": (c_int, [c_void_p]),
     "sc_fno_params": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "sc_fno_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "sc_fno_loss_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),

@@ -19,8 +19,8 @@
 // Every linear map (lift, pointwise, the truncated DFT and its real inverse
 // as separable partial DFTs -- along y, then x; back along x, then y -- the
 // per-mode mixing, projections, readout) is one hand-written tensor-core GEMM: operands rounded to BF16 as they are staged,
-// mma.sync m16n8k16 with FP32 accumulation, FP32 in global memory, arbitrary
-// strides and batches.  Training: relative squared error per sample, Adam on
+// tcgen05.mma kind::f16 with FP32 accumulation in tensor memory, FP32 in global
+// memory, arbitrary strides and batches.  Training: relative squared error per sample, Adam on
 // FP32 master weights.
 #include <cmath>
 #include <cstdint>
@@ -31,6 +31,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace sc {
 namespace fno {
@@ -68,186 +69,183 @@ struct Gemm {
     long long sCm, sCn, sCb;
 };
 
-constexpr int TM = 64, TN = 64, TK = 32, GT = 128, PADK = 8;
+// Tile of the tensor-core GEMM: 128 rows (the TMEM lanes) x 64 columns,
+// staged 32 K values at a time.  Operands are FP32 in global memory, rounded
+// to BF16 as the CTA writes them into shared memory in the UMMA K-major
+// core-matrix layout (8 rows x 16 bytes per core matrix, LBO = 128 B along K,
+// SBO = 512 B between 8-row groups); one thread issues two tcgen05.mma
+// kind::f16 (BF16 x BF16 -> FP32, 128 x 64 x 16) per stage into a TMEM
+// accumulator; two shared-memory stages let the CTA convert and store the
+// next K slice while the tensor core consumes the current one (an mbarrier
+// per stage, signalled by tcgen05.commit).  The epilogue reads the
+// accumulator with tcgen05.ld and writes C with its strides.  Every wait is
+// bounded; a timeout sets the context's error word.
+constexpr int TM = 128, TN = 64, TK = 32, GT = 128;
+constexpr int UA_BYTES = TM * TK * 2, UB_BYTES = TN * TK * 2;   // 8 KB, 4 KB per stage
+constexpr uint32_t U_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                             ((uint32_t)(TM >> 4) << 24);      // F32 accumulate, A = B = BF16, K-major
 
-__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+// byte offset of (row, k) in a K-major BF16 core-matrix tile of TK = 32 columns
+__device__ __forceinline__ int uoff(int r, int kk) { return (r >> 3) * 512 + (kk >> 3) * 128 + (r & 7) * 16 + (kk & 7) * 2; }
+
+__device__ __forceinline__ uint64_t udesc(const void* p) {
+    return (uint64_t)((tc::smem_u32(p) >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) |
+           (1ULL << 46);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem), "l"(adesc),
+        "l"(bdesc), "r"(U_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ uint32_t bf2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
 
 // operand load modes: 0 scalar (any strides), 1 float4 along k (stride_k == 1),
 // 2 float4 along m / n (stride_m or stride_n == 1); the host picks a vector
 // mode only when the base is 16-byte aligned, the other stride is a multiple
 // of 4 and the contiguous extent is a multiple of 4
+template <int V, int R>
+struct Stager {
+    static constexpr int PER = R * TK / GT;   // values per thread
+    float v[PER];
+    __device__ __forceinline__ void load(const float* X, long long s_r, long long s_k, int rows, int kdim, int r0,
+                                         int k0, int tid) {
+        if constexpr (V == 0) {
+            const bool kf = (s_k == 1);
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int e = tid + GT * i;
+                const int r = kf ? e / TK : e % R, kk = kf ? e % TK : e / R;
+                const int gr = r0 + r, gk = k0 + kk;
+                v[i] = (gr < rows && gk < kdim) ? X[gr * s_r + gk * s_k] : 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < PER / 4; ++i) {
+                const int e = tid + GT * i;
+                const int r = (V == 1) ? e / (TK / 4) : (e % (R / 4)) * 4;
+                const int kk = (V == 1) ? (e % (TK / 4)) * 4 : e / (R / 4);
+                const int gr = r0 + r, gk = k0 + kk;
+                float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gr < rows && gk < kdim) x = *reinterpret_cast<const float4*>(X + gr * s_r + gk * s_k);
+                v[4 * i] = x.x;
+                v[4 * i + 1] = x.y;
+                v[4 * i + 2] = x.z;
+                v[4 * i + 3] = x.w;
+            }
+        }
+    }
+    __device__ __forceinline__ void store(unsigned char* tile, long long s_k, int tid) const {
+        if constexpr (V == 0) {
+            const bool kf = (s_k == 1);
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int e = tid + GT * i;
+                const int r = kf ? e / TK : e % R, kk = kf ? e % TK : e / R;
+                *reinterpret_cast<__nv_bfloat16*>(tile + uoff(r, kk)) = __float2bfloat16_rn(v[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < PER / 4; ++i) {
+                const int e = tid + GT * i;
+                const int r = (V == 1) ? e / (TK / 4) : (e % (R / 4)) * 4;
+                const int kk = (V == 1) ? (e % (TK / 4)) * 4 : e / (R / 4);
+                if (V == 1) {
+                    *reinterpret_cast<uint2*>(tile + uoff(r, kk)) =
+                        make_uint2(bf2(v[4 * i], v[4 * i + 1]), bf2(v[4 * i + 2], v[4 * i + 3]));
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        *reinterpret_cast<__nv_bfloat16*>(tile + uoff(r + q, kk)) = __float2bfloat16_rn(v[4 * i + q]);
+                }
+            }
+        }
+    }
+};
+
+// set by a tensor-core GEMM whose pipeline wait timed out; read and cleared by sc_fno_status
+__device__ int g_fno_err;
+
 template <int VA, int VB>
 __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
-    __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PADK];
-    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PADK];
+    __shared__ __align__(1024) unsigned char sm[2][UA_BYTES + UB_BYTES];
+    __shared__ __align__(8) uint64_t mma_bar[2], done_bar;
+    __shared__ uint32_t tmem_base;
     const int b = blockIdx.z;
     const float* A = g.A + b * g.sAb;
     const float* B = g.B + b * g.sBb;
     float* C = g.C + b * g.sCb;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 1, wn = warp >> 1;
-    const int gq = lane >> 2, tq = lane & 3;
-    float ra[TM * TK / GT], rb[TN * TK / GT];
-
-    auto load = [&](int k0) {
-        if constexpr (VA == 0) {
-            const bool kf = (g.sAk == 1);
-#pragma unroll
-            for (int i = 0; i < TM * TK / GT; ++i) {
-                const int e = tid + GT * i;
-                const int r = kf ? e / TK : e % TM, kk = kf ? e % TK : e / TM;
-                const int gm = m0 + r, gk = k0 + kk;
-                ra[i] = (gm < g.m && gk < g.k) ? A[gm * g.sAm + gk * g.sAk] : 0.f;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < TM * TK / GT / 4; ++i) {
-                const int e = tid + GT * i;
-                const int r = (VA == 1) ? e / (TK / 4) : (e % (TM / 4)) * 4;
-                const int kk = (VA == 1) ? (e % (TK / 4)) * 4 : e / (TM / 4);
-                const int gm = m0 + r, gk = k0 + kk;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (gm < g.m && gk < g.k) v = *reinterpret_cast<const float4*>(A + gm * g.sAm + gk * g.sAk);
-                ra[4 * i] = v.x;
-                ra[4 * i + 1] = v.y;
-                ra[4 * i + 2] = v.z;
-                ra[4 * i + 3] = v.w;
-            }
-        }
-        if constexpr (VB == 0) {
-            const bool kf = (g.sBk == 1);
-#pragma unroll
-            for (int i = 0; i < TN * TK / GT; ++i) {
-                const int e = tid + GT * i;
-                const int c = kf ? e / TK : e % TN, kk = kf ? e % TK : e / TN;
-                const int gn = n0 + c, gk = k0 + kk;
-                rb[i] = (gn < g.n && gk < g.k) ? B[gk * g.sBk + gn * g.sBn] : 0.f;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < TN * TK / GT / 4; ++i) {
-                const int e = tid + GT * i;
-                const int c = (VB == 1) ? e / (TK / 4) : (e % (TN / 4)) * 4;
-                const int kk = (VB == 1) ? (e % (TK / 4)) * 4 : e / (TN / 4);
-                const int gn = n0 + c, gk = k0 + kk;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (gn < g.n && gk < g.k) v = *reinterpret_cast<const float4*>(B + gk * g.sBk + gn * g.sBn);
-                rb[4 * i] = v.x;
-                rb[4 * i + 1] = v.y;
-                rb[4 * i + 2] = v.z;
-                rb[4 * i + 3] = v.w;
-            }
-        }
-    };
-    auto store = [&]() {
-        if constexpr (VA == 0) {
-            const bool kf = (g.sAk == 1);
-#pragma unroll
-            for (int i = 0; i < TM * TK / GT; ++i) {
-                const int e = tid + GT * i;
-                const int r = kf ? e / TK : e % TM, kk = kf ? e % TK : e / TM;
-                As[r][kk] = __float2bfloat16_rn(ra[i]);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < TM * TK / GT / 4; ++i) {
-                const int e = tid + GT * i;
-                const int r = (VA == 1) ? e / (TK / 4) : (e % (TM / 4)) * 4;
-                const int kk = (VA == 1) ? (e % (TK / 4)) * 4 : e / (TM / 4);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (VA == 1) As[r][kk + q] = __float2bfloat16_rn(ra[4 * i + q]);
-                    else As[r + q][kk] = __float2bfloat16_rn(ra[4 * i + q]);
-                }
-            }
-        }
-        if constexpr (VB == 0) {
-            const bool kf = (g.sBk == 1);
-#pragma unroll
-            for (int i = 0; i < TN * TK / GT; ++i) {
-                const int e = tid + GT * i;
-                const int c = kf ? e / TK : e % TN, kk = kf ? e % TK : e / TN;
-                Bs[c][kk] = __float2bfloat16_rn(rb[i]);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < TN * TK / GT / 4; ++i) {
-                const int e = tid + GT * i;
-                const int c = (VB == 1) ? e / (TK / 4) : (e % (TN / 4)) * 4;
-                const int kk = (VB == 1) ? (e % (TK / 4)) * 4 : e / (TN / 4);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (VB == 1) Bs[c][kk + q] = __float2bfloat16_rn(rb[4 * i + q]);
-                    else Bs[c + q][kk] = __float2bfloat16_rn(rb[4 * i + q]);
-                }
-            }
-        }
-    };
-
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-
-    const int nk = (g.k + TK - 1) / TK;
-    if (nk > 0) {
-        load(0);
-        store();
+    if (tid == 0) {
+        tc::mbar_init(&mma_bar[0], 1);
+        tc::mbar_init(&mma_bar[1], 1);
+        tc::mbar_init(&done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 64u);
+    tc::fence_before_sync();
     __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    Stager<VA, TM> sa;
+    Stager<VB, TN> sb;
+    const int nk = (g.k + TK - 1) / TK;
+    bool ok = true;
+    if (nk > 0) {
+        sa.load(A, g.sAm, g.sAk, g.m, g.k, m0, 0, tid);
+        sb.load(B, g.sBn, g.sBk, g.n, g.k, n0, 0, tid);
+    }
     for (int t = 0; t < nk; ++t) {
-        if (t + 1 < nk) load((t + 1) * TK);
-#pragma unroll
-        for (int ks = 0; ks < TK; ks += 16) {
-            uint32_t af[2][4], bf[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r0 = wm * 32 + i * 16 + gq;
-                af[i][0] = ld32(&As[r0][ks + 2 * tq]);
-                af[i][1] = ld32(&As[r0 + 8][ks + 2 * tq]);
-                af[i][2] = ld32(&As[r0][ks + 8 + 2 * tq]);
-                af[i][3] = ld32(&As[r0 + 8][ks + 8 + 2 * tq]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int c0 = wn * 32 + j * 8 + gq;
-                bf[j][0] = ld32(&Bs[c0][ks + 2 * tq]);
-                bf[j][1] = ld32(&Bs[c0][ks + 8 + 2 * tq]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-                        "{%8, %9}, {%0, %1, %2, %3};\n"
-                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                        : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bf[j][0]), "r"(bf[j][1]));
-        }
+        const int s = t & 1;
+        // the MMAs of K slice t - 2 read this stage: wait for them
+        if (t >= 2 && !tc::mbar_wait(&mma_bar[s], (uint32_t)(((t - 2) >> 1) & 1))) ok = false;
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        sa.store(sm[s], g.sAk, tid);
+        sb.store(sm[s] + UA_BYTES, g.sBk, tid);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint64_t da = udesc(sm[s]), db = udesc(sm[s] + UA_BYTES);
+            umma_bf16(tmem, da, db, t > 0 ? 1u : 0u);
+            umma_bf16(tmem, da + (256 >> 4), db + (256 >> 4), 1u);   // K 16..31: two core matrices on
+            tc::mma_commit(&mma_bar[s]);
+        }
         if (t + 1 < nk) {
-            store();
-            __syncthreads();
+            sa.load(A, g.sAm, g.sAk, g.m, g.k, m0, (t + 1) * TK, tid);
+            sb.load(B, g.sBn, g.sBk, g.n, g.k, n0, (t + 1) * TK, tid);
         }
     }
+    if (tid == 0) tc::mma_commit(&done_bar);
+    bool ready = ok && tc::mbar_wait(&done_bar, 0);
+    ready = __all_sync(0xffffffffu, ready);
+    if (!ready && lane == 0) atomicExch(&g_fno_err, 1);
+    tc::fence_after_sync();
+    const int gm = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < TN; c0 += 32) {
+        uint32_t r[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+        if (ready && gm < g.m) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int gm = m0 + wm * 32 + i * 16 + gq + ((q & 2) ? 8 : 0);
-                const int gn = n0 + wn * 32 + j * 8 + 2 * tq + (q & 1);
-                if (gm < g.m && gn < g.n) {
+            for (int q = 0; q < 32; ++q) {
+                const int gn = n0 + c0 + q;
+                if (gn < g.n) {
                     float* p = C + gm * g.sCm + gn * g.sCn;
-                    const float v = g.alpha * acc[i][j][q];
+                    const float v = g.alpha * __uint_as_float(r[q]);
                     *p = (g.beta == 0.f) ? v : fmaf(g.beta, *p, v);
                 }
             }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 64u);
 }
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
@@ -917,6 +915,24 @@ sc_status sc_fno_destroy(sc_fno* f) {
         if (f->X[l]) cudaFree(f->X[l]);
     }
     delete f;
+    return SC_OK;
+}
+
+sc_status sc_fno_status(sc_fno* f) {
+    if (!f) {
+        set_error("sc_fno_status: null network");
+        return SC_BADINPUT;
+    }
+    Guard gd(f->device);
+    SC_CUDA_TRY(cudaDeviceSynchronize());
+    int h = 0;
+    SC_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_fno_err, sizeof(int)));
+    if (h) {
+        const int zero = 0;
+        SC_CUDA_TRY(cudaMemcpyToSymbol(g_fno_err, &zero, sizeof(int)));
+        set_error("surrogate: a tensor-core GEMM pipeline wait timed out");
+        return SC_CUDA_ERROR;
+    }
     return SC_OK;
 }
 

@@ -156,6 +156,10 @@ class Surrogate:
     def _p(t):
         return ctypes.c_void_p(t.data_ptr())
 
+    def status(self):
+        """Synchronise and raise if a tensor-core GEMM of this network timed out since the last check."""
+        check(self.lib.sc_fno_status(self.h))
+
     def get_params(self) -> torch.Tensor:
         t = torch.empty(self.n_params, dtype=torch.float32, device="cuda")
         check(self.lib.sc_fno_params(self.h, self._p(t), 0, None))

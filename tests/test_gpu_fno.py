@@ -48,6 +48,7 @@ def test_forward_matches_oracle(net):
     net.set_params(w)
     maps, lams, _ = batch()
     got = net.forward(torch.from_numpy(maps).cuda(), torch.from_numpy(lams).cuda()).cpu().numpy()
+    net.status()
     ref = ofno.Net(w).forward(maps, lams)
     assert np.linalg.norm(got - ref) <= 5e-3 * np.linalg.norm(ref)
 
@@ -58,6 +59,7 @@ def test_gradients_match_oracle(net):
     maps, lams, tgt = batch(5)
     loss, grad = net.loss_grad(torch.from_numpy(maps).cuda(), torch.from_numpy(lams).cuda(),
                                torch.from_numpy(tgt).cuda())
+    net.status()
     rl, rg = ofno.Net(w).loss_grad(maps, lams, tgt)
     assert np.allclose(loss.cpu().numpy(), rl, rtol=5e-3)
     g = grad.cpu().numpy()
@@ -90,6 +92,7 @@ def test_training_lowers_loss(net, solved):
     first = float(fresh.train_step(dm, dl, dt, 1e-3).mean())
     for _ in range(150):
         last = float(fresh.train_step(dm, dl, dt, 1e-3).mean())
+    fresh.status()
     fresh.close()
     assert last < 0.2 * first, (first, last)
 
