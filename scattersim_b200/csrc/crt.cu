@@ -29,10 +29,11 @@
 // the UMMA K-major core-matrix layout (as the digit-sliced engine does for its
 // digit planes).  The MMA kernel is persistent (one CTA per SM); a CTA owns
 // output tiles of 128 rows of C' (64 complex rows) x 256 complex columns and
-// for each tile runs NMOD passes of the K loop: warp 0 streams 12 KB stages
-// (A 4 KB + B 8 KB) through a 16-slot ring with cp.async.bulk, warp 1 issues
-// one 128 x 256 x 32 MMA per stage into one of two 256-column TMEM
-// accumulators, and eight epilogue warps turn a finished accumulator into
+// for each tile runs NMOD passes of the K loop: warp 0 streams 48 KB stages
+// (four K steps: A 16 KB + B 32 KB, two bulk copies) through a 4-slot ring with
+// cp.async.bulk, warp 1 issues four 128 x 256 x 32 MMAs per stage (one commit
+// per stage: committing after every MMA serialised them) into one of two
+// 256-column TMEM accumulators, and eight epilogue warps turn a finished accumulator into
 // int8 residues (written to a per-CTA scratch slot that stays in L2) while the
 // MMAs of the next modulus run in the other accumulator.  After the last
 // modulus the epilogue warps rebuild the tile from the residues in FP64 and
@@ -56,8 +57,12 @@ constexpr int CRT_BN = 256;                  // complex columns per tile
 constexpr int CRT_BK = 32;                   // K' bytes per stage
 constexpr int CRT_ATILE = CRT_BM * CRT_BK;   // 4 KB
 constexpr int CRT_BTILE = CRT_BN * CRT_BK;   // 8 KB
-constexpr int CRT_STAGE = CRT_ATILE + CRT_BTILE;
-constexpr int CRT_NS = 16;                   // ring slots (192 KB)
+constexpr int CRT_STAGE = CRT_ATILE + CRT_BTILE;   // one K step (the probe's operands)
+constexpr int CRT_KSUB = 4;                  // K steps per ring stage: four MMAs per commit
+constexpr int CRT_SA = CRT_KSUB * CRT_ATILE;   // 16 KB: the stage's A tiles, consecutive in memory
+constexpr int CRT_SB = CRT_KSUB * CRT_BTILE;   // 32 KB
+constexpr int CRT_SLOT = CRT_SA + CRT_SB;      // 48 KB
+constexpr int CRT_NS = 4;                    // ring slots (192 KB)
 constexpr int CRT_EPI_WARPS = 8;
 constexpr int CRT_THREADS = 32 * (2 + CRT_EPI_WARPS);
 constexpr int CRT_SCRATCH = CRT_NMOD * CRT_BM * CRT_BN;   // residue bytes per CTA (448 KB)
@@ -348,7 +353,8 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                 for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
                     const int8_t* Ab = g.Aq + ((long long)b * CRT_NMOD + t) * planeA + (long long)rb * KB * CRT_ATILE;
                     const int8_t* Bb = g.Bq + ((long long)b * CRT_NMOD + t) * planeB + (long long)cb * KB * CRT_BTILE;
-                    for (int kb = 0; kb < KB; ++kb, ++stage) {
+                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
+                        const int nsub = min(CRT_KSUB, KB - kb);
                         const int slot = (int)(stage % CRT_NS);
                         if (stage >= CRT_NS && !tc::mbar_wait(&empty[slot], (uint32_t)(((stage / CRT_NS) - 1) & 1))) {
                             atomicExch(g.err, 11);
@@ -356,10 +362,11 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                             break;
                         }
                         if (*aborted) break;
-                        unsigned char* sa = smem_raw + (size_t)slot * CRT_STAGE;
-                        tc::mbar_expect_tx(&full[slot], (uint32_t)CRT_STAGE);
-                        tc::bulk_g2s(sa, Ab + (long long)kb * CRT_ATILE, (uint32_t)CRT_ATILE, &full[slot]);
-                        tc::bulk_g2s(sa + CRT_ATILE, Bb + (long long)kb * CRT_BTILE, (uint32_t)CRT_BTILE, &full[slot]);
+                        unsigned char* sa = smem_raw + (size_t)slot * CRT_SLOT;
+                        tc::mbar_expect_tx(&full[slot], (uint32_t)(nsub * CRT_STAGE));
+                        tc::bulk_g2s(sa, Ab + (long long)kb * CRT_ATILE, (uint32_t)(nsub * CRT_ATILE), &full[slot]);
+                        tc::bulk_g2s(sa + CRT_SA, Bb + (long long)kb * CRT_BTILE, (uint32_t)(nsub * CRT_BTILE),
+                                     &full[slot]);
                     }
                 }
             }
@@ -371,7 +378,7 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
         if (lane == 0) {
             // MMA issuer: accumulator unit u (tile, modulus) in buffer u & 1
             const uint64_t desc0 = tc::smem_desc(smem_raw);
-            const uint64_t slot_step = (uint64_t)(CRT_STAGE >> 4);
+            const uint64_t slot_step = (uint64_t)(CRT_SLOT >> 4);
             long long stage = 0, u = 0;
             for (int tile = blockIdx.x; tile < g.ntiles && !*aborted; tile += gridDim.x) {
                 for (int t = 0; t < CRT_NMOD && !*aborted; ++t, ++u) {
@@ -383,7 +390,8 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                     }
                     tc::fence_after_sync();
                     const uint32_t acc = tmem + (uint32_t)(buf * CRT_BN);
-                    for (int kb = 0; kb < KB; ++kb, ++stage) {
+                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
+                        const int nsub = min(CRT_KSUB, KB - kb);
                         const int slot = (int)(stage % CRT_NS);
                         if (!tc::mbar_wait(&full[slot], (uint32_t)((stage / CRT_NS) & 1))) {
                             atomicExch(g.err, 13);
@@ -392,8 +400,10 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
                         }
                         tc::fence_after_sync();
                         const uint64_t da = desc0 + (uint64_t)slot * slot_step;
-                        const uint64_t db = da + (uint64_t)(CRT_ATILE >> 4);
-                        tc::mma_i8<CRT_IDESC>(acc, da, db, kb > 0 ? 1u : 0u);
+                        const uint64_t db = da + (uint64_t)(CRT_SA >> 4);
+                        for (int j = 0; j < nsub; ++j)
+                            tc::mma_i8<CRT_IDESC>(acc, da + (uint64_t)(j * (CRT_ATILE >> 4)),
+                                                  db + (uint64_t)(j * (CRT_BTILE >> 4)), (kb + j) > 0 ? 1u : 0u);
                         tc::mma_commit(&empty[slot]);
                     }
                     if (*aborted) break;
@@ -583,7 +593,7 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
     if (dev >= 0 && dev < 64 && !g_crt_const_ready[dev]) {
         SC_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &host_const, sizeof(CrtConst)));
         SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         CRT_NS * CRT_STAGE + 1024));
+                                         CRT_NS * CRT_SLOT + 1024));
         g_crt_const_ready[dev] = true;
     }
     int sms = 148;
@@ -654,7 +664,7 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
             const double macs = (double)CRT_NMOD * nb * (double)RB * CRT_BM * (double)CB * CRT_BN * (double)KB * CRT_BK;
             SC_TRY(ws.mark_begin(st, 2, 8.0 * g.m * (double)g.n * g.k * nb, 2.0 * macs, &mark));
         }
-        crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_STAGE + 1024, st>>>(a);
+        crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_SLOT + 1024, st>>>(a);
         count_launch();
         if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark));
         SC_CHECK_LAUNCH("crt mma");
