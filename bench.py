@@ -553,7 +553,7 @@ def run_sweep_ours(args):
     # ---- one instrumented step: per-launch GEMM timing for the roofline (not in the headline)
     ctx.kernel_timing(True)
     _, instr_ms = timed(lambda: solve_share(MIXED))
-    kst = ctx.kernel_stats()
+    kst = ctx.kernel_stats_ex()
     ctx.kernel_timing(False)
 
     # ---- batched FP64, same step count (one warm-up for its own GEMM shapes)
@@ -624,33 +624,36 @@ def run_sweep_ours(args):
     peaks = _peaks()
     fp64_peak = ctx.fp64_peak_tflops()
     int8_peak_meas = ctx.int8_peak_tops() if hasattr(ctx, "int8_peak_tops") else None
-    d8, dd = kst["int8"], kst["dmma"]
-    if d8["ms"] >= dd["ms"]:
-        # the larger of the int8 probe and twice the measured BF16 burst peak (int8 dense is twice BF16
-        # dense on B200), so that a weak probe cannot flatter the fraction
-        bf16x2 = 2.0 * float(peaks.get("bf16_tflops", 1590.0))
-        if int8_peak_meas and int8_peak_meas >= bf16x2:
-            int8_peak, src = int8_peak_meas, ("int8 tcgen05 MMA probe measured in this run (128 x 256 x 32, "
-                                              "operands resident in shared memory, no loads)")
-        else:
-            int8_peak, src = bf16x2, "2 x measured bf16 dense burst peak (MEASURED_PEAKS.json)"
-        achieved = d8["int8_ops"] / (d8["ms"] / 1e3) / 1e12
-        tr = None
+    d8, dd, dc, dcg = kst["int8"], kst["dmma"], kst["crt"], kst["crt_gemm"]
+    # the larger of the int8 probe and twice the measured BF16 burst peak (int8 dense is twice BF16
+    # dense on B200), so that a weak probe cannot flatter the fraction
+    bf16x2 = 2.0 * float(peaks.get("bf16_tflops", 1590.0))
+    if int8_peak_meas and int8_peak_meas >= bf16x2:
+        int8_peak, src = int8_peak_meas, ("int8 tcgen05 MMA probe measured in this run (128 x 256 x 32, "
+                                          "operands resident in shared memory, no loads)")
+    else:
+        int8_peak, src = bf16x2, "2 x measured bf16 dense burst peak (MEASURED_PEAKS.json)"
+    dom = max((("int8", d8), ("crt", dc), ("dmma", dd)), key=lambda kv: kv[1]["ms"])[0]
+    if dom in ("int8", "crt"):
+        st_ = d8 if dom == "int8" else dc
+        achieved = st_["int8_ops"] / (st_["ms"] / 1e3) / 1e12
+        tr, tr_src = None, None
+        rec_name = "int8_gemm_traffic.json" if dom == "int8" else "crt_gemm_traffic.json"
         try:
-            with open(os.path.join(ROOT, "profiles", "int8_gemm_traffic.json")) as f:
+            with open(os.path.join(ROOT, "profiles", rec_name)) as f:
                 rec = json.load(f)
-            tr = rec["bytes_per_fp64_flop"] * d8["flops"] / max(d8["launches"], 1)
+            tr = rec["bytes_per_fp64_flop"] * st_["flops"] / max(st_["launches"], 1)
+            tr_src = (f"ncu dram bytes of one capture ({rec['case']}), scaled by FP64-equivalent flops per "
+                      f"launch (profiles/{rec_name})")
         except Exception:
             pass
+        name = ("oz_mma_kernel (int8 tcgen05 MMA, 7 digit slices, TMEM accumulators)" if dom == "int8" else
+                "crt_mma_kernel (int8 tcgen05 MMA, 14 moduli, persistent 128x256 tiles, TMEM accumulators)")
         roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS (int8)",
-                    "frac": achieved / int8_peak, "traffic": tr,
-                    "kernel": "oz_mma_kernel (int8 tcgen05 MMA, 7 digit slices, TMEM accumulators)",
-                    "peak_source": src,
-                    "launches": int(d8["launches"]), "avg_launch_ms": d8["ms"] / max(d8["launches"], 1),
-                    "fp64_equivalent_tflops": d8["flops"] / (d8["ms"] / 1e3) / 1e12,
-                    "fp64_peak_tflops": fp64_peak,
-                    "traffic_source": "ncu dram bytes of one 1250^3 x 8 capture, scaled by FP64-equivalent "
-                                      "flops per launch (profiles/int8_gemm_traffic.json)"}
+                    "frac": achieved / int8_peak, "traffic": tr, "kernel": name, "peak_source": src,
+                    "launches": int(st_["launches"]), "avg_launch_ms": st_["ms"] / max(st_["launches"], 1),
+                    "fp64_equivalent_tflops": st_["flops"] / (st_["ms"] / 1e3) / 1e12,
+                    "fp64_peak_tflops": fp64_peak, "traffic_source": tr_src}
     else:
         achieved = dd["flops"] / (dd["ms"] / 1e3) / 1e12
         roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
@@ -658,8 +661,13 @@ def run_sweep_ours(args):
                     "kernel": "zgemm_kernel (FP64 mma.sync m8n8k4 complex GEMM)",
                     "peak_source": "FP64 FMA probe measured in this run",
                     "launches": int(dd["launches"]), "avg_launch_ms": dd["ms"] / max(dd["launches"], 1)}
+    # the modular engine's whole products (exponents, packing, MMA kernel) enclose its MMA marks
+    roofline["crt_whole_product_ms_per_step"] = dcg["ms"]
+    roofline["crt_mma_ms_per_step"] = dc["ms"]
+    if dcg["ms"] > 0:
+        roofline["crt_whole_product_fp64_equivalent_tflops"] = dcg["flops"] / (dcg["ms"] / 1e3) / 1e12
     roofline["instrumented_step_ms"] = instr_ms
-    roofline["gemm_time_share"] = (d8["ms"] + dd["ms"]) / (instr_ms or 1.0)
+    roofline["gemm_time_share"] = (d8["ms"] + dd["ms"] + dcg["ms"]) / (instr_ms or 1.0)
     roofline["int8_ms_per_step"] = d8["ms"]
     roofline["fp64_tile_ms_per_step"] = dd["ms"]
 

@@ -145,8 +145,11 @@ __device__ __forceinline__ int sym_res(int x) {
 // split into 17-bit limbs U0 + 2^17 U1 + 2^34 U2
 template <int P>
 __device__ __forceinline__ int sym_res_wide(int U0, int U1, int U2) {
-    constexpr int c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
-    return sym_res<P>(U2 * c34 + U1 * c17 + U0 - c50);
+    constexpr unsigned c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
+    // u = U - 2^50 = U2 2^34 + U1 2^17 + U0 - 2^50 == v (mod P) with v >= 0 (< 2^26), unsigned remainder
+    const unsigned v = (unsigned)U2 * c34 + (unsigned)U1 * c17 + (unsigned)U0 + (unsigned)(P - c50);
+    const int r = (int)(v % (unsigned)P);
+    return r > P / 2 ? r - P : r;
 }
 
 // x (|x| < 2^50, any double) rounded to the nearest integer and returned as
@@ -238,42 +241,39 @@ __global__ void __launch_bounds__(128) crt_pack_a_kernel(int m, int k, const dou
     for_each_mod(one);
 }
 
-// B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB]; a thread takes one
-// column c and 16 complex rows (32 K' bytes: both core matrices along K)
+// B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB]; a block covers
+// half a tile (128 columns), a thread one column and 8 complex rows (one
+// 16-byte core-matrix row per modulus)
 __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const double2* __restrict__ B,
                                                          const double2* const* Bp, int ldb, long long sB,
                                                          const int* __restrict__ colexp, int be, int CB, int KB,
                                                          int8_t* __restrict__ out) {
     const int b = blockIdx.z;
-    const int cb = blockIdx.x, kb = blockIdx.y;
+    const int cb = blockIdx.x >> 1, kb = blockIdx.y;
     const double2* bb = Bp ? Bp[b] : B + b * sB;
-    const int cl = threadIdx.x;
-    const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2);
-    int lx[32][3];
+    const int cl = (blockIdx.x & 1) * 128 + (threadIdx.x & 127), jc = threadIdx.x >> 7;
+    const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2) + 8 * jc;
+    int lx[16][3];
     const int ex = (c < n) ? colexp[(long long)b * n + c] : 0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < 8; ++q) {
         double2 v = make_double2(0.0, 0.0);
         if (c < n && j0 + q < k) v = bb[(long long)c * ldb + j0 + q];
         round_limbs(scale2(v.x, be - ex), lx[2 * q][0], lx[2 * q][1], lx[2 * q][2]);
         round_limbs(scale2(v.y, be - ex), lx[2 * q + 1][0], lx[2 * q + 1][1], lx[2 * q + 1][2]);
     }
-    const int o0 = tc::tile_off(cl, 0), o1 = tc::tile_off(cl, 16);
+    const int o = tc::tile_off(cl, 16 * jc);
     const long long plane = (long long)CB * KB * CRT_BTILE;
     int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)cb * KB + kb) * CRT_BTILE;
     auto one = [&](auto tag) {
         constexpr int T = decltype(tag)::value;
         constexpr int P = crt_mod(T);
-        int d[32];
+        int d[16];
 #pragma unroll
-        for (int q = 0; q < 32; ++q) d[q] = sym_res_wide<P>(lx[q][0], lx[q][1], lx[q][2]);
-        int8_t* pl = base + (long long)T * plane;
-        *reinterpret_cast<uint4*>(pl + o0) = make_uint4(pack4(d[0], d[1], d[2], d[3]), pack4(d[4], d[5], d[6], d[7]),
-                                                       pack4(d[8], d[9], d[10], d[11]),
-                                                       pack4(d[12], d[13], d[14], d[15]));
-        *reinterpret_cast<uint4*>(pl + o1) =
-            make_uint4(pack4(d[16], d[17], d[18], d[19]), pack4(d[20], d[21], d[22], d[23]),
-                       pack4(d[24], d[25], d[26], d[27]), pack4(d[28], d[29], d[30], d[31]));
+        for (int q = 0; q < 16; ++q) d[q] = sym_res_wide<P>(lx[q][0], lx[q][1], lx[q][2]);
+        *reinterpret_cast<uint4*>(base + (long long)T * plane + o) =
+            make_uint4(pack4(d[0], d[1], d[2], d[3]), pack4(d[4], d[5], d[6], d[7]), pack4(d[8], d[9], d[10], d[11]),
+                       pack4(d[12], d[13], d[14], d[15]));
     };
     for_each_mod(one);
 }
@@ -631,7 +631,7 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         if (g.Bp) h.Bp = g.Bp + b0; else h.B = g.B + (long long)b0 * g.sB;
         crt_pack_a_kernel<<<dim3(RB, KB, nb), 128, 0, st>>>(g.m, g.k, h.A, h.Ap, g.lda, g.sA,
                                                            rowexp + (size_t)b0 * g.m, bits, RB, KB, Aq);
-        crt_pack_b_kernel<<<dim3(CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
+        crt_pack_b_kernel<<<dim3(2 * CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
                                                            colexp + (size_t)b0 * g.n, bits, CB, KB, Bq);
         count_launch(2);
         SC_CHECK_LAUNCH("crt pack");
