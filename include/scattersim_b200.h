@@ -274,7 +274,8 @@ sc_status sc_kernel_stats(sc_context* ctx, double* out8);
 sc_status sc_kernel_stats_ex(sc_context* ctx, double* out, int classes);
 
 /* The GEMM autotuner's choices on this context, as 6-int records (m, n, k,
- * batch, slices, variant: 0/1 FP64 tile of 64/128 rows, 2 int8 engine).
+ * batch, slices, variant: 0/1 FP64 tile of 64/128 rows, 2 digit-sliced int8
+ * engine, 3 modular int8 engine).
  * sc_gemm_choices_get writes up to cap records and returns their count in
  * *count; sc_gemm_choices_set replaces the table, so that a later run (a
  * profiler replay, say) makes the same choices without timing them again. */

@@ -482,7 +482,7 @@ sc_status sc_gemm_choices_set(sc_context* ctx, const int* rec, int count) {
         return SC_BADINPUT;
     }
     for (int i = 0; i < count; ++i)
-        if (rec[6 * i + 5] < 0 || rec[6 * i + 5] > 2) {
+        if (rec[6 * i + 5] < 0 || rec[6 * i + 5] > 3) {
             set_error("sc_gemm_choices_set: record %d has unknown variant %d", i, rec[6 * i + 5]);
             return SC_BADINPUT;
         }
