@@ -1247,7 +1247,7 @@ def run_surrogate_ours(args):
 #   gemm          batched complex GEMM throughput at the shapes of the solves
 #   gemm_int8     one int8 digit-sliced GEMM shape (1250^3 x 8) at 7 then 4 slices,
 #                 twice each (the profiling case of the tcgen05 MMA kernel)
-#   gemm_crt [m n k batch reps]  the modular int8 engine (default 1250^3 x 8): time of
+#   gemm_crt [m n k batch reps tiles]  the modular int8 engine (default 1250^3 x 8): time of
 #                 the whole product and of its MMA kernel, error against the FP64 tile
 #   layer [N]     scatterlayer's default stack (4 layers) under an N x N polar beam
 #                 (default 1024: 1,048,576 waves) and a 15-layer stack under a
@@ -1291,7 +1291,7 @@ def run_case(argv):
     if name == "gemm_int8":
         return gemm_int8_case()
     if name == "gemm_crt":
-        return gemm_crt_case(*[int(a) for a in argv[1:6]])
+        return gemm_crt_case(*[int(a) for a in argv[1:7]])
     if name == "layer":
         return layer_case(int(argv[1]) if len(argv) > 1 else 1024)
     if name in ("sweep", "sweep_plain", "sweep_mixed"):
@@ -1451,14 +1451,16 @@ def gemm_int8_case():
     return 0
 
 
-def gemm_crt_case(m=1250, n=1250, k=1250, batch=8, reps=3):
+def gemm_crt_case(m=1250, n=1250, k=1250, batch=8, reps=3, tiles=0):
     """The modular int8 engine on one shape (default 1250^3 x 8, the sweep's largest layer-factor products):
-    FP64-equivalent TFLOP/s of the whole product and of its MMA kernel, int8 TOPS, error vs the FP64 tile."""
+    FP64-equivalent TFLOP/s of the whole product and of its MMA kernel, int8 TOPS, error vs the FP64 tile.
+    tiles: 1 = 256 x 256 tiles on CTA pairs, 0 = 128 x 256 tiles on one CTA."""
     import ctypes
     import torch
     from scattersim_b200 import solver
     from scattersim_b200._lib import check
     ctx = solver.Context(0)
+    ctx.crt_tiles(tiles)
     A = torch.randn(batch, k, m, dtype=torch.complex128, device="cuda")
     B = torch.randn(batch, n, k, dtype=torch.complex128, device="cuda")
     C = torch.empty(batch, n, m, dtype=torch.complex128, device="cuda")
@@ -1478,7 +1480,7 @@ def gemm_crt_case(m=1250, n=1250, k=1250, batch=8, reps=3):
     ctx.kernel_timing(False)
     err = float((C - R).abs().max() / R.abs().max())
     fl = 8.0 * m * n * k * batch * reps
-    print(f"gemm_crt m={m} n={n} k={k} batch={batch}: whole product {st['crt_gemm']['ms'] / reps:.3f} ms "
+    print(f"gemm_crt m={m} n={n} k={k} batch={batch} tiles={'256x256 pair' if tiles else '128x256'}: whole product {st['crt_gemm']['ms'] / reps:.3f} ms "
           f"({fl / (st['crt_gemm']['ms'] / 1e3) / 1e12:.1f} FP64-eq TFLOP/s), MMA kernel "
           f"{st['crt']['ms'] / reps:.3f} ms ({st['crt']['int8_ops'] / (st['crt']['ms'] / 1e3) / 1e12:.0f} int8 TOPS, "
           f"{fl / (st['crt']['ms'] / 1e3) / 1e12:.1f} FP64-eq), max error vs FP64 tile {err:.2e}")

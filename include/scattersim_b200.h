@@ -144,6 +144,10 @@ sc_status sc_zgemm_emulated_batched(sc_context* ctx, int slices, int m, int n, i
 sc_status sc_zgemm_crt_batched(sc_context* ctx, int m, int n, int k, const double* alpha, const void* A, int lda,
                                long long strideA, const void* B, int ldb, long long strideB, const double* beta,
                                void* C, int ldc, long long strideC, int batch, void* stream);
+/* Output tiles of the modular engine's MMA kernel, for this context: 0 (the
+ * default) = 128 x 256 tiles on one CTA, 1 = 256 x 256 tiles on clusters of
+ * two CTAs (tcgen05 cta_group::2).  Both give bit-identical results. */
+sc_status sc_crt_tiles_set(sc_context* ctx, int mode);
 
 /* --------------------------------------------------------- volume solve */
 

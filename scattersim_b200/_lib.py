@@ -114,6 +114,7 @@ _SIGS = {
     "sc_fp64_peak_probe": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_fp64_dmma_probe": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_int8_peak_probe": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_crt_tiles_set": (c_int, [c_void_p, c_int]),
     "sc_qr_stats": (c_int, [c_void_p, POINTER(c_longlong), c_int]),
     "sc_volume_waves": (c_int, [c_void_p, POINTER(VolumeParams), c_int, c_int, c_int, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_int, POINTER(c_longlong), POINTER(c_int), POINTER(c_int),

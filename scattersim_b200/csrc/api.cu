@@ -598,6 +598,15 @@ sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops) {
     return fp64_probe(ctx, true, tflops);
 }
 
+sc_status sc_crt_tiles_set(sc_context* ctx, int mode) {
+    if (!ctx || (mode != 0 && mode != 1)) {
+        set_error("sc_crt_tiles_set: mode must be 0 or 1");
+        return SC_BADINPUT;
+    }
+    ctx->ws.crt_tiles = mode;
+    return SC_OK;
+}
+
 sc_status sc_int8_peak_probe(sc_context* ctx, double* tops) {
     if (!ctx || !tops) {
         set_error("sc_int8_peak_probe: null argument");

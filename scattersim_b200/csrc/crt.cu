@@ -241,13 +241,15 @@ __global__ void __launch_bounds__(128) crt_pack_a_kernel(int m, int k, const dou
     for_each_mod(one);
 }
 
-// B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB]; a block covers
-// half a tile (128 columns), a thread one column and 8 complex rows (one
-// 16-byte core-matrix row per modulus)
+// B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB] of 256 columns, or
+// with `halves` [b][p][2 cb + h][kb][4 KB] of 128 columns (each CTA of a pair
+// then loads its half of a 256-column tile as one contiguous run); a block
+// covers 128 columns, a thread one column and 8 complex rows (one 16-byte
+// core-matrix row per modulus)
 __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const double2* __restrict__ B,
                                                          const double2* const* Bp, int ldb, long long sB,
                                                          const int* __restrict__ colexp, int be, int CB, int KB,
-                                                         int8_t* __restrict__ out) {
+                                                         int halves, int8_t* __restrict__ out) {
     const int b = blockIdx.z;
     const int cb = blockIdx.x >> 1, kb = blockIdx.y;
     const double2* bb = Bp ? Bp[b] : B + b * sB;
@@ -262,9 +264,10 @@ __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const dou
         round_limbs(scale2(v.x, be - ex), lx[2 * q][0], lx[2 * q][1], lx[2 * q][2]);
         round_limbs(scale2(v.y, be - ex), lx[2 * q + 1][0], lx[2 * q + 1][1], lx[2 * q + 1][2]);
     }
-    const int o = tc::tile_off(cl, 16 * jc);
+    const int o = tc::tile_off(halves ? (cl & 127) : cl, 16 * jc);
     const long long plane = (long long)CB * KB * CRT_BTILE;
-    int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)cb * KB + kb) * CRT_BTILE;
+    int8_t* base = out + (long long)b * CRT_NMOD * plane +
+                   (halves ? ((long long)blockIdx.x * KB + kb) * (CRT_BTILE / 2) : ((long long)cb * KB + kb) * CRT_BTILE);
     auto one = [&](auto tag) {
         constexpr int T = decltype(tag)::value;
         constexpr int P = crt_mod(T);
@@ -313,6 +316,91 @@ __device__ __forceinline__ double crt_value(const int (&r)[CRT_NMOD]) {
     const double dm = fma(-q, c_crt.Pm, sm);
     const double dl = fma(-q, c_crt.Pl, sl);
     return fma(dh, 0x1p74, fma(dm, 0x1p37, dl));
+}
+
+// One CTA's epilogue for one output tile: 128 rows of C' (its TMEM lanes; warp
+// w reads lane quarter w % 4, and the two warps of a quarter split the 256
+// columns) for each modulus pass: wait for the accumulator, reduce it to int8
+// residues in the CTA's scratch (which stays in L2) and hand the accumulator
+// back; then rebuild the rows from the residues in FP64 and write C.  rb is
+// the 128-row tile, cb the 256-column tile; u counts accumulator uses.
+// Returns false when a wait gave up (the error word is then set).
+template <typename WaitFull, typename Release>
+__device__ __forceinline__ bool crt_epilogue_tile(const CrtArgs& g, uint32_t tmem, int8_t* scr, int rb, int cb, int b,
+                                                  long long& u, volatile int* aborted, WaitFull wait_full,
+                                                  Release release) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ew = warp - 2;
+    const int quarter = warp & 3;
+    const int half = ew >> 2;
+    const int row = quarter * 32 + lane;                 // row of C' in the tile
+    for (int t = 0; t < CRT_NMOD; ++t, ++u) {
+        const int buf = (int)(u & 1);
+        bool ready = !*aborted && wait_full(buf, (uint32_t)((u >> 1) & 1));
+        ready = __all_sync(0xffffffffu, ready);
+        if (!ready) {
+            if (lane == 0 && !*aborted) atomicExch(g.err, 14);
+            return false;
+        }
+        tc::fence_after_sync();
+        int8_t* dst = scr + ((long long)t * CRT_BM + row) * CRT_BN;
+        auto extract = [&](auto tag) {
+            constexpr int P = crt_mod(decltype(tag)::value);
+#pragma unroll 1
+            for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+                uint32_t r[32];
+                tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * CRT_BN + c0), r);
+                uint32_t w[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    w[q] = pack4(sym_res<P>((int)r[4 * q]), sym_res<P>((int)r[4 * q + 1]),
+                                 sym_res<P>((int)r[4 * q + 2]), sym_res<P>((int)r[4 * q + 3]));
+                *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
+            }
+        };
+        with_mod(t, extract);
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) release(buf);
+    }
+    __syncwarp();
+    // rebuild this warp's rows x columns from the residues (this thread wrote them)
+    const int rowp = rb * CRT_BM + row;
+    const int i = rowp >> 1;
+    const bool im = rowp & 1;
+    double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
+    const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
+    const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
+    const int ex = (i < g.m) ? g.rowexp[(long long)b * g.m + i] : 0;
+#pragma unroll 1
+    for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
+        uint4 rv[CRT_NMOD];
+#pragma unroll
+        for (int t = 0; t < CRT_NMOD; ++t)
+            rv[t] = *reinterpret_cast<const uint4*>(scr + ((long long)t * CRT_BM + row) * CRT_BN + c0);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            int r[CRT_NMOD];
+#pragma unroll
+            for (int t = 0; t < CRT_NMOD; ++t) {
+                const uint32_t word = (q < 4) ? rv[t].x : (q < 8) ? rv[t].y : (q < 12) ? rv[t].z : rv[t].w;
+                r[t] = (int)(int8_t)(word >> (8 * (q & 3)));
+            }
+            const int c = cb * CRT_BN + c0 + q;
+            const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
+            const double v = scale2(crt_value(r), ex + fx - g.shift);
+            const double o = __shfl_xor_sync(0xffffffffu, v, 1);
+            if (!im && i < g.m && c < g.n) {
+                double2* pc = C + (long long)c * g.ldc + i;
+                double2 val = cmul(alpha, make_double2(v, o));
+                if (!beta_zero) val = cfma(g.beta, *pc, val);
+                *pc = val;
+            }
+        }
+    }
+    __syncwarp();
+    return true;
 }
 
 __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
@@ -412,85 +500,17 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
             }
         }
     } else {
-        // epilogue warps: TMEM lane quarter (hardware: warp % 4) and column half
-        const int ew = warp - 2;
-        const int quarter = warp & 3;
-        const int half = ew >> 2;
-        const int row = quarter * 32 + lane;                 // row of C' in the tile
+        // epilogue warps
         int8_t* scr = g.scratch + (long long)blockIdx.x * CRT_SCRATCH;
+        auto wait_full = [&](int buf, uint32_t parity) { return tc::mbar_wait(&accfull[buf], parity); };
+        auto release = [&](int buf) { tc::mbar_arrive(&accempty[buf]); };
         long long u = 0;
         for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
             const int cb = tile % g.CB, rb = (tile / g.CB) % g.RB, b = tile / (g.CB * g.RB);
-            bool ok = true;
-            for (int t = 0; t < CRT_NMOD; ++t, ++u) {
-                const int buf = (int)(u & 1);
-                bool ready = !*aborted && tc::mbar_wait(&accfull[buf], (uint32_t)((u >> 1) & 1));
-                ready = __all_sync(0xffffffffu, ready);
-                if (!ready) {
-                    if (lane == 0 && !*aborted) atomicExch(g.err, 14);
-                    *aborted = 1;
-                    ok = false;
-                    break;
-                }
-                tc::fence_after_sync();
-                int8_t* dst = scr + ((long long)t * CRT_BM + row) * CRT_BN;
-                auto extract = [&](auto tag) {
-                    constexpr int P = crt_mod(decltype(tag)::value);
-#pragma unroll 1
-                    for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
-                        uint32_t r[32];
-                        tc::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * CRT_BN + c0), r);
-                        uint32_t w[8];
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            w[q] = pack4(sym_res<P>((int)r[4 * q]), sym_res<P>((int)r[4 * q + 1]),
-                                         sym_res<P>((int)r[4 * q + 2]), sym_res<P>((int)r[4 * q + 3]));
-                        *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
-                        *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
-                    }
-                };
-                with_mod(t, extract);
-                tc::fence_before_sync();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&accempty[buf]);
+            if (!crt_epilogue_tile(g, tmem, scr, rb, cb, b, u, aborted, wait_full, release)) {
+                *aborted = 1;
+                break;
             }
-            if (!ok) break;
-            __syncwarp();
-            // rebuild this warp's rows x columns from the residues (this thread wrote them)
-            const int rowp = rb * CRT_BM + row;
-            const int i = rowp >> 1;
-            const bool im = rowp & 1;
-            double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
-            const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
-            const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
-            const int ex = (i < g.m) ? g.rowexp[(long long)b * g.m + i] : 0;
-#pragma unroll 1
-            for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
-                uint4 rv[CRT_NMOD];
-#pragma unroll
-                for (int t = 0; t < CRT_NMOD; ++t)
-                    rv[t] = *reinterpret_cast<const uint4*>(scr + ((long long)t * CRT_BM + row) * CRT_BN + c0);
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    int r[CRT_NMOD];
-#pragma unroll
-                    for (int t = 0; t < CRT_NMOD; ++t) {
-                        const uint32_t word = (q < 4) ? rv[t].x : (q < 8) ? rv[t].y : (q < 12) ? rv[t].z : rv[t].w;
-                        r[t] = (int)(int8_t)(word >> (8 * (q & 3)));
-                    }
-                    const int c = cb * CRT_BN + c0 + q;
-                    const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
-                    const double v = scale2(crt_value(r), ex + fx - g.shift);
-                    const double o = __shfl_xor_sync(0xffffffffu, v, 1);
-                    if (!im && i < g.m && c < g.n) {
-                        double2* pc = C + (long long)c * g.ldc + i;
-                        double2 val = cmul(alpha, make_double2(v, o));
-                        if (!beta_zero) val = cfma(g.beta, *pc, val);
-                        *pc = val;
-                    }
-                }
-            }
-            __syncwarp();
         }
     }
     tc::fence_before_sync();
@@ -498,7 +518,188 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
     if (warp == 0) tc::tmem_dealloc(tmem, 512u);
 }
 
+// ---------------------------------------------------------------- CTA-pair MMA kernel
+// The same product with 256 x 256 output tiles on a cluster of two CTAs
+// (tcgen05 cta_group::2): the even CTA's MMA thread issues 256 x 256 x 32
+// MMAs whose A rows 0-127 and B columns 0-127 come from its own shared memory
+// and A rows 128-255 and B columns 128-255 from the odd CTA's, at the same
+// offsets; each CTA's TMEM receives its 128 rows.  Per SM and K step a CTA
+// stages 4 KB of A and 4 KB of B for 128 x 256 multiply-adds (the single-CTA
+// tile stages 4 + 8 KB), so the L2 -> shared-memory traffic that feeds the
+// tensor pipe drops by a third, and the 32 KB stages allow a six-deep ring.
+// Both CTAs load their halves with plain bulk copies (no multicast) on their
+// own barrier; the odd CTA's MMA warp relays each landed stage to the even
+// CTA (a remote mbarrier arrive), whose MMA thread waits for both.  The MMA
+// thread's commits arrive on the barriers of both CTAs (two commits, one per
+// CTA).  Each CTA's epilogue warps drain its own TMEM rows exactly as in the
+// single-CTA kernel and release the accumulator on the even CTA's barrier.
+// Every wait is bounded and also gives up once either CTA has aborted; a CTA
+// that aborts raises the other's flag through distributed shared memory.
+constexpr int C2_BTILE = CRT_BTILE / 2;             // 128 columns x 32 K bytes
+constexpr int C2_SA = CRT_KSUB * CRT_ATILE;         // 16 KB
+constexpr int C2_SB = CRT_KSUB * C2_BTILE;          // 16 KB
+constexpr int C2_SLOT = C2_SA + C2_SB;              // 32 KB
+constexpr int C2_NS = 6;                            // ring slots (192 KB)
+constexpr uint32_t C2_IDESC = tc::idesc_i8(2 * CRT_BM, CRT_BN);
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_mma2_kernel(CrtArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[C2_NS], pfull[C2_NS], empty[C2_NS], accfull[2], accempty[2], done;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    volatile int* aborted = &abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = tc::cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = (int)(blockIdx.x >> 1), npairs = (int)(gridDim.x >> 1);
+    const int KB = g.KB, RB2 = g.RB >> 1;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < C2_NS; ++q) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&pfull[q], 1);
+            tc::mbar_init(&empty[q], 1);
+        }
+        for (int q = 0; q < 2; ++q) {
+            tc::mbar_init(&accfull[q], 1);
+            tc::mbar_init(&accempty[q], 2 * CRT_EPI_WARPS);
+        }
+        tc::mbar_init(&done, 1);
+        *aborted = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc2(&tmem_base, 512u);
+    tc::fence_before_sync();
+    tc::cluster_sync();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    const uint32_t peer_abort = tc::peer_addr(&abort_flag, rank ^ 1u);
+    auto abort_pair = [&](int code) {
+        if (!*aborted) atomicExch(g.err, code);
+        *aborted = 1;
+        tc::st_remote_u32(peer_abort, 1u);
+    };
+    // bounded wait that also gives up when either CTA has aborted
+    auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+        if (tc::mbar_try_cluster(bar, parity)) return true;
+        const unsigned long long t0 = tc::globaltimer_ns();
+        for (long long it = 0; it < tc::TC_SPIN; ++it) {
+            if (tc::mbar_try_cluster(bar, parity)) return true;
+            if (*aborted || tc::globaltimer_ns() - t0 > tc::TC_TIMEOUT_NS) return false;
+        }
+        return false;
+    };
+    const long long planeA = (long long)g.RB * KB * CRT_ATILE;
+    const long long planeB = (long long)g.CB * KB * CRT_BTILE;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer (both CTAs): this CTA's 128 rows of A and 128 columns of B
+            long long stage = 0;
+            for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
+                const int cb = tile % g.CB, rb2 = (tile / g.CB) % RB2, b = tile / (g.CB * RB2);
+                const int rb = 2 * rb2 + (int)rank, cbh = 2 * cb + (int)rank;
+                for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
+                    const int8_t* Ab = g.Aq + ((long long)b * CRT_NMOD + t) * planeA + (long long)rb * KB * CRT_ATILE;
+                    const int8_t* Bb = g.Bq + ((long long)b * CRT_NMOD + t) * planeB + (long long)cbh * KB * C2_BTILE;
+                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
+                        const int nsub = min(CRT_KSUB, KB - kb);
+                        const int slot = (int)(stage % C2_NS);
+                        if (stage >= C2_NS && !wait(&empty[slot], (uint32_t)(((stage / C2_NS) - 1) & 1))) {
+                            abort_pair(21);
+                            break;
+                        }
+                        unsigned char* sa = smem_raw + (size_t)slot * C2_SLOT;
+                        tc::mbar_expect_tx(&full[slot], (uint32_t)(nsub * (CRT_ATILE + C2_BTILE)));
+                        tc::bulk_g2s(sa, Ab + (long long)kb * CRT_ATILE, (uint32_t)(nsub * CRT_ATILE), &full[slot]);
+                        tc::bulk_g2s(sa + C2_SA, Bb + (long long)kb * C2_BTILE, (uint32_t)(nsub * C2_BTILE),
+                                     &full[slot]);
+                    }
+                }
+            }
+            // drain: this CTA's copies in flight must land before it exits
+            for (long long s2 = (stage > C2_NS ? stage - C2_NS : 0); s2 < stage; ++s2)
+                tc::mbar_wait(&full[s2 % C2_NS], (uint32_t)((s2 / C2_NS) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // MMA issuer of the pair
+            const uint64_t desc0 = tc::smem_desc(smem_raw);
+            const uint64_t slot_step = (uint64_t)(C2_SLOT >> 4);
+            long long stage = 0, u = 0;
+            for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
+                for (int t = 0; t < CRT_NMOD && !*aborted; ++t, ++u) {
+                    const int buf = (int)(u & 1);
+                    if (u >= 2 && !wait(&accempty[buf], (uint32_t)(((u >> 1) - 1) & 1))) {
+                        abort_pair(22);
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t acc = tmem + (uint32_t)(buf * CRT_BN);
+                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
+                        const int nsub = min(CRT_KSUB, KB - kb);
+                        const int slot = (int)(stage % C2_NS);
+                        const uint32_t par = (uint32_t)((stage / C2_NS) & 1);
+                        if (!wait(&full[slot], par) || !wait(&pfull[slot], par)) {
+                            abort_pair(23);
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        const uint64_t da = desc0 + (uint64_t)slot * slot_step;
+                        const uint64_t db = da + (uint64_t)(C2_SA >> 4);
+                        for (int j = 0; j < nsub; ++j)
+                            tc::mma2_i8<C2_IDESC>(acc, da + (uint64_t)(j * (CRT_ATILE >> 4)),
+                                                  db + (uint64_t)(j * (C2_BTILE >> 4)), (kb + j) > 0 ? 1u : 0u);
+                        tc::mma2_commit(tc::smem_u32(&empty[slot]));
+                        tc::mma2_commit(tc::peer_addr(&empty[slot], 1u));
+                    }
+                    if (*aborted) break;
+                    tc::mma2_commit(tc::smem_u32(&accfull[buf]));
+                    tc::mma2_commit(tc::peer_addr(&accfull[buf], 1u));
+                }
+            }
+            // every MMA issued must have completed before either CTA releases its TMEM or shared memory
+            tc::mma2_commit(tc::smem_u32(&done));
+            if (!tc::mbar_wait(&done, 0)) atomicExch(g.err, 25);
+        } else if (lane == 0) {
+            // relay (odd CTA): tell the MMA thread when this CTA's half of a stage has landed
+            long long stage = 0;
+            for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
+                for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
+                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
+                        const int slot = (int)(stage % C2_NS);
+                        if (!wait(&full[slot], (uint32_t)((stage / C2_NS) & 1))) {
+                            abort_pair(24);
+                            break;
+                        }
+                        tc::mbar_arrive_remote(tc::peer_addr(&pfull[slot], 0u));
+                    }
+                }
+            }
+        }
+    } else {
+        // epilogue warps: this CTA's 128 rows of each 256-row tile
+        int8_t* scr = g.scratch + (long long)blockIdx.x * CRT_SCRATCH;
+        auto wait_full = [&](int buf, uint32_t parity) { return wait(&accfull[buf], parity); };
+        auto release = [&](int buf) { tc::mbar_arrive_remote(tc::peer_addr(&accempty[buf], 0u)); };
+        long long u = 0;
+        for (int tile = pair; tile < g.ntiles; tile += npairs) {
+            const int cb = tile % g.CB, rb2 = (tile / g.CB) % RB2, b = tile / (g.CB * RB2);
+            if (!crt_epilogue_tile(g, tmem, scr, 2 * rb2 + (int)rank, cb, b, u, aborted, wait_full, release)) {
+                if (lane == 0) abort_pair(14);
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    tc::fence_before_sync();
+    tc::cluster_sync();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_dealloc2(tmem, 512u);
+}
+
 bool g_crt_const_ready[64] = {};
+int g_crt_pairs[64] = {};
 
 // int8 tensor-core throughput probe: one CTA per SM issues `iters` MMAs of
 // 128 x 256 x 32 (the modular engine's shape) on operands resident in shared
@@ -570,9 +771,10 @@ sc_status int8_peak_probe(int device, Workspace& ws, double* tops) {
     return SC_OK;
 }
 
-// packed bytes of the residue operands per batch entry
+// packed bytes of the residue operands per batch entry (row tiles rounded up
+// to an even count, as the CTA-pair kernel needs)
 size_t crt_packed_bytes(int m, int n, int k) {
-    const long long RB = (2LL * m + CRT_BM - 1) / CRT_BM, CB = ((long long)n + CRT_BN - 1) / CRT_BN,
+    const long long RB = 2 * ((2LL * m + 2 * CRT_BM - 1) / (2 * CRT_BM)), CB = ((long long)n + CRT_BN - 1) / CRT_BN,
                     KB = (2LL * k + CRT_BK - 1) / CRT_BK;
     return (size_t)CRT_NMOD * (size_t)KB * ((size_t)RB * CRT_ATILE + (size_t)CB * CRT_BTILE);
 }
@@ -594,13 +796,26 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         SC_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &host_const, sizeof(CrtConst)));
         SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          CRT_NS * CRT_SLOT + 1024));
+        SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         C2_NS * C2_SLOT + 1024));
+        // clusters of two that fit on the device at once (SMs left without a
+        // partner in their GPC cannot hold one): the pair kernel's grid
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2, 1, 1);
+        cfg.blockDim = dim3(CRT_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = C2_NS * C2_SLOT + 1024;
+        int ncl = 0;
+        SC_CUDA_TRY(cudaOccupancyMaxActiveClusters(&ncl, crt_mma2_kernel, &cfg));
+        g_crt_pairs[dev] = ncl;
         g_crt_const_ready[dev] = true;
     }
     int sms = 148;
     SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bits = crt_bits(g.k, host_const.log2P);
-    const int RB = (2 * g.m + CRT_BM - 1) / CRT_BM, CB = (g.n + CRT_BN - 1) / CRT_BN,
-              KB = (2 * g.k + CRT_BK - 1) / CRT_BK;
+    const int npairs = (dev >= 0 && dev < 64) ? g_crt_pairs[dev] : 0;
+    const bool pair = ws.crt_tiles != 0 && npairs > 0;
+    const int RB = pair ? 2 * ((2 * g.m + 2 * CRT_BM - 1) / (2 * CRT_BM)) : (2 * g.m + CRT_BM - 1) / CRT_BM,
+              CB = (g.n + CRT_BN - 1) / CRT_BN, KB = (2 * g.k + CRT_BK - 1) / CRT_BK;
     if (RB > 65535 || KB > 65535) {
         set_error("zgemm_crt: grid too large");
         return SC_BADINPUT;
@@ -632,7 +847,8 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         crt_pack_a_kernel<<<dim3(RB, KB, nb), 128, 0, st>>>(g.m, g.k, h.A, h.Ap, g.lda, g.sA,
                                                            rowexp + (size_t)b0 * g.m, bits, RB, KB, Aq);
         crt_pack_b_kernel<<<dim3(2 * CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
-                                                           colexp + (size_t)b0 * g.n, bits, CB, KB, Bq);
+                                                           colexp + (size_t)b0 * g.n, bits, CB, KB, pair ? 1 : 0,
+                                                           Bq);
         count_launch(2);
         SC_CHECK_LAUNCH("crt pack");
         CrtArgs a;
@@ -643,7 +859,7 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         a.CB = CB;
         a.KB = KB;
         a.batch = nb;
-        a.ntiles = nb * RB * CB;
+        a.ntiles = nb * (pair ? RB / 2 : RB) * CB;
         a.shift = 2 * bits;
         a.Aq = Aq;
         a.Bq = Bq;
@@ -658,13 +874,19 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         a.sC = g.sC;
         a.scratch = scratch;
         a.err = err;
-        const int grid = std::min(a.ntiles, sms);
         size_t mark = 0;
         if (ws.time_kernels) {
             const double macs = (double)CRT_NMOD * nb * (double)RB * CRT_BM * (double)CB * CRT_BN * (double)KB * CRT_BK;
             SC_TRY(ws.mark_begin(st, 2, 8.0 * g.m * (double)g.n * g.k * nb, 2.0 * macs, &mark));
         }
-        crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_SLOT + 1024, st>>>(a);
+        if (pair) {
+            // two CTAs per tile; never more CTAs than SMs (the scratch holds one slot per SM)
+            const int grid = 2 * std::min(a.ntiles, std::min(npairs, sms / 2));
+            crt_mma2_kernel<<<grid, CRT_THREADS, C2_NS * C2_SLOT + 1024, st>>>(a);
+        } else {
+            const int grid = std::min(a.ntiles, sms);
+            crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_SLOT + 1024, st>>>(a);
+        }
         count_launch();
         if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark));
         SC_CHECK_LAUNCH("crt mma");

@@ -67,6 +67,9 @@ struct Gemm {
     long long sBk, sBn, sBb;
     float* C;
     long long sCm, sCn, sCb;
+    // split-K: batch entry b, K chunk s (of kchunk values) writes output entry
+    // b * ksplit + s; ksplit = 1 is the plain batched product
+    int ksplit = 1, kchunk = 0;
 };
 
 // Tile of the tensor-core GEMM: 128 rows (the TMEM lanes) x 64 columns,
@@ -104,65 +107,54 @@ __device__ __forceinline__ uint32_t bf2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// operand load modes: 0 scalar (any strides), 1 float4 along k (stride_k == 1),
-// 2 float4 along m / n (stride_m or stride_n == 1); the host picks a vector
-// mode only when the base is 16-byte aligned, the other stride is a multiple
-// of 4 and the contiguous extent is a multiple of 4
+// operand load modes: 1 float4 along k (stride_k == 1; the host picks it only
+// when the base is 16-byte aligned, the row and batch strides are multiples of
+// 4 and k is), otherwise scalar loads (0: any strides, 2: the row index
+// contiguous, where the scalar loads of a warp coalesce).  A thread stages
+// 16-byte units, one row x 8 K values each; consecutive threads take
+// consecutive rows, so a warp's loads in mode 2 read contiguous rows and its
+// 16-byte shared-memory stores (8 consecutive rows of a core matrix, 128 B)
+// are free of bank conflicts.
 template <int V, int R>
 struct Stager {
-    static constexpr int PER = R * TK / GT;   // values per thread
-    float v[PER];
+    static constexpr int U = R * (TK / 8) / GT;   // units per thread
+    float v[U][8];
     __device__ __forceinline__ void load(const float* X, long long s_r, long long s_k, int rows, int kdim, int r0,
                                          int k0, int tid) {
-        if constexpr (V == 0) {
-            const bool kf = (s_k == 1);
 #pragma unroll
-            for (int i = 0; i < PER; ++i) {
-                const int e = tid + GT * i;
-                const int r = kf ? e / TK : e % R, kk = kf ? e % TK : e / R;
-                const int gr = r0 + r, gk = k0 + kk;
-                v[i] = (gr < rows && gk < kdim) ? X[gr * s_r + gk * s_k] : 0.f;
-            }
-        } else {
+        for (int i = 0; i < U; ++i) {
+            const int u = tid + GT * i;
+            const int r = u % R, o = u / R;
+            const int gr = r0 + r, gk = k0 + 8 * o;
+            if constexpr (V == 1) {
+                float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+                if (gr < rows) {
+                    const float* p = X + gr * s_r + gk;
+                    if (gk < kdim) x0 = *reinterpret_cast<const float4*>(p);
+                    if (gk + 4 < kdim) x1 = *reinterpret_cast<const float4*>(p + 4);
+                }
+                v[i][0] = x0.x;
+                v[i][1] = x0.y;
+                v[i][2] = x0.z;
+                v[i][3] = x0.w;
+                v[i][4] = x1.x;
+                v[i][5] = x1.y;
+                v[i][6] = x1.z;
+                v[i][7] = x1.w;
+            } else {
 #pragma unroll
-            for (int i = 0; i < PER / 4; ++i) {
-                const int e = tid + GT * i;
-                const int r = (V == 1) ? e / (TK / 4) : (e % (R / 4)) * 4;
-                const int kk = (V == 1) ? (e % (TK / 4)) * 4 : e / (R / 4);
-                const int gr = r0 + r, gk = k0 + kk;
-                float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (gr < rows && gk < kdim) x = *reinterpret_cast<const float4*>(X + gr * s_r + gk * s_k);
-                v[4 * i] = x.x;
-                v[4 * i + 1] = x.y;
-                v[4 * i + 2] = x.z;
-                v[4 * i + 3] = x.w;
+                for (int j = 0; j < 8; ++j)
+                    v[i][j] = (gr < rows && gk + j < kdim) ? X[gr * s_r + (long long)(gk + j) * s_k] : 0.f;
             }
         }
     }
-    __device__ __forceinline__ void store(unsigned char* tile, long long s_k, int tid) const {
-        if constexpr (V == 0) {
-            const bool kf = (s_k == 1);
+    __device__ __forceinline__ void store(unsigned char* tile, int tid) const {
 #pragma unroll
-            for (int i = 0; i < PER; ++i) {
-                const int e = tid + GT * i;
-                const int r = kf ? e / TK : e % R, kk = kf ? e % TK : e / R;
-                *reinterpret_cast<__nv_bfloat16*>(tile + uoff(r, kk)) = __float2bfloat16_rn(v[i]);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < PER / 4; ++i) {
-                const int e = tid + GT * i;
-                const int r = (V == 1) ? e / (TK / 4) : (e % (R / 4)) * 4;
-                const int kk = (V == 1) ? (e % (TK / 4)) * 4 : e / (R / 4);
-                if (V == 1) {
-                    *reinterpret_cast<uint2*>(tile + uoff(r, kk)) =
-                        make_uint2(bf2(v[4 * i], v[4 * i + 1]), bf2(v[4 * i + 2], v[4 * i + 3]));
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        *reinterpret_cast<__nv_bfloat16*>(tile + uoff(r + q, kk)) = __float2bfloat16_rn(v[4 * i + q]);
-                }
-            }
+        for (int i = 0; i < U; ++i) {
+            const int u = tid + GT * i;
+            const int r = u % R, o = u / R;
+            *reinterpret_cast<uint4*>(tile + uoff(r, 8 * o)) =
+                make_uint4(bf2(v[i][0], v[i][1]), bf2(v[i][2], v[i][3]), bf2(v[i][4], v[i][5]), bf2(v[i][6], v[i][7]));
         }
     }
 };
@@ -175,10 +167,12 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
     __shared__ __align__(1024) unsigned char sm[2][UA_BYTES + UB_BYTES];
     __shared__ __align__(8) uint64_t mma_bar[2], done_bar;
     __shared__ uint32_t tmem_base;
-    const int b = blockIdx.z;
-    const float* A = g.A + b * g.sAb;
-    const float* B = g.B + b * g.sBb;
-    float* C = g.C + b * g.sCb;
+    const int z = blockIdx.z;
+    const int b = z / g.ksplit, kbeg = (z - b * g.ksplit) * g.kchunk;
+    const int kdim = min(g.k - kbeg, g.kchunk);
+    const float* A = g.A + b * g.sAb + (long long)kbeg * g.sAk;
+    const float* B = g.B + b * g.sBb + (long long)kbeg * g.sBk;
+    float* C = g.C + z * g.sCb;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -194,11 +188,11 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
     const uint32_t tmem = tmem_base;
     Stager<VA, TM> sa;
     Stager<VB, TN> sb;
-    const int nk = (g.k + TK - 1) / TK;
+    const int nk = kdim > 0 ? (kdim + TK - 1) / TK : 0;
     bool ok = true;
     if (nk > 0) {
-        sa.load(A, g.sAm, g.sAk, g.m, g.k, m0, 0, tid);
-        sb.load(B, g.sBn, g.sBk, g.n, g.k, n0, 0, tid);
+        sa.load(A, g.sAm, g.sAk, g.m, kdim, m0, 0, tid);
+        sb.load(B, g.sBn, g.sBk, g.n, kdim, n0, 0, tid);
     }
     for (int t = 0; t < nk; ++t) {
         const int s = t & 1;
@@ -206,8 +200,8 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
         if (t >= 2 && !tc::mbar_wait(&mma_bar[s], (uint32_t)(((t - 2) >> 1) & 1))) ok = false;
         ok = __syncthreads_and(ok);
         if (!ok) break;
-        sa.store(sm[s], g.sAk, tid);
-        sb.store(sm[s] + UA_BYTES, g.sBk, tid);
+        sa.store(sm[s], tid);
+        sb.store(sm[s] + UA_BYTES, tid);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -218,8 +212,8 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
             tc::mma_commit(&mma_bar[s]);
         }
         if (t + 1 < nk) {
-            sa.load(A, g.sAm, g.sAk, g.m, g.k, m0, (t + 1) * TK, tid);
-            sb.load(B, g.sBn, g.sBk, g.n, g.k, n0, (t + 1) * TK, tid);
+            sa.load(A, g.sAm, g.sAk, g.m, kdim, m0, (t + 1) * TK, tid);
+            sb.load(B, g.sBn, g.sBk, g.n, kdim, n0, (t + 1) * TK, tid);
         }
     }
     if (tid == 0) tc::mma_commit(&done_bar);
@@ -228,17 +222,59 @@ __global__ void __launch_bounds__(GT) bf16_gemm_kernel(Gemm g) {
     if (!ready && lane == 0) atomicExch(&g_fno_err, 1);
     tc::fence_after_sync();
     const int gm = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < TN; c0 += 32) {
-        uint32_t r[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-        if (ready && gm < g.m) {
+    if (g.sCn == 1 && g.sCm != 1) {
+        // row-contiguous C: a thread's TMEM row goes through shared memory (the
+        // operand stages are free: every MMA has completed) so that a warp
+        // writes whole rows, 32 columns at a time; [128][33] floats, padded
+        // against bank conflicts
+        float* T = reinterpret_cast<float*>(&sm[0][0]);
+        const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && (g.sCm % 4 == 0);
+        for (int c0 = 0; c0 < TN; c0 += 32) {
+            uint32_t r[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+            __syncthreads();   // the previous half's rows have been written out
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                const int gn = n0 + c0 + q;
-                if (gn < g.n) {
-                    float* p = C + gm * g.sCm + gn * g.sCn;
-                    const float v = g.alpha * __uint_as_float(r[q]);
-                    *p = (g.beta == 0.f) ? v : fmaf(g.beta, *p, v);
+            for (int q = 0; q < 32; ++q) T[(warp * 32 + lane) * 33 + q] = nk > 0 ? g.alpha * __uint_as_float(r[q]) : 0.f;
+            __syncthreads();
+            if (ready) {
+                // thread t: rows t / 8 + 16 i, columns 4 (t % 8) .. + 3
+                const int cq = 4 * (tid & 7);
+                const int gn = n0 + c0 + cq;
+#pragma unroll 4
+                for (int i = 0; i < 8; ++i) {
+                    const int rr = (tid >> 3) + 16 * i;
+                    const int row = m0 + rr;
+                    if (row >= g.m) continue;
+                    const float* t = T + rr * 33 + cq;
+                    float* p = C + row * g.sCm + gn;
+                    if (vec && gn + 3 < g.n) {
+                        float4 v = make_float4(t[0], t[1], t[2], t[3]);
+                        if (g.beta != 0.f) {
+                            const float4 o = *reinterpret_cast<const float4*>(p);
+                            v = make_float4(fmaf(g.beta, o.x, v.x), fmaf(g.beta, o.y, v.y), fmaf(g.beta, o.z, v.z),
+                                            fmaf(g.beta, o.w, v.w));
+                        }
+                        *reinterpret_cast<float4*>(p) = v;
+                    } else {
+                        for (int q = 0; q < 4; ++q)
+                            if (gn + q < g.n) p[q] = (g.beta == 0.f) ? t[q] : fmaf(g.beta, p[q], t[q]);
+                    }
+                }
+            }
+        }
+    } else {
+        for (int c0 = 0; c0 < TN; c0 += 32) {
+            uint32_t r[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+            if (ready && gm < g.m) {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int gn = n0 + c0 + q;
+                    if (gn < g.n) {
+                        float* p = C + gm * g.sCm + gn * g.sCn;
+                        const float v = nk > 0 ? g.alpha * __uint_as_float(r[q]) : 0.f;
+                        *p = (g.beta == 0.f) ? v : fmaf(g.beta, *p, v);
+                    }
                 }
             }
         }
@@ -264,13 +300,38 @@ void launch_gemm(dim3 grid, cudaStream_t st, const Gemm& g) {
     bf16_gemm_kernel<VA, VB><<<grid, GT, 0, st>>>(g);
 }
 
-sc_status gemm(cudaStream_t st, const Gemm& g) {
-    if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return SC_OK;
-    if (g.batch > 65535 || (g.n + TN - 1) / TN > 65535) {
+sc_status gemm(cudaStream_t st, const Gemm& g0) {
+    if (g0.m <= 0 || g0.n <= 0 || g0.batch <= 0) return SC_OK;
+    // the tile has 128 rows (TMEM lanes) and 64 columns: when n > m (the
+    // network's products are mostly 64- or 12-row by thousands of columns)
+    // compute C^T = B^T A^T so that the long dimension fills the rows
+    // (and, for square shapes, when C is row-contiguous: the epilogue's
+    // stores then run along the rows a warp covers)
+    Gemm g = g0;
+    if (g0.n > g0.m || (g0.n == g0.m && g0.sCn == 1 && g0.sCm != 1)) {
+        g.m = g0.n;
+        g.n = g0.m;
+        g.A = g0.B;
+        g.sAm = g0.sBn;
+        g.sAk = g0.sBk;
+        g.sAb = g0.sBb;
+        g.B = g0.A;
+        g.sBn = g0.sAm;
+        g.sBk = g0.sAk;
+        g.sBb = g0.sAb;
+        g.sCm = g0.sCn;
+        g.sCn = g0.sCm;
+    }
+    if (g.ksplit < 1 || (g.ksplit > 1 && g.k % (g.ksplit * TK) != 0)) {
+        set_error("fno gemm: split-K needs k a multiple of 32 x ksplit");
+        return SC_BADINPUT;
+    }
+    g.kchunk = g.k / g.ksplit;
+    if ((long long)g.batch * g.ksplit > 65535 || (g.n + TN - 1) / TN > 65535) {
         set_error("fno gemm: grid too large");
         return SC_BADINPUT;
     }
-    dim3 grid((g.m + TM - 1) / TM, (g.n + TN - 1) / TN, g.batch);
+    dim3 grid((g.m + TM - 1) / TM, (g.n + TN - 1) / TN, g.batch * g.ksplit);
     const int va = vec_mode(g.A, g.sAm, g.sAk, g.batch > 1 ? g.sAb : 0, g.m, g.k);
     const int vb = vec_mode(g.B, g.sBn, g.sBk, g.batch > 1 ? g.sBb : 0, g.n, g.k);
     switch (va * 3 + vb) {
@@ -339,6 +400,7 @@ __global__ void gelu_back_kernel(float* __restrict__ g, const float* __restrict_
 // samples b = s, s + NSPL, ... and all pixels of g[b][c][p] (one CTA each),
 // then db[c] += sum_s partial[c][s] in order
 constexpr int NSPL = 32;
+constexpr int KSPLIT = 8;              // K chunks of the per-sample weight gradients (K = NP)
 __global__ void bias_grad_part_kernel(const float* __restrict__ g, int C, int Bn, float* __restrict__ part) {
     __shared__ float red[8];
     const int c = blockIdx.x, sp = blockIdx.y;
@@ -363,13 +425,30 @@ __global__ void bias_grad_sum_kernel(const float* __restrict__ part, int C, floa
     db[c] += t;
 }
 
-// out[i] += sum_b part[b][i]
-__global__ void batch_sum_kernel(const float* __restrict__ part, int Bn, long long n, float* __restrict__ out) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        float s = 0.f;
-        for (int b = 0; b < Bn; ++b) s += part[(long long)b * n + t];
-        out[t] += s;
+// out[i] += sum_r part[r][i] over R partials (per sample and K chunk): a block
+// of 8 warps per 32 outputs, lanes along i (coalesced), warps splitting r,
+// then a fixed-order sum across the warps (deterministic)
+__global__ void __launch_bounds__(256) batch_sum_kernel(const float* __restrict__ part, int R, long long n,
+                                                        float* __restrict__ out) {
+    __shared__ float red[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long i = blockIdx.x * 32LL + lane;
+    float s = 0.f;
+    if (i < n)
+        for (int r = w; r < R; r += 8) s += part[(long long)r * n + i];
+    red[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && i < n) {
+        float t = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t += red[q][lane];
+        out[i] += t;
     }
+}
+sc_status batch_sum(cudaStream_t st, const float* part, int R, long long n, float* out) {
+    batch_sum_kernel<<<(unsigned)((n + 31) / 32), 256, 0, st>>>(part, R, n, out);
+    count_launch();
+    return SC_OK;
 }
 
 // readout: P[b][12][242] (cos | sin correlations) -> pred[b][6][121][re, im]
@@ -576,6 +655,13 @@ Gemm mk(int m, int n, int k, int batch, float alpha, float beta, const float* A,
         long long sCn, long long sCb) {
     return Gemm{m, n, k, batch, alpha, beta, A, sAm, sAk, sAb, B, sBk, sBn, sBb, C, sCm, sCn, sCb};
 }
+// the weight gradients contract over the 4096 pixels of one sample: split K
+// into KSPLIT chunks (one partial per sample and chunk, summed by batch_sum),
+// so that the product runs on Bn x KSPLIT CTAs instead of Bn
+Gemm ksplit(Gemm g) {
+    g.ksplit = KSPLIT;
+    return g;
+}
 
 // forward pass for Bn samples; keeps every activation for the backward pass
 sc_status forward(sc_fno* f, const float* maps, const float* lam, int Bn, cudaStream_t st) {
@@ -663,20 +749,18 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     SC_TRY(gemm(st, mk(COUT, NP, 2 * NORD, Bn, 1.f, 0.f, f->dP, 2 * NORD, 1, (long long)COUT * 2 * NORD, f->R, 1,
                        2 * NORD, 0, f->do12, NP, 1, so)));
     // Q2, bQ2: per-sample partials, then summed over the batch
-    SC_TRY(gemm(st, mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
-                       (long long)COUT * HID)));
-    batch_sum_kernel<<<blocks((long long)COUT * HID), 256, 0, st>>>(f->part, Bn, (long long)COUT * HID, g + Ly.Q2);
+    SC_TRY(gemm(st, ksplit(mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
+                              (long long)COUT * HID))));
+    SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)COUT * HID, g + Ly.Q2));
     bias_grad(st, f->do12, COUT, Bn, g + Ly.bQ2, f->bpart);
-    count_launch();   // batch_sum_kernel
     // dh_b = Q2^T do12_b, through GELU
     SC_TRY(gemm(st, mk(HID, NP, COUT, Bn, 1.f, 0.f, w + Ly.Q2, 1, HID, 0, f->do12, NP, 1, so, f->dh, NP, 1, sh)));
     gelu_back_kernel<<<blocks((long long)Bn * sh), 256, 0, st>>>(f->dh, f->hpre, (long long)Bn * sh);
     count_launch();
-    SC_TRY(gemm(st, mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
-                       (long long)HID * W)));
-    batch_sum_kernel<<<blocks((long long)HID * W), 256, 0, st>>>(f->part, Bn, (long long)HID * W, g + Ly.Q1);
+    SC_TRY(gemm(st, ksplit(mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
+                              (long long)HID * W))));
+    SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)HID * W, g + Ly.Q1));
     bias_grad(st, f->dh, HID, Bn, g + Ly.bQ1, f->bpart);
-    count_launch();   // batch_sum_kernel
     // dv4 = Q1^T dh
     SC_TRY(gemm(st, mk(W, NP, HID, Bn, 1.f, 0.f, w + Ly.Q1, 1, W, 0, f->dh, NP, 1, sh, f->dact, NP, 1, sv)));
     for (int l = L - 1; l >= 0; --l) {
@@ -689,9 +773,9 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
         bias_grad(st, du, W, Bn, g + Ly.bl[l], f->bpart);
         const float* vin = f->act[l];
         // W_l
-        SC_TRY(gemm(st, mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1, (long long)W * W)));
-        batch_sum_kernel<<<blocks((long long)W * W), 256, 0, st>>>(f->part, Bn, (long long)W * W, g + Ly.Wl[l]);
-        count_launch();
+        SC_TRY(gemm(st, ksplit(mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1,
+                                  (long long)W * W))));
+        SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)W * W, g + Ly.Wl[l]));
         // dv_l = W_l^T du
         SC_TRY(gemm(st, mk(W, NP, W, Bn, 1.f, 0.f, w + Ly.Wl[l], 1, W, 0, du, NP, 1, sv, f->dv, NP, 1, sv)));
         // adjoint of the inverse transform: dZ[x][ky'][channel] = du Gy^T (batched over
@@ -734,11 +818,10 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
         std::swap(f->dact, f->dv);
     }
     // lift
-    SC_TRY(gemm(st, mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part, CIN,
-                       1, (long long)W * CIN)));
-    batch_sum_kernel<<<blocks((long long)W * CIN), 256, 0, st>>>(f->part, Bn, (long long)W * CIN, g + Ly.P);
+    SC_TRY(gemm(st, ksplit(mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part,
+                              CIN, 1, (long long)W * CIN))));
+    SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)W * CIN, g + Ly.P));
     bias_grad(st, f->dact, W, Bn, g + Ly.bP, f->bpart);
-    count_launch();   // batch_sum_kernel
     SC_CHECK_LAUNCH("fno backward");
     return SC_OK;
 }
@@ -879,7 +962,7 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->do12, B * COUT * NP);
     A(&f->dP, B * COUT * 2 * NORD);
     A(&f->dpred, B * NOUT);
-    A(&f->part, B * (long long)HID * W);
+    A(&f->part, B * (long long)KSPLIT * HID * W);
     A(&f->loss, B);
     A(&f->bpart, (long long)HID * NSPL);
     if (s == SC_OK) {

@@ -37,6 +37,8 @@ struct Workspace {
     // tensor-pipe tiles, class 1: int8 tcgen05 MMA kernel): event pairs on the
     // launching stream, summed by sc_kernel_stats after the stream has drained
     bool time_kernels = false;
+    // modular engine's MMA kernel: 0 = one CTA per 128 x 256 tile, 1 = CTA pairs with 256 x 256 tiles
+    int crt_tiles = 0;
     struct KernelMark {
         int cls;
         double flops;      // FP64-equivalent flops of the product (8 m n k per batch entry)

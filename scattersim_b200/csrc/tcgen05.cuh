@@ -9,6 +9,15 @@ namespace sc {
 namespace tc {
 
 constexpr long long TC_SPIN = 1LL << 24;
+// and at most this long: one try_wait may suspend the thread for a
+// hardware-defined time, so the poll count alone does not bound the wait
+constexpr unsigned long long TC_TIMEOUT_NS = 4000000000ULL;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
 
 // byte offset of (row, kk) inside one K-major core-matrix tile of 32 K bytes:
 // core matrices of 8 rows x 16 bytes, the two along K 128 B apart (LBO), the
@@ -40,10 +49,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: false after TC_SPIN polls
+// bounded wait: false after TC_SPIN polls or TC_TIMEOUT_NS
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (long long it = 0; it < TC_SPIN; ++it)
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (long long it = 0; it < TC_SPIN; ++it) {
         if (mbar_try(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > TC_TIMEOUT_NS) return false;
+    }
     return false;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -85,6 +98,79 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t tmem, uint32_t ncols) {
 }
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// ---- CTA pairs (cluster of two; the even CTA issues the MMAs of both)
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+// every thread of both CTAs; orders shared-memory and barrier initialisation across the pair
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void st_remote_u32(uint32_t cluster_addr, uint32_t v) {
+    asm volatile("st.shared::cluster.u32 [%0], %1;\n" ::"r"(cluster_addr), "r"(v) : "memory");
+}
+// try_wait with cluster-scope acquire: for barriers that the other CTA of the pair arrives on
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_cluster(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (long long it = 0; it < TC_SPIN; ++it) {
+        if (mbar_try_cluster(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > TC_TIMEOUT_NS) return false;
+    }
+    return false;
+}
+// 256-row MMA over the pair: A rows 0-127 / 128-255 and B columns 0-N/2-1 / N/2-N-1
+// from the same shared-memory offsets in the even / odd CTA; D rows likewise in
+// each CTA's TMEM
+template <uint32_t IDESC>
+__device__ __forceinline__ void mma2_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}\n" ::"r"(
+            dtmem),
+        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+        "r"(0u), "r"(0u));
+}
+// arrive on a barrier (this CTA's or, through its shared::cluster address, the
+// other's) when the pair MMAs issued so far by this thread have completed
+__device__ __forceinline__ void mma2_commit(uint32_t cluster_addr) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(cluster_addr)
+                 : "memory");
+}
+// TMEM of a pair: one warp of each CTA, the same warp in both, the same destination offset
+__device__ __forceinline__ void tmem_alloc2(uint32_t* dst_smem, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::);
+}
+__device__ __forceinline__ void tmem_dealloc2(uint32_t tmem, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
+}
+
 // 32 lanes x 32 columns of 32-bit TMEM cells into 32 registers per thread
 __device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
     asm volatile(

@@ -107,6 +107,10 @@ class Context:
         check(self.lib.sc_int8_peak_probe(self.handle, ctypes.byref(v)))
         return v.value
 
+    def crt_tiles(self, mode: int) -> None:
+        """Modular engine's MMA tiles: 0 = 128 x 256 on one CTA (default), 1 = 256 x 256 on CTA pairs."""
+        check(self.lib.sc_crt_tiles_set(self.handle, int(mode)))
+
     def fp64_peak_tflops(self, tensor: bool = False) -> float:
         """Measured FP64 throughput: FMA pipe, or mma.sync f64 with tensor=True."""
         v = ctypes.c_double(0.0)

@@ -210,14 +210,16 @@ def train(sur: Surrogate, maps, lams, targets, epochs: int, batch: int = 64, lr:
     hist = []
     for ep in range(epochs):
         perm = torch.from_numpy(rng.permutation(n)).cuda()
-        tot = 0.0
+        # the loss is summed on the device: reading it back every step would
+        # stall the launch queue once per step
+        tot = torch.zeros((), dtype=torch.float32, device="cuda")
         for i0 in range(0, n - batch + 1, batch):
             idx = perm[i0:i0 + batch]
             rate = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(steps, 1)))
             loss = sur.train_step(dm[idx].contiguous(), dl[idx].contiguous(), dt[idx].contiguous(), rate)
-            tot += float(loss.mean())
+            tot += loss.mean()
             step += 1
-        hist.append(tot / max(1, n // batch))
+        hist.append(float(tot) / max(1, n // batch))
         if log:
             log(f"epoch {ep}: train loss {hist[-1]:.3e}")
     torch.cuda.synchronize()

@@ -151,3 +151,23 @@ def test_crt_gemm_many_tiles_persistent(ctx):
     got = run_crt(ctx, A, B)
     ref = A @ B
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("m,n,k,batch", [(1, 1, 1, 1), (130, 300, 97, 3), (200, 129, 260, 2), (441, 441, 441, 2),
+                                         (700, 900, 300, 6)])
+def test_crt_pair_tiles_bit_identical(ctx, m, n, k, batch):
+    """The CTA-pair kernel (256 x 256 tiles over two SMs) and the single-CTA kernel (128 x 256 tiles) form
+    the same exact integer products and the same reconstruction: bit-identical results, including shapes
+    whose row tiles are odd in number and whose last column half-tile is all padding."""
+    rng = np.random.default_rng(m + 3 * n + 5 * k)
+    A, B, C = crand(rng, batch, m, k), crand(rng, batch, k, n), crand(rng, batch, m, n)
+    try:
+        ctx.crt_tiles(0)
+        one = run_crt(ctx, A, B, C, 0.3 + 0.1j, 0.5 - 0.25j)
+        ctx.crt_tiles(1)
+        two = run_crt(ctx, A, B, C, 0.3 + 0.1j, 0.5 - 0.25j)
+    finally:
+        ctx.crt_tiles(0)
+    assert np.array_equal(one, two)
+    ref = (0.3 + 0.1j) * A @ B + (0.5 - 0.25j) * C
+    assert np.linalg.norm(two - ref) / np.linalg.norm(ref) < 1e-13
