@@ -33,12 +33,12 @@
 // (four K steps: A 16 KB + B 32 KB, two bulk copies) through a 4-slot ring with
 // cp.async.bulk, warp 1 issues four 128 x 256 x 32 MMAs per stage (one commit
 // per stage: committing after every MMA serialised them) into one of two
-// 256-column TMEM accumulators, and eight epilogue warps turn a finished accumulator into
-// int8 residues (written to a per-CTA scratch slot that stays in L2) while the
-// MMAs of the next modulus run in the other accumulator.  After the last
-// modulus the epilogue warps rebuild the tile from the residues in FP64 and
-// write C.  All waits are bounded; a timeout sets the error word and the CTA
-// drains its copies, frees its TMEM and returns.
+// 256-column TMEM accumulators, and eight epilogue warps turn a finished
+// accumulator into int8 residues (in a residue buffer, one plane per modulus)
+// while the MMAs of the next modulus run in the other accumulator.  A rebuild
+// kernel then reads each output's 14 residues and writes C in FP64.  All
+// waits are bounded; a timeout sets the error word and the CTA drains its
+// copies, frees its TMEM and returns.
 #include <cmath>
 #include <cstdint>
 #include <type_traits>
@@ -65,7 +65,6 @@ constexpr int CRT_SLOT = CRT_SA + CRT_SB;      // 48 KB
 constexpr int CRT_NS = 4;                    // ring slots (192 KB)
 constexpr int CRT_EPI_WARPS = 8;
 constexpr int CRT_THREADS = 32 * (2 + CRT_EPI_WARPS);
-constexpr int CRT_SCRATCH = CRT_NMOD * CRT_BM * CRT_BN;   // residue bytes per CTA (448 KB)
 constexpr uint32_t CRT_IDESC = tc::idesc_i8(CRT_BM, CRT_BN);
 constexpr int CRT_MODS[CRT_NMOD] = {255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197};
 
@@ -295,7 +294,8 @@ struct CrtArgs {
     double2* const* Cp;
     int ldc;
     long long sC;
-    int8_t* scratch;         // CRT_SCRATCH bytes per CTA
+    int8_t* res;             // residues: [b][p][Mp rows of C'][Np columns] int8
+    int Mp, Np;              // RB x 128, CB x 256
     int* err;
 };
 
@@ -320,15 +320,16 @@ __device__ __forceinline__ double crt_value(const int (&r)[CRT_NMOD]) {
 
 // One CTA's epilogue for one output tile: 128 rows of C' (its TMEM lanes; warp
 // w reads lane quarter w % 4, and the two warps of a quarter split the 256
-// columns) for each modulus pass: wait for the accumulator, reduce it to int8
-// residues in the CTA's scratch (which stays in L2) and hand the accumulator
-// back; then rebuild the rows from the residues in FP64 and write C.  rb is
+// columns).  For each modulus pass: wait for the accumulator, reduce it to
+// int8 residues in the residue buffer and hand the accumulator back.  rb is
 // the 128-row tile, cb the 256-column tile; u counts accumulator uses.
-// Returns false when a wait gave up (the error word is then set).
+// Returns false when a wait gave up (the error word is then set).  The FP64
+// rebuild of C from the residues is crt_rebuild_kernel's: done here it kept
+// the epilogue warps from draining the next tile's accumulators and stalled
+// the MMAs for about a third of the kernel.
 template <typename WaitFull, typename Release>
-__device__ __forceinline__ bool crt_epilogue_tile(const CrtArgs& g, uint32_t tmem, int8_t* scr, int rb, int cb, int b,
-                                                  long long& u, volatile int* aborted, WaitFull wait_full,
-                                                  Release release) {
+__device__ __forceinline__ bool crt_extract_tile(const CrtArgs& g, uint32_t tmem, int rb, int cb, int b, long long& u,
+                                                 volatile int* aborted, WaitFull wait_full, Release release) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ew = warp - 2;
     const int quarter = warp & 3;
@@ -343,7 +344,8 @@ __device__ __forceinline__ bool crt_epilogue_tile(const CrtArgs& g, uint32_t tme
             return false;
         }
         tc::fence_after_sync();
-        int8_t* dst = scr + ((long long)t * CRT_BM + row) * CRT_BN;
+        int8_t* dst = g.res + (((long long)b * CRT_NMOD + t) * g.Mp + (long long)rb * CRT_BM + row) * g.Np +
+                      (long long)cb * CRT_BN;
         auto extract = [&](auto tag) {
             constexpr int P = crt_mod(decltype(tag)::value);
 #pragma unroll 1
@@ -364,43 +366,49 @@ __device__ __forceinline__ bool crt_epilogue_tile(const CrtArgs& g, uint32_t tme
         __syncwarp();
         if (lane == 0) release(buf);
     }
-    __syncwarp();
-    // rebuild this warp's rows x columns from the residues (this thread wrote them)
-    const int rowp = rb * CRT_BM + row;
-    const int i = rowp >> 1;
-    const bool im = rowp & 1;
+    return true;
+}
+
+// C = alpha 2^(e_i + f_c - al - be) C'_int + beta C from the residues: block of
+// 8 warps = 8 complex rows i (C' rows 2i, 2i+1) x 256 columns, a lane 8
+// consecutive columns (8-byte residue loads, coalesced along the rows); the
+// 8 warps of a block write adjacent rows of each column of the column-major C
+__global__ void __launch_bounds__(256) crt_rebuild_kernel(CrtArgs g) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.z;
+    const int i = blockIdx.y * 8 + warp;
+    const int c0 = blockIdx.x * 256 + 8 * lane;
+    if (i >= g.m || c0 >= g.n) return;
+    const long long plane = (long long)g.Mp * g.Np;
+    const int8_t* base = g.res + (long long)b * CRT_NMOD * plane + (long long)(2 * i) * g.Np + c0;
+    uint2 re[CRT_NMOD], im[CRT_NMOD];
+#pragma unroll
+    for (int t = 0; t < CRT_NMOD; ++t) {
+        re[t] = *reinterpret_cast<const uint2*>(base + t * plane);
+        im[t] = *reinterpret_cast<const uint2*>(base + t * plane + g.Np);
+    }
     double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
     const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
     const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
-    const int ex = (i < g.m) ? g.rowexp[(long long)b * g.m + i] : 0;
-#pragma unroll 1
-    for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 16) {
-        uint4 rv[CRT_NMOD];
+    const int ex = g.rowexp[(long long)b * g.m + i] - g.shift;
 #pragma unroll
-        for (int t = 0; t < CRT_NMOD; ++t)
-            rv[t] = *reinterpret_cast<const uint4*>(scr + ((long long)t * CRT_BM + row) * CRT_BN + c0);
+    for (int q = 0; q < 8; ++q) {
+        const int c = c0 + q;
+        if (c >= g.n) break;
+        int rr[CRT_NMOD], ri[CRT_NMOD];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            int r[CRT_NMOD];
-#pragma unroll
-            for (int t = 0; t < CRT_NMOD; ++t) {
-                const uint32_t word = (q < 4) ? rv[t].x : (q < 8) ? rv[t].y : (q < 12) ? rv[t].z : rv[t].w;
-                r[t] = (int)(int8_t)(word >> (8 * (q & 3)));
-            }
-            const int c = cb * CRT_BN + c0 + q;
-            const int fx = (c < g.n) ? g.colexp[(long long)b * g.n + c] : 0;
-            const double v = scale2(crt_value(r), ex + fx - g.shift);
-            const double o = __shfl_xor_sync(0xffffffffu, v, 1);
-            if (!im && i < g.m && c < g.n) {
-                double2* pc = C + (long long)c * g.ldc + i;
-                double2 val = cmul(alpha, make_double2(v, o));
-                if (!beta_zero) val = cfma(g.beta, *pc, val);
-                *pc = val;
-            }
+        for (int t = 0; t < CRT_NMOD; ++t) {
+            const uint32_t wr = (q < 4) ? re[t].x : re[t].y, wi = (q < 4) ? im[t].x : im[t].y;
+            rr[t] = (int)(int8_t)(wr >> (8 * (q & 3)));
+            ri[t] = (int)(int8_t)(wi >> (8 * (q & 3)));
         }
+        const int e = ex + g.colexp[(long long)b * g.n + c];
+        const double vr = scale2(crt_value(rr), e), vi = scale2(crt_value(ri), e);
+        double2* pc = C + (long long)c * g.ldc + i;
+        double2 val = cmul(alpha, make_double2(vr, vi));
+        if (!beta_zero) val = cfma(g.beta, *pc, val);
+        *pc = val;
     }
-    __syncwarp();
-    return true;
 }
 
 __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
@@ -501,13 +509,12 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
         }
     } else {
         // epilogue warps
-        int8_t* scr = g.scratch + (long long)blockIdx.x * CRT_SCRATCH;
         auto wait_full = [&](int buf, uint32_t parity) { return tc::mbar_wait(&accfull[buf], parity); };
         auto release = [&](int buf) { tc::mbar_arrive(&accempty[buf]); };
         long long u = 0;
         for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
             const int cb = tile % g.CB, rb = (tile / g.CB) % g.RB, b = tile / (g.CB * g.RB);
-            if (!crt_epilogue_tile(g, tmem, scr, rb, cb, b, u, aborted, wait_full, release)) {
+            if (!crt_extract_tile(g, tmem, rb, cb, b, u, aborted, wait_full, release)) {
                 *aborted = 1;
                 break;
             }
@@ -679,13 +686,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
         }
     } else {
         // epilogue warps: this CTA's 128 rows of each 256-row tile
-        int8_t* scr = g.scratch + (long long)blockIdx.x * CRT_SCRATCH;
         auto wait_full = [&](int buf, uint32_t parity) { return wait(&accfull[buf], parity); };
         auto release = [&](int buf) { tc::mbar_arrive_remote(tc::peer_addr(&accempty[buf], 0u)); };
         long long u = 0;
         for (int tile = pair; tile < g.ntiles; tile += npairs) {
             const int cb = tile % g.CB, rb2 = (tile / g.CB) % RB2, b = tile / (g.CB * RB2);
-            if (!crt_epilogue_tile(g, tmem, scr, 2 * rb2 + (int)rank, cb, b, u, aborted, wait_full, release)) {
+            if (!crt_extract_tile(g, tmem, 2 * rb2 + (int)rank, cb, b, u, aborted, wait_full, release)) {
                 if (lane == 0) abort_pair(14);
                 break;
             }
@@ -820,18 +826,19 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         set_error("zgemm_crt: grid too large");
         return SC_BADINPUT;
     }
-    // sub-batches so that the packed operands stay within 8 GiB
-    const size_t per = crt_packed_bytes(g.m, g.n, g.k);
+    // sub-batches so that the packed operands and the residues stay within 8 GiB
+    const size_t res_per = (size_t)CRT_NMOD * RB * CRT_BM * (size_t)CB * CRT_BN;
+    const size_t per = crt_packed_bytes(g.m, g.n, g.k) + res_per;
     int sub = (int)std::max<size_t>(1, std::min<size_t>((size_t)batch, (8ULL << 30) / std::max<size_t>(per, 1)));
     if (sub > 65535) sub = 65535;
-    int8_t *Aq, *Bq, *scratch;
+    int8_t *Aq, *Bq, *res;
     int* ex;
     const size_t aq = (size_t)sub * CRT_NMOD * RB * KB * CRT_ATILE;
     const size_t bq = (size_t)sub * CRT_NMOD * CB * KB * CRT_BTILE;
     SC_TRY(ws.get(&Aq, aq, WS_OZ_A, st));
     SC_TRY(ws.get(&Bq, bq, WS_OZ_B, st));
     SC_TRY(ws.get(&ex, (size_t)batch * (g.m + g.n), WS_OZ_E, st));
-    SC_TRY(ws.get(&scratch, (size_t)sms * CRT_SCRATCH, WS_CRT_SCRATCH, st));
+    SC_TRY(ws.get(&res, (size_t)sub * res_per, WS_CRT_RES, st));
     int* rowexp = ex;
     int* colexp = ex + (size_t)batch * g.m;
     size_t mark_all = 0;
@@ -872,7 +879,9 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         a.Cp = g.Cp ? g.Cp + b0 : nullptr;
         a.ldc = g.ldc;
         a.sC = g.sC;
-        a.scratch = scratch;
+        a.res = res;
+        a.Mp = RB * CRT_BM;
+        a.Np = CB * CRT_BN;
         a.err = err;
         size_t mark = 0;
         if (ws.time_kernels) {
@@ -880,7 +889,7 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
             SC_TRY(ws.mark_begin(st, 2, 8.0 * g.m * (double)g.n * g.k * nb, 2.0 * macs, &mark));
         }
         if (pair) {
-            // two CTAs per tile; never more CTAs than SMs (the scratch holds one slot per SM)
+            // two CTAs per tile, at most one CTA per SM
             const int grid = 2 * std::min(a.ntiles, std::min(npairs, sms / 2));
             crt_mma2_kernel<<<grid, CRT_THREADS, C2_NS * C2_SLOT + 1024, st>>>(a);
         } else {
@@ -890,6 +899,9 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         count_launch();
         if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark));
         SC_CHECK_LAUNCH("crt mma");
+        crt_rebuild_kernel<<<dim3((g.n + 255) / 256, (g.m + 7) / 8, nb), 256, 0, st>>>(a);
+        count_launch();
+        SC_CHECK_LAUNCH("crt rebuild");
     }
     if (ws.time_kernels) SC_TRY(ws.mark_end(st, mark_all));
     return SC_OK;
