@@ -39,6 +39,9 @@
 // kernel then reads each output's 14 residues and writes C in FP64.  All
 // waits are bounded; a timeout sets the error word and the CTA drains its
 // copies, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdint>
 #include <type_traits>
@@ -140,17 +143,6 @@ __device__ __forceinline__ int sym_res(int x) {
     if (r < -(P / 2)) r += P;
     return r;
 }
-// symmetric residue of an integer u with |u| < 2^50, given as U = u + 2^50
-// split into 17-bit limbs U0 + 2^17 U1 + 2^34 U2
-template <int P>
-__device__ __forceinline__ int sym_res_wide(int U0, int U1, int U2) {
-    constexpr unsigned c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
-    // u = U - 2^50 = U2 2^34 + U1 2^17 + U0 - 2^50 == v (mod P) with v >= 0 (< 2^26), unsigned remainder
-    const unsigned v = (unsigned)U2 * c34 + (unsigned)U1 * c17 + (unsigned)U0 + (unsigned)(P - c50);
-    const int r = (int)(v % (unsigned)P);
-    return r > P / 2 ? r - P : r;
-}
-
 // x (|x| < 2^50, any double) rounded to the nearest integer and returned as
 // the three 17-bit limbs of x + 2^50: 1.5 2^52 + x places the rounded integer
 // in the low mantissa bits (no FP64 rounding or conversion instruction)
@@ -196,88 +188,140 @@ template <typename F>
 __device__ __forceinline__ void with_mod(int t, F& f) { with_mod_from<0>(t, f); }
 
 // ---------------------------------------------------------------- packing
-// A' residue tiles: [b][p][rb][kb][4 KB]; a thread takes one complex row i and
-// 8 complex columns (16 K' bytes) and writes one 16-byte core-matrix row per
-// modulus for each of A' rows 2i (Re, -Im pairs) and 2i+1 (Im, Re pairs)
-__global__ void __launch_bounds__(128) crt_pack_a_kernel(int m, int k, const double2* __restrict__ A,
+// Residues for packing: r' = (u + h) mod p with h = (p - 1) / 2, so that the
+// symmetric residue (|r| <= h) is r' - h; u (|u| < 2^50) comes as U = u + 2^50
+// in 17-bit limbs, and the constant (p - 2^50 mod p) + h keeps the unsigned
+// sum non-negative.  The subtraction of h (or, for a negated residue, h - r')
+// runs on four packed bytes at once (__vsub4: bytewise, no borrow), so each
+// value costs two multiply-adds, an add and the remainder by a constant.
+template <int P>
+__device__ __forceinline__ uint32_t res_shifted(int U0, int U1, int U2) {
+    constexpr unsigned c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
+    constexpr unsigned K = (unsigned)(P - c50) + (unsigned)(P - 1) / 2;
+    const unsigned v = (unsigned)U2 * c34 + (unsigned)U1 * c17 + ((unsigned)U0 + K);
+    return v % (unsigned)P;
+}
+template <int P>
+__device__ __forceinline__ uint32_t half4() { return (uint32_t)((P - 1) / 2) * 0x01010101u; }
+__device__ __forceinline__ uint32_t bytes4(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) {
+    return b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+}
+
+// copy NP planes of `bytes` contiguous bytes each from shared memory to global
+// (plane t at dst + t * plane) with 16-byte stores, consecutive threads on
+// consecutive addresses
+template <int NP>
+__device__ __forceinline__ void planes_out(const unsigned char* sm, int bytes, int8_t* dst, long long plane) {
+    const int per = bytes / 16;
+    for (int e = threadIdx.x; e < NP * per; e += blockDim.x) {
+        const int t = e / per, o = (e - t * per) * 16;
+        *reinterpret_cast<uint4*>(dst + t * plane + o) = *reinterpret_cast<const uint4*>(sm + t * bytes + o);
+    }
+}
+
+// A' residue tiles: [b][p][rb][kb][4 KB].  A block packs one tile (64 complex
+// rows x 16 complex columns) for all moduli; a thread takes one complex row i
+// and 4 complex columns (8 K' bytes) and writes 8 bytes per modulus to each of
+// A' rows 2i (Re, -Im pairs) and 2i+1 (Im, Re pairs) in shared memory; the
+// block then stores each modulus' 4 KB tile with contiguous 16-byte stores
+// (written directly, 8-byte pieces 32 bytes apart left three quarters of each
+// written sector empty).  Seven moduli per round (28 KB of shared memory).
+__global__ void __launch_bounds__(256) crt_pack_a_kernel(int m, int k, const double2* __restrict__ A,
                                                          const double2* const* Ap, int lda, long long sA,
                                                          const int* __restrict__ rowexp, int al, int RB, int KB,
                                                          int8_t* __restrict__ out) {
+    constexpr int HALF = CRT_NMOD / 2;
+    __shared__ __align__(16) unsigned char sm[HALF * CRT_ATILE];
     const int b = blockIdx.z;
     const int rb = blockIdx.x, kb = blockIdx.y;
     const double2* a = Ap ? Ap[b] : A + b * sA;
-    const int il = threadIdx.x & 63, jc = threadIdx.x >> 6;
-    const int i = rb * (CRT_BM / 2) + il, j0 = kb * (CRT_BK / 2) + 8 * jc;
-    int lr[8][3], li[8][3];
+    const int il = threadIdx.x & 63, jq = threadIdx.x >> 6;
+    const int i = rb * (CRT_BM / 2) + il, j0 = kb * (CRT_BK / 2) + 4 * jq;
+    int lr[4][3], li[4][3];
     const int ex = (i < m) ? rowexp[(long long)b * m + i] : 0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 4; ++q) {
         double2 v = make_double2(0.0, 0.0);
         if (i < m && j0 + q < k) v = a[(long long)(j0 + q) * lda + i];
         round_limbs(scale2(v.x, al - ex), lr[q][0], lr[q][1], lr[q][2]);
         round_limbs(scale2(v.y, al - ex), li[q][0], li[q][1], li[q][2]);
     }
-    const int o0 = tc::tile_off(2 * il, 16 * jc), o1 = tc::tile_off(2 * il + 1, 16 * jc);
+    const int o0 = tc::tile_off(2 * il, 8 * jq), o1 = tc::tile_off(2 * il + 1, 8 * jq);
     const long long plane = (long long)RB * KB * CRT_ATILE;
     int8_t* base = out + (long long)b * CRT_NMOD * plane + ((long long)rb * KB + kb) * CRT_ATILE;
     auto one = [&](auto tag) {
         constexpr int T = decltype(tag)::value;
         constexpr int P = crt_mod(T);
-        int dr[8], di[8];
+        constexpr uint32_t H = (uint32_t)((P - 1) / 2);
+        uint32_t dr[4], di[4];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            dr[q] = sym_res_wide<P>(lr[q][0], lr[q][1], lr[q][2]);
-            di[q] = sym_res_wide<P>(li[q][0], li[q][1], li[q][2]);
+        for (int q = 0; q < 4; ++q) {
+            dr[q] = res_shifted<P>(lr[q][0], lr[q][1], lr[q][2]);
+            di[q] = res_shifted<P>(li[q][0], li[q][1], li[q][2]);
         }
-        const uint4 w0 = make_uint4(pack4(dr[0], -di[0], dr[1], -di[1]), pack4(dr[2], -di[2], dr[3], -di[3]),
-                                    pack4(dr[4], -di[4], dr[5], -di[5]), pack4(dr[6], -di[6], dr[7], -di[7]));
-        const uint4 w1 = make_uint4(pack4(di[0], dr[0], di[1], dr[1]), pack4(di[2], dr[2], di[3], dr[3]),
-                                    pack4(di[4], dr[4], di[5], dr[5]), pack4(di[6], dr[6], di[7], dr[7]));
-        int8_t* pl = base + (long long)T * plane;
-        *reinterpret_cast<uint4*>(pl + o0) = w0;
-        *reinterpret_cast<uint4*>(pl + o1) = w1;
+        // row 2i: Re - h, h - Im ; row 2i+1: Im - h, Re - h
+        unsigned char* st = sm + (T % HALF) * CRT_ATILE;
+        *reinterpret_cast<uint2*>(st + o0) =
+            make_uint2(__vsub4(bytes4(dr[0], H, dr[1], H), bytes4(H, di[0], H, di[1])),
+                       __vsub4(bytes4(dr[2], H, dr[3], H), bytes4(H, di[2], H, di[3])));
+        *reinterpret_cast<uint2*>(st + o1) = make_uint2(__vsub4(bytes4(di[0], dr[0], di[1], dr[1]), half4<P>()),
+                                                        __vsub4(bytes4(di[2], dr[2], di[3], dr[3]), half4<P>()));
+        if constexpr (T % HALF == HALF - 1) {
+            __syncthreads();
+            planes_out<HALF>(sm, CRT_ATILE, base + (long long)(T - (HALF - 1)) * plane, plane);
+            __syncthreads();
+        }
     };
     for_each_mod(one);
 }
 
 // B' residue tiles (N x K', K-major): [b][p][cb][kb][8 KB] of 256 columns, or
 // with `halves` [b][p][2 cb + h][kb][4 KB] of 128 columns (each CTA of a pair
-// then loads its half of a 256-column tile as one contiguous run); a block
-// covers 128 columns, a thread one column and 8 complex rows (one 16-byte
-// core-matrix row per modulus)
+// then loads its half of a 256-column tile as one contiguous run).  A block
+// packs 64 columns of a tile (2 KB per modulus, contiguous in either layout);
+// a thread takes one column and 4 complex rows (8 bytes of one core-matrix row
+// per modulus) into shared memory, and the block stores the 14 runs of 2 KB
+// with contiguous 16-byte stores.
 __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const double2* __restrict__ B,
                                                          const double2* const* Bp, int ldb, long long sB,
                                                          const int* __restrict__ colexp, int be, int CB, int KB,
                                                          int halves, int8_t* __restrict__ out) {
+    constexpr int QB = CRT_BTILE / 4;   // 2 KB: 64 columns x 32 K' bytes
+    __shared__ __align__(16) unsigned char sm[CRT_NMOD * QB];
     const int b = blockIdx.z;
-    const int cb = blockIdx.x >> 1, kb = blockIdx.y;
+    const int cb = blockIdx.x >> 2, qt = blockIdx.x & 3, kb = blockIdx.y;
     const double2* bb = Bp ? Bp[b] : B + b * sB;
-    const int cl = (blockIdx.x & 1) * 128 + (threadIdx.x & 127), jc = threadIdx.x >> 7;
-    const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2) + 8 * jc;
-    int lx[16][3];
+    const int cq = threadIdx.x & 63, jq = threadIdx.x >> 6;
+    const int cl = qt * 64 + cq;
+    const int c = cb * CRT_BN + cl, j0 = kb * (CRT_BK / 2) + 4 * jq;
+    int lx[8][3];
     const int ex = (c < n) ? colexp[(long long)b * n + c] : 0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 4; ++q) {
         double2 v = make_double2(0.0, 0.0);
         if (c < n && j0 + q < k) v = bb[(long long)c * ldb + j0 + q];
         round_limbs(scale2(v.x, be - ex), lx[2 * q][0], lx[2 * q][1], lx[2 * q][2]);
         round_limbs(scale2(v.y, be - ex), lx[2 * q + 1][0], lx[2 * q + 1][1], lx[2 * q + 1][2]);
     }
-    const int o = tc::tile_off(halves ? (cl & 127) : cl, 16 * jc);
+    // the block's 64 columns are 8 core-matrix row groups: offset cq within its 2 KB run
+    const int o = tc::tile_off(cq, 8 * jq);
     const long long plane = (long long)CB * KB * CRT_BTILE;
     int8_t* base = out + (long long)b * CRT_NMOD * plane +
-                   (halves ? ((long long)blockIdx.x * KB + kb) * (CRT_BTILE / 2) : ((long long)cb * KB + kb) * CRT_BTILE);
+                   (halves ? ((long long)(2 * cb + (qt >> 1)) * KB + kb) * (CRT_BTILE / 2) + (qt & 1) * QB
+                           : ((long long)cb * KB + kb) * CRT_BTILE + qt * QB);
     auto one = [&](auto tag) {
         constexpr int T = decltype(tag)::value;
         constexpr int P = crt_mod(T);
-        int d[16];
+        uint32_t d[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) d[q] = sym_res_wide<P>(lx[q][0], lx[q][1], lx[q][2]);
-        *reinterpret_cast<uint4*>(base + (long long)T * plane + o) =
-            make_uint4(pack4(d[0], d[1], d[2], d[3]), pack4(d[4], d[5], d[6], d[7]), pack4(d[8], d[9], d[10], d[11]),
-                       pack4(d[12], d[13], d[14], d[15]));
+        for (int q = 0; q < 8; ++q) d[q] = res_shifted<P>(lx[q][0], lx[q][1], lx[q][2]);
+        *reinterpret_cast<uint2*>(sm + T * QB + o) =
+            make_uint2(__vsub4(bytes4(d[0], d[1], d[2], d[3]), half4<P>()),
+                       __vsub4(bytes4(d[4], d[5], d[6], d[7]), half4<P>()));
     };
     for_each_mod(one);
+    __syncthreads();
+    planes_out<CRT_NMOD>(sm, QB, base, plane);
 }
 
 // ---------------------------------------------------------------- MMA kernel
@@ -371,43 +415,61 @@ __device__ __forceinline__ bool crt_extract_tile(const CrtArgs& g, uint32_t tmem
 
 // C = alpha 2^(e_i + f_c - al - be) C'_int + beta C from the residues: block of
 // 8 warps = 8 complex rows i (C' rows 2i, 2i+1) x 256 columns, a lane 8
-// consecutive columns (8-byte residue loads, coalesced along the rows); the
-// 8 warps of a block write adjacent rows of each column of the column-major C
+// consecutive columns (8-byte residue loads, coalesced along the rows).  The
+// values go through shared memory so that the stores to the column-major C
+// are whole: a quarter-warp writes the block's 8 rows of one column (128
+// contiguous bytes).  Tile [256 columns][8 rows] of double2, the row slot
+// XOR-swizzled by column / 8 so that neither pass has bank conflicts.
 __global__ void __launch_bounds__(256) crt_rebuild_kernel(CrtArgs g) {
+    __shared__ double2 tile[256 * 8];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.z;
-    const int i = blockIdx.y * 8 + warp;
-    const int c0 = blockIdx.x * 256 + 8 * lane;
-    if (i >= g.m || c0 >= g.n) return;
-    const long long plane = (long long)g.Mp * g.Np;
-    const int8_t* base = g.res + (long long)b * CRT_NMOD * plane + (long long)(2 * i) * g.Np + c0;
-    uint2 re[CRT_NMOD], im[CRT_NMOD];
-#pragma unroll
-    for (int t = 0; t < CRT_NMOD; ++t) {
-        re[t] = *reinterpret_cast<const uint2*>(base + t * plane);
-        im[t] = *reinterpret_cast<const uint2*>(base + t * plane + g.Np);
-    }
+    const int i0 = blockIdx.y * 8, cb0 = blockIdx.x * 256;
+    const int i = i0 + warp;
+    const int c0 = cb0 + 8 * lane;
     double2* C = g.Cp ? g.Cp[b] : g.C + b * g.sC;
     const double2 alpha = g.alphas ? cmul(g.alpha, g.alphas[b]) : g.alpha;
     const bool beta_zero = (g.beta.x == 0.0 && g.beta.y == 0.0);
-    const int ex = g.rowexp[(long long)b * g.m + i] - g.shift;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int c = c0 + q;
-        if (c >= g.n) break;
-        int rr[CRT_NMOD], ri[CRT_NMOD];
+    if (i < g.m && c0 < g.n) {
+        const long long plane = (long long)g.Mp * g.Np;
+        const int8_t* base = g.res + (long long)b * CRT_NMOD * plane + (long long)(2 * i) * g.Np + c0;
+        uint2 re[CRT_NMOD], im[CRT_NMOD];
 #pragma unroll
         for (int t = 0; t < CRT_NMOD; ++t) {
-            const uint32_t wr = (q < 4) ? re[t].x : re[t].y, wi = (q < 4) ? im[t].x : im[t].y;
-            rr[t] = (int)(int8_t)(wr >> (8 * (q & 3)));
-            ri[t] = (int)(int8_t)(wi >> (8 * (q & 3)));
+            re[t] = *reinterpret_cast<const uint2*>(base + t * plane);
+            im[t] = *reinterpret_cast<const uint2*>(base + t * plane + g.Np);
         }
-        const int e = ex + g.colexp[(long long)b * g.n + c];
-        const double vr = scale2(crt_value(rr), e), vi = scale2(crt_value(ri), e);
-        double2* pc = C + (long long)c * g.ldc + i;
-        double2 val = cmul(alpha, make_double2(vr, vi));
-        if (!beta_zero) val = cfma(g.beta, *pc, val);
-        *pc = val;
+        const int ex = g.rowexp[(long long)b * g.m + i] - g.shift;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = c0 + q;
+            if (c >= g.n) break;
+            int rr[CRT_NMOD], ri[CRT_NMOD];
+#pragma unroll
+            for (int t = 0; t < CRT_NMOD; ++t) {
+                const uint32_t wr = (q < 4) ? re[t].x : re[t].y, wi = (q < 4) ? im[t].x : im[t].y;
+                rr[t] = (int)(int8_t)(wr >> (8 * (q & 3)));
+                ri[t] = (int)(int8_t)(wi >> (8 * (q & 3)));
+            }
+            const int e = ex + g.colexp[(long long)b * g.n + c];
+            const int cl = 8 * lane + q;
+            tile[cl * 8 + (warp ^ (lane & 7))] = cmul(alpha, make_double2(scale2(crt_value(rr), e),
+                                                                          scale2(crt_value(ri), e)));
+        }
+    }
+    __syncthreads();
+    // quarter-warp per column: lanes 8j..8j+7 write rows i0..i0+7 of column 4 it + j (of this warp's 32)
+    const int r = lane & 7;
+#pragma unroll 4
+    for (int it = 0; it < 8; ++it) {
+        const int cl = warp * 32 + 4 * it + (lane >> 3);
+        const int c = cb0 + cl, row = i0 + r;
+        if (c < g.n && row < g.m) {
+            double2 val = tile[cl * 8 + (r ^ ((cl >> 3) & 7))];
+            double2* pc = C + (long long)c * g.ldc + row;
+            if (!beta_zero) val = cfma(g.beta, *pc, val);
+            *pc = val;
+        }
     }
 }
 
@@ -531,27 +593,29 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
 // MMAs whose A rows 0-127 and B columns 0-127 come from its own shared memory
 // and A rows 128-255 and B columns 128-255 from the odd CTA's, at the same
 // offsets; each CTA's TMEM receives its 128 rows.  Per SM and K step a CTA
-// stages 4 KB of A and 4 KB of B for 128 x 256 multiply-adds (the single-CTA
-// tile stages 4 + 8 KB), so the L2 -> shared-memory traffic that feeds the
-// tensor pipe drops by a third, and the 32 KB stages allow a six-deep ring.
-// Both CTAs load their halves with plain bulk copies (no multicast) on their
-// own barrier; the odd CTA's MMA warp relays each landed stage to the even
-// CTA (a remote mbarrier arrive), whose MMA thread waits for both.  The MMA
-// thread's commits arrive on the barriers of both CTAs (two commits, one per
-// CTA).  Each CTA's epilogue warps drain its own TMEM rows exactly as in the
-// single-CTA kernel and release the accumulator on the even CTA's barrier.
-// Every wait is bounded and also gives up once either CTA has aborted; a CTA
-// that aborts raises the other's flag through distributed shared memory.
+// stages 4 KB of A and 4 KB of B for 128 x 256 multiply-adds where the
+// single-CTA tile stages 4 + 8 KB: the shared-memory traffic of the copies
+// drops by a third (with the operand reads, shared-memory bandwidth is what
+// bounds the single-CTA kernel), and the 32 KB stages allow a six-deep ring.
+// Both CTAs load their halves with 2-D tensor copies (cta_group::2, no
+// multicast) that complete on the even CTA's stage barrier, which expects the
+// bytes of both; the MMA thread's commits arrive on the barriers of both CTAs
+// (one commit per CTA).  Each CTA's epilogue warps drain its own TMEM rows as
+// in the single-CTA kernel and release the accumulator on the even CTA's
+// barrier.  Every wait is bounded and gives up once either CTA has aborted; a
+// CTA that aborts raises the other's flag through distributed shared memory.
 constexpr int C2_BTILE = CRT_BTILE / 2;             // 128 columns x 32 K bytes
 constexpr int C2_SA = CRT_KSUB * CRT_ATILE;         // 16 KB
 constexpr int C2_SB = CRT_KSUB * C2_BTILE;          // 16 KB
 constexpr int C2_SLOT = C2_SA + C2_SB;              // 32 KB
 constexpr int C2_NS = 6;                            // ring slots (192 KB)
+constexpr int C2_ROW = 256;                         // bytes per row of the tensor maps (box 256 x 64 = one stage)
 constexpr uint32_t C2_IDESC = tc::idesc_i8(2 * CRT_BM, CRT_BN);
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_mma2_kernel(CrtArgs g) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1)
+    crt_mma2_kernel(CrtArgs g, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[C2_NS], pfull[C2_NS], empty[C2_NS], accfull[2], accempty[2], done;
+    __shared__ __align__(8) uint64_t full[C2_NS], empty[C2_NS], accfull[2], accempty[2], done;
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     volatile int* aborted = &abort_flag;
@@ -564,7 +628,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
     if (threadIdx.x == 0) {
         for (int q = 0; q < C2_NS; ++q) {
             tc::mbar_init(&full[q], 1);
-            tc::mbar_init(&pfull[q], 1);
             tc::mbar_init(&empty[q], 1);
         }
         for (int q = 0; q < 2; ++q) {
@@ -601,32 +664,33 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer (both CTAs): this CTA's 128 rows of A and 128 columns of B
+            // producer (both CTAs): this CTA's 128 rows of A and 128 columns of B, one 16 KB box each per
+            // stage (a stage of fewer than four K steps loads the box all the same; the MMAs skip the rest)
             long long stage = 0;
             for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
                 const int cb = tile % g.CB, rb2 = (tile / g.CB) % RB2, b = tile / (g.CB * RB2);
                 const int rb = 2 * rb2 + (int)rank, cbh = 2 * cb + (int)rank;
                 for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
-                    const int8_t* Ab = g.Aq + ((long long)b * CRT_NMOD + t) * planeA + (long long)rb * KB * CRT_ATILE;
-                    const int8_t* Bb = g.Bq + ((long long)b * CRT_NMOD + t) * planeB + (long long)cbh * KB * C2_BTILE;
+                    const long long offA = ((long long)b * CRT_NMOD + t) * planeA + (long long)rb * KB * CRT_ATILE;
+                    const long long offB = ((long long)b * CRT_NMOD + t) * planeB + (long long)cbh * KB * C2_BTILE;
                     for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
-                        const int nsub = min(CRT_KSUB, KB - kb);
                         const int slot = (int)(stage % C2_NS);
                         if (stage >= C2_NS && !wait(&empty[slot], (uint32_t)(((stage / C2_NS) - 1) & 1))) {
                             abort_pair(21);
                             break;
                         }
+                        const uint32_t bar = tc::peer_addr(&full[slot], 0u);
+                        if (leader) tc::mbar_expect_tx(&full[slot], (uint32_t)(2 * C2_SLOT));
                         unsigned char* sa = smem_raw + (size_t)slot * C2_SLOT;
-                        tc::mbar_expect_tx(&full[slot], (uint32_t)(nsub * (CRT_ATILE + C2_BTILE)));
-                        tc::bulk_g2s(sa, Ab + (long long)kb * CRT_ATILE, (uint32_t)(nsub * CRT_ATILE), &full[slot]);
-                        tc::bulk_g2s(sa + C2_SA, Bb + (long long)kb * C2_BTILE, (uint32_t)(nsub * C2_BTILE),
-                                     &full[slot]);
+                        tc::tma2d_pair(sa, &tmA, 0, (int)((offA + (long long)kb * CRT_ATILE) / C2_ROW), bar);
+                        tc::tma2d_pair(sa + C2_SA, &tmB, 0, (int)((offB + (long long)kb * C2_BTILE) / C2_ROW), bar);
                     }
                 }
             }
-            // drain: this CTA's copies in flight must land before it exits
-            for (long long s2 = (stage > C2_NS ? stage - C2_NS : 0); s2 < stage; ++s2)
-                tc::mbar_wait(&full[s2 % C2_NS], (uint32_t)((s2 / C2_NS) & 1));
+            // drain: the copies of both CTAs complete on the even CTA's barriers
+            if (leader)
+                for (long long s2 = (stage > C2_NS ? stage - C2_NS : 0); s2 < stage; ++s2)
+                    tc::mbar_wait(&full[s2 % C2_NS], (uint32_t)((s2 / C2_NS) & 1));
         }
     } else if (warp == 1) {
         if (lane == 0 && leader) {
@@ -646,8 +710,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
                     for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
                         const int nsub = min(CRT_KSUB, KB - kb);
                         const int slot = (int)(stage % C2_NS);
-                        const uint32_t par = (uint32_t)((stage / C2_NS) & 1);
-                        if (!wait(&full[slot], par) || !wait(&pfull[slot], par)) {
+                        if (!wait(&full[slot], (uint32_t)((stage / C2_NS) & 1))) {
                             abort_pair(23);
                             break;
                         }
@@ -668,21 +731,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
             // every MMA issued must have completed before either CTA releases its TMEM or shared memory
             tc::mma2_commit(tc::smem_u32(&done));
             if (!tc::mbar_wait(&done, 0)) atomicExch(g.err, 25);
-        } else if (lane == 0) {
-            // relay (odd CTA): tell the MMA thread when this CTA's half of a stage has landed
-            long long stage = 0;
-            for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
-                for (int t = 0; t < CRT_NMOD && !*aborted; ++t) {
-                    for (int kb = 0; kb < KB; kb += CRT_KSUB, ++stage) {
-                        const int slot = (int)(stage % C2_NS);
-                        if (!wait(&full[slot], (uint32_t)((stage / C2_NS) & 1))) {
-                            abort_pair(24);
-                            break;
-                        }
-                        tc::mbar_arrive_remote(tc::peer_addr(&pfull[slot], 0u));
-                    }
-                }
-            }
         }
     } else {
         // epilogue warps: this CTA's 128 rows of each 256-row tile
@@ -702,6 +750,34 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1) crt_
     tc::cluster_sync();
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_dealloc2(tmem, 512u);
+}
+
+// 2-D byte tensor over a packed operand buffer: rows of 256 bytes, boxes of
+// 256 x 64 (one 16 KB stage); the driver's encoder comes through the runtime
+// (no link against the driver library)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+bool byte_tensor_map(CUtensorMap* map, const void* base, size_t bytes) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || bytes % C2_ROW != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)C2_ROW, (cuuint64_t)(bytes / C2_ROW)};
+    const cuuint64_t strides[1] = {(cuuint64_t)C2_ROW};
+    const cuuint32_t box[2] = {(cuuint32_t)C2_ROW, (cuuint32_t)(C2_SA / C2_ROW)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool g_crt_const_ready[64] = {};
@@ -851,9 +927,9 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         GemmArgs h = g;
         if (g.Ap) h.Ap = g.Ap + b0; else h.A = g.A + (long long)b0 * g.sA;
         if (g.Bp) h.Bp = g.Bp + b0; else h.B = g.B + (long long)b0 * g.sB;
-        crt_pack_a_kernel<<<dim3(RB, KB, nb), 128, 0, st>>>(g.m, g.k, h.A, h.Ap, g.lda, g.sA,
+        crt_pack_a_kernel<<<dim3(RB, KB, nb), 256, 0, st>>>(g.m, g.k, h.A, h.Ap, g.lda, g.sA,
                                                            rowexp + (size_t)b0 * g.m, bits, RB, KB, Aq);
-        crt_pack_b_kernel<<<dim3(2 * CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
+        crt_pack_b_kernel<<<dim3(4 * CB, KB, nb), 256, 0, st>>>(g.k, g.n, h.B, h.Bp, g.ldb, g.sB,
                                                            colexp + (size_t)b0 * g.n, bits, CB, KB, pair ? 1 : 0,
                                                            Bq);
         count_launch(2);
@@ -888,10 +964,16 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
             const double macs = (double)CRT_NMOD * nb * (double)RB * CRT_BM * (double)CB * CRT_BN * (double)KB * CRT_BK;
             SC_TRY(ws.mark_begin(st, 2, 8.0 * g.m * (double)g.n * g.k * nb, 2.0 * macs, &mark));
         }
+        CUtensorMap tmA, tmB;
+        if (pair && (!byte_tensor_map(&tmA, Aq, (size_t)nb * CRT_NMOD * RB * KB * CRT_ATILE) ||
+                     !byte_tensor_map(&tmB, Bq, (size_t)nb * CRT_NMOD * CB * KB * CRT_BTILE))) {
+            set_error("zgemm_crt: tensor map of the packed operands could not be encoded");
+            return SC_CUDA_ERROR;
+        }
         if (pair) {
             // two CTAs per tile, at most one CTA per SM
             const int grid = 2 * std::min(a.ntiles, std::min(npairs, sms / 2));
-            crt_mma2_kernel<<<grid, CRT_THREADS, C2_NS * C2_SLOT + 1024, st>>>(a);
+            crt_mma2_kernel<<<grid, CRT_THREADS, C2_NS * C2_SLOT + 1024, st>>>(a, tmA, tmB);
         } else {
             const int grid = std::min(a.ntiles, sms);
             crt_mma_kernel<<<grid, CRT_THREADS, CRT_NS * CRT_SLOT + 1024, st>>>(a);

@@ -51,6 +51,8 @@ constexpr int COUT = 12;              // 6 complex output fields
 constexpr int NO = 11;                // orders per axis
 constexpr int NORD = NO * NO;         // 121
 constexpr int NOUT = 6 * NORD * 2;    // 1452 reals per sample
+constexpr int PW = 2 * NORD + 2;      // 244: readout columns [cos | sin] padded with zeros to a multiple of 4,
+                                      // so that the readout products take the vector operand loads
 // separable-transform operators, packed in one buffer
 constexpr int OP_FY = 0, OP_EX = OP_FY + G * 2 * MY, OP_ER = OP_EX + G * G, OP_EI = OP_ER + G * G,
               OP_GY = OP_EI + G * G, OP_TOTAL = OP_GY + 2 * MY * G;
@@ -445,19 +447,29 @@ __global__ void __launch_bounds__(256) batch_sum_kernel(const float* __restrict_
         out[i] += t;
     }
 }
+// out[b][i] = sum_s part[b S + s][i]: the K chunks of a split product, per sample
+__global__ void ksum_kernel(const float* __restrict__ part, int S, int Bn, long long n, float* __restrict__ out) {
+    const long long tot = (long long)Bn * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long b = t / n, i = t - b * n;
+        float s = 0.f;
+        for (int q = 0; q < S; ++q) s += part[(b * S + q) * n + i];
+        out[t] = s;
+    }
+}
 sc_status batch_sum(cudaStream_t st, const float* part, int R, long long n, float* out) {
     batch_sum_kernel<<<(unsigned)((n + 31) / 32), 256, 0, st>>>(part, R, n, out);
     count_launch();
     return SC_OK;
 }
 
-// readout: P[b][12][242] (cos | sin correlations) -> pred[b][6][121][re, im]
+// readout: P[b][12][244] (cos | sin correlations, 2 zero columns) -> pred[b][6][121][re, im]
 __global__ void readout_kernel(const float* __restrict__ P, int Bn, float* __restrict__ pred) {
     const int tot = Bn * 6 * NORD;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
         const int b = t / (6 * NORD), c = (t / NORD) % 6, j = t % NORD;
-        const float* pr = P + ((long long)b * COUT + 2 * c) * 2 * NORD;
-        const float* pi = pr + 2 * NORD;
+        const float* pr = P + ((long long)b * COUT + 2 * c) * PW;
+        const float* pi = pr + PW;
         float* o = pred + (long long)b * NOUT + 2 * (c * NORD + j);
         o[0] = pr[j] + pi[NORD + j];
         o[1] = pi[j] - pr[NORD + j];
@@ -470,8 +482,8 @@ __global__ void readout_back_kernel(const float* __restrict__ dpred, int Bn, flo
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
         const int b = t / (6 * NORD), c = (t / NORD) % 6, j = t % NORD;
         const float* d = dpred + (long long)b * NOUT + 2 * (c * NORD + j);
-        float* pr = dP + ((long long)b * COUT + 2 * c) * 2 * NORD;
-        float* pi = pr + 2 * NORD;
+        float* pr = dP + ((long long)b * COUT + 2 * c) * PW;
+        float* pi = pr + PW;
         pr[j] = d[0];
         pi[NORD + j] = d[0];
         pi[j] = d[1];
@@ -726,9 +738,12 @@ sc_status forward(sc_fno* f, const float* maps, const float* lam, int Bn, cudaSt
     SC_TRY(gemm(st, mk(COUT, NP, HID, Bn, 1.f, 0.f, w + Ly.Q2, HID, 1, 0, f->h, NP, 1, sh, f->o12, NP, 1, so)));
     bias_act_kernel<<<blocks((long long)Bn * so), 256, 0, st>>>(f->o12, w + Ly.bQ2, COUT, Bn, 0, nullptr);
     count_launch();
-    // readout correlations P_b (12 x 242) = o_b (12 x NP) R (NP x 242)
-    SC_TRY(gemm(st, mk(COUT, 2 * NORD, NP, Bn, 1.f, 0.f, f->o12, NP, 1, so, f->R, 2 * NORD, 1, 0, f->P, 2 * NORD, 1,
-                       (long long)COUT * 2 * NORD)));
+    // readout correlations P_b (12 x 244) = o_b (12 x NP) R (NP x 244): K = NP split into KSPLIT chunks,
+    // the partials summed per sample
+    SC_TRY(gemm(st, ksplit(mk(COUT, PW, NP, Bn, 1.f, 0.f, f->o12, NP, 1, so, f->R, PW, 1, 0, f->part, PW, 1,
+                              (long long)COUT * PW))));
+    ksum_kernel<<<blocks((long long)Bn * COUT * PW), 256, 0, st>>>(f->part, KSPLIT, Bn, (long long)COUT * PW, f->P);
+    count_launch();
     readout_kernel<<<blocks((long long)Bn * 6 * NORD), 256, 0, st>>>(f->P, Bn, f->pred);
     count_launch();
     SC_CHECK_LAUNCH("fno forward");
@@ -745,9 +760,9 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     loss_kernel<<<Bn, 256, 0, st>>>(f->pred, tgt, Bn, f->dpred, f->loss);
     readout_back_kernel<<<blocks((long long)Bn * 6 * NORD), 256, 0, st>>>(f->dpred, Bn, f->dP);
     count_launch(2);
-    // do12_b (12 x NP) = dP_b (12 x 242) R^T
-    SC_TRY(gemm(st, mk(COUT, NP, 2 * NORD, Bn, 1.f, 0.f, f->dP, 2 * NORD, 1, (long long)COUT * 2 * NORD, f->R, 1,
-                       2 * NORD, 0, f->do12, NP, 1, so)));
+    // do12_b (12 x NP) = dP_b (12 x 244) R^T (the zero columns of R and dP add nothing)
+    SC_TRY(gemm(st, mk(COUT, NP, PW, Bn, 1.f, 0.f, f->dP, PW, 1, (long long)COUT * PW, f->R, 1, PW, 0, f->do12, NP,
+                       1, so)));
     // Q2, bQ2: per-sample partials, then summed over the batch
     SC_TRY(gemm(st, ksplit(mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
                               (long long)COUT * HID))));
@@ -852,10 +867,10 @@ void init_params(const Layout& Ly, uint64_t seed, std::vector<float>& w) {
 //   Ex (64 x 64 x): rows q < 32 cos(2 pi kx(q) x / 64), q >= 32 sin  forward along x
 //   Er, Ei (64 x x 64): [cos | -sin], [sin | cos] of kx(k) x           inverse along x
 //   Gy (32 x 64 y): [c cos; -c sin] / 4096, c = 1 for ky = 0 else 2   real inverse along y
-// and R (NP x 242) = [cos | sin] / NP at the 121 orders (readout)
+// and R (NP x 244) = [cos | sin | 0 0] / NP at the 121 orders (readout)
 void build_operators(std::vector<float>& ops, std::vector<float>& R) {
     ops.assign(OP_TOTAL, 0.f);
-    R.assign((size_t)NP * 2 * NORD, 0.f);
+    R.assign((size_t)NP * PW, 0.f);
     const double tp = 2.0 * M_PI / G;
     auto trig = [&](long long ph, double* c, double* s) {
         const double th = tp * (double)(((ph % G) + G) % G);
@@ -889,8 +904,8 @@ void build_operators(std::vector<float>& ops, std::vector<float>& R) {
                 int pp, qq;
                 order_pq(j, &pp, &qq);
                 trig((long long)pp * x + (long long)qq * y, &c, &sn);
-                R[(size_t)p * 2 * NORD + j] = (float)(c / NP);
-                R[(size_t)p * 2 * NORD + NORD + j] = (float)(sn / NP);
+                R[(size_t)p * PW + j] = (float)(c / NP);
+                R[(size_t)p * PW + NORD + j] = (float)(sn / NP);
             }
         }
 }
@@ -941,7 +956,7 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->ops, OP_TOTAL);
     A(&f->S1, B * W * SEP);
     A(&f->S2, B * W * SEP);
-    A(&f->R, (long long)NP * 2 * NORD);
+    A(&f->R, (long long)NP * PW);
     A(&f->in, B * CIN * NP);
     for (int l = 0; l <= L; ++l) A(&f->act[l], B * sv);
     for (int l = 0; l < L; ++l) {
@@ -952,7 +967,7 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->hpre, B * HID * NP);
     A(&f->h, B * HID * NP);
     A(&f->o12, B * COUT * NP);
-    A(&f->P, B * COUT * 2 * NORD);
+    A(&f->P, B * COUT * PW);
     A(&f->pred, B * NOUT);
     A(&f->dact, B * sv);
     A(&f->dv, B * sv);
@@ -960,7 +975,7 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
     A(&f->dY, B * W * NF);
     A(&f->dh, B * HID * NP);
     A(&f->do12, B * COUT * NP);
-    A(&f->dP, B * COUT * 2 * NORD);
+    A(&f->dP, B * COUT * PW);
     A(&f->dpred, B * NOUT);
     A(&f->part, B * (long long)KSPLIT * HID * W);
     A(&f->loss, B);
@@ -973,6 +988,8 @@ sc_status sc_fno_create(sc_fno** out, int device, int max_batch, unsigned long l
         if (e == cudaSuccess) e = cudaMemcpy(f->ops, ops.data(), sizeof(float) * ops.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(f->R, R.data(), sizeof(float) * R.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(f->m, 0, sizeof(float) * Ly.total);
+        // the readout gradient's pad columns are never written: zero once
+        if (e == cudaSuccess) e = cudaMemset(f->dP, 0, sizeof(float) * (size_t)B * COUT * PW);
         if (e == cudaSuccess) e = cudaMemset(f->v, 0, sizeof(float) * Ly.total);
         if (e != cudaSuccess) s = cuda_status(e, "sc_fno_create");
     }

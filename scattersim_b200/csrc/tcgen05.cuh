@@ -155,6 +155,16 @@ __device__ __forceinline__ void mma2_i8(uint32_t dtmem, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
         "r"(0u), "r"(0u));
 }
+// 2-D tensor load (no multicast) into this CTA's shared memory whose completion
+// is counted on a barrier of either CTA of the pair (its shared::cluster
+// address); the tensor map is a kernel parameter (__grid_constant__)
+__device__ __forceinline__ void tma2d_pair(void* dst, const void* tmap, int x, int y, uint32_t bar_cluster) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(bar_cluster)
+        : "memory");
+}
 // arrive on a barrier (this CTA's or, through its shared::cluster address, the
 // other's) when the pair MMAs issued so far by this thread have completed
 __device__ __forceinline__ void mma2_commit(uint32_t cluster_addr) {
