@@ -29,10 +29,13 @@
 // the UMMA K-major core-matrix layout (as the digit-sliced engine does for its
 // digit planes).  The MMA kernel is persistent (one CTA per SM); a CTA owns
 // output tiles of 128 rows of C' (64 complex rows) x 256 complex columns and
-// for each tile runs NMOD passes of the K loop: warp 0 streams 48 KB stages
-// (four K steps: A 16 KB + B 32 KB, two bulk copies) through a 4-slot ring with
-// cp.async.bulk, warp 1 issues four 128 x 256 x 32 MMAs per stage (one commit
-// per stage: committing after every MMA serialised them) into one of two
+// for each tile runs NMOD passes of the K loop: warp 0 streams 72 KB stages
+// (six K steps: A 24 KB + B 48 KB, two bulk copies) through a 3-slot ring with
+// cp.async.bulk, warp 1 issues six 128 x 256 x 32 MMAs per stage (one commit
+// per stage: every stage's copy and barrier round trip costs time that the
+// MMAs do not hide, so fewer, larger stages run faster: 1, 2, 3, 4, 5, 6 K
+// steps per stage measured 2.33, 1.37, 1.12, 0.92, 0.87, 0.85 ms at 1250^3 x 8,
+// and 8 steps in two slots 0.90 ms, the ring then too shallow) into one of two
 // 256-column TMEM accumulators, and eight epilogue warps turn a finished
 // accumulator into int8 residues (in a residue buffer, one plane per modulus)
 // while the MMAs of the next modulus run in the other accumulator.  A rebuild
@@ -61,11 +64,11 @@ constexpr int CRT_BK = 32;                   // K' bytes per stage
 constexpr int CRT_ATILE = CRT_BM * CRT_BK;   // 4 KB
 constexpr int CRT_BTILE = CRT_BN * CRT_BK;   // 8 KB
 constexpr int CRT_STAGE = CRT_ATILE + CRT_BTILE;   // one K step (the probe's operands)
-constexpr int CRT_KSUB = 4;                  // K steps per ring stage: four MMAs per commit
-constexpr int CRT_SA = CRT_KSUB * CRT_ATILE;   // 16 KB: the stage's A tiles, consecutive in memory
-constexpr int CRT_SB = CRT_KSUB * CRT_BTILE;   // 32 KB
-constexpr int CRT_SLOT = CRT_SA + CRT_SB;      // 48 KB
-constexpr int CRT_NS = 4;                    // ring slots (192 KB)
+constexpr int CRT_KSUB = 6;                  // K steps per ring stage: six MMAs per commit
+constexpr int CRT_SA = CRT_KSUB * CRT_ATILE;   // 24 KB: the stage's A tiles, consecutive in memory
+constexpr int CRT_SB = CRT_KSUB * CRT_BTILE;   // 48 KB
+constexpr int CRT_SLOT = CRT_SA + CRT_SB;      // 72 KB
+constexpr int CRT_NS = 3;                    // ring slots (216 KB)
 constexpr int CRT_EPI_WARPS = 8;
 constexpr int CRT_THREADS = 32 * (2 + CRT_EPI_WARPS);
 constexpr uint32_t CRT_IDESC = tc::idesc_i8(CRT_BM, CRT_BN);
@@ -135,13 +138,14 @@ __host__ __device__ constexpr int crt_mod(int t) {
 // 2^e mod p for e = 17, 34, 50 (the limb weights of the operand split below)
 __host__ __device__ constexpr int pow2_mod(int e, int p) { return e == 0 ? 1 % p : (2 * pow2_mod(e - 1, p)) % p; }
 
-// symmetric residue of a 32-bit integer: |r| <= (p - 1) / 2
+// (x + h) mod p, h = (p - 1) / 2, for an int32 accumulator: |x| <= K' 127^2
+// with K' 128^2 < 2^31 (checked on the host), so the offset p floor(2^31 / p)
+// + h (= h mod p) keeps x + offset in [0, 2^32) and one unsigned remainder
+// gives r' = r + h for the symmetric residue r
 template <int P>
-__device__ __forceinline__ int sym_res(int x) {
-    int r = x % P;
-    if (r > P / 2) r -= P;
-    if (r < -(P / 2)) r += P;
-    return r;
+__device__ __forceinline__ uint32_t acc_res_shifted(int x) {
+    constexpr unsigned OFF = (unsigned)P * ((1u << 31) / (unsigned)P) + (unsigned)(P - 1) / 2;
+    return ((unsigned)x + OFF) % (unsigned)P;
 }
 // x (|x| < 2^50, any double) rounded to the nearest integer and returned as
 // the three 17-bit limbs of x + 2^50: 1.5 2^52 + x places the rounded integer
@@ -161,10 +165,6 @@ __device__ __forceinline__ double scale2(double x, int e) {
     return ldexp(x, e);
 }
 
-__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-    return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
-           ((uint32_t)(uint8_t)d << 24);
-}
 
 // f(std::integral_constant<int, t>) for t = 0 .. NMOD-1 (the modulus a compile-time constant in each call)
 template <int T, typename F>
@@ -399,8 +399,9 @@ __device__ __forceinline__ bool crt_extract_tile(const CrtArgs& g, uint32_t tmem
                 uint32_t w[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    w[q] = pack4(sym_res<P>((int)r[4 * q]), sym_res<P>((int)r[4 * q + 1]),
-                                 sym_res<P>((int)r[4 * q + 2]), sym_res<P>((int)r[4 * q + 3]));
+                    w[q] = __vsub4(bytes4(acc_res_shifted<P>((int)r[4 * q]), acc_res_shifted<P>((int)r[4 * q + 1]),
+                                          acc_res_shifted<P>((int)r[4 * q + 2]), acc_res_shifted<P>((int)r[4 * q + 3])),
+                                   half4<P>());
                 *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
                 *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
             }
@@ -594,9 +595,11 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
 // and A rows 128-255 and B columns 128-255 from the odd CTA's, at the same
 // offsets; each CTA's TMEM receives its 128 rows.  Per SM and K step a CTA
 // stages 4 KB of A and 4 KB of B for 128 x 256 multiply-adds where the
-// single-CTA tile stages 4 + 8 KB: the shared-memory traffic of the copies
-// drops by a third (with the operand reads, shared-memory bandwidth is what
-// bounds the single-CTA kernel), and the 32 KB stages allow a six-deep ring.
+// single-CTA tile stages 4 + 8 KB, so the copies per multiply-add drop by a
+// third.  Measured it is the slower of the two (1874 against 2187 int8 TOPS
+// at 1250^3 x 8 with four K steps per stage; neither the copies nor shared-
+// memory bandwidth bound the single-CTA kernel, whose MMA stream probes at
+// full rate beside concurrent copies), so it is opt-in (sc_crt_tiles_set).
 // Both CTAs load their halves with 2-D tensor copies (cta_group::2, no
 // multicast) that complete on the even CTA's stage barrier, which expects the
 // bytes of both; the MMA thread's commits arrive on the barriers of both CTAs
@@ -605,11 +608,13 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
 // barrier.  Every wait is bounded and gives up once either CTA has aborted; a
 // CTA that aborts raises the other's flag through distributed shared memory.
 constexpr int C2_BTILE = CRT_BTILE / 2;             // 128 columns x 32 K bytes
-constexpr int C2_SA = CRT_KSUB * CRT_ATILE;         // 16 KB
-constexpr int C2_SB = CRT_KSUB * C2_BTILE;          // 16 KB
-constexpr int C2_SLOT = C2_SA + C2_SB;              // 32 KB
-constexpr int C2_NS = 6;                            // ring slots (192 KB)
-constexpr int C2_ROW = 256;                         // bytes per row of the tensor maps (box 256 x 64 = one stage)
+constexpr int C2_SA = CRT_KSUB * CRT_ATILE;         // 24 KB
+constexpr int C2_SB = CRT_KSUB * C2_BTILE;          // 24 KB
+constexpr int C2_SLOT = C2_SA + C2_SB;              // 48 KB
+constexpr int C2_NS = (192 * 1024) / C2_SLOT;      // ring slots (192 KB)
+constexpr int C2_ROW = 256;                         // bytes per row of the tensor maps (box 256 x 96 = one stage)
+static_assert(C2_SA % C2_ROW == 0 && C2_SA / C2_ROW <= 256, "tensor box rows");
+static_assert(CRT_NS * CRT_SLOT + 1024 <= 227 * 1024 && C2_NS * C2_SLOT + 1024 <= 227 * 1024, "shared memory");
 constexpr uint32_t C2_IDESC = tc::idesc_i8(2 * CRT_BM, CRT_BN);
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1)
@@ -664,8 +669,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer (both CTAs): this CTA's 128 rows of A and 128 columns of B, one 16 KB box each per
-            // stage (a stage of fewer than four K steps loads the box all the same; the MMAs skip the rest)
+            // producer (both CTAs): this CTA's 128 rows of A and 128 columns of B, one box each per stage
+            // (a stage of fewer than CRT_KSUB K steps loads the whole box; the MMAs skip the rest)
             long long stage = 0;
             for (int tile = pair; tile < g.ntiles && !*aborted; tile += npairs) {
                 const int cb = tile % g.CB, rb2 = (tile / g.CB) % RB2, b = tile / (g.CB * RB2);
@@ -753,7 +758,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1)
 }
 
 // 2-D byte tensor over a packed operand buffer: rows of 256 bytes, boxes of
-// 256 x 64 (one 16 KB stage); the driver's encoder comes through the runtime
+// 256 x C2_SA / 256 rows (one stage); the driver's encoder comes through the runtime
 // (no link against the driver library)
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
