@@ -682,7 +682,7 @@ def run_sweep_ours(args):
                        "sc_volume_solve (--external) each; sweep time = sum over strata of population x mean time")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "strong", "vs_baseline": None, "dtype": "int8 tensor products (7 digit slices) + f64",
+                "scaling": "strong", "vs_baseline": None, "dtype": "int8 tensor products (modular, 14 moduli, or 7 digit slices, per shape) + f64",
                 "data": "synthetic",
                 "config": {"workload": SWEEP_NAME, "seed": SWEEP_SEED, "path": "batched mixed precision",
                            "l2": "flushed between steps (256 MB write, untimed); working set >> L2",
