@@ -1014,7 +1014,17 @@ def run_field_ours(args):
                       [int(sum(1 for zz in wt.z_layers if FIELD_GRID["origin"][2] + FIELD_GRID["step"][2] * i >=
                                zz - 0.001)) for i in planes]) * FIELD_GRID["counts"][0] * FIELD_GRID["counts"][1]
     direct_rate = {"float32_fp64_phase": plane_evals / (t32 / 1e3), "float64": plane_evals / (t64 / 1e3)}
-    nw_table = int(wt.E0.shape[0])
+    # interior planes per layer (the order-sum kernel reads each layer's mode fields once per group of up
+    # to 4 of its planes)
+    zls = [float(z) for z in wt.z_layers]
+    per_layer = {}
+    for i in range(FIELD_GRID["counts"][2]):
+        zi = FIELD_GRID["origin"][2] + FIELD_GRID["step"][2] * i
+        r = sum(1 for zz in zls if zi >= zz - 0.001)
+        if 1 <= r <= len(zls) - 1:
+            per_layer[r - 1] = per_layer.get(r - 1, 0) + 1
+    plane_groups = sum((c + 3) // 4 for c in per_layer.values())
+    interior_planes = sum(per_layer.values())
     del wt
 
     # the thin-volume slice (configs[0]-sized): factorised and direct
@@ -1054,23 +1064,35 @@ def run_field_ours(args):
 
     # roofline: the dominant stage by device time
     st = {k: statistics.mean(s[k] for s in stages) for k in ("fft", "assemble", "eig", "chain", "total")}
-    names = {"fft": "wave table (waves_kernel) + phase tables", "assemble": "order sums (field_h_kernel)",
+    names = {"fft": "boundary wave table + phase tables",
+             "assemble": "order sums (field_hq_kernel from the layers' mode fields, field_h_kernel outside)",
              "eig": "y transform (field_u_kernel)", "chain": "x transform + output (field_e_kernel)"}
     MF, Mx, Ny = sol.dims.MF, sol.dims.Mx, FIELD_GRID["counts"][1]
     dom = max(("fft", "assemble", "eig", "chain"), key=lambda k: st[k])
     nz = FIELD_GRID["counts"][2]
     peak = float(_peaks().get("hbm_gbs", 6650.0))
     zb = sol.shape[0]
-    # algorithmic bytes per stage: table written + solution read; table read per plane's region (two
-    # internal lists); U written; output written + U read
-    bytes_dom = {"fft": nw_table * 96 + 2 * zb * 3 * MF * 2 * MF * 16,
-                 "assemble": nz * 2 * (2 * MF * MF) * 96,
+    # algorithmic bytes per stage: boundary wave table (3 MF waves) + the x / y phase tables; the interior
+    # planes' mode fields (Qc and Qh of the layer, once per group of planes) + the slice partial sums; U
+    # written; output written + U read
+    bytes_dom = {"fft": 3 * MF * 96 + (FIELD_GRID["counts"][0] * Mx + FIELD_GRID["counts"][1] * sol.dims.My) * 16,
+                 "assemble": plane_groups * 2 * (3 * MF * 2 * MF) * 16 + 8 * interior_planes * 3 * MF * 16,
                  "eig": nz * 3 * Mx * Ny * 16,
                  "chain": out_bytes + nz * 3 * Mx * Ny * 16}[dom]
     roofline = {"bound": "hbm", "achieved": bytes_dom / (st[dom] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": bytes_dom / (st[dom] / 1e3) / 1e9 / peak, "traffic": None, "kernel": names[dom],
                 "algorithmic_bytes": bytes_dom, "stage_ms": {names[k]: round(st[k], 3) for k in names},
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if _peaks() else "fallback 6650 GB/s"}
+    if dom == "chain":
+        # the x transform is FP64-bound: 3 Mx complex multiply-adds (8 flops each) per point, against the FP64
+        # FMA rate measured in this run; its output write is reported beside it
+        flops = 8.0 * 3 * Mx * npts
+        fp64_peak = ctx.fp64_peak_tflops()
+        ach = flops / (st[dom] / 1e3) / 1e12
+        roofline.update({"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": ach / fp64_peak, "algorithmic_flops": flops,
+                         "peak_source": "FP64 FMA probe measured in this run",
+                         "hbm_gbs_of_output_write": bytes_dom / (st[dom] / 1e3) / 1e9})
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:

@@ -21,88 +21,101 @@ namespace sc {
 namespace {
 constexpr int ET = 256;
 
-__global__ void waves_kernel(int MF, int Z, const double2* __restrict__ Sx, const double2* __restrict__ Sy,
-                             const double2* __restrict__ Sz0, const double2* __restrict__ Sz1,
-                             const double2* __restrict__ EF, const double2* __restrict__ x,
-                             const double2* __restrict__ evl, const double2* __restrict__ Qc,
-                             const double2* __restrict__ Qh, const double* __restrict__ zpl, double k, double ntop,
-                             double nbot, int external, int ez_mode, long long nw, double2* __restrict__ E0,
-                             double2* __restrict__ K) {
-    const int n2 = 2 * MF, n3 = 3 * MF, n4 = 4 * MF;
-    const long long internal = (long long)n2 * MF;   // waves per internal list
-    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
-         w += (long long)gridDim.x * blockDim.x) {
-        // locate the wave: Pi | (Pr_0, Pt_0) | (Pr_1, Pt_1) | ... | (Pr_Z, Pt_Z)
-        long long o = w;
+struct WaveSrc {
+    int MF, Z, external, ez_mode;
+    const double2 *Sx, *Sy, *Sz0, *Sz1, *EF, *x, *evl, *Qc, *Qh;
+    const double* zpl;
+    double k, ntop, nbot;
+};
+
+// one entry of the table: kind 0 incident, 1 reflected, 2 transmitted (order
+// p), 3 internal (order p, mode jj of `layer`'s list `parity`, e[] already
+// holding the mode's field from Q); returns E0 wound to the origin and k
+__device__ __forceinline__ void wave_entry(const WaveSrc& s, int kind, long long p, long long jj, int layer,
+                                           int parity, double zl, double2 (&e)[3], double2 (&kv)[3]) {
+    const int MF = s.MF;
+    kv[0] = cscale(s.Sx[p], s.k);
+    kv[1] = cscale(s.Sy[p], s.k);
+    if (kind == 0) {
+        kv[2] = cscale(s.Sz0[p], s.k);
+        e[0] = s.EF[p];
+        e[1] = s.EF[MF + p];
+        e[2] = s.EF[2 * MF + p];
+    } else if (kind == 1) {
+        kv[2] = cscale(s.Sz0[p], -s.k * s.ntop);
+        e[0] = s.x[p];
+        e[1] = s.x[MF + p];
+        e[2] = s.x[2 * MF + p];
+    } else if (kind == 2) {
+        kv[2] = cscale(s.Sz1[p], s.k * s.nbot);
+        e[0] = s.x[3 * MF + p];
+        e[1] = s.x[4 * MF + p];
+        e[2] = s.x[5 * MF + p];
+    } else {
+        kv[2] = cscale(s.evl[(long long)layer * 4 * MF + 2 * jj + parity], s.k);
+    }
+    if (s.ez_mode == 1) {
+        // E_z from transversality, as the .cw reader rebuilds it
+        e[2] = cneg(cdiv(cadd(cmul(kv[0], e[0]), cmul(kv[1], e[1])), kv[2]));
+    }
+    if (kind != 0) {
+        // wind(0, 0, -z_l): E0 *= exp(i kz (-z_l))
+        double2 ph = cexp(cmul(make_double2(0.0, 1.0), cscale(kv[2], -zl)));
+        for (int c = 0; c < 3; ++c) e[c] = cmul(e[c], ph);
+    }
+}
+
+// Table layout (cw_unpack order): Pi (MF) | Pr_0 (MF) | layer 0 parity 0,
+// layer 0 parity 1, ..., layer Z-1 parity 1 (2 MF x MF waves each, order p
+// major, mode jj minor; absent with --external) | Pt_Z (MF).
+// The three boundary lists: one thread per wave; Pt_Z starts at t_base
+// (2 MF + the internal lists in the full table, 2 MF in a compact one).
+__global__ void waves_boundary_kernel(WaveSrc s, long long t_base, double2* __restrict__ E0,
+                                      double2* __restrict__ K) {
+    const int MF = s.MF;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * MF; t += gridDim.x * blockDim.x) {
+        const int kind = t / MF;
+        const long long p = t - (long long)kind * MF;
+        const long long w = (kind == 2) ? t_base + p : t;
+        const double zl = (kind == 1) ? s.zpl[0] : (kind == 2) ? s.zpl[s.Z] : 0.0;
         double2 e[3], kv[3];
-        double zl = 0.0;
-        int kind = -1, layer = -1, parity = 0;
-        long long idx = 0;
-        if (o < MF) {
-            kind = 0;  // incident
-            idx = o;
-        } else {
-            o -= MF;
-            for (int l = 0; l <= Z && kind < 0; ++l) {
-                long long npr = (l == 0) ? MF : (external ? 0 : internal);
-                long long npt = (l == Z) ? MF : (external ? 0 : internal);
-                if (o < npr) {
-                    if (l == 0) kind = 1;  // reflected
-                    else { kind = 3; layer = l - 1; parity = 1; }
-                    idx = o;
-                    zl = zpl[l];
-                } else if (o < npr + npt) {
-                    o -= npr;
-                    if (l == Z) kind = 2;  // transmitted
-                    else { kind = 3; layer = l; parity = 0; }
-                    idx = o;
-                    zl = zpl[l];
-                } else {
-                    o -= npr + npt;
-                }
-            }
-        }
-        if (kind <= 2) {
-            const long long p = idx;
-            kv[0] = cscale(Sx[p], k);
-            kv[1] = cscale(Sy[p], k);
-            if (kind == 0) {
-                kv[2] = cscale(Sz0[p], k);
-                e[0] = EF[p];
-                e[1] = EF[MF + p];
-                e[2] = EF[2 * MF + p];
-            } else if (kind == 1) {
-                kv[2] = cscale(Sz0[p], -k * ntop);
-                e[0] = x[p];
-                e[1] = x[MF + p];
-                e[2] = x[2 * MF + p];
-            } else {
-                kv[2] = cscale(Sz1[p], k * nbot);
-                e[0] = x[3 * MF + p];
-                e[1] = x[4 * MF + p];
-                e[2] = x[5 * MF + p];
-            }
-        } else {
-            const long long p = idx / n2, jj = idx % n2;
-            kv[0] = cscale(Sx[p], k);
-            kv[1] = cscale(Sy[p], k);
-            kv[2] = cscale(evl[(long long)layer * n4 + 2 * jj + parity], k);
-            const double2* Q = (parity ? Qh : Qc) + (long long)layer * n3 * n2 + jj * n3;
-            e[0] = Q[p];
-            e[1] = Q[MF + p];
-            e[2] = Q[2 * MF + p];
-        }
-        if (ez_mode == 1) {
-            // E_z from transversality, as the .cw reader rebuilds it
-            e[2] = cneg(cdiv(cadd(cmul(kv[0], e[0]), cmul(kv[1], e[1])), kv[2]));
-        }
-        if (kind != 0) {
-            // wind(0, 0, -z_l): E0 *= exp(i kz (-z_l))
-            double2 ph = cexp(cmul(make_double2(0.0, 1.0), cscale(kv[2], -zl)));
-            for (int c = 0; c < 3; ++c) e[c] = cmul(e[c], ph);
-        }
+        wave_entry(s, kind, p, 0, -1, 0, zl, e, kv);
         for (int c = 0; c < 3; ++c) {
             E0[w * 3 + c] = e[c];
+            K[w * 3 + c] = kv[c];
+        }
+    }
+}
+
+// The internal lists, one block per tile of 16 modes x 32 orders of one list
+// (grid z = 2 layer + parity): the mode fields are read from Q along the
+// order index (contiguous in Q) into shared memory, and the table is written
+// along the mode index (contiguous in the table), both coalesced.
+constexpr int WJ = 16, WP = 32;
+__global__ void __launch_bounds__(256) waves_internal_kernel(WaveSrc s, double2* __restrict__ E0,
+                                                             double2* __restrict__ K) {
+    __shared__ double2 sq[3][WJ][WP + 1];
+    const int MF = s.MF, n2 = 2 * MF, n3 = 3 * MF;
+    const int q = blockIdx.z, layer = q >> 1, parity = q & 1;
+    const int j0 = blockIdx.x * WJ, p0 = blockIdx.y * WP;
+    const double2* Q = (parity ? s.Qh : s.Qc) + (long long)layer * n3 * n2;
+    for (int e = threadIdx.x; e < 3 * WJ * WP; e += blockDim.x) {
+        const int c = e / (WJ * WP), r = (e / WP) % WJ, pp = e % WP;
+        const int jj = j0 + r, p = p0 + pp;
+        sq[c][r][pp] = (jj < n2 && p < MF) ? Q[(long long)jj * n3 + c * MF + p] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const double zl = s.zpl[layer + parity];
+    const long long w0 = 2LL * MF + (long long)q * n2 * MF;
+    for (int e = threadIdx.x; e < WJ * WP; e += blockDim.x) {
+        const int jl = e % WJ, pl = e / WJ;
+        const int jj = j0 + jl, p = p0 + pl;
+        if (jj >= n2 || p >= MF) continue;
+        double2 ev[3] = {sq[0][jl][pl], sq[1][jl][pl], sq[2][jl][pl]}, kv[3];
+        wave_entry(s, 3, p, jj, layer, parity, zl, ev, kv);
+        const long long w = w0 + (long long)p * n2 + jj;
+        for (int c = 0; c < 3; ++c) {
+            E0[w * 3 + c] = ev[c];
             K[w * 3 + c] = kv[c];
         }
     }
@@ -198,14 +211,36 @@ sc_status volume_waves_launch(cudaStream_t st, int MF, int Z, const double2* sve
                               const double2* evl, const double2* Qc, const double2* Qh, const double* zpl,
                               double k, double ntop, double nbot, int external, int ez_mode, long long nw,
                               double2* E0, double2* K) {
-    long long blocks = (nw + 255) / 256;
-    if (blocks > 16384) blocks = 16384;
-    if (blocks < 1) blocks = 1;
-    waves_kernel<<<(unsigned)blocks, 256, 0, st>>>(MF, Z, svec, svec + MF, svec + 2 * MF, svec + 3 * MF,
-                                                   svec + 4 * MF, x, evl, Qc, Qh, zpl, k, ntop, nbot, external,
-                                                   ez_mode, nw, E0, K);
+    const long long internal = external ? 0 : 2LL * Z * (2LL * MF * MF);
+    if (nw != 3LL * MF + internal) {
+        set_error("volume_waves: table of %lld waves, expected %lld", nw, 3LL * MF + internal);
+        return SC_BADINPUT;
+    }
+    WaveSrc s{MF, Z, external, ez_mode, svec, svec + MF, svec + 2 * MF, svec + 3 * MF, svec + 4 * MF,
+              x, evl, Qc, Qh, zpl, k, ntop, nbot};
+    waves_boundary_kernel<<<(3 * MF + 255) / 256, 256, 0, st>>>(s, 2LL * MF + internal, E0, K);
     count_launch();
+    if (internal > 0) {
+        if (2LL * Z > 65535) {
+            set_error("volume_waves: too many layers (%d)", Z);
+            return SC_BADINPUT;
+        }
+        waves_internal_kernel<<<dim3((2 * MF + WJ - 1) / WJ, (MF + WP - 1) / WP, 2 * Z), 256, 0, st>>>(s, E0, K);
+        count_launch();
+    }
     SC_CHECK_LAUNCH("volume_waves");
+    return SC_OK;
+}
+
+// the compact table of the three boundary lists only: Pi | Pr_0 | Pt_Z (3 MF waves)
+sc_status volume_boundary_waves_launch(cudaStream_t st, int MF, int Z, const double2* svec, const double2* x,
+                                       const double* zpl, double k, double ntop, double nbot, int external,
+                                       int ez_mode, double2* E0, double2* K) {
+    WaveSrc s{MF, Z, external, ez_mode, svec, svec + MF, svec + 2 * MF, svec + 3 * MF, svec + 4 * MF,
+              x, nullptr, nullptr, nullptr, zpl, k, ntop, nbot};
+    waves_boundary_kernel<<<(3 * MF + 255) / 256, 256, 0, st>>>(s, 2LL * MF, E0, K);
+    count_launch();
+    SC_CHECK_LAUNCH("volume_boundary_waves");
     return SC_OK;
 }
 

@@ -19,7 +19,7 @@ enum WsSlot {
     WS_EVAL_W, WS_EVAL_IDX, WS_STATS,
     WS_HY, WS_HV, WS_HT, WS_HPART, WS_HW, WS_HW2, WS_INV, WS_TREE, WS_GEMV, WS_BINS,
     WS_SWEEP, WS_SWEEP_PTR, WS_OZ_A, WS_OZ_B, WS_OZ_E, WS_OZ_ERR, WS_TUNE_C, WS_TUNE_P,
-    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR, WS_MFUN_OUT, WS_CHAIN_T, WS_CRT_RES, WS_FIELD_W, WS_FIELD_T, WS_FIELD_H, WS_FIELD_U, WS_CW_STAGE,
+    WS_LAYER, WS_LAYER_STATUS, WS_MFUN_PTR, WS_MFUN_OUT, WS_CHAIN_T, WS_CRT_RES, WS_FIELD_W, WS_FIELD_T, WS_FIELD_H, WS_FIELD_U, WS_FIELD_HP, WS_FIELD_G, WS_CW_STAGE,
     WS_COUNT
 };
 
