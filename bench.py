@@ -32,7 +32,9 @@ map's 256x256 x-z slice beside it.
 --workload surrogate: the learned surrogate: trains the network on
 --train-solves plain solves for --epochs, then times the 2000 held-out maps with
 the energy-balance fallback at several gate tolerances (the headline gate is the
-loosest with p90 error <= 1e-2), beside the fallback-only and per-instance paths.
+fastest with p90 error <= 1e-2), beside the fallback-only and per-instance paths;
+--ensemble 2 trains two networks, predicts their mean and also falls back where
+they disagree.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload sweep|volume|layer|field|surrogate]
 
@@ -1136,6 +1138,7 @@ SUR_NAME = ("FNO surrogate (4 spectral layers, width 64, 16x16 modes) of the thi
             "disk/triangle maps (n 1.0-1.6, 10x10 um, 1 um slab), lambda 0.4-0.8 um, 11x11 orders; trained on "
             "plain batched FP64 solves, evaluated on 2000 held-out maps (seeds 100000-101999)")
 SUR_GATES = (1e-3, 3e-4, 1e-4, 3e-5)
+SUR_SPREADS = (2e-2, 1e-2, 5e-3, 2.5e-3)   # ensemble: largest relative distance of a member from the mean
 
 
 def run_surrogate_reference(args):
@@ -1176,15 +1179,20 @@ def run_surrogate_ours(args):
     tmaps, tlams, tx = sg.generate(ctx, range(args.train_solves))
     maps, lams, xs = sg.generate(ctx, range(100000, 102000))
     gen_s = time.perf_counter() - t0
-    sur = sg.Surrogate(0, max_batch=64, seed=0)
+    # one network, or an ensemble of networks from different initialisations and shuffles
+    surs = [sg.Surrogate(0, max_batch=64, seed=i) for i in range(max(1, args.ensemble))]
     t0 = time.perf_counter()
-    sg.train(sur, tmaps, tlams, np.stack([sg.x_to_target(x) for x in tx]), args.epochs, 64, 1e-3)
-    sur.status()
+    ttgt = np.stack([sg.x_to_target(x) for x in tx])
+    for i, su in enumerate(surs):
+        sg.train(su, tmaps, tlams, ttgt, args.epochs, 64, 1e-3, seed=i)
+        su.status()
     train_s = time.perf_counter() - t0
     dm, dl = torch.from_numpy(maps).cuda(), torch.from_numpy(lams).cuda()
-    pred = sg.target_to_x(sur.forward(dm, dl).cpu().numpy())
+    preds = [sg.target_to_x(su.forward(dm, dl).cpu().numpy()) for su in surs]
+    pred = np.mean(preds, axis=0)
     err_net = sg.rel_err(pred, xs)
     energy = sg.energy_error(pred, lams)
+    sur = surs if len(surs) > 1 else surs[0]
     stream = torch.cuda.current_stream()
 
     def timed(fn):
@@ -1197,18 +1205,22 @@ def run_surrogate_ours(args):
         return out, e0.elapsed_time(e1)
 
     gates = {}
-    for tol in SUR_GATES:
+    # energy-balance gates, and with an ensemble also the members' disagreement (loosest first)
+    combos = [(tol, None) for tol in SUR_GATES]
+    if len(surs) > 1:
+        combos = [(tol, sp) for tol in SUR_GATES[:2] for sp in (None,) + SUR_SPREADS]
+    for tol, sp in combos:
         for _ in range(args.warmup):
-            sg.predict_with_fallback(sur, ctx, maps, lams, tol)
+            sg.predict_with_fallback(sur, ctx, maps, lams, tol, sp)
         ms = []
         for _ in range(args.steps):
-            (out, bad), t = timed(lambda: sg.predict_with_fallback(sur, ctx, maps, lams, tol))
+            (out, bad), t = timed(lambda: sg.predict_with_fallback(sur, ctx, maps, lams, tol, sp))
             ms.append(t)
         err = sg.rel_err(out, xs)
-        gates[f"{tol:g}"] = {"solves_per_s": len(maps) / (statistics.mean(ms) / 1e3),
-                             "fallback_fraction": float(bad.mean()),
-                             "rel_err": {"median": float(np.median(err)), "p90": float(np.quantile(err, 0.9)),
-                                         "max": float(err.max())}}
+        gates[f"{tol:g}" if sp is None else f"{tol:g}, spread {sp:g}"] = {
+            "solves_per_s": len(maps) / (statistics.mean(ms) / 1e3), "fallback_fraction": float(bad.mean()),
+            "rel_err": {"median": float(np.median(err)), "p90": float(np.quantile(err, 0.9)),
+                        "max": float(err.max())}}
     # the same held-out maps through the batched plain solve alone (the fallback-only method), and the plain
     # per-instance path on a sample
     _, t_fb = timed(lambda: sg.solve_plain(ctx, maps, lams))
@@ -1219,16 +1231,19 @@ def run_surrogate_ours(args):
         _, t = timed(lambda: solver.solve(ctx, sg.params_for(float(lams[i])), d, fields=False))
         t_plain += t
     plain = len(sub) / (t_plain / 1e3)
-    # headline gate: the loosest whose p90 error with fallback is within 1e-2
+    # headline gate: the fastest whose p90 error with fallback is within 1e-2
     ok = [k for k in gates if gates[k]["rel_err"]["p90"] <= 1e-2]
-    head = ok[0] if ok else f"{SUR_GATES[-1]:g}"
+    head = max(ok, key=lambda k: gates[k]["solves_per_s"]) if ok else list(gates)[-1]
     value = gates[head]["solves_per_s"]
     line = {"metric": SUR_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": len(maps) / value * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network (fp32 accumulate) + f64 fallback",
             "data": "synthetic",
             "config": {"workload": SUR_NAME, "train_solves": args.train_solves, "epochs": args.epochs,
-                       "gate": f"|energy balance error| <= {head}"},
+                       "networks": len(surs),
+                       "gate": f"|energy balance error| <= {head.split(',')[0]}" +
+                               (f", members' relative disagreement <= {head.split('spread ')[1]}"
+                                if "spread" in head else "")},
             "paths": {"gates": gates, "network_alone_rel_err": {"median": float(np.median(err_net)),
                                                                 "p90": float(np.quantile(err_net, 0.9)),
                                                                 "max": float(err_net.max())},
@@ -1239,7 +1254,8 @@ def run_surrogate_ours(args):
                       "speedup_vs_fallback_only": value / (len(maps) / (t_fb / 1e3)),
                       "generate_s": gen_s, "train_s": train_s}}
     print(json.dumps(line), flush=True)
-    sur.close()
+    for su in surs:
+        su.close()
     ctx.close()
     return 0
 
@@ -1597,6 +1613,9 @@ def main():
     ap.add_argument("--workload", default="sweep", choices=["sweep", "volume", "layer", "field", "surrogate"])
     ap.add_argument("--train-solves", type=int, default=150000, help="surrogate workload: training solves")
     ap.add_argument("--epochs", type=int, default=30, help="surrogate workload: training epochs")
+    ap.add_argument("--ensemble", type=int, default=1,
+                    help="surrogate workload: networks trained from different seeds (their mean is the prediction; "
+                         "with 2 or more, a sample whose members disagree also falls back)")
     ap.add_argument("--case", nargs=argparse.REMAINDER, help="run one named profiling case instead")
     args = ap.parse_args()
     if args.case:

@@ -883,8 +883,9 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         SC_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &host_const, sizeof(CrtConst)));
         SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          CRT_NS * CRT_SLOT + 1024));
-        SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         C2_NS * C2_SLOT + 1024));
+        const bool pair_ok = cudaFuncSetAttribute(crt_mma2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  C2_NS * C2_SLOT + 1024) == cudaSuccess;
+        if (!pair_ok) (void)cudaGetLastError();
         // clusters of two that fit on the device at once (SMs left without a
         // partner in their GPC cannot hold one): the pair kernel's grid
         cudaLaunchConfig_t cfg = {};
@@ -892,7 +893,10 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         cfg.blockDim = dim3(CRT_THREADS, 1, 1);
         cfg.dynamicSmemBytes = C2_NS * C2_SLOT + 1024;
         int ncl = 0;
-        SC_CUDA_TRY(cudaOccupancyMaxActiveClusters(&ncl, crt_mma2_kernel, &cfg));
+        if (!pair_ok || cudaOccupancyMaxActiveClusters(&ncl, crt_mma2_kernel, &cfg) != cudaSuccess) {
+            ncl = 0;                 // no CTA pairs: the single-CTA tiles serve every product
+            (void)cudaGetLastError();
+        }
         g_crt_pairs[dev] = ncl;
         g_crt_const_ready[dev] = true;
     }

@@ -670,7 +670,7 @@ Gemm mk(int m, int n, int k, int batch, float alpha, float beta, const float* A,
 // the weight gradients contract over the 4096 pixels of one sample: split K
 // into KSPLIT chunks (one partial per sample and chunk, summed by batch_sum),
 // so that the product runs on Bn x KSPLIT CTAs instead of Bn
-Gemm ksplit(Gemm g) {
+Gemm split_k(Gemm g) {
     g.ksplit = KSPLIT;
     return g;
 }
@@ -740,7 +740,7 @@ sc_status forward(sc_fno* f, const float* maps, const float* lam, int Bn, cudaSt
     count_launch();
     // readout correlations P_b (12 x 244) = o_b (12 x NP) R (NP x 244): K = NP split into KSPLIT chunks,
     // the partials summed per sample
-    SC_TRY(gemm(st, ksplit(mk(COUT, PW, NP, Bn, 1.f, 0.f, f->o12, NP, 1, so, f->R, PW, 1, 0, f->part, PW, 1,
+    SC_TRY(gemm(st, split_k(mk(COUT, PW, NP, Bn, 1.f, 0.f, f->o12, NP, 1, so, f->R, PW, 1, 0, f->part, PW, 1,
                               (long long)COUT * PW))));
     ksum_kernel<<<blocks((long long)Bn * COUT * PW), 256, 0, st>>>(f->part, KSPLIT, Bn, (long long)COUT * PW, f->P);
     count_launch();
@@ -764,7 +764,7 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     SC_TRY(gemm(st, mk(COUT, NP, PW, Bn, 1.f, 0.f, f->dP, PW, 1, (long long)COUT * PW, f->R, 1, PW, 0, f->do12, NP,
                        1, so)));
     // Q2, bQ2: per-sample partials, then summed over the batch
-    SC_TRY(gemm(st, ksplit(mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
+    SC_TRY(gemm(st, split_k(mk(COUT, HID, NP, Bn, 1.f, 0.f, f->do12, NP, 1, so, f->h, 1, NP, sh, f->part, HID, 1,
                               (long long)COUT * HID))));
     SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)COUT * HID, g + Ly.Q2));
     bias_grad(st, f->do12, COUT, Bn, g + Ly.bQ2, f->bpart);
@@ -772,7 +772,7 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
     SC_TRY(gemm(st, mk(HID, NP, COUT, Bn, 1.f, 0.f, w + Ly.Q2, 1, HID, 0, f->do12, NP, 1, so, f->dh, NP, 1, sh)));
     gelu_back_kernel<<<blocks((long long)Bn * sh), 256, 0, st>>>(f->dh, f->hpre, (long long)Bn * sh);
     count_launch();
-    SC_TRY(gemm(st, ksplit(mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
+    SC_TRY(gemm(st, split_k(mk(HID, W, NP, Bn, 1.f, 0.f, f->dh, NP, 1, sh, f->act[L], 1, NP, sv, f->part, W, 1,
                               (long long)HID * W))));
     SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)HID * W, g + Ly.Q1));
     bias_grad(st, f->dh, HID, Bn, g + Ly.bQ1, f->bpart);
@@ -788,7 +788,7 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
         bias_grad(st, du, W, Bn, g + Ly.bl[l], f->bpart);
         const float* vin = f->act[l];
         // W_l
-        SC_TRY(gemm(st, ksplit(mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1,
+        SC_TRY(gemm(st, split_k(mk(W, W, NP, Bn, 1.f, 0.f, du, NP, 1, sv, vin, 1, NP, sv, f->part, W, 1,
                                   (long long)W * W))));
         SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)W * W, g + Ly.Wl[l]));
         // dv_l = W_l^T du
@@ -833,7 +833,7 @@ sc_status backward(sc_fno* f, const float* tgt, int Bn, cudaStream_t st) {
         std::swap(f->dact, f->dv);
     }
     // lift
-    SC_TRY(gemm(st, ksplit(mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part,
+    SC_TRY(gemm(st, split_k(mk(W, CIN, NP, Bn, 1.f, 0.f, f->dact, NP, 1, sv, f->in, 1, NP, (long long)CIN * NP, f->part,
                               CIN, 1, (long long)W * CIN))));
     SC_TRY(batch_sum(st, f->part, Bn * KSPLIT, (long long)W * CIN, g + Ly.P));
     bias_grad(st, f->dact, W, Bn, g + Ly.bP, f->bpart);

@@ -226,12 +226,21 @@ def train(sur: Surrogate, maps, lams, targets, epochs: int, batch: int = 64, lr:
     return hist
 
 
-def predict_with_fallback(sur: Surrogate, ctx, maps, lams, tol: float = ENERGY_TOL):
-    """Surrogate R/T (N, 726) complex, with the plain solve wherever energy balance fails."""
+def predict_with_fallback(sur, ctx, maps, lams, tol: float = ENERGY_TOL, spread: float | None = None):
+    """Surrogate R/T (N, 726) complex, with the plain solve wherever energy balance fails.
+
+    `sur` is one Surrogate or a list of them (an ensemble trained from different seeds): the prediction is the
+    members' mean, and with `spread` a sample whose members disagree (the largest relative distance of a member
+    from the mean) by more than `spread` falls back as well."""
+    members = list(sur) if isinstance(sur, (list, tuple)) else [sur]
     dm = torch.from_numpy(np.ascontiguousarray(maps, dtype=np.float32)).cuda()
     dl = torch.from_numpy(np.ascontiguousarray(lams, dtype=np.float32)).cuda()
-    pred = target_to_x(sur.forward(dm, dl).cpu().numpy())
+    preds = [target_to_x(m.forward(dm, dl).cpu().numpy()) for m in members]
+    pred = np.mean(preds, axis=0) if len(preds) > 1 else preds[0]
     bad = energy_error(pred, lams) > tol
+    if spread is not None and len(preds) > 1:
+        dis = np.max([rel_err(q, pred) for q in preds], axis=0)
+        bad |= dis > spread
     if bad.any():
         pred[bad] = solve_plain(ctx, np.asarray(maps)[bad], np.asarray(lams)[bad])
     return pred, bad
