@@ -29,7 +29,7 @@ solve of the whole beam (incident waves resident in HBM), in plane waves/s.
 (the work of the direct sum), with the direct evaluator and the 64x64 triangle
 map's 256x256 x-z slice beside it.
 
---workload surrogate: the learned surrogate: trains the network on
+--workload surrogate: the learned surrogate of the thin-volume solve: trains the network on
 --train-solves plain solves for --epochs, then times the 2000 held-out maps with
 the energy-balance fallback at several gate tolerances (the headline gate is the
 fastest with p90 error <= 1e-2), beside the fallback-only and per-instance paths;
@@ -1029,7 +1029,7 @@ def run_field_ours(args):
     interior_planes = sum(per_layer.values())
     del wt
 
-    # the thin-volume slice (configs[0]-sized): factorised and direct
+    # the thin-volume slice (64x64 triangle map, 11x11 orders): factorised and direct
     tsmp = torch.from_numpy(samples.triangle_map(0)).cuda()
     tp = solver.make_params(**THIN_KW)
     tsol = solver.solve(ctx, tp, tsmp)
@@ -1133,7 +1133,7 @@ def run_field_ours(args):
 
 
 # --------------------------------------------------------------------------- surrogate
-SUR_METRIC = "RCWA solves/sec at stated err vs FP64: surrogate with energy-balance fallback (configs[4])"
+SUR_METRIC = "RCWA solves/sec at stated err vs FP64: surrogate with energy-balance fallback (FNO surrogate of the thin-volume solve)"
 SUR_NAME = ("FNO surrogate (4 spectral layers, width 64, 16x16 modes) of the thin-volume solve: 64x64 seeded "
             "disk/triangle maps (n 1.0-1.6, 10x10 um, 1 um slab), lambda 0.4-0.8 um, 11x11 orders; trained on "
             "plain batched FP64 solves, evaluated on 2000 held-out maps (seeds 100000-101999)")

@@ -600,8 +600,8 @@ __global__ void __launch_bounds__(CRT_THREADS, 1) crt_mma_kernel(CrtArgs g) {
 // at 1250^3 x 8 with four K steps per stage; neither the copies nor shared-
 // memory bandwidth bound the single-CTA kernel, whose MMA stream probes at
 // full rate beside concurrent copies), so it is opt-in (sc_crt_tiles_set).
-// Both CTAs load their halves with 2-D tensor copies (cta_group::2, no
-// multicast) that complete on the even CTA's stage barrier, which expects the
+// Both CTAs load their halves with 2-D tensor copies (cta_group::2, each
+// into its own CTA only) that complete on the even CTA's stage barrier, which expects the
 // bytes of both; the MMA thread's commits arrive on the barriers of both CTAs
 // (one commit per CTA).  Each CTA's epilogue warps drain its own TMEM rows as
 // in the single-CTA kernel and release the accumulator on the even CTA's

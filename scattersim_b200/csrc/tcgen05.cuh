@@ -155,7 +155,7 @@ __device__ __forceinline__ void mma2_i8(uint32_t dtmem, uint64_t adesc, uint64_t
         "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
         "r"(0u), "r"(0u));
 }
-// 2-D tensor load (no multicast) into this CTA's shared memory whose completion
+// 2-D tensor load into this CTA's shared memory only, whose completion
 // is counted on a barrier of either CTA of the pair (its shared::cluster
 // address); the tensor map is a kernel parameter (__grid_constant__)
 __device__ __forceinline__ void tma2d_pair(void* dst, const void* tmap, int x, int y, uint32_t bar_cluster) {
