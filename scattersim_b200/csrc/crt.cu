@@ -343,13 +343,14 @@ struct CrtArgs {
     int* err;
 };
 
-// C'_int from its residues (one value): exact limb sums, exact reduction, one rounding
-__device__ __forceinline__ double crt_value(const int (&r)[CRT_NMOD]) {
+// C'_int from its residues (one value), each given as u = r + 128 in [0, 255]:
+// exact limb sums, exact reduction, one rounding
+__device__ __forceinline__ double crt_value(const uint32_t (&u)[CRT_NMOD]) {
     double sh = 0.0, sm = 0.0, sl = 0.0;
 #pragma unroll
     for (int t = 0; t < CRT_NMOD; ++t) {
-        // r + 128 in the low bits of 2^52: an exact int8 -> double without a conversion instruction
-        const double rv = __hiloint2double(0x43300000, r[t] + 128) - 4503599627370624.0;   // 2^52 + 128
+        // u in the low bits of 2^52: an exact int8 -> double without a conversion instruction
+        const double rv = __hiloint2double(0x43300000, (int)u[t]) - 4503599627370624.0;   // 2^52 + 128
         sh = fma(rv, c_crt.wh[t], sh);
         sm = fma(rv, c_crt.wm[t], sm);
         sl = fma(rv, c_crt.wl[t], sl);
@@ -445,12 +446,14 @@ __global__ void __launch_bounds__(256) crt_rebuild_kernel(CrtArgs g) {
         for (int q = 0; q < 8; ++q) {
             const int c = c0 + q;
             if (c >= g.n) break;
-            int rr[CRT_NMOD], ri[CRT_NMOD];
+            uint32_t rr[CRT_NMOD], ri[CRT_NMOD];
 #pragma unroll
             for (int t = 0; t < CRT_NMOD; ++t) {
-                const uint32_t wr = (q < 4) ? re[t].x : re[t].y, wi = (q < 4) ? im[t].x : im[t].y;
-                rr[t] = (int)(int8_t)(wr >> (8 * (q & 3)));
-                ri[t] = (int)(int8_t)(wi >> (8 * (q & 3)));
+                // the residue byte r (two's complement) plus 128 is the byte XOR 0x80, zero-extended
+                const uint32_t wr = ((q < 4) ? re[t].x : re[t].y) ^ 0x80808080u;
+                const uint32_t wi = ((q < 4) ? im[t].x : im[t].y) ^ 0x80808080u;
+                rr[t] = __byte_perm(wr, 0u, 0x4440u | (uint32_t)(q & 3));
+                ri[t] = __byte_perm(wi, 0u, 0x4440u | (uint32_t)(q & 3));
             }
             const int e = ex + g.colexp[(long long)b * g.n + c];
             const int cl = 8 * lane + q;
