@@ -48,12 +48,15 @@ namespace sc {
 
 namespace {
 
-// out_l = c0 I + c1 y + c2 Y2 + c3 Y3 + c4 Y4  (n x n, contiguous, stride n^2)
+// out_l = c0 I + c1 y + c2 Y2 + c3 Y3 + c4 Y4  (inputs n x n, contiguous, stride n^2;
+// out with leading dimension ldo and layer stride so)
 __global__ void poly_block_kernel(int n, const double2* __restrict__ y, const double2* __restrict__ Y2,
                                   const double2* __restrict__ Y3, const double2* __restrict__ Y4, double c0,
-                                  double c1, double c2, double c3, double c4, double2* __restrict__ out) {
+                                  double c1, double c2, double c3, double c4, double2* __restrict__ out, int ldo,
+                                  long long so) {
     const long long nn = (long long)n * n;
     const long long off = (long long)blockIdx.y * nn;
+    double2* o = out + (long long)blockIdx.y * so;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
          t += (long long)gridDim.x * blockDim.x) {
         const long long i = off + t;
@@ -62,15 +65,20 @@ __global__ void poly_block_kernel(int n, const double2* __restrict__ y, const do
         v = cadd(v, cscale(Y3[i], c3));
         if (c4 != 0.0) v = cadd(v, cscale(Y4[i], c4));
         if (t % (n + 1) == 0) v.x += c0;
-        out[i] = v;
+        o[(t / n) * ldo + t % n] = v;
     }
 }
 
-// P[b](i, i) += val for the n x n blocks of a pointer table (leading dimension n)
-__global__ void add_diag_ptr_kernel(int n, double val, double2* const* __restrict__ P) {
+// P[b] <- 2 P[b] - I for the n x n blocks of a pointer table (leading dimension ld)
+__global__ void double_minus_identity_kernel(int n, int ld, double2* const* __restrict__ P) {
     double2* p = P[blockIdx.y];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        p[(long long)i * n + i].x += val;
+    const long long nn = (long long)n * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long r = t % n, c = t / n;
+        double2& v = p[c * ld + r];
+        v = make_double2(2.0 * v.x - (r == c ? 1.0 : 0.0), 2.0 * v.y);
+    }
 }
 
 // A_l *= s_l (real per-layer scale, stored in .x)
@@ -133,10 +141,15 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     double2* Y2 = scr;
     double2* Y3 = scr + (long long)count * nn;
     double2* Y4 = scr + 2LL * count * nn;
-    double2* F = scr + 3LL * count * nn;
-    double2* G = scr + 4LL * count * nn;
-    double2* P1 = scr + 5LL * count * nn;
-    double2* P2 = scr + 6LL * count * nn;
+    // each layer's G and F stacked as one 2 n2 x n2 block [G; F] (leading dimension 2 n2), so that a
+    // double-angle step is one product [G; F] F (F packed once as the right operand); two sets, the
+    // second also holding the Paterson-Stockmeyer temporaries P1, P2 of step 3
+    const int ls = 2 * n2;
+    const long long sS = 2 * nn;
+    double2* S0 = scr + 3LL * count * nn;
+    double2* S1 = scr + 5LL * count * nn;
+    double2* P1 = S1;
+    double2* P2 = S1 + (long long)count * nn;
 
     // 1. scaling per layer: the least s_l >= 1 with (kdz / 2^s_l)^2 ||Omega_l||_1 <= 4
     norm1_kernel<<<count, 256, 0, st>>>(n2, Om, dnorm);
@@ -203,24 +216,23 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     for (int which = 0; which < 2; ++which) {
         double c[13];
         for (int j = 0; j <= 12; ++j) c[j] = 1.0 / factorial(2 * j + which);
-        double2* out = which ? G : F;
-        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[8], c[9], c[10], c[11], c[12], P1);
-        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[4], c[5], c[6], c[7], 0.0, P2);
-        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[0], c[1], c[2], c[3], 0.0, out);
+        double2* out = which ? S0 : S0 + n2;   // G rows, then F rows of the stacked blocks
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[8], c[9], c[10], c[11], c[12], P1, n2, nn);
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[4], c[5], c[6], c[7], 0.0, P2, n2, nn);
+        poly_block_kernel<<<ge, 256, 0, st>>>(n2, y, Y2, Y3, Y4, c[0], c[1], c[2], c[3], 0.0, out, ls, sS);
         count_launch(3);
         SC_CHECK_LAUNCH("poly_block");
         SC_TRY(mm(Y4, n2, nn, P1, n2, nn, P2, n2, nn, one, one, nullptr));
-        SC_TRY(mm(Y4, n2, nn, P2, n2, nn, out, n2, nn, one, one, nullptr));
+        SC_TRY(mm(Y4, n2, nn, P2, n2, nn, out, ls, sS, one, one, nullptr));
     }
 
-    // 4. s_l - 1 double-angle steps per layer.  Each layer's current F and G
-    // live in F or P2 and in G or P1; step j runs over the layers with s_l > j.
-    std::vector<double2*> Fc(count), Fo(count), Gc(count), Go(count);
+    // 4. s_l - 1 double-angle steps per layer: [G; F] <- [G F; 2 F^2 - I].  Each
+    // layer's current stacked block lives in S0 or S1; step j runs over the
+    // layers with s_l > j.
+    std::vector<double2*> Sc(count), So(count);
     for (int l = 0; l < count; ++l) {
-        Fc[l] = F + (long long)l * nn;
-        Fo[l] = P2 + (long long)l * nn;
-        Gc[l] = G + (long long)l * nn;
-        Go[l] = P1 + (long long)l * nn;
+        Sc[l] = S0 + (long long)l * sS;
+        So[l] = S1 + (long long)l * sS;
     }
     std::vector<void*> tab;
     std::vector<std::pair<size_t, int>> steps;   // (table offset, active layers)
@@ -229,29 +241,27 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         for (int l = 0; l < count; ++l)
             if (sl[l] > j) act.push_back(l);
         steps.emplace_back(tab.size(), (int)act.size());
-        for (int l : act) tab.push_back(Gc[l]);
-        for (int l : act) tab.push_back(Fc[l]);
-        for (int l : act) tab.push_back(Go[l]);
-        for (int l : act) tab.push_back(Fo[l]);
-        for (int l : act) {
-            std::swap(Fc[l], Fo[l]);
-            std::swap(Gc[l], Go[l]);
-        }
+        for (int l : act) tab.push_back(Sc[l]);            // [G; F]
+        for (int l : act) tab.push_back(Sc[l] + n2);       // F
+        for (int l : act) tab.push_back(So[l]);            // [G F; F^2]
+        for (int l : act) tab.push_back(So[l] + n2);       // F^2 -> 2 F^2 - I
+        for (int l : act) std::swap(Sc[l], So[l]);
     }
     const size_t last = tab.size();
-    for (int l = 0; l < count; ++l) tab.push_back(Gc[l]);
-    for (int l = 0; l < count; ++l) tab.push_back(Fc[l]);
+    for (int l = 0; l < count; ++l) tab.push_back(Sc[l]);        // G
+    for (int l = 0; l < count; ++l) tab.push_back(Sc[l] + n2);   // F
     void** dtab = nullptr;
     SC_TRY(eng.ws->get(&dtab, tab.size(), WS_MFUN_PTR, st));
     SC_CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(void*) * tab.size(), cudaMemcpyHostToDevice, st));
     auto cp = [&](size_t o) { return reinterpret_cast<const double2* const*>(dtab + o); };
     auto mp = [&](size_t o) { return reinterpret_cast<double2* const*>(dtab + o); };
-    // one batched product with any operand given by a pointer table (Ap/Bp/Cp) or by base + stride
-    auto mmp = [&](const double2* const* Ap, const double2* A, long long sA, const double2* const* Bp,
-                   const double2* Bm, long long sB, double2* const* Cp, double2* Cm, int ldc, long long sC,
-                   double2 alpha, double2 beta, const double2* alphas, int batch) {
+    // one batched product with any operand given by a pointer table (Ap/Bp/Cp) or by base + stride;
+    // m rows, leading dimensions lda / ldb of A and B
+    auto mmp = [&](int m, const double2* const* Ap, const double2* A, int lda, long long sA,
+                   const double2* const* Bp, const double2* Bm, int ldb, long long sB, double2* const* Cp,
+                   double2* Cm, int ldc, long long sC, double2 alpha, double2 beta, const double2* alphas, int batch) {
         GemmArgs g;
-        g.m = n2;
+        g.m = m;
         g.n = n2;
         g.k = n2;
         g.alpha = alpha;
@@ -259,11 +269,11 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         g.alphas = alphas;
         g.Ap = Ap;
         g.A = A;
-        g.lda = n2;
+        g.lda = lda;
         g.sA = sA;
         g.Bp = Bp;
         g.B = Bm;
-        g.ldb = n2;
+        g.ldb = ldb;
         g.sB = sB;
         g.Cp = Cp;
         g.C = Cm;
@@ -271,15 +281,14 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
         g.sC = sC;
         return eng.run(st, g, batch);
     };
-    const double2 two = make_double2(2.0, 0.0);
     for (const auto& sp : steps) {
         const int na = sp.second;
-        const size_t gc = sp.first, fc = gc + na, go = fc + na, fo = go + na;
-        SC_TRY(mmp(cp(gc), nullptr, 0, cp(fc), nullptr, 0, mp(go), nullptr, n2, 0, one, zero, nullptr, na));  // G F
-        SC_TRY(mmp(cp(fc), nullptr, 0, cp(fc), nullptr, 0, mp(fo), nullptr, n2, 0, two, zero, nullptr, na));  // 2 F^2
-        add_diag_ptr_kernel<<<dim3((n2 + 255) / 256, na), 256, 0, st>>>(n2, -1.0, mp(fo));                     // - I
+        const size_t sc = sp.first, fc = sc + na, so = fc + na, fo = so + na;
+        SC_TRY(mmp(ls, cp(sc), nullptr, ls, 0, cp(fc), nullptr, ls, 0, mp(so), nullptr, ls, 0, one, zero, nullptr,
+                   na));                                                                          // [G; F] F
+        double_minus_identity_kernel<<<dim3(nblocks(nn), na), 256, 0, st>>>(n2, ls, mp(fo));        // 2 F^2 - I
         count_launch();
-        SC_CHECK_LAUNCH("add_diag_ptr");
+        SC_CHECK_LAUNCH("double_minus_identity");
     }
 
     // 5. the factored layer: F, G B and C G (half angle) into the layer's block of T
@@ -289,9 +298,11 @@ sc_status transfer_inv_batched(cudaStream_t st, const GemmEngine& eng, int n2, i
     void** dout = nullptr;
     SC_TRY(eng.ws->get(&dout, outp.size(), WS_MFUN_OUT, st));
     SC_CUDA_TRY(cudaMemcpyAsync(dout, outp.data(), sizeof(void*) * outp.size(), cudaMemcpyHostToDevice, st));
-    SC_TRY(copy_blocks(st, n2, n2, cp(lf), n2, reinterpret_cast<double2* const*>(dout), n2, count));        // F
-    SC_TRY(mmp(cp(lg), nullptr, 0, nullptr, B, nn, nullptr, T + nn, n2, sT, one, zero, nullptr, count));   // G B
-    SC_TRY(mmp(nullptr, C, nn, cp(lg), nullptr, 0, nullptr, T + 2 * nn, n2, sT, one, zero, nullptr, count));  // C G
+    SC_TRY(copy_blocks(st, n2, n2, cp(lf), ls, reinterpret_cast<double2* const*>(dout), n2, count));        // F
+    SC_TRY(mmp(n2, cp(lg), nullptr, ls, 0, nullptr, B, n2, nn, nullptr, T + nn, n2, sT, one, zero, nullptr,
+               count));                                                                                     // G B
+    SC_TRY(mmp(n2, nullptr, C, n2, nn, cp(lg), nullptr, ls, 0, nullptr, T + 2 * nn, n2, sT, one, zero, nullptr,
+               count));                                                                                     // C G
     return SC_OK;
 }
 
