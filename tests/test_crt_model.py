@@ -82,6 +82,28 @@ def test_biased_byte_unpacking():
         assert ((w ^ 0x80808080) >> (8 * q)) & 0xFF == r + 128
 
 
+def test_biased_byte_packing_every_residue():
+    """sym4: bytes r' + (128 - h), XOR 0x80 each, are the int8 bytes of r' - h; sym4_alt: the (a - h, h - c) pairs
+    of an A' row 2i, formed by whole-word adds with no carry or borrow between bytes -- all residue pairs, all p."""
+    for p in MODS:
+        h = (p - 1) // 2
+        a, c = np.meshgrid(np.arange(p, dtype=np.int64), np.arange(p, dtype=np.int64), indexing="ij")
+        a, c = a.ravel(), c.ravel()
+        a1, c1 = np.roll(a, 7), np.roll(c, 3)
+        # sym4 on bytes (a, c, a1, c1)
+        w = a | (c << 8) | (a1 << 16) | (c1 << 24)
+        s = ((w + (128 - h) * 0x01010101) & 0xFFFFFFFF) ^ 0x80808080
+        for q, v in enumerate((a, c, a1, c1)):
+            byte = (s >> (8 * q)) & 0xFF
+            assert np.array_equal(np.where(byte > 127, byte - 256, byte), v - h)
+        # sym4_alt
+        L = (128 - h) * 0x00010001 + (128 + h) * 0x01000100
+        t = (((a + (a1 << 16) + L) - ((c << 8) + (c1 << 24))) & 0xFFFFFFFF) ^ 0x80808080
+        for q, v in enumerate((a - h, h - c, a1 - h, h - c1)):
+            byte = (t >> (8 * q)) & 0xFF
+            assert np.array_equal(np.where(byte > 127, byte - 256, byte), v)
+
+
 def limbs37(v):
     m = (1 << 37) - 1
     return float(v >> 74), float((v >> 37) & m), float(v & m)
