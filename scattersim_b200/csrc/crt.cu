@@ -191,9 +191,13 @@ __device__ __forceinline__ void with_mod(int t, F& f) { with_mod_from<0>(t, f); 
 // Residues for packing: r' = (u + h) mod p with h = (p - 1) / 2, so that the
 // symmetric residue (|r| <= h) is r' - h; u (|u| < 2^50) comes as U = u + 2^50
 // in 17-bit limbs, and the constant (p - 2^50 mod p) + h keeps the unsigned
-// sum non-negative.  The subtraction of h (or, for a negated residue, h - r')
-// runs on four packed bytes at once (__vsub4: bytewise, no borrow), so each
-// value costs two multiply-adds, an add and the remainder by a constant.
+// sum non-negative.  Four such residues go into one word with the bias
+// 128 - h added to every byte (128 + h to a byte that carries h - r' for a
+// negated residue): each byte then lies in [128 - h, 128 + h], so the word
+// adds and subtracts without a carry or borrow between bytes, and XOR 0x80 per
+// byte turns r' + 128 - h into the two's-complement byte of r' - h.  Each
+// value costs two multiply-adds, an add and the remainder by a constant; each
+// word a few integer adds and one XOR.
 template <int P>
 __device__ __forceinline__ uint32_t res_shifted(int U0, int U1, int U2) {
     constexpr unsigned c17 = pow2_mod(17, P), c34 = pow2_mod(34, P), c50 = pow2_mod(50, P);
@@ -201,10 +205,20 @@ __device__ __forceinline__ uint32_t res_shifted(int U0, int U1, int U2) {
     const unsigned v = (unsigned)U2 * c34 + (unsigned)U1 * c17 + ((unsigned)U0 + K);
     return v % (unsigned)P;
 }
-template <int P>
-__device__ __forceinline__ uint32_t half4() { return (uint32_t)((P - 1) / 2) * 0x01010101u; }
 __device__ __forceinline__ uint32_t bytes4(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) {
     return b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+}
+// bytes r'_q (each in [0, p)) -> bytes r'_q - h: bias every byte by 128 - h, then flip its top bit
+template <int P>
+__device__ __forceinline__ uint32_t sym4(uint32_t packed) {
+    return (packed + (uint32_t)(128 - (P - 1) / 2) * 0x01010101u) ^ 0x80808080u;
+}
+// bytes (a0 - h, h - c0, a1 - h, h - c1) from a_q, c_q in [0, p): even bytes biased by 128 - h, odd
+// bytes by 128 + h less c_q
+template <int P>
+__device__ __forceinline__ uint32_t sym4_alt(uint32_t a0, uint32_t c0, uint32_t a1, uint32_t c1) {
+    constexpr uint32_t L = (uint32_t)(128 - (P - 1) / 2) * 0x00010001u + (uint32_t)(128 + (P - 1) / 2) * 0x01000100u;
+    return ((a0 + (a1 << 16) + L) - ((c0 << 8) + (c1 << 24))) ^ 0x80808080u;
 }
 
 // copy NP planes of `bytes` contiguous bytes each from shared memory to global
@@ -252,7 +266,6 @@ __global__ void __launch_bounds__(256) crt_pack_a_kernel(int m, int k, const dou
     auto one = [&](auto tag) {
         constexpr int T = decltype(tag)::value;
         constexpr int P = crt_mod(T);
-        constexpr uint32_t H = (uint32_t)((P - 1) / 2);
         uint32_t dr[4], di[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -261,11 +274,10 @@ __global__ void __launch_bounds__(256) crt_pack_a_kernel(int m, int k, const dou
         }
         // row 2i: Re - h, h - Im ; row 2i+1: Im - h, Re - h
         unsigned char* st = sm + (T % HALF) * CRT_ATILE;
-        *reinterpret_cast<uint2*>(st + o0) =
-            make_uint2(__vsub4(bytes4(dr[0], H, dr[1], H), bytes4(H, di[0], H, di[1])),
-                       __vsub4(bytes4(dr[2], H, dr[3], H), bytes4(H, di[2], H, di[3])));
-        *reinterpret_cast<uint2*>(st + o1) = make_uint2(__vsub4(bytes4(di[0], dr[0], di[1], dr[1]), half4<P>()),
-                                                        __vsub4(bytes4(di[2], dr[2], di[3], dr[3]), half4<P>()));
+        *reinterpret_cast<uint2*>(st + o0) = make_uint2(sym4_alt<P>(dr[0], di[0], dr[1], di[1]),
+                                                        sym4_alt<P>(dr[2], di[2], dr[3], di[3]));
+        *reinterpret_cast<uint2*>(st + o1) = make_uint2(sym4<P>(bytes4(di[0], dr[0], di[1], dr[1])),
+                                                        sym4<P>(bytes4(di[2], dr[2], di[3], dr[3])));
         if constexpr (T % HALF == HALF - 1) {
             __syncthreads();
             planes_out<HALF>(sm, CRT_ATILE, base + (long long)(T - (HALF - 1)) * plane, plane);
@@ -316,8 +328,7 @@ __global__ void __launch_bounds__(256) crt_pack_b_kernel(int k, int n, const dou
 #pragma unroll
         for (int q = 0; q < 8; ++q) d[q] = res_shifted<P>(lx[q][0], lx[q][1], lx[q][2]);
         *reinterpret_cast<uint2*>(sm + T * QB + o) =
-            make_uint2(__vsub4(bytes4(d[0], d[1], d[2], d[3]), half4<P>()),
-                       __vsub4(bytes4(d[4], d[5], d[6], d[7]), half4<P>()));
+            make_uint2(sym4<P>(bytes4(d[0], d[1], d[2], d[3])), sym4<P>(bytes4(d[4], d[5], d[6], d[7])));
     };
     for_each_mod(one);
     __syncthreads();
@@ -400,9 +411,8 @@ __device__ __forceinline__ bool crt_extract_tile(const CrtArgs& g, uint32_t tmem
                 uint32_t w[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    w[q] = __vsub4(bytes4(acc_res_shifted<P>((int)r[4 * q]), acc_res_shifted<P>((int)r[4 * q + 1]),
-                                          acc_res_shifted<P>((int)r[4 * q + 2]), acc_res_shifted<P>((int)r[4 * q + 3])),
-                                   half4<P>());
+                    w[q] = sym4<P>(bytes4(acc_res_shifted<P>((int)r[4 * q]), acc_res_shifted<P>((int)r[4 * q + 1]),
+                                          acc_res_shifted<P>((int)r[4 * q + 2]), acc_res_shifted<P>((int)r[4 * q + 3])));
                 *reinterpret_cast<uint4*>(dst + c0) = make_uint4(w[0], w[1], w[2], w[3]);
                 *reinterpret_cast<uint4*>(dst + c0 + 16) = make_uint4(w[4], w[5], w[6], w[7]);
             }
