@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -32,6 +33,19 @@ sc_status cuda_status(cudaError_t e, const char* where) {
 
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 uint64_t launch_total() { return g_launches.load(); }
+
+sc_status smem_opt_in(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> granted;   // (kernel, device) -> bytes
+    int dev = 0;
+    SC_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    int& have = granted[{kernel, dev}];
+    if (have >= bytes) return SC_OK;
+    SC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    have = bytes;
+    return SC_OK;
+}
 
 sc_status set_volume_precision(sc_context* ctx, int precision);
 sc_status sweep_solve(sc_context* ctx, int count, const sc_volume_params* params, const void* const* samples,

@@ -105,6 +105,16 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 void set_error(const char* fmt, ...);
 sc_status cuda_status(cudaError_t e, const char* where);
 
+// Dynamic shared memory above 48 KB is granted per kernel and per device (a
+// function attribute belongs to the current device's context): raise the
+// kernel's limit to `bytes` on the current device unless an earlier call
+// there already granted at least that much.  Thread-safe.
+sc_status smem_opt_in(const void* kernel, int bytes);
+template <typename K>
+sc_status smem_opt_in(K* kernel, int bytes) {
+    return smem_opt_in(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 #define SC_CUDA_TRY(expr)                                                  \
     do {                                                                   \
         cudaError_t _e = (expr);                                           \

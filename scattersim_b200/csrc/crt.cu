@@ -46,6 +46,7 @@
 #include <cudaTypedefs.h>
 
 #include <cmath>
+#include <mutex>
 #include <cstdint>
 #include <type_traits>
 
@@ -774,16 +775,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CRT_THREADS, 1)
 // 256 x C2_SA / 256 rows (one stage); the driver's encoder comes through the runtime
 // (no link against the driver library)
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        (void)cudaGetLastError();
+        return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }();
     return fn;
 }
 bool byte_tensor_map(CUtensorMap* map, const void* base, size_t bytes) {
@@ -798,6 +798,8 @@ bool byte_tensor_map(CUtensorMap* map, const void* base, size_t bytes) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// per device: constants copied, kernel limits raised, CTA-pair capacity found
+std::mutex g_crt_mu;
 bool g_crt_const_ready[64] = {};
 int g_crt_pairs[64] = {};
 
@@ -891,11 +893,15 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
     }
     int dev = 0;
     SC_CUDA_TRY(cudaGetDevice(&dev));
-    static CrtConst host_const = make_constants();
-    if (dev >= 0 && dev < 64 && !g_crt_const_ready[dev]) {
+    if (dev < 0 || dev >= 64) {
+        set_error("zgemm_crt: device %d out of range", dev);
+        return SC_BADINPUT;
+    }
+    static const CrtConst host_const = make_constants();
+    std::unique_lock<std::mutex> init_lock(g_crt_mu);
+    if (!g_crt_const_ready[dev]) {
         SC_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &host_const, sizeof(CrtConst)));
-        SC_CUDA_TRY(cudaFuncSetAttribute(crt_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         CRT_NS * CRT_SLOT + 1024));
+        SC_TRY(smem_opt_in(crt_mma_kernel, CRT_NS * CRT_SLOT + 1024));
         const bool pair_ok = cudaFuncSetAttribute(crt_mma2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   C2_NS * C2_SLOT + 1024) == cudaSuccess;
         if (!pair_ok) (void)cudaGetLastError();
@@ -913,10 +919,11 @@ sc_status zgemm_crt(cudaStream_t st, const GemmArgs& g, int batch, Workspace& ws
         g_crt_pairs[dev] = ncl;
         g_crt_const_ready[dev] = true;
     }
+    const int npairs = g_crt_pairs[dev];
+    init_lock.unlock();
     int sms = 148;
     SC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int bits = crt_bits(g.k, host_const.log2P);
-    const int npairs = (dev >= 0 && dev < 64) ? g_crt_pairs[dev] : 0;
     const bool pair = ws.crt_tiles != 0 && npairs > 0;
     const int RB = pair ? 2 * ((2 * g.m + 2 * CRT_BM - 1) / (2 * CRT_BM)) : (2 * g.m + CRT_BM - 1) / CRT_BM,
               CB = (g.n + CRT_BN - 1) / CRT_BN, KB = (2 * g.k + CRT_BK - 1) / CRT_BK;

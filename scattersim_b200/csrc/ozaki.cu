@@ -356,11 +356,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_mma_kernel(OzArgs g) {
 namespace {
 template <int S>
 sc_status launch_mma_s(dim3 grid, size_t smem, cudaStream_t st, const OzArgs& a) {
-    static bool configured = false;
-    if (!configured) {
-        SC_CUDA_TRY(cudaFuncSetAttribute(oz_mma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
+    SC_TRY(smem_opt_in(oz_mma_kernel<S>, (int)smem));
     oz_mma_kernel<S><<<grid, OZ_THREADS, smem, st>>>(a);
     return SC_OK;
 }

@@ -168,13 +168,8 @@ __global__ void __launch_bounds__(NT, (BM == 64 ? 2 : 1)) zgemm_kernel(GemmArgs 
 
 template <int BM, bool CA, bool CB>
 sc_status launch_tile(cudaStream_t st, const GemmArgs& g, int batch) {
-    static bool configured = false;
     constexpr int bytes = tile_smem_bytes<BM>();
-    if (!configured) {
-        SC_CUDA_TRY(cudaFuncSetAttribute(zgemm_kernel<BM, CA, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         bytes));
-        configured = true;
-    }
+    SC_TRY(smem_opt_in(zgemm_kernel<BM, CA, CB>, bytes));
     dim3 grid((g.m + BM - 1) / BM, (g.n + 63) / 64, batch);
     zgemm_kernel<BM, CA, CB><<<grid, NT, bytes, st>>>(g);
     return SC_OK;
