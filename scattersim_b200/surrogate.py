@@ -136,6 +136,7 @@ class Surrogate:
         h = ctypes.c_void_p()
         check(self.lib.sc_fno_create(ctypes.byref(h), device, max_batch, seed))
         self.h = h
+        self.device = torch.device("cuda", device)
         self.max_batch = max_batch
         n = ctypes.c_longlong(0)
         check(self.lib.sc_fno_param_count(self.h, ctypes.byref(n)))
@@ -156,24 +157,41 @@ class Surrogate:
     def _p(t):
         return ctypes.c_void_p(t.data_ptr())
 
+    def _buf(self, t, shape, name: str) -> torch.Tensor:
+        """`t` as a contiguous float32 tensor on the network's device, after checking its shape: the library
+        reads as many floats as the batch implies from a bare pointer, so a short buffer must not reach it."""
+        t = torch.as_tensor(t)
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"surrogate: {name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+        return t.to(device=self.device, dtype=torch.float32).contiguous()
+
+    def _batch(self, maps, lams, target=None):
+        """(batch, [maps, lams(, target)]) checked and placed for one library call."""
+        maps = torch.as_tensor(maps)
+        B = int(maps.shape[0]) if maps.dim() else 0
+        bufs = [self._buf(maps, (B, 64, 64), "maps"), self._buf(lams, (B,), "lams")]
+        if target is not None:
+            bufs.append(self._buf(target, (B, NOUT), "target"))
+        return B, bufs
+
     def status(self):
         """Synchronise and raise if a tensor-core GEMM of this network timed out since the last check."""
         check(self.lib.sc_fno_status(self.h))
 
     def get_params(self) -> torch.Tensor:
-        t = torch.empty(self.n_params, dtype=torch.float32, device="cuda")
+        t = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
         check(self.lib.sc_fno_params(self.h, self._p(t), 0, None))
         torch.cuda.synchronize()
         return t
 
     def set_params(self, t):
-        t = torch.as_tensor(t, dtype=torch.float32).cuda().contiguous()
+        t = self._buf(torch.as_tensor(t).reshape(-1), (self.n_params,), "parameters")
         check(self.lib.sc_fno_params(self.h, self._p(t), 1, None))
         torch.cuda.synchronize()
 
     def forward(self, maps: torch.Tensor, lams: torch.Tensor) -> torch.Tensor:
-        B = maps.shape[0]
-        out = torch.empty((B, NOUT), dtype=torch.float32, device="cuda")
+        B, (maps, lams) = self._batch(maps, lams)
+        out = torch.empty((B, NOUT), dtype=torch.float32, device=self.device)
         for i0 in range(0, B, self.max_batch):
             m = maps[i0:i0 + self.max_batch].contiguous()
             l = lams[i0:i0 + self.max_batch].contiguous()
@@ -181,17 +199,17 @@ class Surrogate:
         return out
 
     def loss_grad(self, maps, lams, target):
-        B = maps.shape[0]
-        loss = torch.empty(B, dtype=torch.float32, device="cuda")
-        grad = torch.empty(self.n_params, dtype=torch.float32, device="cuda")
-        check(self.lib.sc_fno_loss_grad(self.h, self._p(maps.contiguous()), self._p(lams.contiguous()),
-                                        self._p(target.contiguous()), B, self._p(loss), self._p(grad), None))
+        B, (maps, lams, target) = self._batch(maps, lams, target)
+        loss = torch.empty(B, dtype=torch.float32, device=self.device)
+        grad = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        check(self.lib.sc_fno_loss_grad(self.h, self._p(maps), self._p(lams), self._p(target), B, self._p(loss),
+                                        self._p(grad), None))
         torch.cuda.synchronize()
         return loss, grad
 
     def train_step(self, maps, lams, target, lr: float) -> torch.Tensor:
-        B = maps.shape[0]
-        loss = torch.empty(B, dtype=torch.float32, device="cuda")
+        B, (maps, lams, target) = self._batch(maps, lams, target)
+        loss = torch.empty(B, dtype=torch.float32, device=self.device)
         check(self.lib.sc_fno_train_step(self.h, self._p(maps), self._p(lams), self._p(target), B, float(lr),
                                          self._p(loss), None))
         return loss
@@ -200,19 +218,20 @@ class Surrogate:
 def train(sur: Surrogate, maps, lams, targets, epochs: int, batch: int = 64, lr: float = 1e-3, seed: int = 0,
           log=None):
     """Adam with a cosine rate schedule over `epochs` passes of shuffled batches."""
-    dm = torch.from_numpy(np.ascontiguousarray(maps)).cuda()
-    dl = torch.from_numpy(np.ascontiguousarray(lams)).cuda()
-    dt = torch.from_numpy(np.ascontiguousarray(targets)).cuda()
+    dev = sur.device
+    dm = torch.as_tensor(np.ascontiguousarray(maps, dtype=np.float32), device=dev)
+    dl = torch.as_tensor(np.ascontiguousarray(lams, dtype=np.float32), device=dev)
+    dt = torch.as_tensor(np.ascontiguousarray(targets, dtype=np.float32), device=dev)
     n = len(maps)
     rng = np.random.default_rng(seed)
     steps = epochs * (n // batch)
     step = 0
     hist = []
     for ep in range(epochs):
-        perm = torch.from_numpy(rng.permutation(n)).cuda()
+        perm = torch.from_numpy(rng.permutation(n)).to(dev)
         # the loss is summed on the device: reading it back every step would
         # stall the launch queue once per step
-        tot = torch.zeros((), dtype=torch.float32, device="cuda")
+        tot = torch.zeros((), dtype=torch.float32, device=dev)
         for i0 in range(0, n - batch + 1, batch):
             idx = perm[i0:i0 + batch]
             rate = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(steps, 1)))
@@ -233,8 +252,10 @@ def predict_with_fallback(sur, ctx, maps, lams, tol: float = ENERGY_TOL, spread:
     members' mean, and with `spread` a sample whose members disagree (the largest relative distance of a member
     from the mean) by more than `spread` falls back as well."""
     members = list(sur) if isinstance(sur, (list, tuple)) else [sur]
-    dm = torch.from_numpy(np.ascontiguousarray(maps, dtype=np.float32)).cuda()
-    dl = torch.from_numpy(np.ascontiguousarray(lams, dtype=np.float32)).cuda()
+    if not members:
+        raise ValueError("predict_with_fallback: no network given")
+    dm = torch.as_tensor(np.ascontiguousarray(maps, dtype=np.float32), device=members[0].device)
+    dl = torch.as_tensor(np.ascontiguousarray(lams, dtype=np.float32), device=members[0].device)
     preds = [target_to_x(m.forward(dm, dl).cpu().numpy()) for m in members]
     pred = np.mean(preds, axis=0) if len(preds) > 1 else preds[0]
     bad = energy_error(pred, lams) > tol

@@ -35,3 +35,24 @@ def test_energy_error_of_oracle_solves_is_zero():
     assert err.max() < 1e-9
     # and it detects a 1 % amplitude error
     assert (sg.energy_error(np.stack(xs) * 1.01, np.array(lams)) > 1e-3).all()
+
+
+def test_network_buffers_are_checked_before_the_library():
+    """The library reads batch x 64 x 64 maps, batch wavelengths and batch x 1452 targets from bare pointers:
+    the wrapper converts and places them on the network's device, and refuses a wrong shape."""
+    import pytest
+    import torch
+    net = sg.Surrogate.__new__(sg.Surrogate)        # no library handle: only the buffer checks run
+    net.device = torch.device("cpu")
+    maps = np.ones((3, 64, 64))
+    B, (m, lam, t) = net._batch(maps, [0.5, 0.6, 0.7], np.zeros((3, sg.NOUT)))
+    assert B == 3 and m.dtype == lam.dtype == t.dtype == torch.float32
+    assert m.is_contiguous() and tuple(m.shape) == (3, 64, 64) and tuple(t.shape) == (3, sg.NOUT)
+    with pytest.raises(ValueError, match="maps"):
+        net._batch(np.ones((3, 32, 32)), [0.5, 0.6, 0.7])
+    with pytest.raises(ValueError, match="lams"):
+        net._batch(maps, [0.5, 0.6])
+    with pytest.raises(ValueError, match="target"):
+        net._batch(maps, [0.5, 0.6, 0.7], np.zeros((3, sg.NOUT - 2)))
+    with pytest.raises(ValueError, match="no network"):
+        sg.predict_with_fallback([], None, maps, [0.5, 0.6, 0.7])
