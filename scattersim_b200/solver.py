@@ -27,6 +27,18 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def _checked(ctx, t, shape, name: str, dtype=torch.complex128) -> torch.Tensor:
+    """`t` made contiguous after checking its type, its device (the context's) and its shape (None: any): the
+    library reads as many elements as the sizes imply from a bare pointer, so a short buffer must not reach it."""
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dtype:
+        raise TypeError(f"{name} must be a {dtype} CUDA tensor")
+    if t.device.index != ctx.device:
+        raise ValueError(f"{name} is on {t.device}, the context on cuda:{ctx.device}")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    return t.contiguous()
+
+
 class Context:
     """One sc_context per GPU (pooled device workspace)."""
 
@@ -161,9 +173,7 @@ def solve(ctx: Context, params: VolumeParams, sample: torch.Tensor, fields: bool
     """One scattervolume solve of a device-resident (Z, S1, S2) complex128 sample."""
     if sample.dim() == 2:
         sample = sample.unsqueeze(0)
-    if sample.dtype != torch.complex128 or not sample.is_cuda:
-        raise TypeError("sample must be a complex128 CUDA tensor")
-    sample = sample.contiguous()
+    sample = _checked(ctx, sample, None, "sample")
     shape = tuple(sample.shape)
     d = plan(params, shape)
     MF, Z = d.MF, shape[0]
@@ -185,7 +195,7 @@ def chain_block(ctx: Context, params: VolumeParams, sample: torch.Tensor, layer_
     (4MF, 4MF) tensor read as its transpose) and GD_0 for the block that starts at layer 0 (else None)."""
     if sample.dim() == 2:
         sample = sample.unsqueeze(0)
-    sample = sample.contiguous()
+    sample = _checked(ctx, sample, None, "sample")
     shape = tuple(sample.shape)
     d = plan(params, shape)
     n4 = 4 * d.MF
@@ -200,22 +210,30 @@ def chain_block(ctx: Context, params: VolumeParams, sample: torch.Tensor, layer_
 def boundary_solve(ctx: Context, params: VolumeParams, shape, Gc_static: torch.Tensor, GD0: torch.Tensor,
                    stream=None) -> torch.Tensor:
     """x = [R; T] (6 MF) from the whole chain and GD_0 (storage as chain_block returns them)."""
-    d = plan(params, tuple(shape))
+    shape = tuple(shape)
+    if len(shape) == 2:
+        shape = (1,) + shape
+    d = plan(params, shape)
+    n4 = 4 * d.MF
+    Gc_static = _checked(ctx, Gc_static, (n4, n4), "Gc_static")
+    GD0 = _checked(ctx, GD0, (n4, n4), "GD0")
     x = torch.empty(6 * d.MF, dtype=torch.complex128, device=Gc_static.device)
     info = ctypes.c_int(0)
-    check(ctx.lib.sc_volume_boundary_solve(ctx.handle, ctypes.byref(params), *shape, _ptr(Gc_static.contiguous()),
-                                           _ptr(GD0.contiguous()), _ptr(x), ctypes.byref(info), _stream_ptr(stream)))
+    check(ctx.lib.sc_volume_boundary_solve(ctx.handle, ctypes.byref(params), *shape, _ptr(Gc_static), _ptr(GD0),
+                                           _ptr(x), ctypes.byref(info), _stream_ptr(stream)))
     return x
 
 
 def colmajor_matmul(ctx: Context, A: torch.Tensor, B: torch.Tensor, stream=None) -> torch.Tensor:
     """A B for square matrices held in column-major storage (as chain_block returns them), on the FP64 tile."""
-    n = A.shape[0]
+    n = A.shape[0] if A.dim() == 2 else -1
+    A = _checked(ctx, A, (n, n), "A")
+    B = _checked(ctx, B, (n, n), "B")
     C = torch.empty_like(A)
     one = (ctypes.c_double * 2)(1.0, 0.0)
     zero = (ctypes.c_double * 2)(0.0, 0.0)
-    check(ctx.lib.sc_zgemm_batched(ctx.handle, n, n, n, one, _ptr(A.contiguous()), n, n * n, _ptr(B.contiguous()),
-                                   n, n * n, zero, _ptr(C), n, n * n, 1, _stream_ptr(stream)))
+    check(ctx.lib.sc_zgemm_batched(ctx.handle, n, n, n, one, _ptr(A), n, n * n, _ptr(B), n, n * n, zero, _ptr(C), n,
+                                   n * n, 1, _stream_ptr(stream)))
     return C
 
 
@@ -262,12 +280,20 @@ def evaluate(ctx: Context, E0: torch.Tensor, K: torch.Tensor, z_layers, begin, e
              zeps: float = 0.001, precision: int = 0, stream=None) -> torch.Tensor:
     """E at (P, 3) float64 device points: the gpuEvaluator sum (gpuEvaluator.cu:28-68)."""
     layers = len(z_layers)
+    if len(begin) < layers + 1 or len(end) < layers + 1:
+        raise ValueError(f"begin / end need {layers + 1} region bounds")
     zl = (ctypes.c_double * max(layers, 1))(*list(z_layers))
     b = (ctypes.c_int * (layers + 1))(*[int(v) for v in begin[:layers + 1]])
     e = (ctypes.c_int * (layers + 1))(*[int(v) for v in end[:layers + 1]])
-    points = points.to(torch.float64).contiguous()
+    nw = E0.shape[0] if E0.dim() == 2 else -1
+    E0 = _checked(ctx, E0, (nw, 3), "E0")
+    K = _checked(ctx, K, (nw, 3), "K")
+    if not isinstance(points, torch.Tensor) or not points.is_floating_point() or points.dim() != 2 \
+            or points.shape[1] != 3:
+        raise ValueError("points must be a (P, 3) floating-point tensor")
+    points = _checked(ctx, points.to(torch.float64), None, "points", torch.float64)
     out = torch.empty((points.shape[0], 3), dtype=torch.complex128, device=points.device)
-    check(ctx.lib.sc_cw_evaluate(ctx.handle, _ptr(E0.contiguous()), _ptr(K.contiguous()), int(E0.shape[0]), zl, b,
+    check(ctx.lib.sc_cw_evaluate(ctx.handle, _ptr(E0), _ptr(K), int(E0.shape[0]), zl, b,
                                  e, layers, float(zeps), _ptr(points), int(points.shape[0]), _ptr(out),
                                  int(precision), _stream_ptr(stream)))
     return out
@@ -308,12 +334,10 @@ def sweep(ctx: Context, params, samples, precision: int = _lib.SC_SWEEP_FP64, st
     if len(samples) != n:
         raise ValueError("params and samples differ in length")
     smp = []
-    for t in samples:
-        if t.dim() == 2:
+    for i, t in enumerate(samples):
+        if isinstance(t, torch.Tensor) and t.dim() == 2:
             t = t.unsqueeze(0)
-        if t.dtype != torch.complex128 or not t.is_cuda:
-            raise TypeError("samples must be complex128 CUDA tensors")
-        smp.append(t.contiguous())
+        smp.append(_checked(ctx, t, None, f"samples[{i}]"))
     dims = [plan(p, tuple(t.shape)) for p, t in zip(params, smp)]
     xs = [torch.empty(6 * d.MF, dtype=torch.complex128, device=t.device) for d, t in zip(dims, smp)]
     P = (VolumeParams * max(n, 1))(*params)
@@ -333,6 +357,9 @@ def eigensolve(ctx: Context, A: torch.Tensor, stream=None):
     """Batched eigenvalues / right eigenvectors of (B, n, n) complex128 matrices (row-major torch view)."""
     if A.dim() == 2:
         A = A.unsqueeze(0)
+    if A.dim() != 3 or A.shape[1] != A.shape[2]:
+        raise ValueError(f"A must be (B, n, n) square matrices, got {tuple(A.shape)}")
+    A = _checked(ctx, A, None, "A")
     B, n, _ = A.shape
     # C ABI is column-major: pass A^T's storage, i.e. the transpose of each matrix
     Acm = A.transpose(1, 2).contiguous()

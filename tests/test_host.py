@@ -142,3 +142,27 @@ def test_two_rank_sharding_with_gloo():
         assert count == 8                    # every instance solved exactly once
         flat = sorted(i for part in gathered for i in part)
         assert flat == list(range(8))
+
+
+def test_wrapper_tensor_checks_run_before_the_library():
+    """The solver wrappers refuse CPU tensors, wrong dtypes and wrong shapes before any pointer reaches the
+    library (which reads as many elements as the sizes imply); checked on the CPU with a stand-in context."""
+    import pytest
+    import torch
+    from scattersim_b200 import solver
+
+    class Ctx:
+        device = 0
+    t = torch.zeros((2, 3), dtype=torch.complex128)
+    with pytest.raises(TypeError, match="CUDA"):
+        solver._checked(Ctx(), t, (2, 3), "E0")
+    with pytest.raises(TypeError, match="complex128"):
+        solver._checked(Ctx(), t.real, (2, 3), "E0")
+    with pytest.raises(TypeError):
+        solver.eigensolve(Ctx(), torch.zeros((2, 4, 4), dtype=torch.complex128))
+    with pytest.raises(ValueError, match="square"):
+        solver.eigensolve(Ctx(), torch.zeros((2, 4, 5), dtype=torch.complex128))
+    with pytest.raises(ValueError, match="region bounds"):
+        solver.evaluate(Ctx(), t, t, [0.0, 1.0], [0], [0], torch.zeros((4, 3)))
+    with pytest.raises(TypeError):
+        solver.sweep(Ctx(), [None], [torch.zeros((4, 4), dtype=torch.complex128)])
