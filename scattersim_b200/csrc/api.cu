@@ -614,7 +614,7 @@ sc_status sc_fp64_dmma_probe(sc_context* ctx, double* tflops) {
 
 sc_status sc_crt_tiles_set(sc_context* ctx, int mode) {
     if (!ctx || (mode != 0 && mode != 1)) {
-        set_error("sc_crt_tiles_set: mode must be 0 or 1");
+        set_error(ctx ? "sc_crt_tiles_set: mode %d, must be 0 or 1" : "sc_crt_tiles_set: null context", mode);
         return SC_BADINPUT;
     }
     ctx->ws.crt_tiles = mode;

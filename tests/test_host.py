@@ -166,3 +166,36 @@ def test_wrapper_tensor_checks_run_before_the_library():
         solver.evaluate(Ctx(), t, t, [0.0, 1.0], [0], [0], torch.zeros((4, 3)))
     with pytest.raises(TypeError):
         solver.sweep(Ctx(), [None], [torch.zeros((4, 4), dtype=torch.complex128)])
+
+
+# entry points whose first statement refuses a null handle or buffer (no CUDA call comes before it)
+NULL_CHECKED = [
+    "sc_create", "sc_fft2_crop", "sc_phi", "sc_eigensolve_batched", "sc_linearsolve_batched", "sc_inverse_batched",
+    "sc_zgemm_emulated_batched", "sc_zgemm_crt_batched", "sc_zgemm_batched", "sc_volume_plan", "sc_volume_solve",
+    "sc_volume_chain_block", "sc_volume_boundary_solve", "sc_sweep_solve", "sc_kernel_timing", "sc_kernel_stats",
+    "sc_kernel_stats_ex", "sc_gemm_choices_get", "sc_volume_precision", "sc_volume_stage_ms",
+    "sc_fp64_peak_probe", "sc_fp64_dmma_probe", "sc_crt_tiles_set", "sc_int8_peak_probe", "sc_qr_stats",
+    "sc_volume_waves", "sc_volume_field_grid", "sc_cw_write", "sc_cw_evaluate", "sc_beam_polar", "sc_layer_solve",
+    "sc_mkl_eigensolve", "sc_gpu_initialize", "sc_linearsolve_batched_noalloc", "sc_scatterio_write",
+    "sc_scatterio_read", "sc_fno_create", "sc_fno_status", "sc_fno_param_count", "sc_fno_params",
+    "sc_fno_forward", "sc_fno_loss_grad", "sc_fno_train_step",
+]
+
+
+def test_null_arguments_are_refused_with_a_message(lib):
+    """Every entry point above, called with null pointers and zero sizes, returns SC_BADINPUT and leaves a
+    message for sc_last_error_string -- never a crash or an exit (the reference's HANDLE_ERROR exits)."""
+    import ctypes
+    for name in NULL_CHECKED:
+        restype, argtypes = _lib._SIGS[name]
+        args = []
+        for t in argtypes:
+            if t in (ctypes.c_double, ctypes.c_float):
+                args.append(0.0)
+            elif t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+                args.append(None)
+            else:
+                args.append(0)
+        rc = getattr(lib, name)(*args)
+        assert rc == _lib.SC_BADINPUT, (name, rc)
+        assert lib.sc_last_error_string(), name
