@@ -92,15 +92,29 @@ def get_e0(E2, k):
     return E
 
 
-def tira_frame(k):
+def tira_frame(k, mirror_down=False):
     """Rotation R whose third column is the real propagation direction Re(k)/|Re(k)|.
 
     R is the minimal (Rodrigues) rotation taking z-hat to that direction: about
     the axis z-hat x k-hat by the angle between them.  Straight down (-z-hat)
     has no minimal rotation; a half turn about x is used there (no shipped
     record is exactly vertical downwards, so that case is unpinned).
+
+    mirror_down: for a downward wave (Re k_z < 0) the frame of the z-mirrored
+    direction (Re k_x, Re k_y, -Re k_z) instead -- the frame of the records
+    that tira::planewave's constructor makes from a Cartesian E0 and a
+    downward k (the reflected waves of ScatterLayer.cpp:246-251, and by the
+    same constructor those of ScatterVolume.cpp:469-493, 907-987).  Records of
+    waves made by tira's scatter() (ScatterPlane.cpp:175, 244) keep their own
+    frame.  Pinned by the shipped files: x64/a.cw's reflected records are the
+    restated scatterlayer solve in the mirrored frame (~1e-15; its field is then
+    continuous at every interface, and jumps by up to 15 % in the own frame),
+    data/psf.cw's reflected records the restated scatterplane solve in the own
+    frame (~1e-15; 4 % median off in the mirrored one).
     """
     kr = np.real(np.asarray(k, dtype=np.complex128))
+    if mirror_down and kr[2] < 0:
+        kr = kr * np.array([1.0, 1.0, -1.0])
     kh = kr / np.linalg.norm(kr)
     ax = np.array([-kh[1], kh[0], 0.0])           # z-hat x k-hat
     s2 = ax @ ax
@@ -110,35 +124,36 @@ def tira_frame(k):
     return np.eye(3) + K + (1.0 - kh[2]) / s2 * (K @ K)
 
 
-def get_e0_tira(E2, k):
+def get_e0_tira(E2, k, mirror_down=False):
     """A record's E0 as tira::planewave::getE0() rebuilds it (pinned by the shipped files).
 
     A record stores (E0x, E0y) = the first two components of R^T E in the
-    frame of ``tira_frame(k)``; the third local component is rebuilt from
-    k . E = 0 in that frame (k' = R^T k, complex for absorbing media).  Under
-    this reading every wave of data/psf.cw (scatterplane, 4096 incident,
-    reflected and transmitted records) and every transmitted wave of x64/a.cw
-    (scatterlayer, three boundaries) is reproduced to ~1e-15 by the layer
-    solve of ScatterLayer.cpp:152-266 fed with the file's own incident waves.
+    frame of ``tira_frame(k, mirror_down)``; the third local component is
+    rebuilt from k . E = 0 in that frame (k' = R^T k, complex for absorbing
+    media).  Under this reading every wave of data/psf.cw (scatterplane, 4096
+    incident, reflected and transmitted records; own frame) and every wave of
+    x64/a.cw (scatterlayer, three boundaries; mirror_down for its reflected
+    records) is reproduced to ~1e-15 by the layer solve of
+    ScatterLayer.cpp:152-266 fed with the file's own incident waves.
     """
     E2 = np.asarray(E2, dtype=np.complex128).reshape(-1, 2)
     k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
     out = np.zeros((len(E2), 3), dtype=np.complex128)
     for i in range(len(E2)):
-        R = tira_frame(k[i])
+        R = tira_frame(k[i], mirror_down)
         kp = R.T @ k[i]
         ez = -(kp[0] * E2[i, 0] + kp[1] * E2[i, 1]) / kp[2] if kp[2] != 0 else 0.0
         out[i] = R @ np.array([E2[i, 0], E2[i, 1], ez])
     return out
 
 
-def put_e0_tira(E, k):
+def put_e0_tira(E, k, mirror_down=False):
     """The (E0x, E0y) pair a record stores for a Cartesian E0 (inverse of get_e0_tira)."""
     E = np.asarray(E, dtype=np.complex128).reshape(-1, 3)
     k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
     out = np.zeros((len(E), 2), dtype=np.complex128)
     for i in range(len(E)):
-        out[i] = (tira_frame(k[i]).T @ E[i])[:2]
+        out[i] = (tira_frame(k[i], mirror_down).T @ E[i])[:2]
     return out
 
 

@@ -11,6 +11,14 @@ there), and the file stores the first two components of E0 in that frame.
 getE0() rebuilds the third from k . E = 0 in the same frame.  This reading
 reproduces every record of the reference's shipped data/psf.cw and the
 incident and transmitted records of x64/a.cw from their restated solves.
+
+Downward waves made by tira::planewave's constructor from a Cartesian E0 (the
+reflected waves of ScatterLayer.cpp:246-251) hold their pair in the frame of
+the z-mirrored direction (Re kx, Re ky, -Re kz) instead: with mirror_down=True
+every record of x64/a.cw, the reflected ones included, is reproduced, and its
+field is continuous at every interface (read in the wave's own frame it jumps
+by up to 15 %).  Waves made by tira's scatter() (ScatterPlane.cpp:175, 244)
+keep their own frame (psf.cw's reflected records are 4 % off when mirrored).
 """
 from __future__ import annotations
 
@@ -19,9 +27,13 @@ import struct
 import numpy as np
 
 
-def frames(k):
-    """(N, 3, 3) rotations whose third column is Re(k)/|Re(k)| (minimal rotation from z-hat)."""
+def frames(k, mirror_down: bool = False):
+    """(N, 3, 3) rotations whose third column is Re(k)/|Re(k)| (minimal rotation from z-hat); with mirror_down,
+    a wave with Re kz < 0 takes the rotation of its z-mirrored direction."""
     kr = np.real(np.asarray(k, dtype=np.complex128)).reshape(-1, 3)
+    if mirror_down:
+        kr = kr.copy()
+        kr[:, 2] = np.abs(kr[:, 2])
     kh = kr / np.linalg.norm(kr, axis=1, keepdims=True)
     ax0, ax1, c = -kh[:, 1], kh[:, 0], kh[:, 2]
     s2 = ax0 * ax0 + ax1 * ax1
@@ -43,17 +55,17 @@ def frames(k):
     return R
 
 
-def to_record(E, k):
+def to_record(E, k, mirror_down: bool = False):
     """Cartesian E0 (N, 3) -> the stored pair (N, 2)."""
-    R = frames(k)
+    R = frames(k, mirror_down)
     return np.einsum("nij,ni->nj", R, np.asarray(E, dtype=np.complex128).reshape(-1, 3))[:, :2]
 
 
-def from_record(E2, k):
+def from_record(E2, k, mirror_down: bool = False):
     """Stored pair (N, 2) -> Cartesian E0 (N, 3), the third local component from k . E = 0."""
     k = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
     E2 = np.asarray(E2, dtype=np.complex128).reshape(-1, 2)
-    R = frames(k)
+    R = frames(k, mirror_down)
     kp = np.einsum("nij,ni->nj", R, k)
     ez = np.where(kp[:, 2] != 0, -(kp[:, 0] * E2[:, 0] + kp[:, 1] * E2[:, 1]) / np.where(kp[:, 2] != 0, kp[:, 2], 1),
                   0)
@@ -61,30 +73,32 @@ def from_record(E2, k):
     return np.einsum("nij,nj->ni", R, loc)
 
 
-def _records(E, k):
+def _records(E, k, mirror_down=False):
     E = np.asarray(E, dtype=np.complex128).reshape(-1, 3)
     rec = np.empty((len(E), 5), dtype=np.complex128)
     if len(E):
-        rec[:, 0:2] = to_record(E, k)
+        rec[:, 0:2] = to_record(E, k, mirror_down)
         rec[:, 2:5] = np.asarray(k, dtype=np.complex128).reshape(-1, 3)
     return rec.tobytes()
 
 
-def save(path, Pi_E, Pi_k, layers):
-    """Write a .cw file.  E arguments are Cartesian E0 (N, 3); layers = [(z, Pr_E, Pr_k, Pt_E, Pt_k)]."""
+def save(path, Pi_E, Pi_k, layers, mirror_down: bool = False):
+    """Write a .cw file.  E arguments are Cartesian E0 (N, 3); layers = [(z, Pr_E, Pr_k, Pt_E, Pt_k)];
+    mirror_down: downward waves' pairs in the mirrored frame, as the reference's scatterlayer writes them."""
     with open(path, "wb") as f:
         f.write(struct.pack("<QQ", 8, len(Pi_E)))
-        f.write(_records(Pi_E, Pi_k))
+        f.write(_records(Pi_E, Pi_k, mirror_down))
         f.write(struct.pack("<Q", len(layers)))
         for z, PrE, Prk, PtE, Ptk in layers:
             f.write(struct.pack("<dQ", float(z), len(PrE)))
-            f.write(_records(PrE, Prk))
+            f.write(_records(PrE, Prk, mirror_down))
             f.write(struct.pack("<Q", len(PtE)))
-            f.write(_records(PtE, Ptk))
+            f.write(_records(PtE, Ptk, mirror_down))
 
 
-def load(path):
-    """Read a .cw file: (Pi_E, Pi_k, layers) with Cartesian E0 (N, 3) as getE0() rebuilds it."""
+def load(path, mirror_down: bool = False):
+    """Read a .cw file: (Pi_E, Pi_k, layers) with Cartesian E0 (N, 3) as getE0() rebuilds it (mirror_down for
+    files whose downward waves hold mirrored-frame pairs, such as the reference's scatterlayer output)."""
     b = open(path, "rb").read()
     sz, npi = struct.unpack_from("<QQ", b, 0)
     if sz != 8:
@@ -96,7 +110,7 @@ def load(path):
         r = np.frombuffer(b, dtype=np.complex128, count=5 * count, offset=o).reshape(count, 5)
         o += 80 * count
         k = r[:, 2:5].copy()
-        return from_record(r[:, 0:2], k) if count else np.zeros((0, 3), np.complex128), k
+        return from_record(r[:, 0:2], k, mirror_down) if count else np.zeros((0, 3), np.complex128), k
 
     PiE, Pik = recs(npi)
     (nl,) = struct.unpack_from("<Q", b, o)

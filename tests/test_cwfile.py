@@ -61,3 +61,34 @@ def test_vertical_waves():
     E = np.array([[1.0, 2.0, 0.0], [1.0, 2.0, 0.0], [0.5j, 1.0, 0.0]])
     assert np.allclose(cwfile.from_record(cwfile.to_record(E, k), k), E)
     assert np.allclose(cwfile.to_record(E, k)[1], [1.0, -2.0])         # half turn about x when going down
+
+
+@pytest.mark.parametrize("tag,nl", [("psf", 1), ("acw", 3)])
+def test_mirrored_decode_matches_oracle(fx, tag, nl):
+    """mirror_down reading (downward waves in the frame of their z-mirrored direction) against the oracle's."""
+    for l in range(nl):
+        for w in ("Pr", "Pt"):
+            E2, k = fx[f"{tag}_L{l}_{w}_E"], fx[f"{tag}_L{l}_{w}_k"]
+            got = cwfile.from_record(E2, k, mirror_down=True)
+            ref = ocw.get_e0_tira(E2, k, mirror_down=True)
+            assert np.abs(got - ref).max() <= 1e-15 * max(np.abs(ref).max(), 1e-300)
+            assert np.abs(cwfile.to_record(got, k, mirror_down=True) - E2).max() <= 1e-15 * max(np.abs(E2).max(),
+                                                                                             1e-300)
+            assert np.abs((got * k).sum(1)).max() <= 1e-13 * max(np.abs(got).max(), 1e-300) * np.abs(k).max()
+            if w == "Pt":          # upward waves: the same in either reading
+                assert np.abs(got - cwfile.from_record(E2, k)).max() <= 1e-15 * max(np.abs(got).max(), 1e-300)
+
+
+def test_acw_reflected_records_are_the_restated_solve_in_the_mirrored_frame(fx):
+    """x64/a.cw's reflected records, read with mirror_down, are the restated scatterlayer solve's Cartesian
+    reflected fields; the own-frame reading (right for psf.cw's scatter()-made waves) is not."""
+    from oracle import scatterlayer as osl
+    _, _, layers = osl.scatterlayer(z=(-3.0, 0.0, 3.0))
+    sel = fx["acw_sel"]
+    scale = np.abs(fx["acw_Pi_E"]).max()
+    for l in range(3):
+        PrE = layers[l][1][sel]
+        got = cwfile.from_record(fx[f"acw_L{l}_Pr_E"], fx[f"acw_L{l}_Pr_k"], mirror_down=True)
+        assert np.abs(got - PrE).max() < 1e-13 * scale
+        own = cwfile.from_record(fx[f"acw_L{l}_Pr_E"], fx[f"acw_L{l}_Pr_k"])
+        assert np.abs(own - PrE).max() > 1e-2 * scale

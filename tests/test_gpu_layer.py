@@ -134,9 +134,14 @@ def test_scatterlayer_reproduces_acw(ctx, cwfix):
     assert np.abs(k[sel] - cwfix["acw_Pi_k"].real).max() < 1e-13
     assert np.abs(cwfile.to_record(E[sel], k[sel]) - cwfix["acw_Pi_E"]).max() < 1e-13 * scale
     tE, tk = sol.Pt_E.cpu().numpy(), sol.Pt_k.cpu().numpy()
+    rE, rk = sol.Pr_E.cpu().numpy(), sol.Pr_k.cpu().numpy()
     for l in range(3):
         assert np.abs(tk[sel, l] - cwfix[f"acw_L{l}_Pt_k"]).max() < 1e-13
         assert np.abs(cwfile.to_record(tE[sel, l], tk[sel, l]) - cwfix[f"acw_L{l}_Pt_E"]).max() < 1e-13 * scale
+        # reflected records: the reference's scatterlayer stores them in the z-mirrored direction's frame
+        assert np.abs(rk[sel, l] - cwfix[f"acw_L{l}_Pr_k"]).max() < 1e-13
+        assert np.abs(cwfile.to_record(rE[sel, l], rk[sel, l], mirror_down=True) - cwfix[f"acw_L{l}_Pr_E"]).max() \
+            < 1e-12 * scale
 
 
 @pytest.fixture(scope="module")

@@ -151,12 +151,16 @@ def test_scatterplane_beam_and_solve_reproduce_psf(cwfix, psf_restated):
     assert np.abs(Ptk[sel] - cwfix["psf_L0_Pt_k"]).max() < 1e-13
     assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel]) - cwfix["psf_L0_Pr_E"]).max() < 1e-13 * scale
     assert np.abs(ocw.put_e0_tira(PtE[sel], Ptk[sel]) - cwfix["psf_L0_Pt_E"]).max() < 1e-13 * scale
+    # scatter()-made reflected waves keep their own frame: the mirrored reading is off
+    assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel], mirror_down=True) - cwfix["psf_L0_Pr_E"]).max() > 1e-2 * scale
 
 
 def test_scatterlayer_beam_and_solve_reproduce_acw(cwfix, acw_restated):
     """x64/a.cw = scatterlayer's default stack (n 1, 1.4 + 0.05i, 1.4, 1; z -3, 0, 3) under a
-    polar beam (alpha 1, 64 x 64 about z): incident and transmitted records agree to rounding
-    at every boundary; the reflected records do not match any solve of the stated system."""
+    polar beam (alpha 1, 64 x 64 about z): every record agrees to rounding at every boundary.
+    The reflected (downward) records, made by tira::planewave's constructor from a Cartesian E0
+    (ScatterLayer.cpp:246-251), hold their pair in the frame of the z-mirrored direction; in the
+    wave's own frame (the frame of psf.cw's scatter()-made reflected records) they are off."""
     ks, Es, layers = acw_restated
     sel = cwfix["acw_sel"]
     scale = np.abs(cwfix["acw_Pi_E"]).max()
@@ -168,7 +172,12 @@ def test_scatterlayer_beam_and_solve_reproduce_acw(cwfix, acw_restated):
         assert np.abs(Prk[sel] - cwfix[f"acw_L{l}_Pr_k"]).max() < 1e-13
         assert np.abs(Ptk[sel] - cwfix[f"acw_L{l}_Pt_k"]).max() < 1e-13
         assert np.abs(ocw.put_e0_tira(PtE[sel], Ptk[sel]) - cwfix[f"acw_L{l}_Pt_E"]).max() < 1e-13 * scale
+        assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel], mirror_down=True) - cwfix[f"acw_L{l}_Pr_E"]).max() \
+            < 1e-13 * scale
         assert np.abs(ocw.put_e0_tira(PrE[sel], Prk[sel]) - cwfix[f"acw_L{l}_Pr_E"]).max() > 1e-2 * scale
+        # upward waves are unaffected by the mirrored reading
+        assert np.abs(ocw.put_e0_tira(PtE[sel], Ptk[sel], mirror_down=True) - cwfix[f"acw_L{l}_Pt_E"]).max() \
+            < 1e-13 * scale
 
 
 def test_cw_fixture_field_matches_reference_file(cwfix):
