@@ -145,10 +145,15 @@ inline void write_npy(const std::string& path, const std::string& descr, const s
 // components in that frame; the reader rebuilds the third from k . E = 0 in
 // the same frame.  This is the reading under which every record of the
 // reference's data/psf.cw, and the incident and transmitted records of
-// x64/a.cw, equal the restated solves of their runs, so files written here
-// read correctly in the reference's viewer and vice versa.  Frame::cartesian
-// stores (E_x, E_y) and rebuilds E_z from k . E = 0 (not the reference's
-// convention; kept for files written that way).
+// x64/a.cw, equal the restated solves of their runs.  Frame::tira_mirror
+// ('tira-mirror') takes, for a downward wave (Re k_z < 0), the frame of the
+// z-mirrored direction (Re k_x, Re k_y, -Re k_z): the frame in which the
+// reference's scatterlayer stores its reflected waves (made by tira's
+// planewave constructor, ScatterLayer.cpp:246-251), under which every record
+// of x64/a.cw equals the restated solve; scatterplane's waves (made by tira's
+// scatter(), ScatterPlane.cpp:175, 244) keep their own frame (Frame::tira).
+// Frame::cartesian stores (E_x, E_y) and rebuilds E_z from k . E = 0 (not
+// the reference's convention; kept for files written that way).
 struct Wave {
     cplx E[3];   // Cartesian E0
     cplx k[3];
@@ -162,18 +167,20 @@ struct CoupledWave {
     std::vector<Boundary> layers;
 };
 
-enum class Frame { tira, cartesian };
+enum class Frame { tira, tira_mirror, cartesian };
 
 inline Frame parse_frame(const std::string& s) {
     if (s == "tira") return Frame::tira;
+    if (s == "tira-mirror") return Frame::tira_mirror;
     if (s == "cartesian") return Frame::cartesian;
-    throw std::runtime_error("unknown --cw-frame '" + s + "' (tira or cartesian)");
+    throw std::runtime_error("unknown --cw-frame '" + s + "' (tira, tira-mirror or cartesian)");
 }
 
 // R (row-major) with third column Re(k)/|Re(k)|: minimal rotation from z-hat;
-// straight down is a half turn about x
-inline void record_frame(const cplx k[3], double R[3][3]) {
-    double kh[3] = {k[0].real(), k[1].real(), k[2].real()};
+// straight down is a half turn about x.  mirror_down: a downward wave takes
+// the rotation of its z-mirrored direction.
+inline void record_frame(const cplx k[3], double R[3][3], bool mirror_down = false) {
+    double kh[3] = {k[0].real(), k[1].real(), mirror_down ? std::fabs(k[2].real()) : k[2].real()};
     const double nk = std::sqrt(kh[0] * kh[0] + kh[1] * kh[1] + kh[2] * kh[2]);
     for (double& v : kh) v = nk > 0 ? v / nk : 0.0;
     const double ax0 = -kh[1], ax1 = kh[0], s2 = ax0 * ax0 + ax1 * ax1;
@@ -197,7 +204,7 @@ inline void to_record(const Wave& w, Frame fr, cplx out[2]) {
         return;
     }
     double R[3][3];
-    record_frame(w.k, R);
+    record_frame(w.k, R, fr == Frame::tira_mirror);
     for (int c = 0; c < 2; ++c) out[c] = R[0][c] * w.E[0] + R[1][c] * w.E[1] + R[2][c] * w.E[2];
 }
 
@@ -209,7 +216,7 @@ inline void from_record(const cplx p[2], Wave& w, Frame fr) {
         return;
     }
     double R[3][3];
-    record_frame(w.k, R);
+    record_frame(w.k, R, fr == Frame::tira_mirror);
     cplx kp[3];
     for (int c = 0; c < 3; ++c) kp[c] = R[0][c] * w.k[0] + R[1][c] * w.k[1] + R[2][c] * w.k[2];
     const cplx e2 = (kp[2] == cplx(0.0)) ? cplx(0.0) : -(kp[0] * p[0] + kp[1] * p[1]) / kp[2];

@@ -33,7 +33,7 @@ int main(int argc, char** argv) {
         std::cout << "Allowed options:\n  --input arg (=c.cw)\n  --cuda arg (=0)\n  --size arg (=100)\n"
                      "  --resolution arg (=8)\n  --output arg (=xz.npy)\n  --axis arg (=1)\n"
                      "  --center arg (={0, 0, 0})\n  --slice arg (=0)\n"
-                     "  --cw-frame arg (=tira) record frame of the file ('tira' or 'cartesian')\n";
+                     "  --cw-frame arg (=tira) record frame of the file ('tira', 'tira-mirror' or 'cartesian')\n";
         return 1;
     }
     const std::string in = o.str("input", "c.cw"), out = o.str("output", "xz.npy");

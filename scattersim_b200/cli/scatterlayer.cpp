@@ -43,7 +43,7 @@ int main(int argc, char** argv) {
                      "  --na arg               focus angle expressed as a numerical aperture (overrides --alpha)\n"
                      "  --samples arg (=64 64) number of samples (can be specified in 2 dimensions)\n"
                      "  --mode arg (=polar)    sampling mode (polar)\n"
-                     "  --cw-frame arg (=tira) record frame of the written .cw ('tira' or 'cartesian')\n";
+                     "  --cw-frame arg (=tira) record frame of the written .cw ('tira', 'tira-mirror' or 'cartesian')\n";
         return 1;
     }
     auto t0 = std::chrono::steady_clock::now();

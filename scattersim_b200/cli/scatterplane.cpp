@@ -46,7 +46,7 @@ int main(int argc, char** argv) {
                      "  --wavemask arg (=1 1 1) waves simulated (boolean value for incident, reflected, and "
                      "transmitted)\n"
                      "  --nooutput             save an output file without printing the summary\n"
-                     "  --cw-frame arg (=tira) record frame of the written .cw ('tira' or 'cartesian')\n";
+                     "  --cw-frame arg (=tira) record frame of the written .cw ('tira', 'tira-mirror' or 'cartesian')\n";
         return 1;
     }
     auto t0 = std::chrono::steady_clock::now();

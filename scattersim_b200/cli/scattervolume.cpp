@@ -102,6 +102,11 @@ int main(int argc, char** argv) {
         std::cerr << "ERROR: " << e.what() << std::endl;
         return 1;
     }
+    if (frame == cwio::Frame::tira_mirror) {
+        std::cerr << "ERROR: --cw-frame tira-mirror is not available for the device-side .cw writer "
+                     "(tira or cartesian)" << std::endl;
+        return 1;
+    }
     if (!o.has("sample")) {
         std::cerr << "ERROR: no --sample given" << std::endl;
         return 1;

@@ -92,3 +92,45 @@ def test_acw_reflected_records_are_the_restated_solve_in_the_mirrored_frame(fx):
         assert np.abs(got - PrE).max() < 1e-13 * scale
         own = cwfile.from_record(fx[f"acw_L{l}_Pr_E"], fx[f"acw_L{l}_Pr_k"])
         assert np.abs(own - PrE).max() > 1e-2 * scale
+
+
+@pytest.fixture(scope="module")
+def cwio_frames(tmp_path_factory):
+    """The command-line tools' record-frame code (cli/cwio.hpp) in a small host program."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no host C++ compiler")
+    exe = str(tmp_path_factory.mktemp("cwio") / "cwio_frames")
+    root = os.path.dirname(HERE)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(root, "scattersim_b200", "cli"),
+                    os.path.join(HERE, "cwio_frames.cpp"), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("frame", ["tira", "tira-mirror"])
+def test_cli_record_frames_match_the_oracle(fx, cwio_frames, frame, tmp_path):
+    """a.cw's fixture records through the CLIs' reader: the Cartesian fields equal the oracle's reading in the
+    same frame (own frame, or mirrored for downward waves), and writing them back gives the same bytes."""
+    import subprocess
+    mirror = frame == "tira-mirror"
+    layers = [(float(fx["acw_z"][l]), fx[f"acw_L{l}_Pr_E"], fx[f"acw_L{l}_Pr_k"], fx[f"acw_L{l}_Pt_E"],
+               fx[f"acw_L{l}_Pt_k"]) for l in range(3)]
+    src, out, fields = (str(tmp_path / n) for n in ("in.cw", "out.cw", "fields.bin"))
+    ocw.save(src, fx["acw_Pi_E"], fx["acw_Pi_k"], layers)          # the reference's record pairs, as stored
+    r = subprocess.run([cwio_frames, src, frame, out, fields], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(fields, dtype=np.complex128).reshape(-1, 3)
+    ref = [ocw.get_e0_tira(fx["acw_Pi_E"], fx["acw_Pi_k"], mirror)]
+    for _, PrE, Prk, PtE, Ptk in layers:
+        ref += [ocw.get_e0_tira(PrE, Prk, mirror), ocw.get_e0_tira(PtE, Ptk, mirror)]
+    ref = np.concatenate(ref)
+    assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
+    a, b = open(src, "rb").read(), open(out, "rb").read()
+    assert len(a) == len(b)
+    E_in, _, lay_in = ocw.load(src)
+    E_out, _, lay_out = ocw.load(out)
+    assert np.abs(E_out - E_in).max() <= 1e-15 * np.abs(E_in).max()
+    for x, y in zip(lay_in, lay_out):
+        assert np.abs(y[1] - x[1]).max() <= 1e-15 * np.abs(E_in).max()
+        assert np.abs(y[3] - x[3]).max() <= 1e-15 * np.abs(E_in).max()

@@ -151,7 +151,7 @@ def tools():
     return BIN
 
 
-def _check_file(path, fx, tag, boundaries, check_reflected):
+def _check_file(path, fx, tag, boundaries, check_reflected, reflected_tol=1e-13):
     raw = open(path, "rb").read()
     assert len(raw) == int(fx[f"{tag}_bytes"])          # same list sizes as the reference's file
     PiE, Pik, lay = ocw.load(path)
@@ -165,7 +165,7 @@ def _check_file(path, fx, tag, boundaries, check_reflected):
         assert np.abs(lay[l][3][sel] - fx[f"{tag}_L{l}_Pt_E"]).max() < 1e-13 * scale
         assert np.abs(lay[l][2][sel] - fx[f"{tag}_L{l}_Pr_k"]).max() < 1e-13
         if check_reflected:
-            assert np.abs(lay[l][1][sel] - fx[f"{tag}_L{l}_Pr_E"]).max() < 1e-13 * scale
+            assert np.abs(lay[l][1][sel] - fx[f"{tag}_L{l}_Pr_E"]).max() < reflected_tol * scale
 
 
 def test_cli_scatterplane_writes_psf(tools, cwfix):
@@ -184,6 +184,16 @@ def test_cli_scatterlayer_writes_acw(tools, cwfix):
         _check_file(os.path.join(d, "a.cw"), cwfix, "acw", 3, False)
         smp = np.load(os.path.join(d, "sample.npy"))
         assert smp.shape == (2, 1, 1) and np.allclose(smp.ravel(), [1.4 + 0.05j, 1.4])
+
+
+def test_cli_scatterlayer_mirrored_frame_writes_every_acw_record(tools, cwfix):
+    """--cw-frame tira-mirror: reflected records in the z-mirrored direction's frame, as the reference's
+    scatterlayer stores them -- every record of a.cw, the reflected ones included."""
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([os.path.join(tools, "scatterlayer"), "--z", "-3", "0", "3", "--output", "a.cw",
+                            "--cw-frame", "tira-mirror"], cwd=d, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        _check_file(os.path.join(d, "a.cw"), cwfix, "acw", 3, True, reflected_tol=1e-12)
 
 
 def test_cli_layer_tools_reject_bad_input(tools):
