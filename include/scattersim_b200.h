@@ -313,7 +313,10 @@ sc_status sc_volume_waves(sc_context* ctx, const sc_volume_params* p, int Z, int
  * then per layer its z (z_layers, host), u64 #Pr, records, u64 #Pt, records.
  * counts (host, 1 + 2 layers): #Pi, then #Pr and #Pt per layer.  Records are
  * 80 bytes {E0 pair, kx, ky, kz}; frame 0 stores the E0 pair in tira's record
- * frame (the reference's own files), 1 the Cartesian (E_x, E_y).  Records are
+ * frame (the frame rotated to Re k: the reference's scatterplane files), 1 the
+ * Cartesian (E_x, E_y), 2 tira's frame with a downward wave (Re k_z < 0) in
+ * the frame of its z-mirrored direction (the reference's scatterlayer files,
+ * whose reflected waves tira::planewave's constructor made).  Records are
  * formed on the device and streamed through pinned buffers, the copy of one
  * chunk overlapping the write of the previous (GB-scale files at disk speed).
  * Synchronises the stream. */

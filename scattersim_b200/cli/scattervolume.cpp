@@ -9,8 +9,10 @@
 // sample is one layer, FourierWave.h:291-299).
 //
 // Records are stored in the reference's record frame (--cw-frame tira, the
-// default: the E0 pair in the frame rotated to Re k, which the reference's
-// viewer reads back); --cw-frame cartesian stores (E_x, E_y).
+// default: the E0 pair in the frame rotated to Re k); --cw-frame tira-mirror
+// stores a downward wave's pair in the frame of its z-mirrored direction (the
+// frame of the waves tira::planewave's constructor makes, which the reference
+// uses for these waves); --cw-frame cartesian stores (E_x, E_y).
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -62,7 +64,8 @@ int main(int argc, char** argv) {
                      "  --external             save waves for the external field only\n"
                      "  --log                  produce a log file\n"
                      "  --npz                  calculate Px and Py only\n"
-                     "  --cw-frame arg (=tira)  E pair stored in the record frame ('tira') or as (E_x, E_y) ('cartesian')\n"
+                     "  --cw-frame arg (=tira)  E pair stored in the record frame ('tira'; 'tira-mirror': downward waves in the\n"
+                     "                         frame of their z-mirrored direction) or as (E_x, E_y) ('cartesian')\n"
                      "  --cuda arg (=0)        CUDA device\n";
         return 1;
     }
@@ -100,11 +103,6 @@ int main(int argc, char** argv) {
         frame = cwio::parse_frame(o.str("cw-frame", "tira"));
     } catch (const std::exception& e) {
         std::cerr << "ERROR: " << e.what() << std::endl;
-        return 1;
-    }
-    if (frame == cwio::Frame::tira_mirror) {
-        std::cerr << "ERROR: --cw-frame tira-mirror is not available for the device-side .cw writer "
-                     "(tira or cartesian)" << std::endl;
         return 1;
     }
     if (!o.has("sample")) {
@@ -181,7 +179,8 @@ int main(int argc, char** argv) {
     }
     if (!out.empty()) {
         if ((s = sc_cw_write(ctx, out.c_str(), d_E, d_k, nw, Z + 1, zl.data(), counts.data(),
-                             frame == cwio::Frame::tira ? 0 : 1, nullptr)) != SC_OK)
+                             frame == cwio::Frame::tira ? 0 : (frame == cwio::Frame::cartesian ? 1 : 2),
+                             nullptr)) != SC_OK)
             return fail("sc_cw_write", s);
     }
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

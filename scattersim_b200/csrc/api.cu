@@ -708,7 +708,7 @@ sc_status sc_volume_field_grid(sc_context* ctx, const sc_volume_params* p, int Z
 sc_status sc_cw_write(sc_context* ctx, const char* path, const void* E0, const void* k, long long nw, int layers,
                       const double* z_layers, const long long* counts, int frame, void* stream) {
     if (!ctx || !path || layers < 0 || nw < 0 || !counts || (layers > 0 && !z_layers) || (nw > 0 && (!E0 || !k)) ||
-        (frame != 0 && frame != 1)) {
+        frame < 0 || frame > 2) {
         set_error("sc_cw_write: bad argument");
         return SC_BADINPUT;
     }

@@ -29,7 +29,9 @@ namespace {
 
 constexpr long long CW_CHUNK = 1 << 20;   // records per chunk (80 MB)
 
-// the record pair of one wave: tira frame (frame 0) or Cartesian (frame 1)
+// the record pair of one wave: tira frame (frame 0), Cartesian (frame 1), or
+// tira frame with a downward wave (Re k_z < 0) in the frame of its z-mirrored
+// direction (frame 2: the reference's constructor-made reflected waves)
 __global__ void cw_record_kernel(const double2* __restrict__ E0, const double2* __restrict__ K, long long w0,
                                  long long count, int frame, double2* __restrict__ rec) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -43,7 +45,7 @@ __global__ void cw_record_kernel(const double2* __restrict__ E0, const double2* 
         p1 = e1;
     } else {
         // R with third column Re k / |Re k| (record_frame of the host writer)
-        double kh0 = k0.x, kh1 = k1.x, kh2 = k2.x;
+        double kh0 = k0.x, kh1 = k1.x, kh2 = (frame == 2) ? fabs(k2.x) : k2.x;
         const double nk = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(kh0, kh0), __dmul_rn(kh1, kh1)),
                                                __dmul_rn(kh2, kh2)));
         kh0 = nk > 0 ? __ddiv_rn(kh0, nk) : 0.0;

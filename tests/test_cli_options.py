@@ -62,8 +62,8 @@ def test_refusals_before_device_work(tools, tmp_path):
     assert r.returncode != 0 and "ERROR" in r.stderr
     r = _run(tools, "scattervolume", "--lambda", "0.5", cwd=tmp_path)          # no --sample
     assert r.returncode != 0 and "ERROR" in r.stderr
-    r = _run(tools, "scattervolume", "--sample", "s.npy", "--cw-frame", "tira-mirror", cwd=tmp_path)
-    assert r.returncode != 0 and "tira-mirror" in r.stderr                   # not in the device-side writer
+    r = _run(tools, "scattervolume", "--sample", "s.npy", "--cw-frame", "upside-down", cwd=tmp_path)
+    assert r.returncode != 0 and "tira-mirror" in r.stderr                   # the error names the choices
     r = _run(tools, "scatterlayer", "--cw-frame", "sideways", cwd=tmp_path)
     assert r.returncode != 0 and "ERROR" in r.stderr
     r = _run(tools, "scattereval", "--axis", "5", cwd=tmp_path)

@@ -2,7 +2,8 @@
 
 Small case: every byte of the structure (size field, counts, z planes, wave
 vectors) equals the Python .cw module's file, and the stored E0 pairs agree
-with its record-frame rotation to rounding, in both frames; the file reads
+with its record-frame rotation to rounding, in every frame (own, Cartesian,
+mirrored for downward waves); the file reads
 back through the oracle's reader.  Large case: the 3-D volume workload's full
 wave table (32 layers, 21x21 orders: about 26 million records, 2 GB) streamed
 to disk, its size and sampled records checked.
@@ -52,7 +53,7 @@ def test_cw_write_matches_python_writer(ctx, external):
     E = wt.E0.cpu().numpy()
     K = wt.k.cpu().numpy()
     with tempfile.TemporaryDirectory() as d:
-        for frame in (0, 1):
+        for frame in (0, 1, 2):
             a = os.path.join(d, f"gpu{frame}.cw")
             write(ctx, a, wt, counts, frame)
             raw = open(a, "rb").read()
@@ -81,7 +82,7 @@ def test_cw_write_matches_python_writer(ctx, external):
             assert off == len(raw)
             R = np.concatenate(recs)
             assert np.array_equal(R[:, 2:5], K)                      # wave vectors byte for byte
-            pair = cwfile.to_record(E, K) if frame == 0 else E[:, :2]
+            pair = E[:, :2] if frame == 1 else cwfile.to_record(E, K, mirror_down=(frame == 2))
             scale = np.abs(E).max(axis=1, keepdims=True) + 1e-300
             assert np.all(np.abs(R[:, 0:2] - pair) <= 4e-16 * scale)
             if frame == 1:
