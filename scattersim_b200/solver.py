@@ -316,6 +316,45 @@ def field_grid(ctx: Context, params: VolumeParams, sol: VolumeSolution, origin, 
     return out
 
 
+def empty_solution(ctx: Context, params: VolumeParams, shape, fields: bool = True) -> VolumeSolution:
+    """A VolumeSolution of the planned shapes with uninitialised tensors on the context's device: the buffers a
+    rank receives a solution into."""
+    shape = tuple(shape)
+    if len(shape) == 2:
+        shape = (1,) + shape
+    d = plan(params, shape)
+    MF, Z = d.MF, shape[0]
+    dev = torch.device("cuda", ctx.device)
+    want = fields and not params.external
+
+    def z(*s):
+        return torch.empty(s, dtype=torch.complex128, device=dev)
+    return VolumeSolution(d, shape, z(6 * MF), z(Z, 4 * MF), z(Z, 2 * MF, 3 * MF) if want else None,
+                          z(Z, 2 * MF, 3 * MF) if want else None)
+
+
+def split_field_grid(ctx: Context, params: VolumeParams, sol: VolumeSolution, origin, step, counts, dist=None,
+                     gather: bool = True, ez_mode: int = 0, zeps: float = 0.001, precision: int = 0, stream=None):
+    """field_grid with the grid's z-planes split over the ranks of `dist` (contiguous slabs).
+
+    Rank 0's solution is broadcast once to the other ranks (which pass a solution of the same shapes, for
+    example from empty_solution); each rank evaluates its slab of planes; with gather every rank returns the
+    whole (Nz, Ny, Nx, 3) grid, without it (its slab or None, (first plane, end plane)).
+    """
+    from . import fieldsplit
+    if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        fieldsplit.broadcast_tensors([sol.x, sol.evl, sol.Qc, sol.Qh], dist, src=0)
+    o = [float(v) for v in origin]
+    st = [float(v) for v in step]
+    nx, ny, nz = (int(c) for c in counts)
+
+    def slab(b, e):
+        return field_grid(ctx, params, sol, (o[0], o[1], o[2] + b * st[2]), st, (nx, ny, e - b), ez_mode, zeps,
+                          precision, stream)
+    dt = torch.complex128 if precision == 0 else torch.complex64
+    return fieldsplit.split_grid(slab, (nx, ny, nz), dist, torch.device("cuda", ctx.device), dt, gather)
+
+
 @dataclass
 class SweepResult:
     x: list                  # per instance: (6 MF,) complex128 device tensor [R; T]

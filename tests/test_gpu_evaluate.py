@@ -118,3 +118,29 @@ def test_field_grid_equals_direct_sum(ctx, kw, counts):
     # complex64 output: the same values rounded
     g32 = solver.field_grid(ctx, p, sol, origin, step, counts, precision=1).cpu().numpy().reshape(-1, 3)
     assert np.linalg.norm(g32 - grid) / np.linalg.norm(grid) < 1e-7
+
+
+def test_field_grid_slabs_equal_the_whole_grid(ctx):
+    """The z-plane split on one GPU, without collectives: the grid evaluated in three slabs (each from its first
+    plane, as three ranks would), from a solution copied into empty_solution's buffers (as a rank receives it),
+    equals the whole grid; split_field_grid without a process group is field_grid."""
+    from scattersim_b200 import fieldsplit
+    smp = samples.sphere_volume(4, nxy=24, nz=5, size=(20.0, 20.0, 8.0))
+    p = solver.make_params(lambda_=0.6, size=(20, 20, 8), coef=(7, 5), direction=(0.17, 0.05, 0.98), ex=(1, 0),
+                           ey=(0, 0))
+    sol = solver.solve(ctx, p, torch.from_numpy(smp).cuda())
+    origin, step, counts = (1.3, 2.1, -6.5), (1.1, 1.7, 0.55), (9, 7, 23)
+    whole = solver.field_grid(ctx, p, sol, origin, step, counts)
+    scale = whole.abs().max()
+    assert (solver.split_field_grid(ctx, p, sol, origin, step, counts) - whole).abs().max() <= 1e-14 * scale
+    recv = solver.empty_solution(ctx, p, smp.shape)
+    for dst, src in ((recv.x, sol.x), (recv.evl, sol.evl), (recv.Qc, sol.Qc), (recv.Qh, sol.Qh)):
+        assert dst.shape == src.shape
+        dst.copy_(src)
+
+    def slab(b, e):
+        return solver.field_grid(ctx, p, recv, (origin[0], origin[1], origin[2] + b * step[2]), step,
+                                 (counts[0], counts[1], e - b))
+    got = fieldsplit.slab_grid(slab, counts, fieldsplit.plane_blocks(counts[2], 3))
+    assert got.shape == whole.shape
+    assert (got - whole).abs().max() <= 1e-12 * scale

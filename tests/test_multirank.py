@@ -176,3 +176,120 @@ def test_layer_split_equals_unsplit_chain(world):
     ref = osv.solve(smp, p, keep=False).x
     for rank, blk, x in res:
         assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-12, (rank, blk)
+
+
+# ---------------------------------------------------------------- field grid split by z-planes
+FIELD_COUNTS = (6, 5, 11)          # nx, ny, nz
+FIELD_ORIGIN, FIELD_STEP = (-1.3, 0.4, -2.0), (0.37, 0.29, 0.41)
+
+
+def field_table(seed=3):
+    """A seeded wave table of three boundaries (incident, reflected and transmitted lists), unpacked."""
+    from oracle import cw as ocw
+    rng = np.random.default_rng(seed)
+
+    def waves(n, down):
+        kt = rng.uniform(-2.0, 2.0, (n, 2))
+        kz = np.sqrt(40.0 - (kt ** 2).sum(1)) * (-1 if down else 1)
+        k = np.c_[kt, kz].astype(np.complex128)
+        E = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
+        return E, k
+    PiE, Pik = waves(4, False)
+    layers = []
+    for z in (-1.0, 0.0, 1.5):
+        PrE, Prk = waves(3, True)
+        PtE, Ptk = waves(5, False)
+        layers.append((z, PrE, Prk, PtE, Ptk))
+    return ocw.unpack(PiE, Pik, layers)
+
+
+def field_planes(WE, Wk, zl, b, e, lo, hi):
+    """The oracle's evaluator on planes lo .. hi-1 of the test grid: (hi - lo, ny, nx, 3) (planes beyond the
+    test grid's count follow the same spacing)."""
+    import torch
+    from oracle import cw as ocw
+    nx, ny, _ = FIELD_COUNTS
+    zz, yy, xx = np.meshgrid(FIELD_ORIGIN[2] + FIELD_STEP[2] * np.arange(lo, hi),
+                             FIELD_ORIGIN[1] + FIELD_STEP[1] * np.arange(ny),
+                             FIELD_ORIGIN[0] + FIELD_STEP[0] * np.arange(nx), indexing="ij")
+    pts = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], -1)
+    return torch.from_numpy(ocw.evaluate(pts, zl, b, e, WE, Wk).reshape(hi - lo, ny, nx, 3))
+
+
+def _field_worker(rank, world, port, q, nz=FIELD_COUNTS[2]):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from scattersim_b200 import fieldsplit
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        zl, b, e, WE, Wk = field_table()
+        # only rank 0 holds the table; the others receive it
+        tE, tk = torch.from_numpy(WE.copy()), torch.from_numpy(Wk.copy())
+        if rank != 0:
+            tE.zero_()
+            tk.zero_()
+        fieldsplit.broadcast_tensors([tE, None, tk], dist)
+
+        def fn(lo, hi):
+            return field_planes(tE.numpy(), tk.numpy(), zl, b, e, lo, hi)
+        counts = FIELD_COUNTS[:2] + (nz,)
+        full = fieldsplit.split_grid(fn, counts, dist, "cpu")
+        local, rng_ = fieldsplit.split_grid(fn, counts, dist, "cpu", gather=False)
+        q.put((rank, full.numpy(), None if local is None else local.numpy(), rng_))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_plane_blocks_partition_in_order():
+    from scattersim_b200 import fieldsplit
+    for nz, w in [(11, 2), (64, 8), (5, 5), (3, 4), (0, 2)]:
+        bl = fieldsplit.plane_blocks(nz, w)
+        assert len(bl) == w and bl[0][0] == 0 and bl[-1][1] == nz
+        assert all(a[1] == c[0] for a, c in zip(bl, bl[1:]))
+        sizes = [hi - lo for lo, hi in bl]
+        assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        fieldsplit.plane_blocks(4, 0)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_field_grid_split_equals_the_whole_grid(world):
+    """z-slabs on 2 and 3 gloo ranks, the wave table broadcast from rank 0, the slabs all-gathered: every rank
+    holds the single-process grid; without the gather each rank holds its own slab."""
+    from scattersim_b200 import fieldsplit
+    res = run_ranks(_field_worker, world)
+    zl, b, e, WE, Wk = field_table()
+    ref = field_planes(WE, Wk, zl, b, e, 0, FIELD_COUNTS[2]).numpy()
+    blocks = fieldsplit.plane_blocks(FIELD_COUNTS[2], world)
+    for rank, full, local, (lo, hi) in res:
+        assert full.shape == ref.shape
+        assert np.abs(full - ref).max() <= 1e-13 * np.abs(ref).max(), rank
+        assert (lo, hi) == blocks[rank]
+        assert np.abs(local - ref[lo:hi]).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_field_grid_split_with_a_rank_holding_no_planes():
+    """3 ranks, 2 planes: the last rank evaluates nothing yet takes part in the gather."""
+    import functools
+    from scattersim_b200 import fieldsplit
+    res = run_ranks(functools.partial(_field_worker, nz=2), 3)
+    zl, b, e, WE, Wk = field_table()
+    ref = field_planes(WE, Wk, zl, b, e, 0, 2).numpy()
+    for rank, full, local, (lo, hi) in res:
+        assert np.abs(full - ref).max() <= 1e-13 * np.abs(ref).max(), rank
+        assert (lo, hi) == fieldsplit.plane_blocks(2, 3)[rank]
+        assert (local is None) == (hi == lo)
+
+
+def test_slab_grid_assembles_blocks_in_order():
+    from scattersim_b200 import fieldsplit
+    zl, b, e, WE, Wk = field_table()
+    ref = field_planes(WE, Wk, zl, b, e, 0, FIELD_COUNTS[2]).numpy()
+    got = fieldsplit.slab_grid(lambda lo, hi: field_planes(WE, Wk, zl, b, e, lo, hi), FIELD_COUNTS,
+                               fieldsplit.plane_blocks(FIELD_COUNTS[2], 4)).numpy()
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
