@@ -104,8 +104,12 @@ sc_status sc_linearsolve_batched(sc_context* ctx, void* A, int n, void* B, int n
  * a device looks the array's device address up for that device and keeps it
  * (make that call before any stream capture, and none after cudaDeviceReset).
  * Like the allocating entry, each call copies the status words back into the
- * host array info and synchronises the stream.  All calls share the array:
- * calls whose work overlaps on the GPU race. */
+ * host array info and synchronises the stream -- except while the stream is
+ * capturing into a CUDA graph: the call then only records the solve's kernels
+ * (make one uncaptured call with the same n and batch on the device first),
+ * leaves info untouched and returns SC_OK, and every replay of the graph
+ * solves again.  All calls share the array: calls whose work overlaps on the
+ * GPU race. */
 sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int nrhs, int batch, int* info,
                                          void* stream);
 

@@ -26,7 +26,13 @@
 // point after resetting the device.
 //
 // Each call ends by copying the status words back to the host and
-// synchronising `stream` (info is a host array, as in the allocating entry).
+// synchronising `stream` (info is a host array, as in the allocating entry),
+// except while `stream` is capturing into a CUDA graph: a capture accepts
+// neither a copy into pageable host memory nor a synchronisation, so the call
+// then records only its clear of the status words and its LU kernels (no
+// allocation, and no other driver call once a first call on the device has
+// looked up the array and raised the kernels' shared-memory limits), leaves
+// info untouched and returns SC_OK; each replay of the graph solves again.
 //
 // All calls share the one array and keep the last call's contents: the status
 // words are cleared on the stream at the start of every call, and calls whose
@@ -90,11 +96,14 @@ extern "C" sc_status sc_linearsolve_batched_noalloc(void* A, int n, void* B, int
     int* piv = base;
     int* dinfo = base + NOALLOC_MAX_PIVOTS;
     cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    SC_CUDA_TRY(cudaStreamIsCapturing(st, &capture));
     // the previous call's status words are still in the array
     SC_CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int) * batch, st));
     const long long sA = (long long)n * n, sB = (long long)n * nrhs;
     SC_TRY(getrf(st, (double2*)A, n, sA, n, batch, piv, dinfo));
     SC_TRY(getrs(st, (const double2*)A, n, sA, n, piv, (double2*)B, n, sB, nrhs, batch));
+    if (capture != cudaStreamCaptureStatusNone) return SC_OK;   // recorded into the caller's graph
     int hinfo[NOALLOC_MAX_BATCH];
     SC_CUDA_TRY(cudaMemcpyAsync(hinfo, dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st));
     SC_CUDA_TRY(cudaStreamSynchronize(st));

@@ -124,3 +124,35 @@ def test_noalloc_rejects_a_stream_of_another_device():
         other = torch.cuda.Stream()
     torch.cuda.set_device(0)
     assert _noalloc(a, a, 2, 1, 1, info, other) == SC_BADINPUT
+
+
+def test_noalloc_records_into_a_cuda_graph():
+    """Captured on a side stream into a CUDA graph, after one uncaptured call with the same sizes: the capture
+    records the solve without a readback or a synchronisation (info untouched), and each replay, with fresh
+    systems copied into the captured buffers, solves them."""
+    rng = np.random.default_rng(7)
+    batch, n, nrhs = 4, 64, 2
+
+    def systems():
+        A = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+        return A, rng.standard_normal((batch, n, nrhs)) + 1j * rng.standard_normal((batch, n, nrhs))
+    A, Bm = systems()
+    a, b = _colmajor(A), _colmajor(Bm)
+    info = (ctypes.c_int * batch)()
+    assert _noalloc(a, b, n, nrhs, batch, info) == SC_OK
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    untouched = (ctypes.c_int * batch)(*([-7] * batch))
+    with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+        rc = _noalloc(a, b, n, nrhs, batch, untouched, s)
+    assert rc == SC_OK and list(untouched) == [-7] * batch
+    for _ in range(2):
+        A, Bm = systems()
+        a.copy_(_colmajor(A))
+        b.copy_(_colmajor(Bm))
+        g.replay()
+        torch.cuda.synchronize()
+        x = np.swapaxes(b.cpu().numpy().reshape(batch, nrhs, n), -1, -2)
+        assert np.abs(x - np.linalg.solve(A, Bm)).max() <= 1e-10 * np.abs(x).max()
+    del g
