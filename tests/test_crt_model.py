@@ -4,7 +4,9 @@ Restates with exact integers the steps the kernels take, so that each trick is p
 without a GPU: operand splitting into 17-bit limbs and the residue with a folded offset
 (pack kernels), the accumulator residue with an offset (MMA epilogue), the biased byte
 unpacking and the three-limb FP64 reconstruction (rebuild kernel), and a whole emulated
-complex product against numpy within the scaling's error bound.
+complex product against numpy within the scaling's error bound -- for the engine's 14
+moduli and for the first 13 and 12 (smaller P, fewer operand bits), the arithmetic a
+count chosen per product would use.
 """
 import math
 
@@ -35,8 +37,8 @@ def acc_res_shifted(x, p):
     return ((x + off) & 0xFFFFFFFF) % p
 
 
-def crt_bits(k):
-    return min(49, int((math.log2(P) - 3 - math.log2(2 * max(k, 1))) // 2))
+def crt_bits(k, nmod=len(MODS)):
+    return min(49, int((math.log2(math.prod(MODS[:nmod])) - 3 - math.log2(2 * max(k, 1))) // 2))
 
 
 def test_moduli_pairwise_coprime_and_range():
@@ -109,18 +111,24 @@ def limbs37(v):
     return float(v >> 74), float((v >> 37) & m), float(v & m)
 
 
-def test_three_limb_reconstruction_is_exact():
-    """S = sum r_p w_p and its reduction by the nearest multiple of P are exact in FP64 limbs."""
+@pytest.mark.parametrize("nmod", [14, 13, 12])
+def test_three_limb_reconstruction_is_exact(nmod):
+    """S = sum r_p w_p and its reduction by the nearest multiple of P are exact in FP64 limbs -- for the 14
+    moduli of the engine and for the first 13 and 12 (a smaller P, fewer residue products)."""
+    mods = MODS[:nmod]
+    P = math.prod(mods)
     w = []
-    for p in MODS:
+    for p in mods:
         Mp = P // p
         w.append((Mp * pow(Mp, -1, p)) % P)
     W = [limbs37(v) for v in w]
     PL = limbs37(P)
     rng = np.random.default_rng(2)
-    for _ in range(3000):
-        x = int(rng.integers(-(2 ** 62), 2 ** 62)) * int(rng.integers(1, 2 ** 44))   # up to ~2^106 < P / 4
-        r = [sym(x, p) for p in MODS]
+    top = (P.bit_length() - 3) - 62                  # |x| up to ~P / 8
+    xs = [int(rng.integers(-(2 ** 62), 2 ** 62)) * int(rng.integers(1, 2 ** top)) for _ in range(3000)]
+    xs += [0, 1, -1, 2 ** 20 + 7, -(2 ** 60) + 3, 2 ** 75 + 1]       # small values: the absolute error regime
+    for x in xs:
+        r = [sym(x, p) for p in mods]
         sh = sum(ri * Wi[0] for ri, Wi in zip(r, W))
         sm = sum(ri * Wi[1] for ri, Wi in zip(r, W))
         sl = sum(ri * Wi[2] for ri, Wi in zip(r, W))
@@ -133,12 +141,18 @@ def test_three_limb_reconstruction_is_exact():
             assert abs(d) < 2 ** 53 and d == int(d)
         exact = int(dh) * 2 ** 74 + int(dm) * 2 ** 37 + int(dl)
         assert exact == x
+        # the kernel's two roundings: fma(dm, 2^37, dl), then fma(dh, 2^74, that) -- the result's own rounding
+        # (relative to |x|) plus the inner term's, whose value stays below 2^88 (absolute error < 2^35, far
+        # below the operands' rounding: ~2^58 for 14 moduli at k = 1250, ~2^42 and more for 12)
+        inner = abs(dm) * 2.0 ** 37 + abs(dl)
+        assert inner < 2.0 ** 88
         approx = dh * 2.0 ** 74 + (dm * 2.0 ** 37 + dl)
-        assert abs(approx - x) <= 2.0 ** -51 * abs(x) + 1.0
+        assert abs(approx - x) <= 2.0 ** -52 * (abs(x) + inner) + 1.0
 
 
+@pytest.mark.parametrize("nmod", [14, 13, 12])
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 9), (24, 17, 33)])
-def test_emulated_complex_product(m, n, k):
+def test_emulated_complex_product(m, n, k, nmod):
     """The whole modular product on small operands: scale rows / columns by powers of two, round to integers
     of `bits` bits, form the interleaved real embedding, multiply residues mod each p exactly, rebuild by CRT
     and scale back -- within the bound the GPU tests state."""
@@ -146,7 +160,9 @@ def test_emulated_complex_product(m, n, k):
     A = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
     B = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
     A[0] *= 1e-30
-    bits = crt_bits(k)
+    mods = MODS[:nmod]
+    P = math.prod(mods)
+    bits = crt_bits(k, nmod)
     ea = [math.frexp(max(np.abs(A[i].real).max(), np.abs(A[i].imag).max()))[1] for i in range(m)]
     eb = [math.frexp(max(np.abs(B[:, c].real).max(), np.abs(B[:, c].imag).max()))[1] for c in range(n)]
     ai = [[(int(round(math.ldexp(z.real, bits - ea[i]))), int(round(math.ldexp(z.imag, bits - ea[i]))))
@@ -158,7 +174,7 @@ def test_emulated_complex_product(m, n, k):
         for c in range(n):
             # rows 2i (Re, -Im) and 2i+1 (Im, Re) of A' against the interleaved column of B'
             re_p, im_p = [], []
-            for p in MODS:
+            for p in mods:
                 sr = si = 0
                 for j in range(k):
                     ar, aim = sym(ai[i][j][0], p), sym(ai[i][j][1], p)
@@ -169,7 +185,7 @@ def test_emulated_complex_product(m, n, k):
                 im_p.append(sym(si, p))
 
             def rebuild(res):
-                s = sum(r * ((P // p) * pow(P // p, -1, p)) for r, p in zip(res, MODS)) % P
+                s = sum(r * ((P // p) * pow(P // p, -1, p)) for r, p in zip(res, mods)) % P
                 return s - P if s > P // 2 else s
             cr, ci = rebuild(re_p), rebuild(im_p)
             # the exact integer products
