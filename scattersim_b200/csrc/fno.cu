@@ -1,7 +1,7 @@
 // Fourier-neural-operator surrogate of the thin-volume solve: a 64 x 64 index
 // map plus the wavelength in, the R/T amplitudes of the 11 x 11 orders out
 // (the x vector of ScatterVolume.cpp:739 for --coef 11 11).  The plain solve is
-// its training data, its fallback and the judge of its error.
+// its training data, its fallback and the measure of its error.
 //
 // Network (width W = 64, 4 spectral layers, 16 x 16 retained modes):
 //   in  = [n(x, y), (lambda - 0.6) / 0.2, x / 63, y / 63,
