@@ -4,6 +4,7 @@
 // read/write, and the coupled-wave (.cw) file of CoupledWaveStructure.h:63-125.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -167,13 +168,20 @@ struct CoupledWave {
     std::vector<Boundary> layers;
 };
 
-enum class Frame { tira, tira_mirror, cartesian };
+// Frame::automatic is for readers only: the file's own convention, decided
+// from the field's continuity at its first interface (load_cw).
+enum class Frame { tira, tira_mirror, cartesian, automatic };
 
 inline Frame parse_frame(const std::string& s) {
     if (s == "tira") return Frame::tira;
     if (s == "tira-mirror") return Frame::tira_mirror;
     if (s == "cartesian") return Frame::cartesian;
     throw std::runtime_error("unknown --cw-frame '" + s + "' (tira, tira-mirror or cartesian)");
+}
+inline Frame parse_read_frame(const std::string& s) {
+    if (s == "auto") return Frame::automatic;
+    if (s == "tira" || s == "tira-mirror" || s == "cartesian") return parse_frame(s);
+    throw std::runtime_error("unknown --cw-frame '" + s + "' (tira, tira-mirror, cartesian or auto)");
 }
 
 // R (row-major) with third column Re(k)/|Re(k)|: minimal rotation from z-hat;
@@ -198,6 +206,7 @@ inline void record_frame(const cplx k[3], double R[3][3], bool mirror_down = fal
 }
 
 inline void to_record(const Wave& w, Frame fr, cplx out[2]) {
+    if (fr == Frame::automatic) throw std::runtime_error("a .cw file is written in one named record frame");
     if (fr == Frame::cartesian) {
         out[0] = w.E[0];
         out[1] = w.E[1];
@@ -267,7 +276,67 @@ inline std::vector<Wave> get_records(std::ifstream& f, Frame fr) {
     return w;
 }
 
+// Largest jump of the tangential (x, y) field across the first interface,
+// relative to the field there, with the stored pairs (held in E[0], E[1] of
+// `raw`) read in frame fr: the plane-wave sum of region 0 (incident +
+// reflected at z_0) against region 1 (transmitted at z_0 + reflected at z_1),
+// on the plane z = z_0 at eight points within a wavelength of the axis (the
+// regions of cpuEvaluator.cpp:34-102).  The reading a file was written in
+// gives a continuous field.
+inline double interface_jump(const CoupledWave& raw, Frame fr) {
+    if (raw.layers.empty()) return 0.0;
+    const Boundary& L0 = raw.layers[0];
+    std::vector<const std::vector<Wave>*> above = {&raw.Pi, &L0.Pr}, below = {&L0.Pt};
+    if (raw.layers.size() > 1) below.push_back(&raw.layers[1].Pr);
+    double kmax = 1.0;
+    for (auto* ws : {&raw.Pi, &L0.Pr, &L0.Pt})
+        for (auto& w : *ws) kmax = std::max(kmax, std::abs(w.k[0]) + std::abs(w.k[1]) + std::abs(w.k[2]));
+    const double off[8][2] = {{0.13, -0.71}, {-0.52, 0.38}, {0.91, 0.07}, {-0.26, -0.44},
+                              {0.47, 0.83}, {-0.88, -0.19}, {0.05, 0.56}, {0.64, -0.33}};
+    const double wl = 2.0 * M_PI / kmax;
+    double jump = 0.0, scale = 0.0;
+    for (auto& o : off) {
+        const double r[3] = {o[0] * wl, o[1] * wl, L0.z};
+        cplx Ea[2] = {0.0, 0.0}, Eb[2] = {0.0, 0.0};
+        auto add = [&](const std::vector<const std::vector<Wave>*>& lists, cplx E[2]) {
+            for (auto* ws : lists)
+                for (const Wave& w0 : *ws) {
+                    Wave w = w0;
+                    const cplx p[2] = {w0.E[0], w0.E[1]};
+                    from_record(p, w, fr);
+                    const cplx ph = std::exp(cplx(0.0, 1.0) * (w.k[0] * r[0] + w.k[1] * r[1] + w.k[2] * r[2]));
+                    E[0] += w.E[0] * ph;
+                    E[1] += w.E[1] * ph;
+                }
+        };
+        add(above, Ea);
+        add(below, Eb);
+        for (int c = 0; c < 2; ++c) {
+            jump = std::max(jump, std::abs(Ea[c] - Eb[c]));
+            scale = std::max(scale, std::max(std::abs(Ea[c]), std::abs(Eb[c])));
+        }
+    }
+    return scale > 0.0 ? jump / scale : 0.0;
+}
+
 inline CoupledWave load_cw(const std::string& path, Frame fr = Frame::tira) {
+    if (fr == Frame::automatic) {
+        CoupledWave cw = load_cw(path, Frame::cartesian);     // E[0], E[1]: the stored pairs
+        const Frame use = interface_jump(cw, Frame::tira_mirror) < interface_jump(cw, Frame::tira)
+                              ? Frame::tira_mirror : Frame::tira;
+        auto conv = [&](std::vector<Wave>& ws) {
+            for (Wave& w : ws) {
+                const cplx p[2] = {w.E[0], w.E[1]};
+                from_record(p, w, use);
+            }
+        };
+        conv(cw.Pi);
+        for (auto& L : cw.layers) {
+            conv(L.Pr);
+            conv(L.Pt);
+        }
+        return cw;
+    }
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("file " + path + " not found");
     uint64_t sz = 0;

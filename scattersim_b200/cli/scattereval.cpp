@@ -33,7 +33,7 @@ int main(int argc, char** argv) {
         std::cout << "Allowed options:\n  --input arg (=c.cw)\n  --cuda arg (=0)\n  --size arg (=100)\n"
                      "  --resolution arg (=8)\n  --output arg (=xz.npy)\n  --axis arg (=1)\n"
                      "  --center arg (={0, 0, 0})\n  --slice arg (=0)\n"
-                     "  --cw-frame arg (=tira) record frame of the file ('tira', 'tira-mirror' or 'cartesian')\n";
+                     "  --cw-frame arg (=tira) record frame of the file ('tira', 'tira-mirror', 'cartesian', or 'auto': the one that makes the field continuous at the first interface)\n";
         return 1;
     }
     const std::string in = o.str("input", "c.cw"), out = o.str("output", "xz.npy");
@@ -48,7 +48,7 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     cwio::CoupledWave cw;
     try {
-        cw = cwio::load_cw(in, cwio::parse_frame(o.str("cw-frame", "tira")));
+        cw = cwio::load_cw(in, cwio::parse_read_frame(o.str("cw-frame", "tira")));
     } catch (const std::exception& e) {
         std::cout << "ERROR: " << e.what() << std::endl;
         return 1;

@@ -96,9 +96,8 @@ def save(path, Pi_E, Pi_k, layers, mirror_down: bool = False):
             f.write(_records(PtE, Ptk, mirror_down))
 
 
-def load(path, mirror_down: bool = False):
-    """Read a .cw file: (Pi_E, Pi_k, layers) with Cartesian E0 (N, 3) as getE0() rebuilds it (mirror_down for
-    files whose downward waves hold mirrored-frame pairs, such as the reference's scatterlayer output)."""
+def _read_raw(path):
+    """(Pi pairs, Pi k, [(z, Pr pairs, Pr k, Pt pairs, Pt k)]) as stored."""
     b = open(path, "rb").read()
     sz, npi = struct.unpack_from("<QQ", b, 0)
     if sz != 8:
@@ -109,19 +108,70 @@ def load(path, mirror_down: bool = False):
         nonlocal o
         r = np.frombuffer(b, dtype=np.complex128, count=5 * count, offset=o).reshape(count, 5)
         o += 80 * count
-        k = r[:, 2:5].copy()
-        return from_record(r[:, 0:2], k, mirror_down) if count else np.zeros((0, 3), np.complex128), k
+        return r[:, 0:2].copy(), r[:, 2:5].copy()
 
-    PiE, Pik = recs(npi)
+    Pi = recs(npi)
     (nl,) = struct.unpack_from("<Q", b, o)
     o += 8
     layers = []
     for _ in range(nl):
         z, npr = struct.unpack_from("<dQ", b, o)
         o += 16
-        PrE, Prk = recs(npr)
+        Pr = recs(npr)
         (npt,) = struct.unpack_from("<Q", b, o)
         o += 8
-        PtE, Ptk = recs(npt)
-        layers.append((z, PrE, Prk, PtE, Ptk))
-    return PiE, Pik, layers
+        Pt = recs(npt)
+        layers.append((z,) + Pr + Pt)
+    return Pi, layers
+
+
+def interface_jump(Pi, layers, mirror_down: bool, points: int = 8) -> float:
+    """Largest jump of the tangential (x, y) field across the first interface, relative to the field there, with
+    the stored pairs read in the given frame: the plane-wave sum of region 0 (incident + reflected at z_0)
+    against that of region 1 (transmitted at z_0 + reflected at z_1), both on the plane z = z_0 (the regions of
+    cpuEvaluator.cpp:34-102).  The reading the file was written in gives a continuous field."""
+    if not layers:
+        return 0.0
+
+    def waves(pk):
+        E2, k = pk
+        return (from_record(E2, k, mirror_down), k) if len(E2) else (np.zeros((0, 3), complex), k)
+    z0 = layers[0][0]
+    above = [waves(Pi), waves(layers[0][1:3])]
+    below = [waves(layers[0][3:5])] + ([waves(layers[1][1:3])] if len(layers) > 1 else [])
+    kmax = max([np.abs(k).max() for _, k in above + below if len(k)] + [1.0])
+    rng = np.random.default_rng(0)
+    xy = rng.uniform(-1.0, 1.0, (points, 2)) * (2 * np.pi / kmax)
+    r = np.c_[xy, np.full(points, z0)]
+
+    def field(parts):
+        out = np.zeros((points, 3), complex)
+        for E, k in parts:
+            if len(E):
+                out += np.exp(1j * (r @ k.T)) @ E
+        return out
+    a, b = field(above)[:, :2], field(below)[:, :2]
+    scale = max(np.abs(a).max(), np.abs(b).max())
+    return float(np.abs(a - b).max() / scale) if scale > 0 else 0.0
+
+
+def detect_mirror_down(path) -> bool:
+    """Which record frame a file's downward waves were written in, from the physics: True when reading them in
+    the z-mirrored direction's frame makes the field continuous across the first interface and the own frame
+    does not (the reference's scatterlayer files), False otherwise (its scatterplane files, this package's)."""
+    Pi, layers = _read_raw(path)
+    return interface_jump(Pi, layers, True) < interface_jump(Pi, layers, False)
+
+
+def load(path, mirror_down=False):
+    """Read a .cw file: (Pi_E, Pi_k, layers) with Cartesian E0 (N, 3) as getE0() rebuilds it.  mirror_down: True
+    for files whose downward waves hold mirrored-frame pairs (the reference's scatterlayer output), "auto" to
+    decide from the field's continuity at the first interface (detect_mirror_down)."""
+    Pi, raw = _read_raw(path)
+    if mirror_down == "auto":
+        mirror_down = interface_jump(Pi, raw, True) < interface_jump(Pi, raw, False)
+
+    def conv(E2, k):
+        return from_record(E2, k, bool(mirror_down)) if len(E2) else np.zeros((0, 3), np.complex128)
+    layers = [(z, conv(a, ak), ak, conv(c, ck), ck) for z, a, ak, c, ck in raw]
+    return conv(*Pi), Pi[1], layers

@@ -1,10 +1,11 @@
 // Test harness for the command-line tools' .cw record frames (cli/cwio.hpp),
 // built and run on the CPU by tests/test_cwfile.py:
 //   cwio_frames <in.cw> <frame> <out.cw> <fields.bin>
-// loads <in.cw> reading its records in <frame> (tira, tira-mirror or
-// cartesian), writes the Cartesian E0 of every wave (incident, then per
-// boundary reflected and transmitted; 3 complex128 each) to <fields.bin> and
-// saves the waves again to <out.cw> in the same frame.
+// loads <in.cw> reading its records in <frame> (tira, tira-mirror,
+// cartesian, or auto: decided from the field's continuity at the first
+// interface), writes the Cartesian E0 of every wave (incident, then per
+// boundary reflected and transmitted; 3 complex128 each) to <fields.bin> and,
+// for a named frame, saves the waves again to <out.cw> in that frame.
 #include "cwio.hpp"
 
 int main(int argc, char** argv) {
@@ -13,7 +14,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     try {
-        const cwio::Frame fr = cwio::parse_frame(argv[2]);
+        const cwio::Frame fr = cwio::parse_read_frame(argv[2]);
         const cwio::CoupledWave cw = cwio::load_cw(argv[1], fr);
         std::ofstream f(argv[4], std::ios::binary);
         auto dump = [&](const std::vector<cwio::Wave>& w) {
@@ -24,7 +25,7 @@ int main(int argc, char** argv) {
             dump(L.Pr);
             dump(L.Pt);
         }
-        cwio::save_cw(argv[3], cw, fr);
+        if (fr != cwio::Frame::automatic) cwio::save_cw(argv[3], cw, fr);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "ERROR: %s\n", e.what());
         return 1;
